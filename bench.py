@@ -1,0 +1,361 @@
+#!/usr/bin/env python3
+"""Benchmark: MITM records joined/s on B200 -- single-modulus k=64 solves (r = 5).
+
+Workload ("k64_r5_single_modulus"): each step solves one seeded modulus
+M = 2^a 3^b 5^c 7^d * (4-6 primes from 11..43) in [10^15, 2^62), pool
+Q(M) = primes <= 5518 with (q-1) | M (capped at 320), B0 = the 64 smallest,
+r = 5, B = 10^148: D side C(64,5) = 7,624,512 records, I side C(|INS|,5)
+(10^7 .. 6.8*10^8).  value = (N_D + N_I) summed over all ranks / max-over-ranks
+device time.  With N GPUs each rank solves its own moduli (the portfolio
+shards by modulus; no data-path collective): weak scaling.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU engine (src/mitm64.cpp built
+from source into oracle/_ref/, all host threads) on a bounded sample of the
+same workload and prints the same JSON line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MITM records joined/s (N_D + N_I per second, k=64 r=5 single-modulus solves)"
+UNIT = "records/s"
+WORKLOAD = "k64_r5_single_modulus"
+SEED_POOL = 64          # candidate seeds for the step sequence
+BYTES_PER_RECORD = 32   # algorithmic: one 16-B {key,id} write + one 16-B read per record entering the join
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="CPU-baseline budget (seconds of work)")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def step_seeds(steps: int, world: int, rank: int):
+    """Balanced weak-scaling schedule: blocks of `world` seeds of similar I-side size per step."""
+    from carmichael_frontier_b200 import workloads as W
+    cands = W.config2_seeds(SEED_POOL)
+    need = steps * world
+    pool = list(cands)
+    while len(pool) < need:
+        pool += cands
+    pool = pool[:need]
+    # sort each consecutive block of `world` by size so ranks get similar work; deterministic
+    order = sorted(range(len(pool)), key=lambda i: (pool[i].n_I, i))
+    blocks = [order[i:i + world] for i in range(0, need, world)]
+    blocks.sort(key=lambda b: min(b))           # restore the seed sequence order across steps
+    return [pool[b[rank]] for b in blocks]
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.gpu_id:
+                cmd += ["-i", self.gpu_id]
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[j] for _, _, rs in rows for j, v in enumerate(rs) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def gpu_uuid(torch, dev) -> str | None:
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------------ CPU baseline (reference engine)
+def cpu_sample(w, cores: int, seconds: float):
+    """Bounded sample of one modulus for the CPU engine: the full D side and the I side over the
+    n' smallest insertion primes, n' the largest with C(n',5) <= ~seconds of work on `cores`."""
+    ins = list(w.INS)
+    budget = max(1_000_000, int(seconds * 4.0e6 * cores))   # ~4M I leaves/s per core (measured mitm64 rate)
+    n2 = w.r
+    while n2 < len(ins) and math.comb(n2 + 1, w.r) <= budget:
+        n2 += 1
+    return ins[:n2]
+
+
+def run_cpu_engine(w, cores: int, seconds: float):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from carmichael_frontier_b200.workloads import product
+    ins = cpu_sample(w, cores, seconds)
+    P0 = product(w.B0)
+    Icap = product(ins[-w.r:]) + 1         # unpruned I side (every r-subset), as the GPU join
+    n_rec = math.comb(len(w.B0), w.r) + math.comb(len(ins), w.r)
+    sample = (f"{w.name}: full D side C({len(w.B0)},{w.r}) + I side over the {len(ins)} smallest of "
+              f"{len(w.INS)} insertion primes (C({len(ins)},{w.r}) = {math.comb(len(ins), w.r):,})")
+    if O.ref_binary("mitm64"):
+        t0 = time.perf_counter()
+        O.run_ref_mitm64(w.M, list(w.B0), ins, w.r, P0, Icap, 1, cores)
+        dt = time.perf_counter() - t0
+        return n_rec, dt, "reference", cores, sample
+    t0 = time.perf_counter()                # the C restatement (single thread) when the binary is absent
+    O.mitm64_matches(w.B0, ins, w.r, w.M, P0, Icap)
+    dt = time.perf_counter() - t0
+    return n_rec, dt, "port", 1, sample + " [oracle port, 1 thread]"
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    seeds = step_seeds(args.steps + args.warmup, 1, 0)
+    per_step = max(2.0, min(8.0, 150.0 / max(1, args.steps + args.warmup)))
+    recs = tsum = 0.0
+    kind = ncores = sample = None
+    for i, w in enumerate(seeds):
+        n, dt, kind, ncores, sample = run_cpu_engine(w, cores, per_step)
+        if i >= args.warmup:
+            recs += n
+            tsum += dt
+    value = recs / tsum
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tsum / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded moduli)",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "engine": "src/mitm64.cpp (built from source, -O3, all host threads)",
+                       "sample_per_step": "bounded: " + (sample or "")},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args):
+    import torch
+    from carmichael_frontier_b200 import Solver, _lib
+    from carmichael_frontier_b200 import solve as public_solve
+    from carmichael_frontier_b200.solve import Instance, _default_solvers
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def allmax(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def allsum(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    seq = step_seeds(args.steps + args.warmup, world, rank)
+    warm, timed = seq[:args.warmup], seq[args.warmup:]
+    solver = Solver(dev)
+    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in seq]
+    # inputs resident in HBM for the device-timed region: pool tables uploaded before timing
+    for inst in insts:
+        solver.tables.pool(inst.B0, inst.r, inst.M, pow(inst.P0, -1, inst.M))
+        solver.tables.pool(inst.INS, inst.r, inst.M, 1)
+        solver.tables.screen(inst.P0, inst.B, 1e-6)
+    solver.tables.max_entries = 10 ** 6
+    clocks = ClockSampler(gpu_uuid(torch, dev))
+    clocks.start()
+    for inst in insts[:args.warmup]:
+        solver.solve_instance(inst, verify=True)
+    # ---- device-timed region: K solves, inputs resident
+    stream = torch.cuda.current_stream(dev)
+    kt = {"gen_D": 0.0, "gen_I": 0.0, "join": 0.0, "check": 0.0}
+    recs = 0
+    launches = 0
+    hits = 0
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    marks_all = []
+    for inst in insts[args.warmup:]:
+        marks = []
+        res = solver.solve_instance(inst, verify=True, marks=marks)
+        marks_all.append(marks)
+        recs += res.records
+        launches += res.launches
+        hits += len(res.hits)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    t_local = e0.elapsed_time(e1) / 1e3
+    for marks in marks_all:
+        for (t0, a), (tag, b) in zip(marks, marks[1:]):
+            kt[tag] += a.elapsed_time(b) / 1e3
+    t_max = allmax(t_local)
+    recs_all = allsum(recs)
+    value = recs_all / t_max
+
+    # ---- end-to-end region: the public API from host inputs (tables built and copied every step)
+    _default_solvers.clear()
+    barrier()
+    torch.cuda.synchronize(dev)
+    h2d = d2h = 0
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    t_wall0 = time.perf_counter()
+    for w in timed:
+        res = public_solve(w.M, w.Q, w.B0, w.r, w.B, device=dev)
+        s = next(iter(_default_solvers.values()))
+        s.tables._cache.clear()              # the next step uploads its inputs again
+        n_b0, n_ins = len(w.B0), len(w.INS)
+        lib = _lib.load()
+        h2d += lib.cf_pool_bytes(n_b0, w.r) + lib.cf_pool_bytes(n_ins, w.r) + lib.cf_screen_bytes()
+        d2h += 8 + res.residue_pairs * lib.cf_pair_result_bytes()
+    f1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    t_e2e = allmax(f0.elapsed_time(f1) / 1e3)
+    t_e2e_wall = allmax(time.perf_counter() - t_wall0)
+    clk = clocks.stop()
+    e2e_value = recs_all / max(t_e2e, t_e2e_wall)
+
+    # ---- roofline of the join path (partitioned generation + partition join)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    t_path = kt["gen_D"] + kt["gen_I"] + kt["join"]
+    achieved = BYTES_PER_RECORD * recs / t_path / 1e9 if t_path > 0 else None
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            tj = json.load(open(tfile))
+            traffic = tj["bytes_per_record"] * recs / len(timed)     # per step (one launch sequence)
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            n, dt, kind, cores, sample = run_cpu_engine(timed[0], os.cpu_count() or 1, args.cpu_seconds)
+            cpu = {"value": n / dt, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        except Exception as e:            # report, never fail the GPU line
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None, "sample": f"failed: {e}"}
+
+    if rank == 0:
+        kern = {k: {"ms_total": 1e3 * v} for k, v in kt.items()}
+        n_d = sum(math.comb(len(w.B0), w.r) for w in timed)
+        n_i = sum(math.comb(len(w.INS), w.r) for w in timed)
+        if kt["gen_I"] > 0:
+            kern["gen_I"]["GB_s"] = 16 * n_i / kt["gen_I"] / 1e9
+        if kt["join"] > 0:
+            kern["join"]["GB_s"] = 16 * (n_i + n_d) / kt["join"] / 1e9
+        if kt["gen_D"] > 0:
+            kern["gen_D"]["GB_s"] = 16 * n_d / kt["gen_D"] / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded moduli)",
+            "config": {"workload": WORKLOAD, "r": 5, "k": 64, "B": "10^148", "moduli_per_step_per_gpu": 1,
+                       "seeds": [w.name for w in timed][:8], "l2": "inputs larger than L2 (I side 0.17-11 GB per step)",
+                       "parallelism": f"modulus-sharded x{world}", "records_per_gpu": recs},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "kernel": "k_gen_part + k_join_part (join path, 32 B/record)", "peak_source": peak_src},
+            "kernels": kern,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // max(1, len(timed)),
+                    "d2h_bytes_per_step": d2h // max(1, len(timed)), "api": "carmichael_frontier_b200.solve"},
+            "gpu_launches": launches,
+            "hits": hits,
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                       "samples": clk["samples"]},
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,114 @@
+"""ctypes binding of the C ABI in ``include/cfmitm.h`` (``libcfmitm.so``).
+
+The library is the only compute path: if it is missing or a call fails, an
+exception is raised.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcfmitm.so")
+
+CF_OK = 0
+CF_EBADARG = -1
+CF_ENOMEM = -2
+CF_ECUDA = -3
+CF_EOVERFLOW = -4
+CF_ETIMEOUT = -5
+
+ERR_PART_OVERFLOW = 1
+ERR_PAIR_OVERFLOW = 2
+ERR_TABLE_FULL = 4
+ERR_SPIN_LIMIT = 8
+ERR_KEY_MISMATCH = 16
+
+HIT_KEY_EQUAL = 1
+HIT_SCREEN = 2
+HIT_SIZE_EXACT = 4
+HIT_KORSELT = 8
+HIT_DISJOINT = 16
+
+u64 = C.c_uint64
+u32 = C.c_uint32
+vp = C.c_void_p
+sz = C.c_size_t
+
+
+class CfError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where}: status {status}: {msg}")
+        self.status = status
+
+
+# (name, restype, argtypes) for every symbol in include/cfmitm.h
+SIGNATURES = [
+    ("cf_version", C.c_int, []),
+    ("cf_last_error_string", C.c_char_p, []),
+    ("cf_pool_bytes", sz, [C.c_int, C.c_int]),
+    ("cf_pool_prepare", C.c_int, [vp, C.c_int, C.c_int, u64, u64, vp, sz]),
+    ("cf_key_of", u64, [u64, u64]),
+    ("cf_canon_of", u64, [u64, u64]),
+    ("cf_key_mul", u64, [u64, u64, u64]),
+    ("cf_part_multiplier", u64, [u64, u32]),
+    ("cf_screen_bytes", sz, []),
+    ("cf_screen_prepare", C.c_int, [vp, C.c_int, C.c_double, C.c_double, C.c_double, vp, sz]),
+    ("cf_gen_subsets", C.c_int, [vp, C.c_int, C.c_int, u64, u64, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
+    ("cf_gen_part_smem_bytes", sz, [C.c_int, u32]),
+    ("cf_gen_part", C.c_int, [vp, C.c_int, C.c_int, u64, u64, u32, u64, u32, vp, vp, vp, vp]),
+    ("cf_join_part_smem_bytes", sz, [C.c_int]),
+    ("cf_join_part", C.c_int, [vp, vp, u32, vp, vp, u32, u32, u64, C.c_int, u32, u32, vp, u32, vp, vp, vp]),
+    ("cf_pair_result_bytes", sz, []),
+    ("cf_check_pairs", C.c_int, [vp, vp, vp, C.c_int, vp, vp, u32, vp, vp, vp]),
+    ("cf_sort_tmp_bytes", sz, [u64]),
+    ("cf_sort_pairs", C.c_int, [vp, vp, u64, C.c_int, vp, sz, vp]),
+    ("cf_merge_run_bytes", sz, []),
+    ("cf_merge_join_runs", C.c_int, [vp, u64, vp, u64, vp, u64, vp, vp, vp, vp]),
+]
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load() -> C.CDLL:
+    """Load libcfmitm.so (built by ``carmichael_frontier_b200._build``)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"{LIB_PATH} is missing: build it with `python -m carmichael_frontier_b200._build` "
+                    "(the join has no CPU fallback)")
+            lib = C.CDLL(LIB_PATH)
+            for name, res, args in SIGNATURES:
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def check(status: int, where: str) -> None:
+    if status != CF_OK:
+        msg = load().cf_last_error_string().decode(errors="replace")
+        raise CfError(status, where, msg)
+
+
+def ptr(t) -> int | None:
+    """Device (or host) address of a torch tensor / numpy array, None for None."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return t.ctypes.data
+
+
+def stream_handle(stream=None) -> int | None:
+    """cudaStream_t of a torch stream (current stream when None)."""
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream

@@ -1,0 +1,157 @@
+// cf_check.cu -- exact verification of candidate pairs on the device.
+//
+// For each (D, I) pair from the join: unrank both lexicographic ranks, recompute
+// both residues from scratch (they must be equal), run the conservative fp64
+// log-size pre-screen  log2 P0 - sum log2 d + sum log2 i <= log2 B + eps, and for
+// every survivor the exact checks:
+//   size     n = prod(B0 \ D) * prod(I) <= B      (32-bit limbs, exact)
+//   Korselt  prod(S) == 1 (mod p-1) for every p in S
+//   distinct the k primes of S are pairwise distinct.
+// The reference performs the same checks on the host in Python integers
+// (gpu/mitm_gpu_mstar_driver.py:226-237) and by ref/ref_carmichael.py:55-72.
+#include "cf_abi_internal.h"
+#include "cf_enum.cuh"
+
+namespace {
+
+template <int R>
+__global__ void __launch_bounds__(128)
+k_check_pairs(const u64* __restrict__ poolD, const u64* __restrict__ poolI, const CfScreen* __restrict__ scr,
+              const CfPair* __restrict__ pairs, const u32* __restrict__ npairs, u32 max_pairs,
+              CfPairResult* __restrict__ res, u32* __restrict__ err) {
+  const CfPoolHdr* hD = (const CfPoolHdr*)poolD;
+  const CfPoolHdr* hI = (const CfPoolHdr*)poolI;
+  const int nD = (int)hD->n, nI = (int)hI->n;
+  const CfMod md = cf_mod_from_hdr(hD);
+  const u64* bD = poolD + cf_pool_off_binom(nD);
+  const u64* bI = poolI + cf_pool_off_binom(nI);
+  const u64* kD = poolD + cf_pool_off_pkey(nD);
+  const u64* kI = poolI + cf_pool_off_pkey(nI);
+  const u64* pD = poolD + cf_pool_off_prime(nD);
+  const u64* pI = poolI + cf_pool_off_prime(nI);
+  const double* lD = (const double*)(poolD + cf_pool_off_lg(nD));
+  const double* lI = (const double*)(poolI + cf_pool_off_lg(nI));
+  const u32 np = min(*npairs, max_pairs);
+  for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < np; t += gridDim.x * blockDim.x) {
+    const CfPair pr = pairs[t];
+    CfPairResult out;
+    out.flags = 0;
+    out.r = R;
+    for (int j = 0; j < CF_MAX_R; ++j) { out.d_idx[j] = 0; out.i_idx[j] = 0; }
+    int di[R], ii[R];
+    cf_unrank_lex<R>(pr.d_id, nD, bD, di);
+    cf_unrank_lex<R>(pr.i_id, nI, bI, ii);
+    u64 kd = hD->mult_key, ki = hI->mult_key;
+    double lg = scr->lgP0;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      kd = cf_mul_key(kd, kD[di[j]], md);
+      ki = cf_mul_key(ki, kI[ii[j]], md);
+      lg += lI[ii[j]] - lD[di[j]];
+      out.d_idx[j] = (unsigned short)di[j];
+      out.i_idx[j] = (unsigned short)ii[j];
+    }
+    if (kd == ki) out.flags |= CF_HIT_KEY_EQUAL;
+    else atomicOr(err, CF_ERR_KEY_MISMATCH);
+    if (lg <= scr->lgB + scr->eps) {
+      out.flags |= CF_HIT_SCREEN;
+      // --- distinctness of S = (B0 \ D) u I: D indices are distinct by construction
+      //     (strictly increasing), I primes must avoid B0 and each other.
+      bool distinct = true;
+      for (int j = 0; j < R; ++j) {
+        const u64 q = pI[ii[j]];
+        for (int x = 0; x < nD; ++x) distinct &= (pD[x] != q);
+        for (int y = 0; y < j; ++y) distinct &= (pI[ii[y]] != q);
+      }
+      if (distinct) out.flags |= CF_HIT_DISJOINT;
+      // --- exact size: n = prod(S) in 32-bit limbs against B
+      u32 limb[CF_SCREEN_MAX_LIMBS];
+      const int L = CF_SCREEN_MAX_LIMBS;
+      for (int l = 0; l < L; ++l) limb[l] = 0;
+      limb[0] = 1;
+      bool over = false;
+      int dpos = 0;
+      for (int x = 0; x < nD + R; ++x) {
+        u64 q;
+        if (x < nD) {
+          if (dpos < R && di[dpos] == x) { ++dpos; continue; }
+          q = pD[x];
+        } else {
+          q = pI[ii[x - nD]];
+        }
+        if (q >> 32) { over = true; continue; }
+        u64 carry = 0;
+        for (int l = 0; l < L; ++l) {
+          const u64 v = (u64)limb[l] * q + carry;
+          limb[l] = (u32)v;
+          carry = v >> 32;
+        }
+        if (carry) over = true;
+      }
+      if (!over) {
+        // compare n <= B
+        int cmp = 0;   // -1 n<B, 0 equal, 1 n>B
+        for (int l = L - 1; l >= 0 && cmp == 0; --l) {
+          const u32 b = (l < (int)scr->nlimbs) ? scr->limbsB[l] : 0u;
+          if (limb[l] != b) cmp = (limb[l] < b) ? -1 : 1;
+        }
+        if (cmp <= 0) out.flags |= CF_HIT_SIZE_EXACT;
+      }
+      // --- Korselt: prod(S) == 1 mod (p-1) for every p in S
+      bool korselt = true;
+      int dp1 = 0;
+      for (int x = 0; x < nD + R && korselt; ++x) {
+        u64 p;
+        if (x < nD) {
+          if (dp1 < R && di[dp1] == x) { ++dp1; continue; }
+          p = pD[x];
+        } else {
+          p = pI[ii[x - nD]];
+        }
+        const u64 mod = p - 1;
+        if (mod == 0) { korselt = false; break; }
+        u64 prod = 1 % mod;
+        int dq = 0;
+        for (int y = 0; y < nD + R; ++y) {
+          u64 q;
+          if (y < nD) {
+            if (dq < R && di[dq] == y) { ++dq; continue; }
+            q = pD[y];
+          } else {
+            q = pI[ii[y - nD]];
+          }
+          prod = (u64)(((unsigned __int128)prod * (q % mod)) % mod);
+        }
+        korselt = (prod == 1 % mod);
+      }
+      if (korselt) out.flags |= CF_HIT_KORSELT;
+    }
+    res[t] = out;
+  }
+}
+
+template <int R>
+void launch_check(const u64* poolD, const u64* poolI, const CfScreen* scr, const CfPair* pairs, const u32* npairs,
+                  u32 max_pairs, CfPairResult* res, u32* err, cudaStream_t st) {
+  const u32 grid = max_pairs ? (u32)((max_pairs + 127) / 128) : 1u;
+  k_check_pairs<R><<<grid < 1024u ? grid : 1024u, 128, 0, st>>>(poolD, poolI, scr, pairs, npairs, max_pairs, res,
+                                                                err);
+}
+
+}  // namespace
+
+extern "C" size_t cf_pair_result_bytes(void) { return sizeof(CfPairResult); }
+
+extern "C" int cf_check_pairs(const void* poolD, const void* poolI, const void* screen, int r, const void* pairs,
+                              const u32* npairs, u32 max_pairs, void* results, u32* err, void* stream) {
+  if (!poolD || !poolI || !screen || !npairs || !err || r < 1 || r > CF_MAX_DISPATCH_R) {
+    cf_set_error("cf_check_pairs: bad arguments%s", "");
+    return CF_EBADARG;
+  }
+  if (max_pairs == 0) return CF_OK;
+  if (!pairs || !results) { cf_set_error("cf_check_pairs: null buffer%s", ""); return CF_EBADARG; }
+  CF_DISPATCH_R(r, launch_check, (const u64*)poolD, (const u64*)poolI, (const CfScreen*)screen,
+                (const CfPair*)pairs, npairs, max_pairs, (CfPairResult*)results, err, (cudaStream_t)stream);
+  CF_LAUNCH_CHECK("cf_check_pairs");
+  return CF_OK;
+}

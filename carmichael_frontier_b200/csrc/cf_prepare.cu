@@ -1,0 +1,154 @@
+// cf_prepare.cu -- host-side preparation of the small tables the kernels read
+// (pool tables and the size-screen table), plus the library's error string.
+// Pure host code: exact 128-bit integer arithmetic, no device calls.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+#include "cf_abi_internal.h"
+
+static thread_local char g_err[512] = "ok";
+
+void cf_set_error(const char* fmt, const char* detail) {
+  snprintf(g_err, sizeof g_err, fmt, detail ? detail : "");
+}
+
+extern "C" const char* cf_last_error_string(void) { return g_err; }
+
+extern "C" int cf_version(void) { return CF_ABI_VERSION; }
+
+typedef unsigned __int128 u128;
+
+static u64 inv_mod_2_64(u64 m) {           // m odd
+  u64 x = m;                               // correct to 3 bits
+  for (int i = 0; i < 6; ++i) x *= 2 - m * x;
+  return x;
+}
+
+static u64 mod_pow(u64 b, u64 e, u64 m) {
+  if (m == 1) return 0;
+  u64 r = 1 % m;
+  b %= m;
+  while (e) {
+    if (e & 1) r = (u64)((u128)r * b % m);
+    b = (u64)((u128)b * b % m);
+    e >>= 1;
+  }
+  return r;
+}
+
+struct HostMod {
+  u64 M, m, minv, mask2, Rm, r2;
+  int a;
+};
+
+static int host_mod_init(u64 M, HostMod* h) {
+  if (M < 2 || M >= (1ull << 62)) return CF_EBADARG;
+  h->M = M;
+  h->a = __builtin_ctzll(M);
+  h->m = M >> h->a;
+  h->minv = inv_mod_2_64(h->m);
+  h->mask2 = (h->a == 0) ? 0 : ((1ull << h->a) - 1);
+  h->Rm = (u64)((((u128)1) << 64) % h->m);
+  h->r2 = (u64)((u128)h->Rm * h->Rm % h->m);
+  return CF_OK;
+}
+
+static u64 host_key(const HostMod& h, u64 v) {
+  const u64 X = (u64)((u128)(v % h.m) * h.Rm % h.m);
+  return (X << h.a) | (v & h.mask2);
+}
+
+extern "C" size_t cf_pool_bytes(int n, int r) {
+  if (n < 1 || n > CF_MAX_POOL || r < 1 || r > CF_MAX_R) return 0;
+  return cf_pool_words(n, r) * sizeof(u64);
+}
+
+extern "C" int cf_pool_prepare(const u64* primes, int n, int r, u64 M, u64 mult, void* out,
+                               size_t out_bytes) {
+  if (!primes || !out) { cf_set_error("cf_pool_prepare: null pointer%s", ""); return CF_EBADARG; }
+  if (n < 1 || n > CF_MAX_POOL) { cf_set_error("cf_pool_prepare: pool size out of range (1..1024)%s", ""); return CF_EBADARG; }
+  if (r < 1 || r > CF_MAX_R || r > n) { cf_set_error("cf_pool_prepare: radius out of range (1..16, <= n)%s", ""); return CF_EBADARG; }
+  if (out_bytes < cf_pool_bytes(n, r)) { cf_set_error("cf_pool_prepare: table buffer too small%s", ""); return CF_EBADARG; }
+  HostMod h;
+  if (host_mod_init(M, &h) != CF_OK) { cf_set_error("cf_pool_prepare: need 2 <= M < 2^62%s", ""); return CF_EBADARG; }
+  u64* w = (u64*)out;
+  memset(w, 0, cf_pool_bytes(n, r));
+  CfPoolHdr* hd = (CfPoolHdr*)w;
+  hd->magic = CF_POOL_MAGIC;
+  hd->M = M; hd->m = h.m; hd->minv = h.minv; hd->mask2 = h.mask2;
+  hd->a = (u64)h.a; hd->n = (u64)n; hd->R = (u64)r;
+  hd->mult_key = host_key(h, mult % M);
+  hd->one_key = host_key(h, 1 % M);
+  hd->r2 = h.r2;
+  const u64 half = (h.m + 1) / 2;          // 2^-1 mod m (m odd)
+  hd->inv2a = mod_pow(half, (u64)h.a, h.m);
+  hd->inv2aR = (u64)((u128)hd->inv2a * h.Rm % h.m);
+  u64* pkey = w + cf_pool_off_pkey(n);
+  u64* prime = w + cf_pool_off_prime(n);
+  double* lg = (double*)(w + cf_pool_off_lg(n));
+  u64* binom = w + cf_pool_off_binom(n);
+  for (int i = 0; i < n; ++i) {
+    pkey[i] = host_key(h, primes[i]);
+    prime[i] = primes[i];
+    lg[i] = primes[i] ? log2((double)primes[i]) : -INFINITY;
+  }
+  const u64 SAT = ~0ull;
+  for (int x = 0; x <= n; ++x) {
+    for (int y = 0; y <= r; ++y) {
+      u64 v;
+      if (y == 0) v = 1;
+      else if (x == 0) v = 0;
+      else {
+        const u64 p = binom[(size_t)(x - 1) * (r + 1) + (y - 1)];
+        const u64 q = binom[(size_t)(x - 1) * (r + 1) + y];
+        v = (p > SAT - q) ? SAT : p + q;
+      }
+      binom[(size_t)x * (r + 1) + y] = v;
+    }
+  }
+  hd->total = binom[(size_t)n * (r + 1) + r];
+  return CF_OK;
+}
+
+extern "C" u64 cf_key_of(u64 M, u64 v) {
+  HostMod h;
+  if (host_mod_init(M, &h) != CF_OK) return ~0ull;
+  return host_key(h, v);
+}
+
+extern "C" u64 cf_canon_of(u64 M, u64 k) {
+  HostMod h;
+  if (host_mod_init(M, &h) != CF_OK) return ~0ull;
+  CfMod md;
+  md.m = h.m; md.minv = h.minv; md.mask2 = h.mask2; md.a = h.a;
+  const u64 inv2a = mod_pow((h.m + 1) / 2, (u64)h.a, h.m);
+  const u64 inv2aR = (u64)((u128)inv2a * h.Rm % h.m);
+  return cf_key_to_canon(k, md, inv2a, inv2aR);
+}
+
+extern "C" u64 cf_key_mul(u64 M, u64 kx, u64 ky) {
+  HostMod h;
+  if (host_mod_init(M, &h) != CF_OK) return ~0ull;
+  CfMod md;
+  md.m = h.m; md.minv = h.minv; md.mask2 = h.mask2; md.a = h.a;
+  return cf_mul_key(kx, ky, md);
+}
+
+extern "C" u64 cf_part_multiplier(u64 M, u32 nparts) {
+  if (M < 2 || nparts == 0 || (u64)nparts >= M) return 0;
+  return (u64)((((u128)nparts) << 64) / M);
+}
+
+extern "C" size_t cf_screen_bytes(void) { return sizeof(CfScreen); }
+
+extern "C" int cf_screen_prepare(const u32* limbsB, int nlimbs, double lgP0, double lgB, double eps,
+                                 void* out, size_t out_bytes) {
+  if (!limbsB || !out || out_bytes < sizeof(CfScreen)) { cf_set_error("cf_screen_prepare: bad buffer%s", ""); return CF_EBADARG; }
+  if (nlimbs < 1 || nlimbs > CF_SCREEN_MAX_LIMBS) { cf_set_error("cf_screen_prepare: B needs 1..64 limbs of 32 bits%s", ""); return CF_EBADARG; }
+  if (!(eps >= 0.0)) { cf_set_error("cf_screen_prepare: eps must be >= 0%s", ""); return CF_EBADARG; }
+  CfScreen* s = (CfScreen*)out;
+  memset(s, 0, sizeof *s);
+  s->lgP0 = lgP0; s->lgB = lgB; s->eps = eps; s->nlimbs = (u32)nlimbs;
+  for (int i = 0; i < nlimbs; ++i) s->limbsB[i] = limbsB[i];
+  return CF_OK;
+}

@@ -1,0 +1,338 @@
+// cf_sort.cu -- stable LSD onesweep radix sort of (u64 key, u64 id) records and
+// the sorted-side merge join: the drop-ins for the reference's sort_side
+// (gpu/mitm_gpu2.py:101-104, a stable argsort plus two gathers) and
+// join_sorted (gpu/mitm_gpu2.py:107-119).
+//
+// Sort: one histogram kernel reads every key once and counts all 8-bit digits
+// of all passes; each pass is then ONE kernel (onesweep): a CTA takes the next
+// tile ticket, ranks its keys stably in shared memory (warp match_any
+// ranking over a warp-striped tile, so equal digits keep input order),
+// publishes its per-digit counts, resolves its global digit offsets by
+// decoupled look-back over the tiles before it (bounded spin), and scatters
+// keys, then ids.  Passes whose digit is equal for every key are skipped by the
+// host, so keys below M < 2^62 cost at most ceil(log2 M / 8) passes.
+//
+// Merge join: every thread takes a run of consecutive sorted I keys, finds the
+// first D key >= its first key by binary search and then gallops forward;
+// every I row with at least one equal D key is appended as (row, first D
+// position, count) to a compact run list (pairs are rare).  The host expands
+// runs into pairs in I-row order, which is join_sorted's output order.
+#include "cf_abi_internal.h"
+
+namespace {
+
+constexpr int kSortBlock = 512;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortBlock * kSortItems;  // 8192
+constexpr int kRadix = 256;
+constexpr int kWarps = kSortBlock / 32;
+constexpr u64 kFlagAgg = 1ull << 62;
+constexpr u64 kFlagInc = 2ull << 62;
+constexpr u64 kValMask = (1ull << 62) - 1;
+constexpr u32 kSpinLimit = 1u << 24;
+
+__global__ void __launch_bounds__(kSortBlock)
+k_sort_hist(const u64* __restrict__ keys, u64 n, u64* __restrict__ hist /*[8][256]*/) {
+  __shared__ u32 s_h[8][kRadix];
+  for (int i = threadIdx.x; i < 8 * kRadix; i += kSortBlock) (&s_h[0][0])[i] = 0;
+  __syncthreads();
+  for (u64 i = (u64)blockIdx.x * kSortBlock + threadIdx.x; i < n; i += (u64)gridDim.x * kSortBlock) {
+    const u64 k = keys[i];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) atomicAdd(&s_h[p][(k >> (8 * p)) & 0xff], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 8 * kRadix; i += kSortBlock) {
+    const u32 v = (&s_h[0][0])[i];
+    if (v) atomicAdd((unsigned long long*)&hist[i], (unsigned long long)v);
+  }
+}
+
+// exclusive scan of each pass's 256-bin histogram (one warp per pass)
+__global__ void k_sort_hist_scan(const u64* __restrict__ hist, u64* __restrict__ excl) {
+  const int p = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  u64 run = 0;
+  for (int c = 0; c < kRadix; c += 32) {
+    const u64 v = hist[p * kRadix + c + lane];
+    u64 incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u64 x = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += x;
+    }
+    excl[p * kRadix + c + lane] = run + incl - v;
+    run += __shfl_sync(0xffffffffu, incl, 31);
+  }
+}
+
+__device__ __forceinline__ u32 lanemask_lt() {
+  u32 m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+constexpr size_t kPassSmem = (size_t)kSortTile * 8 + (size_t)kSortTile + (size_t)kWarps * kRadix * 4;
+
+// One onesweep pass over the digit at bit `shift`.
+__global__ void __launch_bounds__(kSortBlock)
+k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __restrict__ kout,
+            u64* __restrict__ iout, u64 n, int shift, const u64* __restrict__ gexcl /*[256]*/,
+            u64* __restrict__ status /*[tiles][256]*/, u32* __restrict__ ticket, u32* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  u64* s_buf = (u64*)smem;                                   // kSortTile words (keys, then ids)
+  unsigned char* s_dj = smem + (size_t)kSortTile * 8;        // digit of staged element j
+  u32* s_wc = (u32*)(s_dj + kSortTile);                      // [kWarps][256] warp digit counts
+  __shared__ u32 s_tile;
+  __shared__ u32 s_dcnt[kRadix];
+  __shared__ u32 s_doff[kRadix];
+  __shared__ u64 s_gbase[kRadix];
+  __shared__ u32 s_scan[kWarps];
+
+  if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+  for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortBlock) s_wc[i] = 0;
+  __syncthreads();
+  const u32 tile = s_tile;
+  const u64 base = (u64)tile * kSortTile;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  u64 key[kSortItems];
+  u32 loc[kSortItems];
+  u32 dig[kSortItems];
+  const u32 lt = lanemask_lt();
+  u32* wc = s_wc + wid * kRadix;
+#pragma unroll
+  for (int it = 0; it < kSortItems; ++it) {
+    const u64 e = base + (u64)wid * 32 * kSortItems + (u64)it * 32 + lane;
+    const bool valid = e < n;
+    key[it] = valid ? kin[e] : 0ull;
+    const u32 d = valid ? (u32)((key[it] >> shift) & 0xff) : 0x100u;
+    dig[it] = d;
+    const u32 peers = __match_any_sync(0xffffffffu, d);
+    u32 cnt = 0;
+    if (valid) cnt = wc[d];
+    __syncwarp();
+    const u32 r = __popc(peers & lt);
+    if (valid && r == 0) wc[d] = cnt + __popc(peers);
+    __syncwarp();
+    loc[it] = cnt + r;
+  }
+  __syncthreads();
+  if (threadIdx.x < kRadix) {                 // per digit: exclusive over warps, tile total
+    const int d = threadIdx.x;
+    u32 run = 0;
+    for (int w = 0; w < kWarps; ++w) {
+      const u32 v = s_wc[w * kRadix + d];
+      s_wc[w * kRadix + d] = run;
+      run += v;
+    }
+    s_dcnt[d] = run;
+    const u64 pub = (tile == 0) ? (kFlagInc | (u64)run) : (kFlagAgg | (u64)run);
+    __threadfence();
+    ((volatile u64*)status)[(u64)tile * kRadix + d] = pub;
+    u32 incl = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u32 x = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += x;
+    }
+    if (lane == 31) s_scan[wid] = incl;
+    s_doff[d] = incl - run;
+  }
+  __syncthreads();
+  if (threadIdx.x < kRadix) {
+    const int d = threadIdx.x;
+    u32 add = 0;
+    for (int w = 0; w < wid; ++w) add += s_scan[w];
+    s_doff[d] += add;
+    u64 excl = 0;
+    if (tile > 0) {                           // decoupled look-back, bounded
+      int j = (int)tile - 1;
+      u32 spins = 0;
+      while (j >= 0) {
+        const u64 v = ((volatile u64*)status)[(u64)j * kRadix + d];
+        const u64 f = v & ~kValMask;
+        if (f == 0) {
+          if (++spins > kSpinLimit) { atomicOr(err, CF_ERR_SPIN_LIMIT); break; }
+          continue;
+        }
+        excl += v & kValMask;
+        if (f == kFlagInc) break;
+        --j;
+      }
+      __threadfence();
+      ((volatile u64*)status)[(u64)tile * kRadix + d] = kFlagInc | (excl + s_dcnt[d]);
+    }
+    s_gbase[d] = gexcl[d] + excl;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < kSortItems; ++it) {
+    if (dig[it] < 0x100u) {
+      loc[it] += s_doff[dig[it]] + wc[dig[it]];
+      s_buf[loc[it]] = key[it];
+      s_dj[loc[it]] = (unsigned char)dig[it];
+    }
+  }
+  __syncthreads();
+  const u64 left = n - base;
+  const int tv = (int)(left < (u64)kSortTile ? left : (u64)kSortTile);
+  for (int j = threadIdx.x; j < tv; j += kSortBlock) {
+    const u32 d = s_dj[j];
+    kout[s_gbase[d] + (u64)(j - (int)s_doff[d])] = s_buf[j];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < kSortItems; ++it) {
+    if (dig[it] < 0x100u) {
+      const u64 e = base + (u64)wid * 32 * kSortItems + (u64)it * 32 + lane;
+      s_buf[loc[it]] = iin[e];
+    }
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < tv; j += kSortBlock) {
+    const u32 d = s_dj[j];
+    iout[s_gbase[d] + (u64)(j - (int)s_doff[d])] = s_buf[j];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Merge join of two sorted key arrays.
+// ---------------------------------------------------------------------------
+constexpr int kMergeBlock = 256;
+constexpr int kMergeRun = 16;
+
+struct CfRun {
+  u64 irow, dlo, cnt;
+};
+
+__device__ __forceinline__ u64 lower_bound_u64(const u64* __restrict__ a, u64 lo, u64 hi, u64 key) {
+  while (lo < hi) {
+    const u64 mid = lo + ((hi - lo) >> 1);
+    if (a[mid] < key) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kMergeBlock)
+k_merge_runs(const u64* __restrict__ Dk, u64 nD, const u64* __restrict__ Ik, u64 nI, CfRun* __restrict__ runs,
+             u64 max_runs, unsigned long long* __restrict__ nruns, u64* __restrict__ npairs, u32* __restrict__ err) {
+  const u64 t = (u64)blockIdx.x * kMergeBlock + threadIdx.x;
+  const u64 r0 = t * kMergeRun;
+  if (r0 >= nI) return;
+  const u64 r1 = (r0 + kMergeRun < nI) ? r0 + kMergeRun : nI;
+  u64 pos = lower_bound_u64(Dk, 0, nD, Ik[r0]);
+  u64 local_pairs = 0;
+  for (u64 r = r0; r < r1; ++r) {
+    const u64 key = Ik[r];
+    if (pos < nD && Dk[pos] < key) {          // gallop to the first D key >= key
+      u64 step = 1, lo = pos + 1, hi = pos + 1;
+      while (hi < nD && Dk[hi] < key) { lo = hi + 1; hi = pos + (step <<= 1); }
+      if (hi > nD) hi = nD;
+      pos = lower_bound_u64(Dk, lo, hi, key);
+    }
+    u64 q = pos;
+    while (q < nD && Dk[q] == key) ++q;
+    if (q > pos) {
+      const u64 k = atomicAdd(nruns, 1ull);
+      if (k < max_runs) {
+        CfRun run;
+        run.irow = r; run.dlo = pos; run.cnt = q - pos;
+        runs[k] = run;
+      } else {
+        atomicOr(err, CF_ERR_PAIR_OVERFLOW);
+      }
+      local_pairs += q - pos;
+    }
+  }
+  if (local_pairs) atomicAdd((unsigned long long*)npairs, (unsigned long long)local_pairs);
+}
+
+}  // namespace
+
+// Workspace of one sort of n records: second key/id buffers, histograms, the
+// look-back status words of every pass and the tile tickets.
+extern "C" size_t cf_sort_tmp_bytes(u64 n) {
+  const u64 tiles = (n + kSortTile - 1) / kSortTile;
+  return (size_t)(2 * n * 8) + 2 * 8 * kRadix * 8 + (size_t)(8 * tiles * kRadix * 8) + 8 * 4 + 64;
+}
+
+// Sort (keys, ids) of length n by key, stably, in place (results end in the
+// caller's arrays).  key_bits: bits of the largest key (1..64); passes whose
+// digit is constant are skipped.  Synchronises the stream once (to read the
+// digit histogram).
+extern "C" int cf_sort_pairs(u64* keys, u64* ids, u64 n, int key_bits, void* tmp, size_t tmp_bytes, void* stream) {
+  if (n <= 1) return CF_OK;
+  if (!keys || !ids || !tmp) { cf_set_error("cf_sort_pairs: null buffer%s", ""); return CF_EBADARG; }
+  if (key_bits < 1 || key_bits > 64) { cf_set_error("cf_sort_pairs: key_bits must be 1..64%s", ""); return CF_EBADARG; }
+  if (n > (1ull << 40)) { cf_set_error("cf_sort_pairs: n too large%s", ""); return CF_EBADARG; }
+  if (tmp_bytes < cf_sort_tmp_bytes(n)) { cf_set_error("cf_sort_pairs: workspace too small%s", ""); return CF_ENOMEM; }
+  cudaStream_t st = (cudaStream_t)stream;
+  const u64 tiles = (n + kSortTile - 1) / kSortTile;
+  unsigned char* w = (unsigned char*)tmp;
+  u64* k2 = (u64*)w; w += n * 8;
+  u64* i2 = (u64*)w; w += n * 8;
+  u64* hist = (u64*)w; w += 8 * kRadix * 8;
+  u64* excl = (u64*)w; w += 8 * kRadix * 8;
+  u64* status = (u64*)w; w += 8 * tiles * kRadix * 8;
+  u32* tickets = (u32*)w; w += 8 * 4;
+  u32* errw = (u32*)w;
+  const int npass = (key_bits + 7) / 8;
+  cudaError_t e = cudaMemsetAsync(hist, 0, 8 * kRadix * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, (size_t)8 * tiles * kRadix * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(tickets, 0, 8 * 4 + 4, st);
+  if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: memset");
+  const unsigned hgrid = (unsigned)((n + kSortBlock * 8 - 1) / (kSortBlock * 8));
+  k_sort_hist<<<hgrid < 2048 ? hgrid : 2048, kSortBlock, 0, st>>>(keys, n, hist);
+  k_sort_hist_scan<<<1, 256, 0, st>>>(hist, excl);
+  CF_LAUNCH_CHECK("cf_sort_pairs: histogram");
+  u64 hh[8 * kRadix];
+  e = cudaMemcpyAsync(hh, hist, sizeof hh, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: histogram read");
+  e = cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPassSmem);
+  if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: smem attribute");
+  u64 *ka = keys, *ia = ids, *kb = k2, *ib = i2;
+  int done = 0;
+  for (int p = 0; p < npass; ++p) {
+    bool trivial = false;
+    for (int d = 0; d < kRadix; ++d) if (hh[p * kRadix + d] == n) trivial = true;
+    if (trivial) continue;
+    k_sort_pass<<<(unsigned)tiles, kSortBlock, kPassSmem, st>>>(ka, ia, kb, ib, n, 8 * p, excl + p * kRadix,
+                                                                 status + (u64)p * tiles * kRadix, tickets + p, errw);
+    CF_LAUNCH_CHECK("cf_sort_pairs: pass");
+    u64* t = ka; ka = kb; kb = t;
+    t = ia; ia = ib; ib = t;
+    ++done;
+  }
+  if (done & 1) {      // result sits in the workspace: copy back
+    e = cudaMemcpyAsync(keys, ka, n * 8, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ids, ia, n * 8, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: copy back");
+  }
+  u32 herr = 0;
+  e = cudaMemcpyAsync(&herr, errw, 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: error word");
+  if (herr & CF_ERR_SPIN_LIMIT) { cf_set_error("cf_sort_pairs: look-back wait exceeded its limit%s", ""); return CF_ETIMEOUT; }
+  return CF_OK;
+}
+
+extern "C" size_t cf_merge_run_bytes(void) { return sizeof(CfRun); }
+
+// Equal-key runs between sorted Dk[nD] and sorted Ik[nI]: runs[k] = (I row, first
+// D position, count), unordered; *nruns and *npairs (device u64 counters,
+// zeroed by the caller) receive the run and pair totals.
+extern "C" int cf_merge_join_runs(const u64* Dk, u64 nD, const u64* Ik, u64 nI, void* runs, u64 max_runs,
+                                  u64* nruns, u64* npairs, u32* err, void* stream) {
+  if (nD == 0 || nI == 0) return CF_OK;
+  if (!Dk || !Ik || !nruns || !npairs || !err || (max_runs && !runs)) {
+    cf_set_error("cf_merge_join_runs: null buffer%s", "");
+    return CF_EBADARG;
+  }
+  const u64 threads = (nI + kMergeRun - 1) / kMergeRun;
+  const u64 grid = (threads + kMergeBlock - 1) / kMergeBlock;
+  if (grid > 0x7fffffffull) { cf_set_error("cf_merge_join_runs: n too large%s", ""); return CF_EBADARG; }
+  k_merge_runs<<<(unsigned)grid, kMergeBlock, 0, (cudaStream_t)stream>>>(
+      Dk, nD, Ik, nI, (CfRun*)runs, max_runs, (unsigned long long*)nruns, npairs, err);
+  CF_LAUNCH_CHECK("cf_merge_join_runs");
+  return CF_OK;
+}

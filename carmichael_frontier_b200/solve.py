@@ -1,0 +1,351 @@
+"""solve(M, Q, B0, r, B) -> Carmichael hits: the exchange meet-in-the-middle join on one B200.
+
+A candidate is S = (B0 \\ D) u I with D an r-subset of the base B0 and I an
+r-subset of INS = Q \\ B0.  Because every prime q of the pool Q = Q(M) has
+(q-1) | M, prod(S) == 1 (mod M) makes S Carmichael by Korselt
+(src/mitm64.cpp:12-16).  The congruence is the residue join
+
+    prod(I) == prod(D) * (prod B0)^-1   (mod M)
+
+(the reference matches P0 * prod(I) == prod(D), gpu/mitm_gpu_mstar_driver.py:214-237;
+both sides here carry the constant on the D side, so the large I side needs no
+multiplier).  Device pipeline, all on one stream:
+
+  1. k_gen_part(D)  : every r-subset of B0, key form, scattered into residue partitions
+  2. k_gen_part(I)  : every r-subset of INS (in rank chunks if the side exceeds the budget)
+  3. k_join_part    : per partition, shared-memory table of D, stream I, emit equal pairs
+  4. k_check_pairs  : recompute residues, fp64 size screen, exact size, Korselt
+
+then one synchronisation, a copy of the (rare) checked pairs, and host
+certification of every hit by ``certify.verify_certificate``.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .certify import verify_certificate
+from .tables import DeviceTables, ncomb, unrank_lex
+
+RESULT_DTYPE = np.dtype([("flags", "<u4"), ("r", "<u4"), ("d_idx", "<u2", (16,)), ("i_idx", "<u2", (16,))])
+ALL_FLAGS = (_lib.HIT_KEY_EQUAL | _lib.HIT_SCREEN | _lib.HIT_SIZE_EXACT | _lib.HIT_KORSELT | _lib.HIT_DISJOINT)
+
+
+@dataclass(frozen=True)
+class Hit:
+    """One Carmichael number found by the join."""
+    D: tuple[int, ...]        # deleted base primes (ascending)
+    I: tuple[int, ...]        # inserted primes (ascending)
+    n: int                    # prod(S)
+    factors: tuple[int, ...]  # S, ascending
+
+
+@dataclass
+class SolveResult:
+    hits: list[Hit]
+    n_D: int                  # D-side records (C(|B0|, r))
+    n_I: int                  # I-side records (C(|INS|, r))
+    residue_pairs: int        # equal-residue (D, I) pairs (join_sorted's pair count)
+    screened: int             # pairs surviving the fp64 log-size screen
+    above_bound: int          # equal-residue pairs with prod(S) > B
+    rejected: int             # pairs failing the device or host checks (0 unless a bug)
+    device_ms: float | None = None
+    plan: dict = field(default_factory=dict)
+    pairs: list = field(default_factory=list)   # every equal-residue (D primes, I primes) pair
+    launches: int = 0                           # kernels of this library launched by the solve
+
+    @property
+    def records(self) -> int:
+        return self.n_D + self.n_I
+
+
+@dataclass
+class Tuning:
+    """Launch shape of the partitioned join (chosen by autotune.py when tuned)."""
+    d_per_part: int = 7000          # target D records per partition
+    max_parts: int = 4096
+    max_sbits: int = 14             # shared table of 2^sbits slots (4 B) per CTA
+    isplit: int = 0                 # CTAs per partition in the join (0 = automatic)
+    i_chunk_records: int = 1 << 31  # I-side records per generation/join chunk
+    pair_capacity: int = 1 << 14    # initial candidate-pair buffer (grown on overflow)
+    sigma: float = 6.0              # partition capacity = mean + sigma*sqrt(mean) + 16
+
+
+def _pow2ceil(x: int) -> int:
+    return 1 if x <= 1 else 1 << (x - 1).bit_length()
+
+
+def _cap(mean: float, sigma: float) -> int:
+    return int(math.ceil(mean + sigma * math.sqrt(max(mean, 1.0)) + 16))
+
+
+@dataclass
+class Instance:
+    M: int
+    B0: list[int]
+    INS: list[int]
+    r: int
+    B: int
+    P0: int
+
+    @staticmethod
+    def build(M: int, Q, B0, r: int, B: int) -> "Instance":
+        M, r, B = int(M), int(r), int(B)
+        if not (2 <= M < (1 << 62)):
+            raise ValueError("M must satisfy 2 <= M < 2^62 (keys are u64 residues)")
+        base = sorted(int(p) for p in B0)
+        if len(set(base)) != len(base):
+            raise ValueError("B0 has repeated primes")
+        bset = set(base)
+        ins = sorted(set(int(q) for q in Q) - bset)
+        if not (0 <= r <= 10):
+            raise ValueError("radius r must be 0..10")
+        if len(base) > 1024 or len(ins) > 1024:
+            raise ValueError("B0 and Q \\ B0 are limited to 1024 primes each")
+        if B < 1:
+            raise ValueError("size bound B must be >= 1")
+        P0 = 1
+        for p in base:
+            P0 *= p
+        if math.gcd(P0, M) != 1 or any(math.gcd(q, M) != 1 for q in ins):
+            raise ValueError("every pool prime must be coprime to M (q does not divide M)")
+        return Instance(M, base, ins, r, B, P0)
+
+
+class Solver:
+    """Reusable device state for repeated solves on one device and stream."""
+
+    def __init__(self, device=None, stream=None, tuning: Tuning | None = None):
+        import torch
+        self.torch = torch
+        self.lib = _lib.load()
+        self.device = torch.device(device if device is not None else "cuda")
+        if self.device.type != "cuda":
+            raise RuntimeError("the join runs on a CUDA device only")
+        self.stream = stream
+        self.tuning = tuning or Tuning()
+        self.tables = DeviceTables(self.device)
+        self._bufs: dict[str, object] = {}
+        self.result_bytes = self.lib.cf_pair_result_bytes()
+        assert self.result_bytes == RESULT_DTYPE.itemsize
+
+    # -- buffers -----------------------------------------------------------
+    def _buf(self, name: str, nbytes: int):
+        t = self._bufs.get(name)
+        if t is None or t.numel() < nbytes:
+            t = self.torch.empty(max(nbytes, 16), dtype=self.torch.uint8, device=self.device)
+            self._bufs[name] = t
+        return t
+
+    def _sh(self):
+        return _lib.stream_handle(self.stream)
+
+    # -- planning ------------------------------------------------------------
+    def plan(self, nD: int, nI: int, capD: int | None = None, capI: int | None = None,
+             pairs: int | None = None) -> dict:
+        tu = self.tuning
+        nparts = min(tu.max_parts, _pow2ceil(-(-nD // tu.d_per_part)))
+        chunk = min(nI, tu.i_chunk_records)
+        cD = capD or _cap(nD / nparts, tu.sigma)
+        cI = capI or _cap(chunk / nparts, tu.sigma)
+        cD = min(cD, nD)
+        cI = min(cI, chunk) if chunk else 1
+        sbits = 4
+        while sbits < tu.max_sbits and (1 << (sbits - 1)) < cD:
+            sbits += 1
+        isplit = tu.isplit or max(1, min(16, (2 * 148 * 2) // max(1, nparts)))
+        return dict(nparts=nparts, capD=max(cD, 1), capI=max(cI, 1), chunk=max(chunk, 1), sbits=sbits,
+                    isplit=isplit, pairs=pairs or tu.pair_capacity)
+
+    # -- one solve -----------------------------------------------------------
+    def _mark(self, marks, tag):
+        if marks is not None:
+            ev = self.torch.cuda.Event(enable_timing=True)
+            ev.record(self._torch_stream())
+            marks.append((tag, ev))
+
+    def enqueue(self, inst: Instance, plan: dict, marks: list | None = None):
+        """Queue the whole device pipeline for `inst` on the stream (no host sync).
+        `marks` (optional list) receives (tag, CUDA event) pairs around every kernel."""
+        torch, lib = self.torch, self.lib
+        r, M = inst.r, inst.M
+        nD, nIt = ncomb(len(inst.B0), r), ncomb(len(inst.INS), r)
+        P = plan["nparts"]
+        cpart = lib.cf_part_multiplier(M, P)
+        poolD = self.tables.pool(inst.B0, r, M, pow(inst.P0, -1, M))
+        poolI = self.tables.pool(inst.INS, r, M, 1)
+        screen = self.tables.screen(inst.P0, inst.B, 1e-6)
+        capD, capI, chunk = plan["capD"], plan["capI"], plan["chunk"]
+        Dbuf = self._buf("D", P * capD * 16)
+        Ibuf = self._buf("I", P * capI * 16)
+        ctr = self._buf("ctr", (2 * P + 8) * 4)
+        ctr_u32 = ctr[: (2 * P + 8) * 4].view(torch.int32)
+        dcnt = ctr_u32[:P]
+        icnt = ctr_u32[P:2 * P]
+        misc = ctr_u32[2 * P:]          # [0] npairs, [1] err
+        maxp = plan["pairs"]
+        pairs = self._buf("pairs", maxp * 16)
+        res = self._buf("res", maxp * self.result_bytes)
+        sh = self._sh()
+        dp = _lib.ptr
+        ctr_u32.zero_()
+        ck = _lib.check
+        launches = 0
+        self._mark(marks, "start")
+        ck(lib.cf_gen_part(dp(poolD), len(inst.B0), r, 0, nD, P, cpart, capD, dp(dcnt), dp(Dbuf),
+                           dp(misc) + 4, sh), "cf_gen_part(D)")
+        launches += 1
+        self._mark(marks, "gen_D")
+        for lo in range(0, nIt, chunk):
+            cnt = min(chunk, nIt - lo)
+            if lo:
+                icnt.zero_()
+            ck(lib.cf_gen_part(dp(poolI), len(inst.INS), r, lo, cnt, P, cpart, capI, dp(icnt), dp(Ibuf),
+                               dp(misc) + 4, sh), "cf_gen_part(I)")
+            self._mark(marks, "gen_I")
+            ck(lib.cf_join_part(dp(Dbuf), dp(dcnt), capD, dp(Ibuf), dp(icnt), capI, P, cpart, plan["sbits"],
+                                plan["isplit"], 0, dp(pairs), maxp, dp(misc), dp(misc) + 4, sh),
+               "cf_join_part")
+            self._mark(marks, "join")
+            launches += 2
+        ck(lib.cf_check_pairs(dp(poolD), dp(poolI), dp(screen), r, dp(pairs), dp(misc), maxp, dp(res),
+                              dp(misc) + 4, sh), "cf_check_pairs")
+        launches += 1
+        self._mark(marks, "check")
+        return dict(misc=misc, dcnt=dcnt, icnt=icnt, res=res, nD=nD, nI=nIt, plan=plan, launches=launches)
+
+    def collect(self, inst: Instance, h: dict, verify: bool = True) -> tuple[SolveResult | None, dict | None]:
+        """Synchronise, read counters; returns (result, None) or (None, bigger plan) on overflow."""
+        self._torch_stream().synchronize()
+        misc = h["misc"][:2].cpu().numpy().view(np.uint32)
+        npairs, err = int(misc[0]), int(misc[1])
+        plan = h["plan"]
+        if err & (_lib.ERR_PART_OVERFLOW | _lib.ERR_PAIR_OVERFLOW):
+            dmax = int(h["dcnt"].max().item())
+            imax = int(h["icnt"].max().item())
+            newp = dict(plan)
+            if err & _lib.ERR_PART_OVERFLOW:
+                newp["capD"] = max(plan["capD"], dmax + 16)
+                newp["capI"] = max(plan["capI"], imax + 16)
+            if err & _lib.ERR_PAIR_OVERFLOW:
+                newp["pairs"] = max(plan["pairs"] * 2, npairs + 16)
+            return None, newp
+        if err & _lib.ERR_SPIN_LIMIT:
+            raise _lib.CfError(_lib.CF_ETIMEOUT, "solve", "a bounded device wait gave up")
+        if err & _lib.ERR_KEY_MISMATCH:
+            raise _lib.CfError(_lib.CF_EBADARG, "solve", "checked pair with unequal residues (internal error)")
+        res = np.frombuffer(h["res"][: npairs * self.result_bytes].cpu().numpy().tobytes(), dtype=RESULT_DTYPE)
+        return self._finish(inst, h, res, verify), None
+
+    def _finish(self, inst: Instance, h: dict, res: np.ndarray, verify: bool) -> SolveResult:
+        r = inst.r
+        hits, screened, above, rejected, pairs = [], 0, 0, 0, []
+        bset = inst.B0
+        for row in res:
+            f = int(row["flags"])
+            if not f & _lib.HIT_KEY_EQUAL:
+                rejected += 1
+                continue
+            pairs.append((tuple(bset[int(x)] for x in row["d_idx"][:r]),
+                          tuple(inst.INS[int(x)] for x in row["i_idx"][:r])))
+            if not f & _lib.HIT_SCREEN:
+                above += 1
+                continue
+            screened += 1
+            if not f & _lib.HIT_SIZE_EXACT:
+                above += 1
+                continue
+            if (f & ALL_FLAGS) != ALL_FLAGS:
+                rejected += 1
+                continue
+            di = [int(x) for x in row["d_idx"][:r]]
+            ii = [int(x) for x in row["i_idx"][:r]]
+            D = tuple(bset[i] for i in di)
+            I = tuple(inst.INS[i] for i in ii)
+            dset = set(D)
+            fac = tuple(sorted([p for p in bset if p not in dset] + list(I)))
+            n = 1
+            for p in fac:
+                n *= p
+            ok = n <= inst.B and (n - 1) % inst.M == 0
+            if verify and ok:
+                ok, n2, _why = verify_certificate(fac)
+                ok = ok and n2 == n
+            if not ok:
+                rejected += 1
+                continue
+            hits.append(Hit(D, I, n, fac))
+        hits.sort(key=lambda x: (x.n, x.D, x.I))
+        pairs.sort()
+        return SolveResult(hits=hits, n_D=h["nD"], n_I=h["nI"], residue_pairs=len(res), screened=screened,
+                           above_bound=above, rejected=rejected, plan=dict(h["plan"]), pairs=pairs)
+
+    def solve_instance(self, inst: Instance, verify: bool = True, timed: bool = False,
+                       marks: list | None = None) -> SolveResult:
+        if inst.r == 0:
+            return self._solve_r0(inst)
+        nD, nI = ncomb(len(inst.B0), inst.r), ncomb(len(inst.INS), inst.r)
+        if nI == 0 or nD == 0:
+            return SolveResult([], nD, nI, 0, 0, 0, 0)
+        plan = self.plan(nD, nI)
+        for _attempt in range(6):
+            ev0 = ev1 = None
+            if timed:
+                ev0 = self.torch.cuda.Event(enable_timing=True)
+                ev1 = self.torch.cuda.Event(enable_timing=True)
+                ev0.record(self._torch_stream())
+            if marks is not None:
+                marks.clear()
+            h = self.enqueue(inst, plan, marks)
+            if timed:
+                ev1.record(self._torch_stream())
+            out, newp = self.collect(inst, h, verify)
+            if out is not None:
+                if timed:
+                    out.device_ms = ev0.elapsed_time(ev1)
+                out.launches = h["launches"]
+                return out
+            plan = self.plan(nD, nI, newp["capD"], newp["capI"], newp["pairs"])
+        raise _lib.CfError(_lib.CF_EOVERFLOW, "solve", "capacities kept overflowing")
+
+    def _torch_stream(self):
+        return self.stream if self.stream is not None else self.torch.cuda.current_stream(self.device)
+
+    def _solve_r0(self, inst: Instance) -> SolveResult:
+        n = inst.P0
+        hits = []
+        if n % inst.M == 1 % inst.M and n <= inst.B:
+            ok, _, _ = verify_certificate(inst.B0)
+            if ok:
+                hits.append(Hit((), (), n, tuple(inst.B0)))
+        return SolveResult(hits, 1, 1, int(n % inst.M == 1 % inst.M), len(hits), 0, 0)
+
+    def solve(self, M: int, Q, B0, r: int, B: int, verify: bool = True, timed: bool = False) -> SolveResult:
+        return self.solve_instance(Instance.build(M, Q, B0, r, B), verify=verify, timed=timed)
+
+
+_default_solvers: dict = {}
+
+
+def solve(M: int, Q, B0, r: int, B: int, device=None, verify: bool = True) -> SolveResult:
+    """Every Carmichael hit S = (B0 \\ D) u I with |D| = |I| = r, prod(S) == 1 (mod M), prod(S) <= B.
+
+    Q is the eligible pool Q(M) (primes q with (q-1) | M and q not dividing M);
+    INS = Q \\ B0.  Hits are certified on the host and returned ascending by n."""
+    import torch
+    dev = torch.device(device if device is not None else "cuda")
+    key = (dev.type, dev.index)
+    s = _default_solvers.get(key)
+    if s is None:
+        s = _default_solvers[key] = Solver(dev)
+    return s.solve(M, Q, B0, r, B, verify=verify)
+
+
+def decode_pair(inst: Instance, d_rank: int, i_rank: int):
+    """(D primes, I primes) of a pair of lexicographic ranks."""
+    di = unrank_lex(d_rank, len(inst.B0), inst.r)
+    ii = unrank_lex(i_rank, len(inst.INS), inst.r)
+    return tuple(inst.B0[i] for i in di), tuple(inst.INS[i] for i in ii)

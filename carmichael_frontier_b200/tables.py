@@ -1,0 +1,141 @@
+"""Host-side tables for the kernels: pool tables, screen tables, exact helpers.
+
+Pool tables are filled by the C ABI (``cf_pool_prepare``) into host buffers and
+copied to the device once per (prime list, radius, modulus, multiplier); the
+copies are cached by content so repeated solves at one modulus reuse them.
+"""
+from __future__ import annotations
+
+import math
+from functools import lru_cache
+from math import comb
+
+import numpy as np
+
+from . import _lib
+
+MAX_POOL = 1024
+MAX_R = 10
+M_LIMIT = 1 << 62
+
+
+def pool_table_host(primes, r: int, M: int, mult: int) -> np.ndarray:
+    """Pool table (uint8 host array) for the r-subsets of `primes` modulo M."""
+    lib = _lib.load()
+    n = len(primes)
+    nbytes = lib.cf_pool_bytes(n, r)
+    if nbytes == 0:
+        raise ValueError(f"pool of {n} primes at radius {r} is outside 1..{MAX_POOL} x 1..16")
+    pr = np.ascontiguousarray(np.asarray([int(p) for p in primes], dtype=np.uint64))
+    out = np.zeros(nbytes, dtype=np.uint8)
+    _lib.check(lib.cf_pool_prepare(pr.ctypes.data, n, r, M, int(mult) % M, out.ctypes.data, nbytes),
+               "cf_pool_prepare")
+    return out
+
+
+class DeviceTables:
+    """Content-keyed cache of device copies of small host tables."""
+
+    def __init__(self, device, max_entries: int = 64):
+        self.device = device
+        self.max_entries = max_entries
+        self._cache: dict = {}
+
+    def get(self, key, make):
+        import torch
+        t = self._cache.get(key)
+        if t is None:
+            host = make()
+            t = torch.from_numpy(host).to(self.device, non_blocking=False)
+            if len(self._cache) >= self.max_entries:
+                self._cache.pop(next(iter(self._cache)))
+            self._cache[key] = t
+        return t
+
+    def pool(self, primes, r: int, M: int, mult: int):
+        key = ("pool", tuple(int(p) for p in primes), r, M, int(mult) % M)
+        return self.get(key, lambda: pool_table_host(primes, r, M, mult))
+
+    def screen(self, P0: int, B: int, eps: float):
+        key = ("screen", P0, B, eps)
+        return self.get(key, lambda: screen_table_host(P0, B, eps))
+
+
+def limbs32(x: int, nlimbs: int | None = None) -> np.ndarray:
+    """Little-endian base-2^32 limbs of a non-negative integer."""
+    if x < 0:
+        raise ValueError("negative")
+    n = max(1, (x.bit_length() + 31) // 32) if nlimbs is None else nlimbs
+    return np.array([(x >> (32 * i)) & 0xFFFFFFFF for i in range(n)], dtype=np.uint32)
+
+
+def screen_table_host(P0: int, B: int, eps: float) -> np.ndarray:
+    lib = _lib.load()
+    if B < 1:
+        raise ValueError("size bound B must be >= 1")
+    if B.bit_length() > 2048:
+        raise ValueError("size bound B must be below 2^2048")
+    lb = limbs32(B)
+    nbytes = lib.cf_screen_bytes()
+    out = np.zeros(nbytes, dtype=np.uint8)
+    _lib.check(lib.cf_screen_prepare(lb.ctypes.data, len(lb), math.log2(P0), math.log2(B), eps,
+                                     out.ctypes.data, nbytes), "cf_screen_prepare")
+    return out
+
+
+@lru_cache(maxsize=4096)
+def ncomb(n: int, r: int) -> int:
+    return comb(n, r)
+
+
+def unrank_lex(rank: int, n: int, r: int) -> tuple[int, ...]:
+    """Subset at lexicographic CNS rank (the order of gen_records, gpu/mitm_gpu2.py:40-52)."""
+    idx = []
+    start = 0
+    for pos in range(r):
+        rem = r - pos - 1
+        for c in range(start, n):
+            cnt = ncomb(n - 1 - c, rem)
+            if rank < cnt:
+                idx.append(c)
+                start = c + 1
+                break
+            rank -= cnt
+    return tuple(idx)
+
+
+def rank_lex(idx, n: int) -> int:
+    """Inverse of unrank_lex."""
+    r = len(idx)
+    rank = 0
+    start = 0
+    for pos, c in enumerate(idx):
+        rem = r - pos - 1
+        for c2 in range(start, c):
+            rank += ncomb(n - 1 - c2, rem)
+        start = c + 1
+    return rank
+
+
+def unrank_colex(v: int, r: int, n: int) -> tuple[int, ...]:
+    """Inverse of the colex rank sum_j C(i_j, j+1) (src/mitm64_idump_stream2.cpp:26-29)."""
+    v = int(v)
+    idx = []
+    x = n - 1
+    for j in range(r - 1, -1, -1):
+        while ncomb(x, j + 1) > v:
+            x -= 1
+        idx.append(x)
+        v -= ncomb(x, j + 1)
+        x -= 1
+    if v != 0:
+        raise ValueError("not a colex rank")
+    return tuple(reversed(idx))
+
+
+def key_of(M: int, v: int) -> int:
+    return int(_lib.load().cf_key_of(M, v % M))
+
+
+def canon_of(M: int, k: int) -> int:
+    return int(_lib.load().cf_canon_of(M, k))

@@ -1,0 +1,154 @@
+/* cfmitm.h -- C ABI of the B200 exchange meet-in-the-middle residue join.
+ *
+ * Every function is extern "C", takes plain pointers and sizes, and returns an
+ * int status (0 = ok, negative = error; cf_last_error_string() says why).
+ * Device buffers are owned by the caller; functions that need scratch take a
+ * (tmp, tmp_bytes) workspace whose size a *_tmp_bytes / *_bytes query gives.
+ * Work is queued on the caller's CUDA stream (`stream`, a cudaStream_t, may be
+ * NULL for the legacy default stream); only the calls documented as
+ * synchronising wait for the device.  The library never throws.
+ *
+ * Residues are held in "key form" (see carmichael_frontier_b200/csrc/cf_common.cuh):
+ * a bijection of [0, M) onto itself, so equal keys <=> equal residues mod M.
+ * cf_gen_subsets(..., canon=1) emits canonical residues instead.
+ *
+ * Reference interfaces replaced (paths inside AlexanderEastwood/carmichael-frontier):
+ *   gen_records / generate()   gpu/mitm_gpu2.py:24-98
+ *   sort_side()                gpu/mitm_gpu2.py:101-104
+ *   join_sorted()              gpu/mitm_gpu2.py:107-119
+ *   exact pair re-check        gpu/mitm_gpu_mstar_driver.py:226-237, ref/ref_carmichael.py:55-72
+ *   CPU join engine            src/mitm64.cpp:50-121 (recD / worker)
+ */
+#ifndef CFMITM_H
+#define CFMITM_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CF_OK 0
+#define CF_EBADARG -1
+#define CF_ENOMEM -2
+#define CF_ECUDA -3
+#define CF_EOVERFLOW -4
+#define CF_ETIMEOUT -5
+
+/* error-word bits written by kernels into the caller's u32 `err` word */
+#define CF_ERR_PART_OVERFLOW 1u
+#define CF_ERR_PAIR_OVERFLOW 2u
+#define CF_ERR_TABLE_FULL 4u
+#define CF_ERR_SPIN_LIMIT 8u
+#define CF_ERR_KEY_MISMATCH 16u
+
+/* pair-check result flags (CfPairResult.flags) */
+#define CF_HIT_KEY_EQUAL 1u
+#define CF_HIT_SCREEN 2u
+#define CF_HIT_SIZE_EXACT 4u
+#define CF_HIT_KORSELT 8u
+#define CF_HIT_DISJOINT 16u
+
+/* ABI version of this header (1). */
+int cf_version(void);
+
+/* Human-readable reason for the last non-zero status on this host thread.
+ * Replaces the reference's Python assertion messages (gpu/mitm_gpu2.py:83-85,
+ * gpu/igen_gpu.py:103-105). */
+const char* cf_last_error_string(void);
+
+/* ---- host-side table preparation (no device calls) ---------------------- */
+
+/* Bytes of the pool table for n primes and radius r (0 if out of range). */
+size_t cf_pool_bytes(int n, int r);
+
+/* Fill a pool table (host buffer) for the r-subsets of primes[0..n-1] modulo M
+ * (2 <= M < 2^62) with leading multiplier `mult` (the D side of a solve uses
+ * (prod B0)^-1 mod M, the I side 1; gen_records' `mult` argument otherwise).
+ * Holds each prime in key form, log2 of each prime and the binomial table.
+ * Replaces the host half of generate(): gpu/mitm_gpu2.py:70-93. */
+int cf_pool_prepare(const uint64_t* primes, int n, int r, uint64_t M, uint64_t mult, void* out,
+                    size_t out_bytes);
+
+/* key(v mod M), its inverse, and the product of two keys computed by the
+ * kernels' own Montgomery/CRT code compiled for the host (host helpers). */
+uint64_t cf_key_of(uint64_t M, uint64_t v);
+uint64_t cf_canon_of(uint64_t M, uint64_t key);
+uint64_t cf_key_mul(uint64_t M, uint64_t kx, uint64_t ky);
+
+/* floor(2^64 * nparts / M): residue partition p(key) = mulhi(key, multiplier). */
+uint64_t cf_part_multiplier(uint64_t M, uint32_t nparts);
+
+/* Size-screen table for cf_check_pairs: B as little-endian 32-bit limbs
+ * (1..64 limbs), log2(prod B0), log2(B) and the fp64 margin eps. */
+size_t cf_screen_bytes(void);
+int cf_screen_prepare(const uint32_t* limbsB, int nlimbs, double lgP0, double lgB, double eps, void* out,
+                      size_t out_bytes);
+
+/* ---- generation ---------------------------------------------------------- */
+
+/* gen_records drop-in (gpu/mitm_gpu2.py:24-98): record t is the r-subset at
+ * lexicographic rank lo+t of the pool in `pool_dev` (a cf_pool_prepare table
+ * copied to the device).  keys[t] = mult * prod(p) mod M (canonical residue if
+ * canon != 0, else key form).  ids[t]: id_mode 0 = indices packed `bits` per
+ * position (gen_records' id), 1 = lexicographic rank, 2 = colexicographic rank
+ * sum C(i_j, j+1) (the rank id of src/mitm64_idump_stream2.cpp:26-29).
+ * Requires 1 <= r <= 10 and lo + count <= C(n, r). */
+int cf_gen_subsets(const void* pool_dev, int n, int r, uint64_t lo, uint64_t count, int id_mode, int bits,
+                   int canon, uint64_t* keys, uint64_t* ids, void* stream);
+
+/* Partitioned generation for the solve path: the records of ranks [lo, lo+count)
+ * (key form, id = lexicographic rank) are scattered into nparts (1..4096)
+ * residue partitions of capacity cap records each: partition p occupies
+ * out[p*cap .. p*cap+cap) as 16-byte {key, id} records (the reference's record
+ * layout, src/mitm64_idump_stream.cpp:6-12).  counts[p] (device, zeroed by the
+ * caller) receives the number of records routed to p, even beyond cap; then
+ * CF_ERR_PART_OVERFLOW is set in *err and the caller retries with a larger cap.
+ * Replaces generate() + sort_side() as the producer of a joinable side. */
+size_t cf_gen_part_smem_bytes(int n, uint32_t nparts);
+int cf_gen_part(const void* pool_dev, int n, int r, uint64_t lo, uint64_t count, uint32_t nparts, uint64_t cpart,
+                uint32_t cap, uint32_t* counts, void* out, uint32_t* err, void* stream);
+
+/* ---- join ---------------------------------------------------------------- */
+
+/* Partitioned equal-residue join: for every partition, every (D, I) record pair
+ * with equal keys is appended to pairs[] as {D id, I id} (16 bytes) through the
+ * device counter *npairs (zeroed by the caller); beyond max_pairs the count
+ * keeps growing and CF_ERR_PAIR_OVERFLOW is set.  sbits (4..15): shared-memory
+ * table of 2^sbits slots (4 bytes each) per CTA; isplit: CTAs per partition;
+ * grid: 0 = one CTA per (partition, split).  Replaces join_sorted
+ * (gpu/mitm_gpu2.py:107-119) and mitm64.cpp's hash probe (src/mitm64.cpp:85-101). */
+size_t cf_join_part_smem_bytes(int sbits);
+int cf_join_part(const void* D, const uint32_t* dcount, uint32_t capD, const void* I, const uint32_t* icount,
+                 uint32_t capI, uint32_t nparts, uint64_t cpart, int sbits, uint32_t isplit, uint32_t grid,
+                 void* pairs, uint32_t max_pairs, uint32_t* npairs, uint32_t* err, void* stream);
+
+/* Exact check of candidate pairs (lexicographic-rank ids): recomputed residues,
+ * conservative fp64 log-size screen, exact size n <= B, Korselt, distinctness.
+ * results[t] (cf_pair_result_bytes() each) for t < min(*npairs, max_pairs).
+ * Replaces the driver's exact re-check (gpu/mitm_gpu_mstar_driver.py:226-237). */
+size_t cf_pair_result_bytes(void);
+int cf_check_pairs(const void* poolD, const void* poolI, const void* screen, int r, const void* pairs,
+                   const uint32_t* npairs, uint32_t max_pairs, void* results, uint32_t* err, void* stream);
+
+/* ---- sorted-side drop-ins ------------------------------------------------ */
+
+/* Stable LSD radix sort of (keys, ids)[n] by key over key_bits bits, in place;
+ * workspace cf_sort_tmp_bytes(n).  Synchronises `stream` once.
+ * Replaces sort_side (gpu/mitm_gpu2.py:101-104). */
+size_t cf_sort_tmp_bytes(uint64_t n);
+int cf_sort_pairs(uint64_t* keys, uint64_t* ids, uint64_t n, int key_bits, void* tmp, size_t tmp_bytes,
+                  void* stream);
+
+/* Equal-key runs between sorted Dk[nD] and sorted Ik[nI]: runs (24 bytes each,
+ * {I row, first D position, count}), unordered, counted in the device u64
+ * counters *nruns and *npairs (zeroed by the caller).  The count/emit core of
+ * join_sorted (gpu/mitm_gpu2.py:107-119). */
+size_t cf_merge_run_bytes(void);
+int cf_merge_join_runs(const uint64_t* Dk, uint64_t nD, const uint64_t* Ik, uint64_t nI, void* runs,
+                       uint64_t max_runs, uint64_t* nruns, uint64_t* npairs, uint32_t* err, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFMITM_H */

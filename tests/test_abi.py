@@ -1,0 +1,135 @@
+"""C-ABI library: loads without a GPU, exports every declared symbol, host helpers are exact."""
+import ctypes as C
+import math
+import os
+import random
+import re
+
+import numpy as np
+import pytest
+
+from carmichael_frontier_b200 import _lib, tables
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    out = []
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if h.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", h)).read()
+            txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+            out += re.findall(r"\b(cf_[a-z0-9_]+)\s*\(", txt)
+    return sorted(set(out))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    syms = declared_symbols()
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(lib, s), s
+    bound = {name for name, _, _ in _lib.SIGNATURES}
+    assert set(syms) <= bound
+
+
+def test_version_and_error_string():
+    lib = _lib.load()
+    assert lib.cf_version() == 1
+    assert isinstance(lib.cf_last_error_string(), bytes)
+
+
+def test_bad_arguments_fail_loudly_without_gpu():
+    lib = _lib.load()
+    buf = np.zeros(64, dtype=np.uint8)
+    pr = np.array([3, 5, 7], dtype=np.uint64)
+    assert lib.cf_pool_prepare(pr.ctypes.data, 3, 2, 1 << 62, 1, buf.ctypes.data, 64) == _lib.CF_EBADARG
+    assert b"table buffer too small" in lib.cf_last_error_string() or b"M < 2^62" in lib.cf_last_error_string()
+    assert lib.cf_gen_subsets(None, 3, 2, 0, 1, 0, 8, 1, None, None, None) == _lib.CF_EBADARG
+    assert lib.cf_join_part(None, None, 1, None, None, 1, 1, 1, 2, 1, 0, None, 0, None, None, None) == _lib.CF_EBADARG
+    with pytest.raises(_lib.CfError):
+        _lib.check(lib.cf_gen_subsets(None, 3, 2, 0, 1, 0, 8, 1, None, None, None), "probe")
+
+
+def _hostkey(M, v):
+    a = (M & -M).bit_length() - 1
+    m = M >> a
+    X = (v % m) * pow(2, 64, m) % m if m > 1 else 0
+    return (X << a) | (v & ((1 << a) - 1))
+
+
+@pytest.mark.parametrize("M", [21621600, 9025877244384000, 1768248177696000, (1 << 62) - 2, 3 * (1 << 50),
+                               1 << 40, 135137, 2, 6])
+def test_key_form_is_a_bijection_and_round_trips(M):
+    rng = random.Random(M)
+    for _ in range(200):
+        v = rng.randrange(M)
+        k = tables.key_of(M, v)
+        assert k == _hostkey(M, v)
+        assert 0 <= k < M
+        assert tables.canon_of(M, k) == v
+
+
+@pytest.mark.parametrize("M", [21621600, 9025877244384000, (1 << 62) - 2, 3 * (1 << 50), 1 << 40, 135137, 6])
+def test_key_product_is_the_residue_product(M):
+    # cf_key_mul runs the kernels' Montgomery/CRT product (same inline code) on the host
+    lib = _lib.load()
+    rng = random.Random(M + 1)
+    for _ in range(300):
+        x, y = rng.randrange(M), rng.randrange(M)
+        k = lib.cf_key_mul(M, tables.key_of(M, x), tables.key_of(M, y))
+        assert tables.canon_of(M, k) == x * y % M
+
+
+def test_pool_table_layout():
+    lib = _lib.load()
+    primes = [11, 13, 17, 19, 23, 29, 31]
+    M = 21621600
+    t = tables.pool_table_host(primes, 3, M, 5)
+    w = t.view(np.uint64)
+    assert w[0] == 0x43464d49544d3031
+    assert int(w[1]) == M and int(w[5]) == 5 and int(w[6]) == 7 and int(w[7]) == 3   # M, a, n, R
+    assert int(w[8]) == tables.key_of(M, 5)                 # mult_key
+    assert int(w[9]) == math.comb(7, 3)                     # total
+    n = 7
+    pkey = w[32:32 + n]
+    assert [int(x) for x in pkey] == [tables.key_of(M, p) for p in primes]
+    assert [int(x) for x in w[32 + n:32 + 2 * n]] == primes
+    lg = w[32 + 2 * n:32 + 3 * n].view(np.float64)
+    assert np.allclose(lg, np.log2(primes), rtol=0, atol=1e-15)
+    binom = w[32 + 3 * n:].reshape(n + 1, 4)
+    for x in range(n + 1):
+        for y in range(4):
+            assert int(binom[x, y]) == math.comb(x, y)
+
+
+def test_partition_multiplier():
+    lib = _lib.load()
+    for M in (21621600, 9025877244384000, (1 << 62) - 2):
+        for P in (1, 2, 1024, 4096):
+            c = lib.cf_part_multiplier(M, P)
+            assert c == (P << 64) // M
+            for key in (0, 1, M // 2, M - 1):
+                assert (key * c) >> 64 < P
+
+
+def test_screen_table():
+    lib = _lib.load()
+    B = 10 ** 148
+    t = tables.screen_table_host(3 ** 300, B, 1e-6)
+    assert len(t) == lib.cf_screen_bytes()
+    d = t[:24].view(np.float64)
+    assert abs(d[0] - 300 * math.log2(3)) < 1e-9 and abs(d[1] - 148 * math.log2(10)) < 1e-9 and d[2] == 1e-6
+    with pytest.raises(ValueError):
+        tables.screen_table_host(3, 1 << 3000, 1e-6)
+
+
+def test_unrank_rank_lex_round_trip():
+    for n, r in [(10, 3), (29, 2), (64, 5), (150, 5)]:
+        total = math.comb(n, r)
+        for rank in [0, 1, total // 3, total - 1]:
+            idx = tables.unrank_lex(rank, n, r)
+            assert list(idx) == sorted(set(idx)) and len(idx) == r
+            assert tables.rank_lex(idx, n) == rank
+    assert tables.unrank_lex(0, 10, 3) == (0, 1, 2)
+    assert tables.unrank_lex(math.comb(10, 3) - 1, 10, 3) == (7, 8, 9)

@@ -1,0 +1,95 @@
+"""solve(): the partitioned join against the oracle and the reference's own results."""
+import math
+import random
+
+import pytest
+
+import oracle as O
+from carmichael_frontier_b200 import Solver, Tuning, workloads as W
+from carmichael_frontier_b200.solve import Instance
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def solver(cuda):
+    return Solver(cuda)
+
+
+def as_lists(pairs):
+    return sorted([list(D), list(I)] for D, I in pairs)
+
+
+def test_config1_two_hits(solver, golden):
+    w = W.config1()
+    res = solver.solve(w.M, w.Q, w.B0, w.r, w.B)
+    g = golden["config1"]
+    assert res.residue_pairs == 2 and res.rejected == 0
+    assert as_lists(res.pairs) == g["pairs"]
+    assert sorted([list(h.D), list(h.I), str(h.n)] for h in res.hits) == g["hits"]
+    assert res.n_D == 406 and res.n_I == math.comb(157, 2)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_small_instances_vs_exhaustive(solver, seed):
+    rng = random.Random(seed)
+    M = W.draw_modulus(100 + seed)
+    Q = W.eligible_pool(M, 5518)
+    k = rng.randint(12, 24)
+    r = rng.randint(1, 3)
+    Qs = Q[: k + rng.randint(r, 50)]
+    B0 = Qs[:k]
+    P0 = W.product(B0)
+    # a bound that cuts the pair set somewhere in the middle, and an unbounded one
+    for B in (P0 * 10 ** rng.randint(0, 12), 1 << 2040):
+        res = solver.solve(M, Qs, B0, r, B)
+        pairs, hits = O.solve_exhaustive(M, Qs, B0, r, B)
+        assert as_lists(res.pairs) == as_lists(pairs)
+        assert [(h.D, h.I, h.n) for h in res.hits] == [(tuple(D), tuple(I), n) for D, I, n in hits]
+        assert res.rejected == 0
+
+
+def test_small_modulus_many_pairs_grows_buffers(cuda):
+    # tiny M: residues collide massively, so partitions and the pair buffer overflow and are regrown
+    s = Solver(cuda, tuning=Tuning(d_per_part=64, pair_capacity=16, sigma=0.0))
+    M = 2 ** 5 * 3 ** 2 * 5 * 7 * 11 * 13
+    Q = W.eligible_pool(M)
+    B0 = Q[:20]
+    res = s.solve(M, Q, B0, 3, 1 << 2040)
+    pairs, hits = O.solve_exhaustive(M, Q, B0, 3, 1 << 2040)
+    assert len(pairs) > 200
+    assert as_lists(res.pairs) == as_lists(pairs)
+    assert len(res.hits) == len(hits) and res.rejected == 0
+
+
+@pytest.mark.parametrize("idx", [1, 4, 0])
+def test_config2_full_size_matches_reference_mitm64(solver, golden, idx):
+    g = golden["config2"][idx]
+    w = W.Workload(g["name"], g["M"], tuple(g["Q"]), tuple(g["B0"]), g["r"], int(g["B"]))
+    res = solver.solve(w.M, w.Q, w.B0, w.r, w.B)
+    assert res.n_D == g["d_leaves"] and res.n_I == g["i_leaves"]
+    assert res.residue_pairs == g["matches"]
+    assert as_lists(res.pairs) == g["pairs"]
+    assert sorted([list(h.D), list(h.I), str(h.n)] for h in res.hits) == g["hits"]
+
+
+def test_positive_control_recovers_previous_incumbent(solver, golden):
+    pc = golden["positive_control"]
+    N = int(pc["N"])
+    res = solver.solve(pc["M"], pc["B0"] + pc["INS"], pc["B0"], pc["r"], N)
+    assert res.n_D == math.comb(64, 7) and res.n_I == math.comb(30, 7)
+    assert any(h.n == N for h in res.hits)
+    assert (tuple(pc["D_need"]), tuple(pc["I_need"])) in set(res.pairs)
+    assert res.rejected == 0
+
+
+def test_edge_cases(solver):
+    w = W.config1()
+    res = solver.solve(w.M, w.B0, w.B0, 2, w.B)          # no insertions
+    assert res.hits == [] and res.n_I == 0
+    res = solver.solve(w.M, w.Q, w.B0, 0, w.B)           # radius 0: the base itself
+    assert res.n_D == 1
+    with pytest.raises(ValueError):
+        solver.solve(w.M * 2 ** 40, w.Q, w.B0, 2, w.B)   # M >= 2^62
+    with pytest.raises(ValueError):
+        solver.solve(w.M, w.Q + (13,), w.B0, 2, w.B)   # 13 divides M

@@ -1,0 +1,79 @@
+"""sort_side / join_sorted drop-ins against the numpy restatements (stable order, every pair)."""
+import random
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from carmichael_frontier_b200 import mitm_gpu2 as G
+from carmichael_frontier_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+def to_dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint64)).cuda()
+
+
+@pytest.mark.parametrize("n,bits", [(1, 62), (2, 8), (1000, 62), (8193, 20), (300_000, 62), (2_000_003, 64),
+                                    (100_000, 4)])
+def test_sort_side_is_numpy_stable_sort(cuda, n, bits):
+    rng = np.random.default_rng(n + bits)
+    keys = rng.integers(0, 1 << min(bits, 63), size=n, dtype=np.uint64)
+    if bits == 64:
+        keys |= rng.integers(0, 2, size=n, dtype=np.uint64) << np.uint64(63)
+    ids = np.arange(n, dtype=np.uint64) * np.uint64(7919)
+    ks, is_ = G.sort_side(to_dev(keys), to_dev(ids))
+    ek, ei = O.sort_side(keys, ids)
+    assert np.array_equal(host(ks), ek)
+    assert np.array_equal(host(is_), ei)    # stability: ties keep input order
+
+
+def test_sort_side_all_equal_keys(cuda):
+    keys = np.full(50_000, 123456789, dtype=np.uint64)
+    ids = np.arange(50_000, dtype=np.uint64)
+    ks, is_ = G.sort_side(to_dev(keys), to_dev(ids))
+    assert np.array_equal(host(is_), ids)
+
+
+def test_join_sorted_config1_and_random(cuda):
+    w = W.config1()
+    P0 = O.product(w.B0)
+    Dk, Did = G.generate(list(w.B0), 2, w.M, 1, 6)
+    Ik, Iid = G.generate(list(w.INS), 2, w.M, P0 % w.M, 8)
+    Dk, Did = G.sort_side(Dk, Did)
+    Ik, Iid = G.sort_side(Ik, Iid)
+    pd, pi = G.join_sorted(Dk, Did, Ik, Iid)
+    ed, ei = O.join_sorted(*O.sort_side(*O.gen_records(w.B0, 2, w.M, 1, 6)),
+                           *O.sort_side(*O.gen_records(w.INS, 2, w.M, P0 % w.M, 8)))
+    assert np.array_equal(host(pd), ed) and np.array_equal(host(pi), ei)
+    assert len(ed) == 2
+    # dense duplicates on both sides
+    rng = np.random.default_rng(5)
+    for nD, nI, span in [(1000, 50_000, 3000), (70_000, 900, 500), (5, 5, 2), (100_000, 100_000, 1 << 40)]:
+        dk = np.sort(rng.integers(0, span, nD, dtype=np.uint64))
+        ik = np.sort(rng.integers(0, span, nI, dtype=np.uint64))
+        did = rng.integers(0, 1 << 62, nD, dtype=np.uint64)
+        iid = rng.integers(0, 1 << 62, nI, dtype=np.uint64)
+        pd, pi = G.join_sorted(to_dev(dk), to_dev(did), to_dev(ik), to_dev(iid))
+        ed, ei = O.join_sorted(dk, did, ik, iid)
+        assert np.array_equal(host(pd), ed) and np.array_equal(host(pi), ei)
+
+
+def test_join_sorted_empty(cuda):
+    e = to_dev(np.zeros(0, np.uint64))
+    one = to_dev(np.array([5], np.uint64))
+    pd, pi = G.join_sorted(e, e, one, one)
+    assert pd.numel() == 0 and pi.numel() == 0
+    pd, pi = G.join_sorted(one, one, to_dev(np.array([4], np.uint64)), one)
+    assert pd.numel() == 0
+
+
+def test_decode_ids_matches_reference_packing(cuda):
+    k, i = G.generate([3, 5, 7, 11, 13], 3, 1000, 1, 6)
+    assert G.decode_ids(i, 3, 6)[:2] == [(0, 1, 2), (0, 1, 3)]
