@@ -45,6 +45,8 @@ def parse_args():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="CPU-baseline budget (seconds of work)")
+    ap.add_argument("--case", type=int, default=None,
+                    help="profile a single seeded modulus (every step solves config-2 seed CASE)")
     return ap.parse_args()
 
 
@@ -55,9 +57,11 @@ def dist_env():
     return rank, world, local
 
 
-def step_seeds(steps: int, world: int, rank: int):
+def step_seeds(steps: int, world: int, rank: int, case: int | None = None):
     """Balanced weak-scaling schedule: blocks of `world` seeds of similar I-side size per step."""
     from carmichael_frontier_b200 import workloads as W
+    if case is not None:
+        return [W.config2(case)] * steps
     cands = W.config2_seeds(SEED_POOL)
     need = steps * world
     pool = list(cands)
@@ -220,7 +224,7 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         return float(t.item())
 
-    seq = step_seeds(args.steps + args.warmup, world, rank)
+    seq = step_seeds(args.steps + args.warmup, world, rank, args.case)
     warm, timed = seq[:args.warmup], seq[args.warmup:]
     solver = Solver(dev)
     insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in seq]

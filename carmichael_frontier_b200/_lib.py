@@ -54,14 +54,15 @@ SIGNATURES = [
     ("cf_key_of", u64, [u64, u64]),
     ("cf_canon_of", u64, [u64, u64]),
     ("cf_key_mul", u64, [u64, u64, u64]),
-    ("cf_part_multiplier", u64, [u64, u32]),
+    ("cf_key32_mul", u64, [u64, u64, u64]),
     ("cf_screen_bytes", sz, []),
     ("cf_screen_prepare", C.c_int, [vp, C.c_int, C.c_double, C.c_double, C.c_double, vp, sz]),
     ("cf_gen_subsets", C.c_int, [vp, C.c_int, C.c_int, u64, u64, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
-    ("cf_gen_part_smem_bytes", sz, [C.c_int, u32]),
-    ("cf_gen_part", C.c_int, [vp, C.c_int, C.c_int, u64, u64, u32, u64, u32, vp, vp, vp, vp]),
+    ("cf_gen_part_shapes", C.c_int, []),
+    ("cf_gen_part_smem_bytes", sz, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    ("cf_gen_part", C.c_int, [vp, C.c_int, C.c_int, u64, u64, C.c_int, u32, vp, vp, vp, C.c_int, vp]),
     ("cf_join_part_smem_bytes", sz, [C.c_int]),
-    ("cf_join_part", C.c_int, [vp, vp, u32, vp, vp, u32, u32, u64, C.c_int, u32, u32, vp, u32, vp, vp, vp]),
+    ("cf_join_part", C.c_int, [vp, vp, u32, vp, vp, u32, C.c_int, C.c_int, u32, u32, vp, u32, vp, vp, vp]),
     ("cf_pair_result_bytes", sz, []),
     ("cf_check_pairs", C.c_int, [vp, vp, vp, C.c_int, vp, vp, u32, vp, vp, vp]),
     ("cf_sort_tmp_bytes", sz, [u64]),

@@ -22,13 +22,23 @@ k_check_pairs(const u64* __restrict__ poolD, const u64* __restrict__ poolI, cons
   const CfPoolHdr* hD = (const CfPoolHdr*)poolD;
   const CfPoolHdr* hI = (const CfPoolHdr*)poolI;
   const int nD = (int)hD->n, nI = (int)hI->n;
-  const CfMod md = cf_mod_from_hdr(hD);
+  const bool fast = hD->fast32 && hI->fast32;
+  CfArithFast fD, fI;
+  fD.md = cf_mod32_from_hdr(hD);
+  fI.md = fD.md;
+  fD.p = nullptr;
+  fI.p = nullptr;
+  CfArithWide wD, wI;
+  wD.md = cf_mod_from_hdr(hD);
+  wI.md = wD.md;
   const u64* bD = poolD + cf_pool_off_binom(nD);
   const u64* bI = poolI + cf_pool_off_binom(nI);
   const u64* kD = poolD + cf_pool_off_pkey(nD);
   const u64* kI = poolI + cf_pool_off_pkey(nI);
   const u64* pD = poolD + cf_pool_off_prime(nD);
   const u64* pI = poolI + cf_pool_off_prime(nI);
+  wD.pk = kD;
+  wI.pk = kI;
   const double* lD = (const double*)(poolD + cf_pool_off_lg(nD));
   const double* lI = (const double*)(poolI + cf_pool_off_lg(nI));
   const u32 np = min(*npairs, max_pairs);
@@ -41,12 +51,25 @@ k_check_pairs(const u64* __restrict__ poolD, const u64* __restrict__ poolI, cons
     int di[R], ii[R];
     cf_unrank_lex<R>(pr.d_id, nD, bD, di);
     cf_unrank_lex<R>(pr.i_id, nI, bI, ii);
-    u64 kd = hD->mult_key, ki = hI->mult_key;
+    u64 kd, ki;
+    if (fast) {
+      CfElt32 eD, eI;
+      eD.X = hD->X0; eD.x2 = hD->x20;
+      eI.X = hI->X0; eI.x2 = hI->x20;
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        eD = cf_mul32(eD, (u32)pD[di[j]], fD.md);
+        eI = cf_mul32(eI, (u32)pI[ii[j]], fI.md);
+      }
+      kd = cf_key32(eD, fD.md);
+      ki = cf_key32(eI, fI.md);
+    } else {
+      kd = cf_subset_key<R>(di, wD, hD->mult_key);
+      ki = cf_subset_key<R>(ii, wI, hI->mult_key);
+    }
     double lg = scr->lgP0;
 #pragma unroll
     for (int j = 0; j < R; ++j) {
-      kd = cf_mul_key(kd, kD[di[j]], md);
-      ki = cf_mul_key(ki, kI[ii[j]], md);
       lg += lI[ii[j]] - lD[di[j]];
       out.d_idx[j] = (unsigned short)di[j];
       out.i_idx[j] = (unsigned short)ii[j];

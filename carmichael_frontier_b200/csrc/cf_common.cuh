@@ -57,6 +57,57 @@ CF_HD u64 cf_mul_key(u64 kx, u64 ky, const CfMod& md) {
 }
 
 // ---------------------------------------------------------------------------
+// Fast path for pool primes p < 2^31 (every pool of the search): a lazy
+// Montgomery step with a 32-bit radix.  For x < 2m and p < 2^31,
+//     cf_redc32(x, p) = x * p * 2^-32 mod m,  result in [0, 2m),
+// in five 32x32->64 multiply(-add)s.  A product of R primes therefore carries
+// the constant 2^(-32R); the start value is pre-scaled by 2^(32R) so that the
+// final value, reduced once to [0, m), is exactly mult * prod(p) mod m.
+// Together with the 2-adic part x mod 2^a the pair is the canonical residue
+// mod M (Chinese remainder theorem), packed as key = (x mod m) << a | x mod 2^a.
+// ---------------------------------------------------------------------------
+struct CfMod32 {
+  u64 m;      // odd part of M (< 2^62)
+  u64 mask2;  // 2^a - 1
+  u32 ninv;   // -m^-1 mod 2^32
+  u32 ml, mh; // low and high 32-bit halves of m
+  int a;
+};
+
+CF_HD u64 cf_redc32(u64 x, u32 p, const CfMod32& md) {
+  const u32 xl = (u32)x, xh = (u32)(x >> 32);
+  const u64 lo = (u64)xl * p;                  // x = xh*2^32 + xl
+  const u32 u = (u32)lo * md.ninv;             // t + u*m == 0 (mod 2^32)
+  const u64 s1 = (u64)u * md.ml + (u32)lo;     // < 2^64; its low 32 bits are 0
+  u64 r = (u64)xh * p + (lo >> 32);
+  r += (u64)u * md.mh;
+  return r + (s1 >> 32);
+}
+
+// Element of the fast path: odd part X in [0, 2m) (lazily reduced), 2-adic part x2.
+struct CfElt32 {
+  u64 X, x2;
+};
+
+CF_HD CfElt32 cf_mul32(CfElt32 e, u32 p, const CfMod32& md) {
+  CfElt32 o;
+  o.X = cf_redc32(e.X, p, md);
+  o.x2 = (e.x2 * (u64)p) & md.mask2;
+  return o;
+}
+
+CF_HD u64 cf_key32(CfElt32 e, const CfMod32& md) {
+  const u64 X = (e.X >= md.m) ? e.X - md.m : e.X;
+  return (X << md.a) | e.x2;
+}
+
+// Residue partitions and in-partition hash: a multiplicative (Fibonacci) hash
+// of the key, so partitions are balanced whatever the structure of M.
+#define CF_HASH_MULT 0x9E3779B97F4A7C15ull
+CF_HD u64 cf_hash(u64 key) { return key * CF_HASH_MULT; }
+CF_HD u32 cf_part_of(u64 h, int pbits) { return pbits ? (u32)(h >> (64 - pbits)) : 0u; }
+
+// ---------------------------------------------------------------------------
 // Pool table: one blob per (prime list, radius, modulus, multiplier), prepared
 // on the host by cf_pool_prepare() and copied to the device by the caller.
 // Layout (u64 words):
@@ -81,7 +132,11 @@ struct CfPoolHdr {
   u64 inv2aR;      // (2^a)^-1 * 2^64 mod m           (canonical conversion)
   u64 r2;          // 2^128 mod m
   u64 one_key;     // key(1)
-  u64 reserved[CF_POOL_HDR_WORDS - 14];
+  u64 fast32;      // 1 if every prime < 2^31 (fast path available)
+  u64 X0;          // fast path start: (mult mod m) * 2^(32R) mod m
+  u64 x20;         // fast path start: mult mod 2^a
+  u64 ninv32;      // -m^-1 mod 2^32
+  u64 reserved[CF_POOL_HDR_WORDS - 18];
 };
 
 CF_HD size_t cf_pool_words(int n, int R) {
@@ -91,6 +146,17 @@ CF_HD size_t cf_pool_off_pkey(int) { return CF_POOL_HDR_WORDS; }
 CF_HD size_t cf_pool_off_prime(int n) { return CF_POOL_HDR_WORDS + (size_t)n; }
 CF_HD size_t cf_pool_off_lg(int n) { return CF_POOL_HDR_WORDS + 2 * (size_t)n; }
 CF_HD size_t cf_pool_off_binom(int n) { return CF_POOL_HDR_WORDS + 3 * (size_t)n; }
+
+CF_HD CfMod32 cf_mod32_from_hdr(const CfPoolHdr* h) {
+  CfMod32 md;
+  md.m = h->m;
+  md.mask2 = h->mask2;
+  md.ninv = (u32)h->ninv32;
+  md.ml = (u32)h->m;
+  md.mh = (u32)(h->m >> 32);
+  md.a = (int)h->a;
+  return md;
+}
 
 CF_HD CfMod cf_mod_from_hdr(const CfPoolHdr* h) {
   CfMod md;

@@ -1,7 +1,7 @@
 // cf_enum.cuh -- per-thread enumeration of r-subsets in lexicographic
 // combinatorial-number-system (CNS) rank order, the order of the reference's
 // gen_records kernel (gpu/mitm_gpu2.py:40-52), with the running product kept
-// in key form.
+// in residue form.
 //
 // A thread owns a contiguous rank range.  It unranks the first rank by binary
 // search over the hockey-stick identity (O(R log n) table reads instead of the
@@ -24,7 +24,7 @@ __device__ __forceinline__ void cf_unrank_lex(u64 rank, int n, const u64* __rest
                                               int (&idx)[R]) {
   int start = 0;
 #pragma unroll
-  for (int pos = 0; pos < R; ++pos) {
+  for (int pos = 0; pos < R - 1; ++pos) {
     const int rem = R - pos - 1;
     // number of subsets whose index at `pos` lies in [start, c) is
     //   cum(c) = C(n-start, rem+1) - C(n-c, rem+1)
@@ -39,6 +39,7 @@ __device__ __forceinline__ void cf_unrank_lex(u64 rank, int n, const u64* __rest
     rank -= total - cf_binom(binom, R, n - lo, rem + 1);
     start = lo + 1;
   }
+  idx[R - 1] = start + (int)rank;             // last position: one subset per index
 }
 
 // Colexicographic rank sum_j C(i_j, j+1) (the id of the reference's rank-mode
@@ -51,26 +52,42 @@ __device__ __forceinline__ u64 cf_colex_rank(const int (&idx)[R], const u64* __r
   return v;
 }
 
-// Lexicographic walker over r-subsets of an n-element pool with running key
-// products.  pk = key form of each pool prime (shared memory or global).
-template <int R>
+// Arithmetic policies for the walker.
+// Fast: primes < 2^31, lazy 32-bit-radix Montgomery (cf_redc32); key = CRT pair.
+struct CfArithFast {
+  CfMod32 md;
+  const u32* p;
+  typedef CfElt32 E;
+  __device__ __forceinline__ E mul(E a, int i) const { return cf_mul32(a, p[i], md); }
+  __device__ __forceinline__ u64 key(E a) const { return cf_key32(a, md); }
+};
+// Wide: any prime below 2^64 (reduced mod M on the host), 64-bit Montgomery keys.
+struct CfArithWide {
+  CfMod md;
+  const u64* pk;
+  typedef u64 E;
+  __device__ __forceinline__ E mul(E a, int i) const { return cf_mul_key(a, pk[i], md); }
+  __device__ __forceinline__ u64 key(E a) const { return a; }
+};
+
+// Lexicographic walker over r-subsets of an n-element pool with running products.
+template <int R, class Ar>
 struct CfLexWalker {
   int idx[R];
-  u64 A[R];     // prefix products; A[0] = mult
-  u64 key;      // A[R-1] * pk[idx[R-1]]
+  typename Ar::E A[R];   // prefix products; A[0] = mult
+  u64 key;               // key of A[R-1] * p[idx[R-1]]
 
-  __device__ __forceinline__ void init(u64 rank, int n, const u64* __restrict__ binom,
-                                       const u64* pk, u64 mult_key, const CfMod& md) {
+  __device__ __forceinline__ void init(u64 rank, int n, const u64* __restrict__ binom, const Ar& ar,
+                                       typename Ar::E start) {
     cf_unrank_lex<R>(rank, n, binom, idx);
-    A[0] = mult_key;
+    A[0] = start;
 #pragma unroll
-    for (int j = 1; j < R; ++j) A[j] = cf_mul_key(A[j - 1], pk[idx[j - 1]], md);
-    key = cf_mul_key(A[R - 1], pk[idx[R - 1]], md);
+    for (int j = 1; j < R; ++j) A[j] = ar.mul(A[j - 1], idx[j - 1]);
+    key = ar.key(ar.mul(A[R - 1], idx[R - 1]));
   }
 
-  // Advance to the lexicographic successor.  The caller guarantees a
-  // successor exists (rank + 1 < C(n, R)).
-  __device__ __forceinline__ void next(int n, const u64* pk, const CfMod& md) {
+  // Advance to the lexicographic successor (the caller guarantees one exists).
+  __device__ __forceinline__ void next(int n, const Ar& ar) {
     if (idx[R - 1] < n - 1) {
       idx[R - 1] += 1;
     } else {
@@ -79,7 +96,6 @@ struct CfLexWalker {
 #pragma unroll
       for (int t = R - 2; t >= 0; --t)
         if (t == j && idx[t] == n - R + t) j = t - 1;
-      // j >= 0 because a successor exists
 #pragma unroll
       for (int t = 0; t < R; ++t) {
         if (t == j) idx[t] += 1;
@@ -87,9 +103,9 @@ struct CfLexWalker {
       }
 #pragma unroll
       for (int t = 1; t < R; ++t)
-        if (t > j) A[t] = cf_mul_key(A[t - 1], pk[idx[t - 1]], md);
+        if (t > j) A[t] = ar.mul(A[t - 1], idx[t - 1]);
     }
-    key = cf_mul_key(A[R - 1], pk[idx[R - 1]], md);
+    key = ar.key(ar.mul(A[R - 1], idx[R - 1]));
   }
 
   // Index word with `bits` bits per position, position order (gen_records' id,
@@ -101,6 +117,15 @@ struct CfLexWalker {
     return id;
   }
 };
+
+// Product of the subset idx under a policy (used by the pair check).
+template <int R, class Ar>
+__device__ __forceinline__ u64 cf_subset_key(const int (&idx)[R], const Ar& ar, typename Ar::E start) {
+  typename Ar::E a = start;
+#pragma unroll
+  for (int j = 0; j < R; ++j) a = ar.mul(a, idx[j]);
+  return ar.key(a);
+}
 
 // Dispatch a templated functor over the supported radii 1..CF_MAX_DISPATCH_R.
 #define CF_MAX_DISPATCH_R 10

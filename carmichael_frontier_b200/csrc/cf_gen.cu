@@ -2,13 +2,14 @@
 //
 //  k_gen_linear : drop-in for the reference's gen_records (gpu/mitm_gpu2.py:24-66).
 //                 Record t of a launch is the subset at lexicographic rank lo+t;
-//                 key = mult * prod(p) mod M (canonical residue, or key form),
+//                 key = mult * prod(p) mod M (canonical residue, or internal key),
 //                 id  = packed indices (`bits` per position), lex rank or colex rank.
-//  k_gen_part   : the solve path's generator.  Same enumeration, but each CTA
-//                 scatters its tile of records straight into `nparts` residue
-//                 partitions (partition = floor(key * nparts / M)), staged in
-//                 shared memory so that every (tile, partition) run is written
-//                 contiguously after ONE global atomic reservation.
+//  k_gen_part   : the solve path's generator.  Same enumeration (fast arithmetic,
+//                 primes < 2^31), but each CTA scatters its tile of records straight
+//                 into 2^pbits residue partitions (partition = top bits of a
+//                 multiplicative hash of the key), staged in shared memory so that
+//                 every (tile, partition) run is written contiguously after ONE
+//                 global atomic reservation.
 #include "cf_abi_internal.h"
 #include "cf_enum.cuh"
 
@@ -16,6 +17,40 @@ namespace {
 
 constexpr int kLinBlock = 256;
 constexpr int kLinItems = 8;
+constexpr size_t kBinomSmemMax = 24 * 1024;
+
+// Stage the pool's primes (u32 for the fast path, key form otherwise) and, when
+// small enough, its binomial table into shared memory.
+template <int R, class Ar>
+__device__ __forceinline__ void cf_gen_linear_body(const u64* __restrict__ pool, const Ar& ar,
+                                                   typename Ar::E start, const u64* binom, int n, u64 lo,
+                                                   u64 count, int id_mode, int bits, int canon,
+                                                   u64* s_k, u64* s_i) {
+  const CfPoolHdr* hd = (const CfPoolHdr*)pool;
+  const u64 tile0 = (u64)blockIdx.x * (kLinBlock * kLinItems);
+  const u64 my0 = tile0 + (u64)threadIdx.x * kLinItems;
+  if (my0 >= count) return;
+  const int nv = (int)((count - my0) < (u64)kLinItems ? (count - my0) : (u64)kLinItems);
+  const CfMod md = cf_mod_from_hdr(hd);
+  const bool fast = hd->fast32 != 0;
+  const u64 inv2a = hd->inv2a, inv2aR = hd->inv2aR;
+  CfLexWalker<R, Ar> w;
+  w.init(lo + my0, n, binom, ar, start);
+  for (int i = 0; i < nv; ++i) {
+    u64 k = w.key;
+    if (canon) {
+      // fast keys hold (x mod m) in standard form, wide keys in Montgomery form
+      k = fast ? cf_key_to_canon(k, md, inv2aR, inv2aR) : cf_key_to_canon(k, md, inv2a, inv2aR);
+    }
+    u64 id;
+    if (id_mode == 0) id = w.packed(bits);
+    else if (id_mode == 1) id = lo + my0 + (u64)i;
+    else id = cf_colex_rank<R>(w.idx, binom);
+    s_k[threadIdx.x * (kLinItems + 1) + i] = k;
+    s_i[threadIdx.x * (kLinItems + 1) + i] = id;
+    if (i + 1 < nv) w.next(n, ar);
+  }
+}
 
 template <int R>
 __global__ void __launch_bounds__(kLinBlock)
@@ -26,31 +61,33 @@ k_gen_linear(const u64* __restrict__ pool, u64 lo, u64 count, int id_mode, int b
   __shared__ u64 s_i[kLinBlock * (kLinItems + 1)];
   const CfPoolHdr* hd = (const CfPoolHdr*)pool;
   const int n = (int)hd->n;
-  const CfMod md = cf_mod_from_hdr(hd);
-  const u64 mult = hd->mult_key, inv2a = hd->inv2a, inv2aR = hd->inv2aR;
+  const bool fast = hd->fast32 != 0;
   const u64* binom = pool + cf_pool_off_binom(n);
-  const u64* pk = pool + cf_pool_off_pkey(n);
-  for (int i = threadIdx.x; i < n; i += kLinBlock) s_pk[i] = pk[i];
-  __syncthreads();
-
-  const u64 tile0 = (u64)blockIdx.x * (kLinBlock * kLinItems);
-  const u64 my0 = tile0 + (u64)threadIdx.x * kLinItems;
-  if (my0 < count) {
-    const int nv = (int)((count - my0) < (u64)kLinItems ? (count - my0) : (u64)kLinItems);
-    CfLexWalker<R> w;
-    w.init(lo + my0, n, binom, s_pk, mult, md);
-    for (int i = 0; i < nv; ++i) {
-      const u64 k = canon ? cf_key_to_canon(w.key, md, inv2a, inv2aR) : w.key;
-      u64 id;
-      if (id_mode == 0) id = w.packed(bits);
-      else if (id_mode == 1) id = lo + my0 + (u64)i;
-      else id = cf_colex_rank<R>(w.idx, binom);
-      s_k[threadIdx.x * (kLinItems + 1) + i] = k;
-      s_i[threadIdx.x * (kLinItems + 1) + i] = id;
-      if (i + 1 < nv) w.next(n, s_pk, md);
-    }
+  if (fast) {
+    const u64* pr = pool + cf_pool_off_prime(n);
+    u32* s_p = (u32*)s_pk;
+    for (int i = threadIdx.x; i < n; i += kLinBlock) s_p[i] = (u32)pr[i];
+  } else {
+    const u64* pk = pool + cf_pool_off_pkey(n);
+    for (int i = threadIdx.x; i < n; i += kLinBlock) s_pk[i] = pk[i];
   }
   __syncthreads();
+  if (fast) {
+    CfArithFast ar;
+    ar.md = cf_mod32_from_hdr(hd);
+    ar.p = (const u32*)s_pk;
+    CfElt32 st;
+    st.X = hd->X0;
+    st.x2 = hd->x20;
+    cf_gen_linear_body<R>(pool, ar, st, binom, n, lo, count, id_mode, bits, canon, s_k, s_i);
+  } else {
+    CfArithWide ar;
+    ar.md = cf_mod_from_hdr(hd);
+    ar.pk = s_pk;
+    cf_gen_linear_body<R>(pool, ar, hd->mult_key, binom, n, lo, count, id_mode, bits, canon, s_k, s_i);
+  }
+  __syncthreads();
+  const u64 tile0 = (u64)blockIdx.x * (kLinBlock * kLinItems);
   for (int j = threadIdx.x; j < kLinBlock * kLinItems; j += kLinBlock) {
     const u64 g = tile0 + (u64)j;
     if (g < count) {
@@ -102,27 +139,61 @@ __device__ __forceinline__ void block_exclusive_scan(u32* a, int len, u32* s_war
   __syncthreads();
 }
 
+struct GenPartSmem {
+  size_t stage, p32, binom, hist, total;
+};
+
+__host__ __device__ inline GenPartSmem gen_part_layout(int block, int items, int n, int R, int pbits) {
+  GenPartSmem L;
+  const size_t T = (size_t)block * items;
+  L.stage = 0;
+  L.p32 = L.stage + T * sizeof(CfRec);
+  size_t b = L.p32 + (((size_t)n * 4 + 15) & ~(size_t)15);
+  const size_t binom_bytes = (size_t)(n + 1) * (R + 1) * 8;
+  L.binom = (binom_bytes <= kBinomSmemMax) ? b : (size_t)-1;
+  if (binom_bytes <= kBinomSmemMax) b += binom_bytes;
+  L.hist = b;
+  L.total = b + (size_t)3 * ((size_t)1 << pbits) * 4;
+  return L;
+}
+
 template <int R, int BLOCK, int ITEMS>
 __global__ void __launch_bounds__(BLOCK)
-k_gen_part(const u64* __restrict__ pool, u64 lo, u64 count, u32 nparts, u64 cpart, u32 cap,
-           u32* __restrict__ counts, CfRec* __restrict__ out, u32* __restrict__ err) {
+k_gen_part(const u64* __restrict__ pool, u64 lo, u64 count, int pbits, u32 cap, u32* __restrict__ counts,
+           CfRec* __restrict__ out, u32* __restrict__ err) {
   constexpr int T = BLOCK * ITEMS;
   extern __shared__ __align__(16) unsigned char smem[];
-  CfRec* s_stage = (CfRec*)smem;                          // T records
+  __shared__ u32 s_warp[BLOCK / 32];
   const CfPoolHdr* hd = (const CfPoolHdr*)pool;
   const int n = (int)hd->n;
-  u64* s_pk = (u64*)(s_stage + T);                         // n keys
-  u32* s_hist = (u32*)(s_pk + n);                          // nparts
-  u32* s_loff = s_hist + nparts;                           // nparts
-  u32* s_gbase = s_loff + nparts;                          // nparts
-  __shared__ u32 s_warp[BLOCK / 32];
-
-  const CfMod md = cf_mod_from_hdr(hd);
-  const u64 mult = hd->mult_key;
-  const u64* binom = pool + cf_pool_off_binom(n);
-  const u64* pk = pool + cf_pool_off_pkey(n);
-  for (int i = threadIdx.x; i < n; i += BLOCK) s_pk[i] = pk[i];
+  if (!hd->fast32) {            // the solve path requires pool primes < 2^31
+    if (threadIdx.x == 0) atomicOr(err, CF_ERR_BAD_ARG);
+    return;
+  }
+  const u32 nparts = 1u << pbits;
+  const GenPartSmem L = gen_part_layout(BLOCK, ITEMS, n, R, pbits);
+  CfRec* s_stage = (CfRec*)(smem + L.stage);
+  u32* s_p = (u32*)(smem + L.p32);
+  u32* s_hist = (u32*)(smem + L.hist);
+  u32* s_loff = s_hist + nparts;
+  u32* s_gbase = s_loff + nparts;
+  const u64* g_binom = pool + cf_pool_off_binom(n);
+  const u64* binom = g_binom;
+  if (L.binom != (size_t)-1) {
+    u64* sb = (u64*)(smem + L.binom);
+    const int nb = (n + 1) * (R + 1);
+    for (int i = threadIdx.x; i < nb; i += BLOCK) sb[i] = g_binom[i];
+    binom = sb;
+  }
+  const u64* pr = pool + cf_pool_off_prime(n);
+  for (int i = threadIdx.x; i < n; i += BLOCK) s_p[i] = (u32)pr[i];
   for (u32 i = threadIdx.x; i < nparts; i += BLOCK) s_hist[i] = 0;
+  CfArithFast ar;
+  ar.md = cf_mod32_from_hdr(hd);
+  ar.p = s_p;
+  CfElt32 st;
+  st.X = hd->X0;
+  st.x2 = hd->x20;
   __syncthreads();
 
   const u64 tile0 = (u64)blockIdx.x * T;
@@ -132,31 +203,44 @@ k_gen_part(const u64* __restrict__ pool, u64 lo, u64 count, u32 nparts, u64 cpar
   u64 key[ITEMS];
   u32 pos[ITEMS];
   if (nv > 0) {
-    CfLexWalker<R> w;
-    w.init(lo + my0, n, binom, s_pk, mult, md);
+    CfLexWalker<R, CfArithFast> w;
+    w.init(lo + my0, n, binom, ar, st);
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
       if (i < nv) {
         key[i] = w.key;
-        const u32 p = (u32)cf_mulhi(w.key, cpart);
-        pos[i] = atomicAdd(&s_hist[p], 1u);
-        if (i + 1 < nv) w.next(n, s_pk, md);
+        pos[i] = atomicAdd(&s_hist[cf_part_of(cf_hash(w.key), pbits)], 1u);
+        if (i + 1 < nv) w.next(n, ar);
       }
     }
   }
   __syncthreads();
-  // reserve one global run per non-empty partition (before the scan overwrites s_hist)
-  for (u32 p = threadIdx.x; p < nparts; p += BLOCK) {
-    const u32 h = s_hist[p];
-    s_loff[p] = h;
-    s_gbase[p] = h ? atomicAdd(&counts[p], h) : 0u;
+  // reserve one global run per non-empty partition; independent atomics in flight together
+  constexpr int PER = 4;
+  for (u32 p0 = threadIdx.x; p0 < nparts; p0 += BLOCK * PER) {
+    u32 res[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const u32 p = p0 + (u32)u * BLOCK;
+      res[u] = 0;
+      if (p < nparts) {
+        const u32 h = s_hist[p];
+        s_loff[p] = h;
+        if (h) res[u] = atomicAdd(&counts[p], h);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const u32 p = p0 + (u32)u * BLOCK;
+      if (p < nparts) s_gbase[p] = res[u];
+    }
   }
   __syncthreads();
   block_exclusive_scan<BLOCK>(s_loff, (int)nparts, s_warp);
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
     if (i < nv) {
-      const u32 p = (u32)cf_mulhi(key[i], cpart);
+      const u32 p = cf_part_of(cf_hash(key[i]), pbits);
       CfRec rc;
       rc.key = key[i];
       rc.id = lo + my0 + (u64)i;
@@ -169,7 +253,7 @@ k_gen_part(const u64* __restrict__ pool, u64 lo, u64 count, u32 nparts, u64 cpar
   bool ovf = false;
   for (int j = threadIdx.x; j < tv; j += BLOCK) {
     const CfRec rc = s_stage[j];
-    const u32 p = (u32)cf_mulhi(rc.key, cpart);
+    const u32 p = cf_part_of(cf_hash(rc.key), pbits);
     const u32 dst = s_gbase[p] + ((u32)j - s_loff[p]);
     if (dst < cap) out[(size_t)p * cap + dst] = rc;
     else ovf = true;
@@ -185,23 +269,33 @@ void launch_gen_linear(const u64* pool, u64 lo, u64 count, int id_mode, int bits
   k_gen_linear<R><<<grid, kLinBlock, 0, st>>>(pool, lo, count, id_mode, bits, canon, keys, ids);
 }
 
-constexpr int kPartBlock = 256;
-constexpr int kPartItems = 16;
+// Launch shapes (threads per CTA, records per thread) the autotuner chooses from.
+constexpr int kShapes[][2] = {{256, 16}, {512, 8}, {512, 16}, {1024, 8}};
+constexpr int kNumShapes = 4;
 
-size_t gen_part_smem(int n, u32 nparts) {
-  return (size_t)kPartBlock * kPartItems * sizeof(CfRec) + (size_t)n * 8 + (size_t)nparts * 12;
+template <int R, int BLOCK, int ITEMS>
+int launch_gen_part_shape(const u64* pool, int n, u64 lo, u64 count, int pbits, u32 cap, u32* counts, CfRec* out,
+                          u32* err, cudaStream_t st) {
+  const size_t smem = gen_part_layout(BLOCK, ITEMS, n, R, pbits).total;
+  if (smem > 227 * 1024) { cf_set_error("cf_gen_part: shared memory budget exceeded%s", ""); return CF_EBADARG; }
+  auto kern = k_gen_part<R, BLOCK, ITEMS>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cf_cuda_status(e, "cf_gen_part: smem attribute");
+  const u64 per = (u64)BLOCK * ITEMS;
+  const unsigned grid = (unsigned)((count + per - 1) / per);
+  kern<<<grid, BLOCK, smem, st>>>(pool, lo, count, pbits, cap, counts, out, err);
+  return CF_OK;
 }
 
 template <int R>
-void launch_gen_part(const u64* pool, int n, u64 lo, u64 count, u32 nparts, u64 cpart, u32 cap, u32* counts,
-                     CfRec* out, u32* err, cudaStream_t st, int* rc) {
-  const size_t smem = gen_part_smem(n, nparts);
-  auto kern = k_gen_part<R, kPartBlock, kPartItems>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) { *rc = cf_cuda_status(e, "cf_gen_part: smem attribute"); return; }
-  const u64 per = (u64)kPartBlock * kPartItems;
-  const unsigned grid = (unsigned)((count + per - 1) / per);
-  kern<<<grid, kPartBlock, smem, st>>>(pool, lo, count, nparts, cpart, cap, counts, out, err);
+void launch_gen_part(const u64* pool, int n, u64 lo, u64 count, int pbits, u32 cap, u32* counts, CfRec* out,
+                     u32* err, cudaStream_t st, int shape, int* rc) {
+  switch (shape) {
+    case 0: *rc = launch_gen_part_shape<R, 256, 16>(pool, n, lo, count, pbits, cap, counts, out, err, st); break;
+    case 1: *rc = launch_gen_part_shape<R, 512, 8>(pool, n, lo, count, pbits, cap, counts, out, err, st); break;
+    case 2: *rc = launch_gen_part_shape<R, 512, 16>(pool, n, lo, count, pbits, cap, counts, out, err, st); break;
+    default: *rc = launch_gen_part_shape<R, 1024, 8>(pool, n, lo, count, pbits, cap, counts, out, err, st); break;
+  }
 }
 
 }  // namespace
@@ -225,25 +319,27 @@ extern "C" int cf_gen_subsets(const void* pool_dev, int n, int r, u64 lo, u64 co
   return CF_OK;
 }
 
-extern "C" size_t cf_gen_part_smem_bytes(int n, u32 nparts) { return gen_part_smem(n, nparts); }
+extern "C" int cf_gen_part_shapes(void) { return kNumShapes; }
 
-extern "C" int cf_gen_part(const void* pool_dev, int n, int r, u64 lo, u64 count, u32 nparts, u64 cpart, u32 cap,
-                           u32* counts, void* out, u32* err, void* stream) {
+extern "C" size_t cf_gen_part_smem_bytes(int n, int r, int pbits, int shape) {
+  if (shape < 0 || shape >= kNumShapes || pbits < 0 || pbits > 12) return 0;
+  return gen_part_layout(kShapes[shape][0], kShapes[shape][1], n, r, pbits).total;
+}
+
+extern "C" int cf_gen_part(const void* pool_dev, int n, int r, u64 lo, u64 count, int pbits, u32 cap,
+                           u32* counts, void* out, u32* err, int shape, void* stream) {
   if (!pool_dev || n < 1 || n > CF_MAX_POOL || r < 1 || r > CF_MAX_DISPATCH_R || r > n) {
     cf_set_error("cf_gen_part: bad pool arguments (n 1..1024, r 1..10)%s", "");
     return CF_EBADARG;
   }
-  if (nparts < 1 || nparts > 4096 || (cpart == 0 && nparts > 1)) {
-    cf_set_error("cf_gen_part: nparts must be 1..4096 with its multiplier%s", "");
-    return CF_EBADARG;
-  }
-  if (gen_part_smem(n, nparts) > 220 * 1024) { cf_set_error("cf_gen_part: shared memory budget exceeded%s", ""); return CF_EBADARG; }
+  if (pbits < 0 || pbits > 12) { cf_set_error("cf_gen_part: pbits must be 0..12%s", ""); return CF_EBADARG; }
+  if (shape < 0 || shape >= kNumShapes) { cf_set_error("cf_gen_part: unknown launch shape%s", ""); return CF_EBADARG; }
   if (count == 0) return CF_OK;
   if (!counts || !out || !err) { cf_set_error("cf_gen_part: null buffer%s", ""); return CF_EBADARG; }
   if (count > (1ull << 40)) { cf_set_error("cf_gen_part: count too large for one launch%s", ""); return CF_EBADARG; }
   int rc = CF_OK;
-  CF_DISPATCH_R(r, launch_gen_part, (const u64*)pool_dev, n, lo, count, nparts, cpart, cap, counts, (CfRec*)out,
-                err, (cudaStream_t)stream, &rc);
+  CF_DISPATCH_R(r, launch_gen_part, (const u64*)pool_dev, n, lo, count, pbits, cap, counts, (CfRec*)out, err,
+                (cudaStream_t)stream, shape, &rc);
   if (rc != CF_OK) return rc;
   CF_LAUNCH_CHECK("cf_gen_part");
   return CF_OK;

@@ -19,19 +19,21 @@ constexpr u32 kEmpty = 0xffffffffu;
 constexpr int kJoinBlock = 512;
 constexpr int kUnroll = 4;
 
-__device__ __forceinline__ void slot_fp(u64 key, u64 cpart, int sbits, u32& slot, u32& fp) {
-  const u64 frac = key * cpart;               // position of the key inside its partition, scaled to 2^64
-  slot = (u32)(frac >> (64 - sbits));
-  fp = (u32)(frac >> (48 - sbits)) & 0xffffu;
+// Slot and 16-bit fingerprint from the hash bits just below the partition bits.
+__device__ __forceinline__ void slot_fp(u64 key, int pbits, int sbits, u32& slot, u32& fp) {
+  const u64 h = cf_hash(key) << pbits;
+  slot = (u32)(h >> (64 - sbits));
+  fp = (u32)(h >> (48 - sbits)) & 0xffffu;
 }
 
 __global__ void __launch_bounds__(kJoinBlock)
 k_join_part(const CfRec* __restrict__ D, const u32* __restrict__ dcount, u32 capD,
-            const CfRec* __restrict__ I, const u32* __restrict__ icount, u32 capI, u32 nparts, u64 cpart,
+            const CfRec* __restrict__ I, const u32* __restrict__ icount, u32 capI, int pbits,
             int sbits, u32 isplit, CfPair* __restrict__ pairs, u32 max_pairs, u32* __restrict__ npairs,
             u32* __restrict__ err) {
   extern __shared__ u32 s_tab[];
   const u32 S = 1u << sbits, smask = S - 1, dmax = S >> 1;
+  const u32 nparts = 1u << pbits;
   const u32 nwork = nparts * isplit;
   for (u32 w = blockIdx.x; w < nwork; w += gridDim.x) {
     const u32 p = w / isplit, part = w % isplit;
@@ -46,7 +48,7 @@ k_join_part(const CfRec* __restrict__ D, const u32* __restrict__ dcount, u32 cap
       __syncthreads();
       for (u32 d = d0 + threadIdx.x; d < d1; d += kJoinBlock) {
         u32 slot, fp;
-        slot_fp(Dp[d].key, cpart, sbits, slot, fp);
+        slot_fp(Dp[d].key, pbits, sbits, slot, fp);
         const u32 v = (fp << 16) | (d - d0);
         for (u32 tries = 0; tries < S; ++tries) {      // load <= 1/2: always finds a slot
           const u32 old = atomicCAS(&s_tab[slot], kEmpty, v);
@@ -67,7 +69,7 @@ k_join_part(const CfRec* __restrict__ D, const u32* __restrict__ dcount, u32 cap
           const u32 i = ib + (u32)u * kJoinBlock;
           if (i >= i1) continue;
           u32 slot, fp;
-          slot_fp(rc[u].key, cpart, sbits, slot, fp);
+          slot_fp(rc[u].key, pbits, sbits, slot, fp);
           for (u32 tries = 0; tries < S; ++tries) {
             const u32 v = s_tab[slot];
             if (v == kEmpty) break;
@@ -100,10 +102,11 @@ k_join_part(const CfRec* __restrict__ D, const u32* __restrict__ dcount, u32 cap
 extern "C" size_t cf_join_part_smem_bytes(int sbits) { return (size_t)4 << sbits; }
 
 extern "C" int cf_join_part(const void* D, const u32* dcount, u32 capD, const void* I, const u32* icount, u32 capI,
-                            u32 nparts, u64 cpart, int sbits, u32 isplit, u32 grid, void* pairs, u32 max_pairs,
+                            int pbits, int sbits, u32 isplit, u32 grid, void* pairs, u32 max_pairs,
                             u32* npairs, u32* err, void* stream) {
   if (sbits < 4 || sbits > 15) { cf_set_error("cf_join_part: sbits must be 4..15%s", ""); return CF_EBADARG; }
-  if (nparts < 1 || isplit < 1 || (u64)nparts * isplit > (1ull << 31)) { cf_set_error("cf_join_part: bad partition counts%s", ""); return CF_EBADARG; }
+  if (pbits < 0 || pbits > 12 || isplit < 1 || isplit > 4096) { cf_set_error("cf_join_part: bad partition counts%s", ""); return CF_EBADARG; }
+  const u32 nparts = 1u << pbits;
   if (!D || !dcount || !I || !icount || !npairs || !err || (max_pairs && !pairs)) {
     cf_set_error("cf_join_part: null buffer%s", "");
     return CF_EBADARG;
@@ -114,7 +117,7 @@ extern "C" int cf_join_part(const void* D, const u32* dcount, u32 capD, const vo
   const u32 nwork = nparts * isplit;
   const u32 g = (grid == 0 || grid > nwork) ? nwork : grid;
   k_join_part<<<g, kJoinBlock, smem, (cudaStream_t)stream>>>((const CfRec*)D, dcount, capD, (const CfRec*)I, icount,
-                                                            capI, nparts, cpart, sbits, isplit, (CfPair*)pairs,
+                                                            capI, pbits, sbits, isplit, (CfPair*)pairs,
                                                             max_pairs, npairs, err);
   CF_LAUNCH_CHECK("cf_join_part");
   return CF_OK;

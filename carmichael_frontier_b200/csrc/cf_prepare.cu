@@ -83,6 +83,12 @@ extern "C" int cf_pool_prepare(const u64* primes, int n, int r, u64 M, u64 mult,
   const u64 half = (h.m + 1) / 2;          // 2^-1 mod m (m odd)
   hd->inv2a = mod_pow(half, (u64)h.a, h.m);
   hd->inv2aR = (u64)((u128)hd->inv2a * h.Rm % h.m);
+  u64 maxp = 0;
+  for (int i = 0; i < n; ++i) maxp = primes[i] > maxp ? primes[i] : maxp;
+  hd->fast32 = (maxp < (1ull << 31)) ? 1 : 0;
+  hd->ninv32 = (u64)(u32)(0u - (u32)h.minv);                 // -m^-1 mod 2^32
+  hd->X0 = (u64)((u128)((mult % M) % h.m) * mod_pow(2, 32ull * (u64)r, h.m) % h.m);
+  hd->x20 = (mult % M) & h.mask2;
   u64* pkey = w + cf_pool_off_pkey(n);
   u64* prime = w + cf_pool_off_prime(n);
   double* lg = (double*)(w + cf_pool_off_lg(n));
@@ -134,9 +140,20 @@ extern "C" u64 cf_key_mul(u64 M, u64 kx, u64 ky) {
   return cf_mul_key(kx, ky, md);
 }
 
-extern "C" u64 cf_part_multiplier(u64 M, u32 nparts) {
-  if (M < 2 || nparts == 0 || (u64)nparts >= M) return 0;
-  return (u64)((((u128)nparts) << 64) / M);
+// Product of the residues x and y mod M through the fast path (two cf_mul32 steps
+// from the scaled start), returned as a key: host mirror for tests.
+extern "C" u64 cf_key32_mul(u64 M, u64 x, u64 y) {
+  HostMod h;
+  if (host_mod_init(M, &h) != CF_OK || x >= (1ull << 31) || y >= (1ull << 31)) return ~0ull;
+  CfMod32 md;
+  md.m = h.m; md.mask2 = h.mask2; md.ninv = (u32)(0u - (u32)h.minv); md.ml = (u32)h.m; md.mh = (u32)(h.m >> 32);
+  md.a = h.a;
+  CfElt32 e;
+  e.X = mod_pow(2, 64, h.m);
+  e.x2 = 1 & h.mask2;
+  e = cf_mul32(e, (u32)x, md);
+  e = cf_mul32(e, (u32)y, md);
+  return cf_key32(e, md);
 }
 
 extern "C" size_t cf_screen_bytes(void) { return sizeof(CfScreen); }

@@ -130,7 +130,8 @@ def join_sorted(Dk, Did, Ik, Iid):
     within = np.arange(len(irow), dtype=np.int64) - np.repeat(np.cumsum(rv[:, 2].astype(np.int64)) - rv[:, 2].astype(np.int64), rv[:, 2].astype(np.int64))
     dpos = torch.from_numpy(starts + within).to(dev)
     ir = torch.from_numpy(irow).to(dev)
-    return Did[dpos], Iid[ir]
+    # torch has no uint64 gather on CUDA: gather the same 8-byte words viewed as int64
+    return (Did.view(torch.int64)[dpos].view(torch.uint64), Iid.view(torch.int64)[ir].view(torch.uint64))
 
 
 def decode_ids(ids, r: int, bits: int):

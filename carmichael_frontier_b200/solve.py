@@ -66,7 +66,8 @@ class SolveResult:
 class Tuning:
     """Launch shape of the partitioned join (chosen by autotune.py when tuned)."""
     d_per_part: int = 7000          # target D records per partition
-    max_parts: int = 4096
+    max_pbits: int = 12             # at most 2^12 partitions
+    gen_shape: int = 1              # cf_gen_part launch shape (threads x records per thread)
     max_sbits: int = 14             # shared table of 2^sbits slots (4 B) per CTA
     isplit: int = 0                 # CTAs per partition in the join (0 = automatic)
     i_chunk_records: int = 1 << 31  # I-side records per generation/join chunk
@@ -112,6 +113,8 @@ class Instance:
             P0 *= p
         if math.gcd(P0, M) != 1 or any(math.gcd(q, M) != 1 for q in ins):
             raise ValueError("every pool prime must be coprime to M (q does not divide M)")
+        if any(p >= 1 << 31 for p in base) or any(q >= 1 << 31 for q in ins):
+            raise ValueError("pool primes must be below 2^31")
         return Instance(M, base, ins, r, B, P0)
 
 
@@ -147,7 +150,8 @@ class Solver:
     def plan(self, nD: int, nI: int, capD: int | None = None, capI: int | None = None,
              pairs: int | None = None) -> dict:
         tu = self.tuning
-        nparts = min(tu.max_parts, _pow2ceil(-(-nD // tu.d_per_part)))
+        pbits = min(tu.max_pbits, (_pow2ceil(-(-nD // tu.d_per_part))).bit_length() - 1)
+        nparts = 1 << pbits
         chunk = min(nI, tu.i_chunk_records)
         cD = capD or _cap(nD / nparts, tu.sigma)
         cI = capI or _cap(chunk / nparts, tu.sigma)
@@ -157,8 +161,8 @@ class Solver:
         while sbits < tu.max_sbits and (1 << (sbits - 1)) < cD:
             sbits += 1
         isplit = tu.isplit or max(1, min(16, (2 * 148 * 2) // max(1, nparts)))
-        return dict(nparts=nparts, capD=max(cD, 1), capI=max(cI, 1), chunk=max(chunk, 1), sbits=sbits,
-                    isplit=isplit, pairs=pairs or tu.pair_capacity)
+        return dict(pbits=pbits, nparts=nparts, capD=max(cD, 1), capI=max(cI, 1), chunk=max(chunk, 1), sbits=sbits,
+                    isplit=isplit, pairs=pairs or tu.pair_capacity, shape=tu.gen_shape)
 
     # -- one solve -----------------------------------------------------------
     def _mark(self, marks, tag):
@@ -174,7 +178,7 @@ class Solver:
         r, M = inst.r, inst.M
         nD, nIt = ncomb(len(inst.B0), r), ncomb(len(inst.INS), r)
         P = plan["nparts"]
-        cpart = lib.cf_part_multiplier(M, P)
+        pbits, shape = plan["pbits"], plan["shape"]
         poolD = self.tables.pool(inst.B0, r, M, pow(inst.P0, -1, M))
         poolI = self.tables.pool(inst.INS, r, M, 1)
         screen = self.tables.screen(inst.P0, inst.B, 1e-6)
@@ -195,18 +199,18 @@ class Solver:
         ck = _lib.check
         launches = 0
         self._mark(marks, "start")
-        ck(lib.cf_gen_part(dp(poolD), len(inst.B0), r, 0, nD, P, cpart, capD, dp(dcnt), dp(Dbuf),
-                           dp(misc) + 4, sh), "cf_gen_part(D)")
+        ck(lib.cf_gen_part(dp(poolD), len(inst.B0), r, 0, nD, pbits, capD, dp(dcnt), dp(Dbuf),
+                           dp(misc) + 4, shape, sh), "cf_gen_part(D)")
         launches += 1
         self._mark(marks, "gen_D")
         for lo in range(0, nIt, chunk):
             cnt = min(chunk, nIt - lo)
             if lo:
                 icnt.zero_()
-            ck(lib.cf_gen_part(dp(poolI), len(inst.INS), r, lo, cnt, P, cpart, capI, dp(icnt), dp(Ibuf),
-                               dp(misc) + 4, sh), "cf_gen_part(I)")
+            ck(lib.cf_gen_part(dp(poolI), len(inst.INS), r, lo, cnt, pbits, capI, dp(icnt), dp(Ibuf),
+                               dp(misc) + 4, shape, sh), "cf_gen_part(I)")
             self._mark(marks, "gen_I")
-            ck(lib.cf_join_part(dp(Dbuf), dp(dcnt), capD, dp(Ibuf), dp(icnt), capI, P, cpart, plan["sbits"],
+            ck(lib.cf_join_part(dp(Dbuf), dp(dcnt), capD, dp(Ibuf), dp(icnt), capI, pbits, plan["sbits"],
                                 plan["isplit"], 0, dp(pairs), maxp, dp(misc), dp(misc) + 4, sh),
                "cf_join_part")
             self._mark(marks, "join")
@@ -235,6 +239,8 @@ class Solver:
             return None, newp
         if err & _lib.ERR_SPIN_LIMIT:
             raise _lib.CfError(_lib.CF_ETIMEOUT, "solve", "a bounded device wait gave up")
+        if err & 32:
+            raise _lib.CfError(_lib.CF_EBADARG, "solve", "a kernel rejected its arguments (pool primes >= 2^31?)")
         if err & _lib.ERR_KEY_MISMATCH:
             raise _lib.CfError(_lib.CF_EBADARG, "solve", "checked pair with unequal residues (internal error)")
         res = np.frombuffer(h["res"][: npairs * self.result_bytes].cpu().numpy().tobytes(), dtype=RESULT_DTYPE)

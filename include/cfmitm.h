@@ -76,8 +76,10 @@ uint64_t cf_key_of(uint64_t M, uint64_t v);
 uint64_t cf_canon_of(uint64_t M, uint64_t key);
 uint64_t cf_key_mul(uint64_t M, uint64_t kx, uint64_t ky);
 
-/* floor(2^64 * nparts / M): residue partition p(key) = mulhi(key, multiplier). */
-uint64_t cf_part_multiplier(uint64_t M, uint32_t nparts);
+/* Key of x*y mod M computed by the solve path's fast arithmetic (pool primes
+ * below 2^31: lazy 32-bit-radix Montgomery steps), for host-side tests.  The
+ * solve path's key is (x mod m) << a | (x mod 2^a) for M = 2^a * m, m odd. */
+uint64_t cf_key32_mul(uint64_t M, uint64_t x, uint64_t y);
 
 /* Size-screen table for cf_check_pairs: B as little-endian 32-bit limbs
  * (1..64 limbs), log2(prod B0), log2(B) and the fp64 margin eps. */
@@ -97,31 +99,36 @@ int cf_screen_prepare(const uint32_t* limbsB, int nlimbs, double lgP0, double lg
 int cf_gen_subsets(const void* pool_dev, int n, int r, uint64_t lo, uint64_t count, int id_mode, int bits,
                    int canon, uint64_t* keys, uint64_t* ids, void* stream);
 
-/* Partitioned generation for the solve path: the records of ranks [lo, lo+count)
- * (key form, id = lexicographic rank) are scattered into nparts (1..4096)
- * residue partitions of capacity cap records each: partition p occupies
- * out[p*cap .. p*cap+cap) as 16-byte {key, id} records (the reference's record
- * layout, src/mitm64_idump_stream.cpp:6-12).  counts[p] (device, zeroed by the
- * caller) receives the number of records routed to p, even beyond cap; then
- * CF_ERR_PART_OVERFLOW is set in *err and the caller retries with a larger cap.
- * Replaces generate() + sort_side() as the producer of a joinable side. */
-size_t cf_gen_part_smem_bytes(int n, uint32_t nparts);
-int cf_gen_part(const void* pool_dev, int n, int r, uint64_t lo, uint64_t count, uint32_t nparts, uint64_t cpart,
-                uint32_t cap, uint32_t* counts, void* out, uint32_t* err, void* stream);
+/* Partitioned generation for the solve path (pool primes below 2^31): the
+ * records of ranks [lo, lo+count) (id = lexicographic rank) are scattered into
+ * 2^pbits (pbits 0..12) residue partitions -- the top pbits bits of
+ * key * 0x9E3779B97F4A7C15 mod 2^64 -- of capacity cap records each: partition
+ * p occupies out[p*cap .. p*cap+cap) as 16-byte {key, id} records (the
+ * reference's record layout, src/mitm64_idump_stream.cpp:6-12).  counts[p]
+ * (device, zeroed by the caller) receives the number of records routed to p,
+ * even beyond cap; then CF_ERR_PART_OVERFLOW is set in *err and the caller
+ * retries with a larger cap.  shape selects the launch shape (0..
+ * cf_gen_part_shapes()-1: threads x records per thread).  Replaces generate()
+ * + sort_side() as the producer of a joinable side. */
+int cf_gen_part_shapes(void);
+size_t cf_gen_part_smem_bytes(int n, int r, int pbits, int shape);
+int cf_gen_part(const void* pool_dev, int n, int r, uint64_t lo, uint64_t count, int pbits, uint32_t cap,
+                uint32_t* counts, void* out, uint32_t* err, int shape, void* stream);
 
 /* ---- join ---------------------------------------------------------------- */
 
-/* Partitioned equal-residue join: for every partition, every (D, I) record pair
- * with equal keys is appended to pairs[] as {D id, I id} (16 bytes) through the
- * device counter *npairs (zeroed by the caller); beyond max_pairs the count
- * keeps growing and CF_ERR_PAIR_OVERFLOW is set.  sbits (4..15): shared-memory
- * table of 2^sbits slots (4 bytes each) per CTA; isplit: CTAs per partition;
- * grid: 0 = one CTA per (partition, split).  Replaces join_sorted
- * (gpu/mitm_gpu2.py:107-119) and mitm64.cpp's hash probe (src/mitm64.cpp:85-101). */
+/* Partitioned equal-residue join over the 2^pbits partitions of cf_gen_part:
+ * every (D, I) record pair with equal keys is appended to pairs[] as
+ * {D id, I id} (16 bytes) through the device counter *npairs (zeroed by the
+ * caller); beyond max_pairs the count keeps growing and CF_ERR_PAIR_OVERFLOW is
+ * set.  sbits (4..15): shared-memory table of 2^sbits slots (4 bytes each) per
+ * CTA; isplit: CTAs per partition; grid: 0 = one CTA per (partition, split).
+ * Replaces join_sorted (gpu/mitm_gpu2.py:107-119) and mitm64.cpp's hash probe
+ * (src/mitm64.cpp:85-101). */
 size_t cf_join_part_smem_bytes(int sbits);
 int cf_join_part(const void* D, const uint32_t* dcount, uint32_t capD, const void* I, const uint32_t* icount,
-                 uint32_t capI, uint32_t nparts, uint64_t cpart, int sbits, uint32_t isplit, uint32_t grid,
-                 void* pairs, uint32_t max_pairs, uint32_t* npairs, uint32_t* err, void* stream);
+                 uint32_t capI, int pbits, int sbits, uint32_t isplit, uint32_t grid, void* pairs,
+                 uint32_t max_pairs, uint32_t* npairs, uint32_t* err, void* stream);
 
 /* Exact check of candidate pairs (lexicographic-rank ids): recomputed residues,
  * conservative fp64 log-size screen, exact size n <= B, Korselt, distinctness.

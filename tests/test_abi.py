@@ -46,7 +46,7 @@ def test_bad_arguments_fail_loudly_without_gpu():
     assert lib.cf_pool_prepare(pr.ctypes.data, 3, 2, 1 << 62, 1, buf.ctypes.data, 64) == _lib.CF_EBADARG
     assert b"table buffer too small" in lib.cf_last_error_string() or b"M < 2^62" in lib.cf_last_error_string()
     assert lib.cf_gen_subsets(None, 3, 2, 0, 1, 0, 8, 1, None, None, None) == _lib.CF_EBADARG
-    assert lib.cf_join_part(None, None, 1, None, None, 1, 1, 1, 2, 1, 0, None, 0, None, None, None) == _lib.CF_EBADARG
+    assert lib.cf_join_part(None, None, 1, None, None, 1, 1, 2, 1, 0, None, 0, None, None, None) == _lib.CF_EBADARG
     with pytest.raises(_lib.CfError):
         _lib.check(lib.cf_gen_subsets(None, 3, 2, 0, 1, 0, 8, 1, None, None, None), "probe")
 
@@ -103,14 +103,18 @@ def test_pool_table_layout():
             assert int(binom[x, y]) == math.comb(x, y)
 
 
-def test_partition_multiplier():
+@pytest.mark.parametrize("M", [21621600, 9025877244384000, 1768248177696000, (1 << 62) - 2, 3 * (1 << 50),
+                               1 << 40, 135137, 6, 2])
+def test_fast_path_product_is_the_crt_residue(M):
+    # the solve path's lazy 32-bit Montgomery product, run on the host, against Python integers
     lib = _lib.load()
-    for M in (21621600, 9025877244384000, (1 << 62) - 2):
-        for P in (1, 2, 1024, 4096):
-            c = lib.cf_part_multiplier(M, P)
-            assert c == (P << 64) // M
-            for key in (0, 1, M // 2, M - 1):
-                assert (key * c) >> 64 < P
+    a = (M & -M).bit_length() - 1
+    m = M >> a
+    rng = random.Random(M + 7)
+    for _ in range(300):
+        x, y = rng.randrange(1, 1 << 31), rng.randrange(1, 1 << 31)
+        v = x * y % M
+        assert lib.cf_key32_mul(M, x, y) == ((v % m) << a) | (v & ((1 << a) - 1))
 
 
 def test_screen_table():
