@@ -58,9 +58,11 @@ SIGNATURES = [
     ("cf_screen_bytes", sz, []),
     ("cf_screen_prepare", C.c_int, [vp, C.c_int, C.c_double, C.c_double, C.c_double, vp, sz]),
     ("cf_gen_subsets", C.c_int, [vp, C.c_int, C.c_int, u64, u64, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
+    ("cf_tail_bytes", sz, [C.c_int, C.c_int]),
+    ("cf_build_tail", C.c_int, [vp, C.c_int, C.c_int, vp, vp]),
     ("cf_gen_part_shapes", C.c_int, []),
     ("cf_gen_part_smem_bytes", sz, [C.c_int, C.c_int, C.c_int, C.c_int]),
-    ("cf_gen_part", C.c_int, [vp, C.c_int, C.c_int, u64, u64, C.c_int, u32, vp, vp, vp, C.c_int, vp]),
+    ("cf_gen_part", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, C.c_int, u32, vp, vp, vp, C.c_int, vp]),
     ("cf_join_part_smem_bytes", sz, [C.c_int]),
     ("cf_join_part", C.c_int, [vp, vp, u32, vp, vp, u32, C.c_int, C.c_int, u32, u32, vp, u32, vp, vp, vp]),
     ("cf_pair_result_bytes", sz, []),

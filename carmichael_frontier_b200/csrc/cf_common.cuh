@@ -136,7 +136,11 @@ struct CfPoolHdr {
   u64 X0;          // fast path start: (mult mod m) * 2^(32R) mod m
   u64 x20;         // fast path start: mult mod 2^a
   u64 ninv32;      // -m^-1 mod 2^32
-  u64 reserved[CF_POOL_HDR_WORDS - 18];
+  u64 tail_b;      // suffix length b of the tail table (0: no tail table for this pool)
+  u64 tail_n;      // C(n, b): entries of the tail table
+  u64 X0s;         // tail path start: (mult mod m) * 2^(32(R-b)) mod m
+  u64 S0;          // tail table start: 2^(64 + 32b) mod m
+  u64 reserved[CF_POOL_HDR_WORDS - 22];
 };
 
 CF_HD size_t cf_pool_words(int n, int R) {
@@ -177,6 +181,15 @@ CF_HD u64 cf_key_to_canon(u64 k, const CfMod& md, u64 inv2a, u64 inv2aR) {
   const u64 q = (t >= s) ? (t - s) : (t + md.m - s);     // (x_m - x_2) * 2^-a mod m
   return x2 + (q << md.a);
 }
+
+// Tail table entry: the product of one b-subset (b <= 3) of the pool, lexicographic
+// order, as odd part in Montgomery form (x * 2^64 mod m, canonical) and 2-adic
+// part; the subset's indices packed 10 bits each.
+struct __align__(16) CfTailEnt {
+  u64 X;
+  u32 x2;
+  u32 ij;
+};
 
 // Record of one subset: residue key and the subset's identifier (its
 // lexicographic combinatorial-number-system rank, or a packed index word).

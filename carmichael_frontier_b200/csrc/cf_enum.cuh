@@ -1,14 +1,13 @@
-// cf_enum.cuh -- per-thread enumeration of r-subsets in lexicographic
+// cf_enum.cuh -- enumeration of r-subsets in lexicographic
 // combinatorial-number-system (CNS) rank order, the order of the reference's
 // gen_records kernel (gpu/mitm_gpu2.py:40-52), with the running product kept
 // in residue form.
 //
-// A thread owns a contiguous rank range.  It unranks the first rank by binary
+// A warp owns a contiguous rank range.  It unranks the first rank by binary
 // search over the hockey-stick identity (O(R log n) table reads instead of the
-// reference's O(n) scan), keeps the prefix products A[j] = mult * p[i_0] ...
-// p[i_{j-1}], and steps to the lexicographic successor.  The common step only
-// moves the last index, so a record costs exactly one modular product
-// (A[R-1] * p[i_{R-1}]); a carry at position j costs R-j products.
+// reference's O(n) scan per record), keeps the prefix products
+// A[j] = mult * p[i_0] ... p[i_{j-1}], and its lanes take consecutive ranks, so
+// a record costs exactly one modular product (A[R-1] * p[i_{R-1}]).
 #pragma once
 #include "cf_common.cuh"
 
@@ -42,6 +41,41 @@ __device__ __forceinline__ void cf_unrank_lex(u64 rank, int n, const u64* __rest
   idx[R - 1] = start + (int)rank;             // last position: one subset per index
 }
 
+// Lexicographic rank of the ascending K-subset idx of {0..n-1}; the binomial
+// table has R+1 columns (K <= R).
+template <int K, int R>
+__device__ __forceinline__ u64 cf_rank_lex(const int* idx, int n, const u64* __restrict__ binom) {
+  u64 rank = 0;
+  int start = 0;
+#pragma unroll
+  for (int pos = 0; pos < K; ++pos) {
+    rank += cf_binom(binom, R, n - start, K - pos) - cf_binom(binom, R, n - idx[pos], K - pos);
+    start = idx[pos] + 1;
+  }
+  return rank;
+}
+
+// Unrank a K-subset of {0..n-1} (lexicographic) with a table of R+1 columns.
+template <int K, int R>
+__device__ __forceinline__ void cf_unrank_lex_k(u64 rank, int n, const u64* __restrict__ binom, int* idx) {
+  int start = 0;
+#pragma unroll
+  for (int pos = 0; pos < K - 1; ++pos) {
+    const int rem = K - pos - 1;
+    const u64 total = cf_binom(binom, R, n - start, rem + 1);
+    const u64 Y = total - rank;
+    int lo = start, hi = n - 1 - rem;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cf_binom(binom, R, n - mid, rem + 1) >= Y) lo = mid; else hi = mid - 1;
+    }
+    idx[pos] = lo;
+    rank -= total - cf_binom(binom, R, n - lo, rem + 1);
+    start = lo + 1;
+  }
+  idx[K - 1] = start + (int)rank;
+}
+
 // Colexicographic rank sum_j C(i_j, j+1) (the id of the reference's rank-mode
 // dumpers, src/mitm64_idump_stream2.cpp:26-29).
 template <int R>
@@ -70,53 +104,190 @@ struct CfArithWide {
   __device__ __forceinline__ u64 key(E a) const { return a; }
 };
 
-// Lexicographic walker over r-subsets of an n-element pool with running products.
+// Warp-cooperative lexicographic walker: the 32 lanes of a warp produce 32
+// CONSECUTIVE ranks per step.  The state is uniform across the warp: the
+// current prefix idx[0..R-2] with its product A[R-1] and the next last index
+// c.  A step hands lanes f..f+take-1 the current prefix with last indices
+// c..c+take-1 and moves to the successor prefix whenever the run of last
+// indices ends, so every lane does exactly one modular product per record, the
+// warp never diverges, and lane-consecutive records are rank-consecutive
+// (coalesced stores).  Unranking happens once per warp range.
 template <int R, class Ar>
-struct CfLexWalker {
-  int idx[R];
-  typename Ar::E A[R];   // prefix products; A[0] = mult
-  u64 key;               // key of A[R-1] * p[idx[R-1]]
+struct CfWarpWalker {
+  int idx[R > 1 ? R - 1 : 1];     // prefix indices (R-1 of them)
+  typename Ar::E A[R];            // A[j] = mult * p[idx[0]] ... p[idx[j-1]]
+  int c;                          // next last index of the current prefix
 
   __device__ __forceinline__ void init(u64 rank, int n, const u64* __restrict__ binom, const Ar& ar,
                                        typename Ar::E start) {
-    cf_unrank_lex<R>(rank, n, binom, idx);
+    int full[R];
+    cf_unrank_lex<R>(rank, n, binom, full);
+#pragma unroll
+    for (int j = 0; j < R - 1; ++j) idx[j] = full[j];
+    c = full[R - 1];
     A[0] = start;
 #pragma unroll
     for (int j = 1; j < R; ++j) A[j] = ar.mul(A[j - 1], idx[j - 1]);
-    key = ar.key(ar.mul(A[R - 1], idx[R - 1]));
   }
 
-  // Advance to the lexicographic successor (the caller guarantees one exists).
-  __device__ __forceinline__ void next(int n, const Ar& ar) {
-    if (idx[R - 1] < n - 1) {
-      idx[R - 1] += 1;
+  // Move to the successor prefix (R-1 subset of {0..n-2} in lexicographic
+  // order); returns false when there is none.  The common case only bumps the
+  // last prefix index (one modular product); a deeper carry is rare.
+  __device__ __forceinline__ bool next_prefix(int n, const Ar& ar) {
+    if constexpr (R == 1) {
+      return false;
     } else {
-      // largest j < R-1 with idx[j] < n - R + j
-      int j = R - 2;
+      if (idx[R - 2] < n - 2) {
+        idx[R - 2] += 1;
+        A[R - 1] = ar.mul(A[R - 2], idx[R - 2]);
+        c = idx[R - 2] + 1;
+        return true;
+      }
+      return carry(n, ar);
+    }
+  }
+
+  __device__ __forceinline__ bool carry(int n, const Ar& ar) {
+    if constexpr (R == 1) {
+      return false;
+    } else {
+      int j = R - 3;                    // idx[R-2] is at its maximum n-2
 #pragma unroll
-      for (int t = R - 2; t >= 0; --t)
+      for (int t = R - 3; t >= 0; --t)
         if (t == j && idx[t] == n - R + t) j = t - 1;
+      if (j < 0) return false;
 #pragma unroll
-      for (int t = 0; t < R; ++t) {
+      for (int t = 0; t < R - 1; ++t) {
         if (t == j) idx[t] += 1;
         else if (t > j) idx[t] = idx[t - 1] + 1;
       }
 #pragma unroll
       for (int t = 1; t < R; ++t)
         if (t > j) A[t] = ar.mul(A[t - 1], idx[t - 1]);
+      c = idx[R - 2] + 1;
+      return true;
     }
-    key = ar.key(ar.mul(A[R - 1], idx[R - 1]));
   }
 
-  // Index word with `bits` bits per position, position order (gen_records' id,
-  // gpu/mitm_gpu2.py:61).
-  __device__ __forceinline__ u64 packed(int bits) const {
-    u64 id = 0;
+  // One warp step: this lane's prefix product and last index for record
+  // (current position + lane).  Lanes past the end of the enumeration get
+  // last = -1.
+  __device__ __forceinline__ void step(int n, const Ar& ar, int lane, typename Ar::E& myA, int& mylast) {
+    int dummy[R > 1 ? R - 1 : 1];
+    step_idx<false>(n, ar, lane, myA, mylast, dummy);
+  }
+
+  // As step(), also copying this lane's prefix indices (for index-word ids).
+  template <bool WANT_IDX>
+  __device__ __forceinline__ void step_idx(int n, const Ar& ar, int lane, typename Ar::E& myA, int& mylast,
+                                           int (&myidx)[R > 1 ? R - 1 : 1]) {
+    int f = 0;
+    mylast = -1;
+    do {
+      if (c >= n && !next_prefix(n, ar)) break;
+      const int take = min(n - c, 32 - f);
+      if ((unsigned)(lane - f) < (unsigned)take) {
+        myA = A[R - 1];
+        mylast = c + (lane - f);
+        if (WANT_IDX) {
 #pragma unroll
-    for (int j = 0; j < R; ++j) id |= ((u64)idx[j]) << (j * bits);
-    return id;
+          for (int j = 0; j < R - 1; ++j) myidx[j] = idx[j];
+        }
+      }
+      f += take;
+      c += take;
+    } while (f < 32);
   }
 };
+
+// ---------------------------------------------------------------------------
+// Tail-table walker (fast arithmetic).  A subset of size R is split into a
+// prefix of A = R - B indices and a suffix of B indices.  The suffix products
+// of all B-subsets sit in a lexicographic table (CfTailEnt, C(n, B) entries,
+// L1/L2-resident), and the records of one prefix are exactly the table's tail
+// from the first suffix whose smallest index exceeds the prefix's largest.  A
+// warp's 32 lanes read 32 consecutive table entries per step (coalesced) and
+// do one 64-bit Montgomery product each; the prefix changes once every
+// C(n - i_last - 1, B) records, so the per-step bookkeeping is negligible.
+// ---------------------------------------------------------------------------
+template <int R, int B>
+struct CfTailWalker {
+  static constexpr int A = R - B;
+  int idx[A > 0 ? A : 1];        // prefix indices
+  CfElt32 Q[A + 1];              // Q[j] = start * p[idx[0]] ... p[idx[j-1]] (lazy, 32-bit radix)
+  u64 cur, tend;                 // position in the tail table and its end
+
+  __device__ __forceinline__ void init(u64 rank, int n, const u64* __restrict__ binom, const CfArithFast& ar,
+                                       CfElt32 start, u64 tail_n) {
+    int full[R];
+    cf_unrank_lex<R>(rank, n, binom, full);
+#pragma unroll
+    for (int j = 0; j < A; ++j) idx[j] = full[j];
+    Q[0] = start;
+#pragma unroll
+    for (int j = 1; j <= A; ++j) Q[j] = ar.mul(Q[j - 1], idx[j - 1]);
+    cur = cf_rank_lex<B, R>(full + A, n, binom);
+    tend = tail_n;
+  }
+
+  __device__ __forceinline__ bool next_prefix(int n, const u64* __restrict__ binom, const CfArithFast& ar) {
+    if constexpr (A == 0) {
+      return false;
+    } else {
+      const int np = n - B;                       // prefix indices lie in 0..np-1
+      if (idx[A - 1] < np - 1) {
+        idx[A - 1] += 1;
+        Q[A] = ar.mul(Q[A - 1], idx[A - 1]);
+      } else {
+        int j = A - 2;
+#pragma unroll
+        for (int t = A - 2; t >= 0; --t)
+          if (t == j && idx[t] == np - A + t) j = t - 1;
+        if (j < 0) return false;
+#pragma unroll
+        for (int t = 0; t < A; ++t) {
+          if (t == j) idx[t] += 1;
+          else if (t > j) idx[t] = idx[t - 1] + 1;
+        }
+#pragma unroll
+        for (int t = 1; t <= A; ++t)
+          if (t > j) Q[t] = ar.mul(Q[t - 1], idx[t - 1]);
+      }
+      cur = tend - cf_binom(binom, R, n - idx[A - 1] - 1, B);
+      return true;
+    }
+  }
+
+  // This lane's prefix product and tail index for record (position + lane);
+  // lanes past the end of the enumeration get j = ~0.
+  template <bool WANT_IDX>
+  __device__ __forceinline__ void step(int n, const u64* __restrict__ binom, const CfArithFast& ar, int lane,
+                                       CfElt32& myQ, u64& myj, int (&myidx)[A > 0 ? A : 1]) {
+    int f = 0;
+    myj = ~0ull;
+    do {
+      if (cur >= tend && !next_prefix(n, binom, ar)) break;
+      const u64 avail = tend - cur;
+      const int take = avail < (u64)(32 - f) ? (int)avail : 32 - f;
+      if ((unsigned)(lane - f) < (unsigned)take) {
+        myQ = Q[A];
+        myj = cur + (u64)(lane - f);
+        if (WANT_IDX) {
+#pragma unroll
+          for (int j = 0; j < A; ++j) myidx[j] = idx[j];
+        }
+      }
+      f += take;
+      cur += (u64)take;
+    } while (f < 32);
+  }
+};
+
+// Key of prefix product q times tail entry e: canonical (x mod m) << a | x mod 2^a.
+__device__ __forceinline__ u64 cf_tail_key(CfElt32 q, const CfTailEnt& e, const CfMod32& md, u64 minv) {
+  const u64 X = cf_redc_mul(q.X, e.X, md.m, minv);   // q.X < 2m, e.X < m: result canonical in [0, m)
+  return (X << md.a) | ((q.x2 * (u64)e.x2) & md.mask2);
+}
 
 // Product of the subset idx under a policy (used by the pair check).
 template <int R, class Ar>

@@ -16,39 +16,53 @@
 namespace {
 
 constexpr int kLinBlock = 256;
-constexpr int kLinItems = 8;
+constexpr int kLinSteps = 16;              // 32 x 16 = 512 consecutive records per warp
 constexpr size_t kBinomSmemMax = 24 * 1024;
 
-// Stage the pool's primes (u32 for the fast path, key form otherwise) and, when
-// small enough, its binomial table into shared memory.
+// One warp writes 32 rank-consecutive records per step straight to global
+// memory (coalesced); keys converted to canonical residues when asked.
 template <int R, class Ar>
-__device__ __forceinline__ void cf_gen_linear_body(const u64* __restrict__ pool, const Ar& ar,
-                                                   typename Ar::E start, const u64* binom, int n, u64 lo,
-                                                   u64 count, int id_mode, int bits, int canon,
-                                                   u64* s_k, u64* s_i) {
-  const CfPoolHdr* hd = (const CfPoolHdr*)pool;
-  const u64 tile0 = (u64)blockIdx.x * (kLinBlock * kLinItems);
-  const u64 my0 = tile0 + (u64)threadIdx.x * kLinItems;
-  if (my0 >= count) return;
-  const int nv = (int)((count - my0) < (u64)kLinItems ? (count - my0) : (u64)kLinItems);
+__device__ __forceinline__ void cf_gen_linear_warp(const CfPoolHdr* hd, const Ar& ar, typename Ar::E start,
+                                                   const u64* binom, int n, u64 lo, u64 count, int id_mode,
+                                                   int bits, int canon, u64* __restrict__ keys,
+                                                   u64* __restrict__ ids) {
+  const int lane = threadIdx.x & 31;
+  const u64 wbase = ((u64)blockIdx.x * (kLinBlock / 32) + (threadIdx.x >> 5)) * (32u * kLinSteps);
+  if (wbase >= count) return;
   const CfMod md = cf_mod_from_hdr(hd);
   const bool fast = hd->fast32 != 0;
   const u64 inv2a = hd->inv2a, inv2aR = hd->inv2aR;
-  CfLexWalker<R, Ar> w;
-  w.init(lo + my0, n, binom, ar, start);
-  for (int i = 0; i < nv; ++i) {
-    u64 k = w.key;
-    if (canon) {
-      // fast keys hold (x mod m) in standard form, wide keys in Montgomery form
-      k = fast ? cf_key_to_canon(k, md, inv2aR, inv2aR) : cf_key_to_canon(k, md, inv2a, inv2aR);
+  CfWarpWalker<R, Ar> w;
+  w.init(lo + wbase, n, binom, ar, start);
+  for (int s = 0; s < kLinSteps; ++s) {
+    const u64 t0 = wbase + (u64)s * 32;
+    if (t0 >= count) break;                       // uniform across the warp
+    typename Ar::E myA = start;
+    int last;
+    int myidx[R > 1 ? R - 1 : 1];
+    w.template step_idx<true>(n, ar, lane, myA, last, myidx);
+    const u64 t = t0 + lane;
+    if (t < count) {
+      u64 k = ar.key(ar.mul(myA, last));
+      if (canon) {
+        // fast keys hold (x mod m) in standard form, wide keys in Montgomery form
+        k = fast ? cf_key_to_canon(k, md, inv2aR, inv2aR) : cf_key_to_canon(k, md, inv2a, inv2aR);
+      }
+      u64 id = 0;
+      if (id_mode == 1) {
+        id = lo + t;
+      } else if (id_mode == 0) {
+#pragma unroll
+        for (int j = 0; j < R - 1; ++j) id |= ((u64)myidx[j]) << (j * bits);
+        id |= ((u64)last) << ((R - 1) * bits);
+      } else {
+#pragma unroll
+        for (int j = 0; j < R - 1; ++j) id += cf_binom(binom, R, myidx[j], j + 1);
+        id += cf_binom(binom, R, last, R);
+      }
+      keys[t] = k;
+      ids[t] = id;
     }
-    u64 id;
-    if (id_mode == 0) id = w.packed(bits);
-    else if (id_mode == 1) id = lo + my0 + (u64)i;
-    else id = cf_colex_rank<R>(w.idx, binom);
-    s_k[threadIdx.x * (kLinItems + 1) + i] = k;
-    s_i[threadIdx.x * (kLinItems + 1) + i] = id;
-    if (i + 1 < nv) w.next(n, ar);
   }
 }
 
@@ -57,8 +71,6 @@ __global__ void __launch_bounds__(kLinBlock)
 k_gen_linear(const u64* __restrict__ pool, u64 lo, u64 count, int id_mode, int bits, int canon,
              u64* __restrict__ keys, u64* __restrict__ ids) {
   __shared__ u64 s_pk[CF_MAX_POOL];
-  __shared__ u64 s_k[kLinBlock * (kLinItems + 1)];
-  __shared__ u64 s_i[kLinBlock * (kLinItems + 1)];
   const CfPoolHdr* hd = (const CfPoolHdr*)pool;
   const int n = (int)hd->n;
   const bool fast = hd->fast32 != 0;
@@ -79,22 +91,12 @@ k_gen_linear(const u64* __restrict__ pool, u64 lo, u64 count, int id_mode, int b
     CfElt32 st;
     st.X = hd->X0;
     st.x2 = hd->x20;
-    cf_gen_linear_body<R>(pool, ar, st, binom, n, lo, count, id_mode, bits, canon, s_k, s_i);
+    cf_gen_linear_warp<R>(hd, ar, st, binom, n, lo, count, id_mode, bits, canon, keys, ids);
   } else {
     CfArithWide ar;
     ar.md = cf_mod_from_hdr(hd);
     ar.pk = s_pk;
-    cf_gen_linear_body<R>(pool, ar, hd->mult_key, binom, n, lo, count, id_mode, bits, canon, s_k, s_i);
-  }
-  __syncthreads();
-  const u64 tile0 = (u64)blockIdx.x * (kLinBlock * kLinItems);
-  for (int j = threadIdx.x; j < kLinBlock * kLinItems; j += kLinBlock) {
-    const u64 g = tile0 + (u64)j;
-    if (g < count) {
-      const int t = j / kLinItems, i = j % kLinItems;
-      keys[g] = s_k[t * (kLinItems + 1) + i];
-      ids[g] = s_i[t * (kLinItems + 1) + i];
-    }
+    cf_gen_linear_warp<R>(hd, ar, hd->mult_key, binom, n, lo, count, id_mode, bits, canon, keys, ids);
   }
 }
 
@@ -140,14 +142,15 @@ __device__ __forceinline__ void block_exclusive_scan(u32* a, int len, u32* s_war
 }
 
 struct GenPartSmem {
-  size_t stage, p32, binom, hist, total;
+  size_t stage, part, p32, binom, hist, total;
 };
 
-__host__ __device__ inline GenPartSmem gen_part_layout(int block, int items, int n, int R, int pbits) {
+__host__ __device__ inline GenPartSmem gen_part_layout(int block, int steps, int n, int R, int pbits) {
   GenPartSmem L;
-  const size_t T = (size_t)block * items;
+  const size_t T = (size_t)block * steps;
   L.stage = 0;
-  L.p32 = L.stage + T * sizeof(CfRec);
+  L.part = L.stage + T * sizeof(CfRec);
+  L.p32 = L.part + ((T * 2 + 15) & ~(size_t)15);
   size_t b = L.p32 + (((size_t)n * 4 + 15) & ~(size_t)15);
   const size_t binom_bytes = (size_t)(n + 1) * (R + 1) * 8;
   L.binom = (binom_bytes <= kBinomSmemMax) ? b : (size_t)-1;
@@ -157,22 +160,24 @@ __host__ __device__ inline GenPartSmem gen_part_layout(int block, int items, int
   return L;
 }
 
-template <int R, int BLOCK, int ITEMS>
+template <int R, int BLOCK, int STEPS>
 __global__ void __launch_bounds__(BLOCK)
-k_gen_part(const u64* __restrict__ pool, u64 lo, u64 count, int pbits, u32 cap, u32* __restrict__ counts,
-           CfRec* __restrict__ out, u32* __restrict__ err) {
-  constexpr int T = BLOCK * ITEMS;
+k_gen_part(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo, u64 count, int pbits,
+           u32 cap, u32* __restrict__ counts, CfRec* __restrict__ out, u32* __restrict__ err) {
+  constexpr int T = BLOCK * STEPS;
+  constexpr int B = R < 2 ? R : 2;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ u32 s_warp[BLOCK / 32];
   const CfPoolHdr* hd = (const CfPoolHdr*)pool;
   const int n = (int)hd->n;
-  if (!hd->fast32) {            // the solve path requires pool primes < 2^31
+  if (!hd->fast32 || hd->tail_b != (u64)B) {   // the solve path needs primes < 2^31 and the tail table
     if (threadIdx.x == 0) atomicOr(err, CF_ERR_BAD_ARG);
     return;
   }
   const u32 nparts = 1u << pbits;
-  const GenPartSmem L = gen_part_layout(BLOCK, ITEMS, n, R, pbits);
+  const GenPartSmem L = gen_part_layout(BLOCK, STEPS, n, R, pbits);
   CfRec* s_stage = (CfRec*)(smem + L.stage);
+  unsigned short* s_part = (unsigned short*)(smem + L.part);
   u32* s_p = (u32*)(smem + L.p32);
   u32* s_hist = (u32*)(smem + L.hist);
   u32* s_loff = s_hist + nparts;
@@ -191,26 +196,35 @@ k_gen_part(const u64* __restrict__ pool, u64 lo, u64 count, int pbits, u32 cap, 
   CfArithFast ar;
   ar.md = cf_mod32_from_hdr(hd);
   ar.p = s_p;
+  const u64 minv = hd->minv;
   CfElt32 st;
-  st.X = hd->X0;
+  st.X = hd->X0s;
   st.x2 = hd->x20;
   __syncthreads();
 
+  // warp w of this CTA owns the 32*STEPS consecutive ranks starting at wbase
+  const int lane = threadIdx.x & 31;
   const u64 tile0 = (u64)blockIdx.x * T;
-  const u64 my0 = tile0 + (u64)threadIdx.x * ITEMS;
-  int nv = 0;
-  if (my0 < count) nv = (int)((count - my0) < (u64)ITEMS ? (count - my0) : (u64)ITEMS);
-  u64 key[ITEMS];
-  u32 pos[ITEMS];
-  if (nv > 0) {
-    CfLexWalker<R, CfArithFast> w;
-    w.init(lo + my0, n, binom, ar, st);
+  const u64 wbase = tile0 + (u64)(threadIdx.x >> 5) * (32u * STEPS);
+  u64 key[STEPS];
+  u32 pos[STEPS];
+  u32 part[STEPS];
+  if (wbase < count) {
+    CfTailWalker<R, B> w;
+    w.init(lo + wbase, n, binom, ar, st, hd->tail_n);
 #pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-      if (i < nv) {
-        key[i] = w.key;
-        pos[i] = atomicAdd(&s_hist[cf_part_of(cf_hash(w.key), pbits)], 1u);
-        if (i + 1 < nv) w.next(n, ar);
+    for (int s = 0; s < STEPS; ++s) {
+      const u64 t0 = wbase + (u64)s * 32;
+      if (t0 < count) {                         // uniform across the warp
+        CfElt32 q = st;
+        u64 j;
+        int unused[R - B > 0 ? R - B : 1];
+        w.template step<false>(n, binom, ar, lane, q, j, unused);
+        if (t0 + lane < count) {
+          key[s] = cf_tail_key(q, tail[j], ar.md, minv);
+          part[s] = cf_part_of(cf_hash(key[s]), pbits);
+          pos[s] = atomicAdd(&s_hist[part[s]], 1u);
+        }
       }
     }
   }
@@ -238,13 +252,15 @@ k_gen_part(const u64* __restrict__ pool, u64 lo, u64 count, int pbits, u32 cap, 
   __syncthreads();
   block_exclusive_scan<BLOCK>(s_loff, (int)nparts, s_warp);
 #pragma unroll
-  for (int i = 0; i < ITEMS; ++i) {
-    if (i < nv) {
-      const u32 p = cf_part_of(cf_hash(key[i]), pbits);
+  for (int s = 0; s < STEPS; ++s) {
+    const u64 t = wbase + (u64)s * 32 + lane;
+    if (t < count) {
+      const u32 slot = s_loff[part[s]] + pos[s];
       CfRec rc;
-      rc.key = key[i];
-      rc.id = lo + my0 + (u64)i;
-      s_stage[s_loff[p] + pos[i]] = rc;
+      rc.key = key[s];
+      rc.id = lo + t;
+      s_stage[slot] = rc;
+      s_part[slot] = (unsigned short)part[s];
     }
   }
   __syncthreads();
@@ -253,7 +269,7 @@ k_gen_part(const u64* __restrict__ pool, u64 lo, u64 count, int pbits, u32 cap, 
   bool ovf = false;
   for (int j = threadIdx.x; j < tv; j += BLOCK) {
     const CfRec rc = s_stage[j];
-    const u32 p = cf_part_of(cf_hash(rc.key), pbits);
+    const u32 p = s_part[j];
     const u32 dst = s_gbase[p] + ((u32)j - s_loff[p]);
     if (dst < cap) out[(size_t)p * cap + dst] = rc;
     else ovf = true;
@@ -264,38 +280,75 @@ k_gen_part(const u64* __restrict__ pool, u64 lo, u64 count, int pbits, u32 cap, 
 template <int R>
 void launch_gen_linear(const u64* pool, u64 lo, u64 count, int id_mode, int bits, int canon, u64* keys,
                        u64* ids, cudaStream_t st) {
-  const u64 per = (u64)kLinBlock * kLinItems;
+  const u64 per = (u64)kLinBlock * kLinSteps;
   const unsigned grid = (unsigned)((count + per - 1) / per);
   k_gen_linear<R><<<grid, kLinBlock, 0, st>>>(pool, lo, count, id_mode, bits, canon, keys, ids);
 }
 
-// Launch shapes (threads per CTA, records per thread) the autotuner chooses from.
+// Launch shapes (threads per CTA, warp steps per tile) the autotuner chooses from.
 constexpr int kShapes[][2] = {{256, 16}, {512, 8}, {512, 16}, {1024, 8}};
 constexpr int kNumShapes = 4;
 
-template <int R, int BLOCK, int ITEMS>
-int launch_gen_part_shape(const u64* pool, int n, u64 lo, u64 count, int pbits, u32 cap, u32* counts, CfRec* out,
-                          u32* err, cudaStream_t st) {
-  const size_t smem = gen_part_layout(BLOCK, ITEMS, n, R, pbits).total;
+template <int R, int BLOCK, int STEPS>
+int launch_gen_part_shape(const u64* pool, const CfTailEnt* tail, int n, u64 lo, u64 count, int pbits, u32 cap,
+                          u32* counts, CfRec* out, u32* err, cudaStream_t st) {
+  const size_t smem = gen_part_layout(BLOCK, STEPS, n, R, pbits).total;
   if (smem > 227 * 1024) { cf_set_error("cf_gen_part: shared memory budget exceeded%s", ""); return CF_EBADARG; }
-  auto kern = k_gen_part<R, BLOCK, ITEMS>;
+  auto kern = k_gen_part<R, BLOCK, STEPS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cf_cuda_status(e, "cf_gen_part: smem attribute");
-  const u64 per = (u64)BLOCK * ITEMS;
+  const u64 per = (u64)BLOCK * STEPS;
   const unsigned grid = (unsigned)((count + per - 1) / per);
-  kern<<<grid, BLOCK, smem, st>>>(pool, lo, count, pbits, cap, counts, out, err);
+  kern<<<grid, BLOCK, smem, st>>>(pool, tail, lo, count, pbits, cap, counts, out, err);
   return CF_OK;
 }
 
 template <int R>
-void launch_gen_part(const u64* pool, int n, u64 lo, u64 count, int pbits, u32 cap, u32* counts, CfRec* out,
-                     u32* err, cudaStream_t st, int shape, int* rc) {
+void launch_gen_part(const u64* pool, const CfTailEnt* tail, int n, u64 lo, u64 count, int pbits, u32 cap,
+                     u32* counts, CfRec* out, u32* err, cudaStream_t st, int shape, int* rc) {
   switch (shape) {
-    case 0: *rc = launch_gen_part_shape<R, 256, 16>(pool, n, lo, count, pbits, cap, counts, out, err, st); break;
-    case 1: *rc = launch_gen_part_shape<R, 512, 8>(pool, n, lo, count, pbits, cap, counts, out, err, st); break;
-    case 2: *rc = launch_gen_part_shape<R, 512, 16>(pool, n, lo, count, pbits, cap, counts, out, err, st); break;
-    default: *rc = launch_gen_part_shape<R, 1024, 8>(pool, n, lo, count, pbits, cap, counts, out, err, st); break;
+    case 0: *rc = launch_gen_part_shape<R, 256, 16>(pool, tail, n, lo, count, pbits, cap, counts, out, err, st); break;
+    case 1: *rc = launch_gen_part_shape<R, 512, 8>(pool, tail, n, lo, count, pbits, cap, counts, out, err, st); break;
+    case 2: *rc = launch_gen_part_shape<R, 512, 16>(pool, tail, n, lo, count, pbits, cap, counts, out, err, st); break;
+    default: *rc = launch_gen_part_shape<R, 1024, 8>(pool, tail, n, lo, count, pbits, cap, counts, out, err, st); break;
   }
+}
+
+// Tail table: entry t = product of the t-th B-subset (lexicographic) of the pool.
+template <int R>
+__global__ void k_build_tail(const u64* __restrict__ pool, CfTailEnt* __restrict__ tail) {
+  constexpr int B = R < 2 ? R : 2;
+  const CfPoolHdr* hd = (const CfPoolHdr*)pool;
+  if (hd->tail_b != (u64)B) return;
+  const int n = (int)hd->n;
+  const u64* binom = pool + cf_pool_off_binom(n);
+  const u64* pr = pool + cf_pool_off_prime(n);
+  const CfMod32 md = cf_mod32_from_hdr(hd);
+  const u64 tn = hd->tail_n;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tn; t += (u64)gridDim.x * blockDim.x) {
+    int idx[B];
+    cf_unrank_lex_k<B, R>(t, n, binom, idx);
+    CfElt32 e;
+    e.X = hd->S0;
+    e.x2 = 1ull & md.mask2;
+    u32 ij = 0;
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+      e = cf_mul32(e, (u32)pr[idx[j]], md);
+      ij |= (u32)idx[j] << (10 * j);
+    }
+    CfTailEnt ent;
+    ent.X = (e.X >= md.m) ? e.X - md.m : e.X;
+    ent.x2 = (u32)e.x2;
+    ent.ij = ij;
+    tail[t] = ent;
+  }
+}
+
+template <int R>
+void launch_build_tail(const u64* pool, CfTailEnt* tail, u64 tn, cudaStream_t st) {
+  const u64 g = (tn + 255) / 256;
+  k_build_tail<R><<<(unsigned)(g < 4096 ? (g ? g : 1) : 4096), 256, 0, st>>>(pool, tail);
 }
 
 }  // namespace
@@ -326,8 +379,31 @@ extern "C" size_t cf_gen_part_smem_bytes(int n, int r, int pbits, int shape) {
   return gen_part_layout(kShapes[shape][0], kShapes[shape][1], n, r, pbits).total;
 }
 
-extern "C" int cf_gen_part(const void* pool_dev, int n, int r, u64 lo, u64 count, int pbits, u32 cap,
-                           u32* counts, void* out, u32* err, int shape, void* stream) {
+static u64 host_binom(int n, int k) {
+  if (k < 0 || k > n) return 0;
+  unsigned __int128 v = 1;
+  for (int i = 1; i <= k; ++i) v = v * (unsigned)(n - k + i) / (unsigned)i;
+  return (u64)v;
+}
+
+extern "C" size_t cf_tail_bytes(int n, int r) {
+  if (n < 1 || n > CF_MAX_POOL || r < 1 || r > CF_MAX_DISPATCH_R) return 0;
+  return (size_t)host_binom(n, r < 2 ? r : 2) * sizeof(CfTailEnt);
+}
+
+extern "C" int cf_build_tail(const void* pool_dev, int n, int r, void* tail, void* stream) {
+  if (!pool_dev || !tail || n < 1 || n > CF_MAX_POOL || r < 1 || r > CF_MAX_DISPATCH_R || r > n) {
+    cf_set_error("cf_build_tail: bad arguments%s", "");
+    return CF_EBADARG;
+  }
+  CF_DISPATCH_R(r, launch_build_tail, (const u64*)pool_dev, (CfTailEnt*)tail, host_binom(n, r < 2 ? r : 2),
+                (cudaStream_t)stream);
+  CF_LAUNCH_CHECK("cf_build_tail");
+  return CF_OK;
+}
+
+extern "C" int cf_gen_part(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count, int pbits,
+                           u32 cap, u32* counts, void* out, u32* err, int shape, void* stream) {
   if (!pool_dev || n < 1 || n > CF_MAX_POOL || r < 1 || r > CF_MAX_DISPATCH_R || r > n) {
     cf_set_error("cf_gen_part: bad pool arguments (n 1..1024, r 1..10)%s", "");
     return CF_EBADARG;
@@ -335,11 +411,11 @@ extern "C" int cf_gen_part(const void* pool_dev, int n, int r, u64 lo, u64 count
   if (pbits < 0 || pbits > 12) { cf_set_error("cf_gen_part: pbits must be 0..12%s", ""); return CF_EBADARG; }
   if (shape < 0 || shape >= kNumShapes) { cf_set_error("cf_gen_part: unknown launch shape%s", ""); return CF_EBADARG; }
   if (count == 0) return CF_OK;
-  if (!counts || !out || !err) { cf_set_error("cf_gen_part: null buffer%s", ""); return CF_EBADARG; }
+  if (!counts || !out || !err || !tail) { cf_set_error("cf_gen_part: null buffer%s", ""); return CF_EBADARG; }
   if (count > (1ull << 40)) { cf_set_error("cf_gen_part: count too large for one launch%s", ""); return CF_EBADARG; }
   int rc = CF_OK;
-  CF_DISPATCH_R(r, launch_gen_part, (const u64*)pool_dev, n, lo, count, pbits, cap, counts, (CfRec*)out, err,
-                (cudaStream_t)stream, shape, &rc);
+  CF_DISPATCH_R(r, launch_gen_part, (const u64*)pool_dev, (const CfTailEnt*)tail, n, lo, count, pbits, cap, counts,
+                (CfRec*)out, err, (cudaStream_t)stream, shape, &rc);
   if (rc != CF_OK) return rc;
   CF_LAUNCH_CHECK("cf_gen_part");
   return CF_OK;

@@ -89,6 +89,13 @@ extern "C" int cf_pool_prepare(const u64* primes, int n, int r, u64 M, u64 mult,
   hd->ninv32 = (u64)(u32)(0u - (u32)h.minv);                 // -m^-1 mod 2^32
   hd->X0 = (u64)((u128)((mult % M) % h.m) * mod_pow(2, 32ull * (u64)r, h.m) % h.m);
   hd->x20 = (mult % M) & h.mask2;
+  // tail table: b = min(R, 2) primes per entry when the fast path applies and 2^a fits 32 bits
+  const int b = (hd->fast32 && h.a <= 32) ? (r < 2 ? r : 2) : 0;
+  hd->tail_b = (u64)b;
+  if (b) {
+    hd->X0s = (u64)((u128)((mult % M) % h.m) * mod_pow(2, 32ull * (u64)(r - b), h.m) % h.m);
+    hd->S0 = mod_pow(2, 64ull + 32ull * (u64)b, h.m);
+  }
   u64* pkey = w + cf_pool_off_pkey(n);
   u64* prime = w + cf_pool_off_prime(n);
   double* lg = (double*)(w + cf_pool_off_lg(n));
@@ -113,6 +120,7 @@ extern "C" int cf_pool_prepare(const u64* primes, int n, int r, u64 M, u64 mult,
     }
   }
   hd->total = binom[(size_t)n * (r + 1) + r];
+  hd->tail_n = b ? binom[(size_t)n * (r + 1) + b] : 0;
   return CF_OK;
 }
 

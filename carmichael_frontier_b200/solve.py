@@ -115,6 +115,8 @@ class Instance:
             raise ValueError("every pool prime must be coprime to M (q does not divide M)")
         if any(p >= 1 << 31 for p in base) or any(q >= 1 << 31 for q in ins):
             raise ValueError("pool primes must be below 2^31")
+        if M % (1 << 33) == 0:
+            raise ValueError("2^33 divides M: the solve path needs the 2-adic part of M below 2^33")
         return Instance(M, base, ins, r, B, P0)
 
 
@@ -179,8 +181,11 @@ class Solver:
         nD, nIt = ncomb(len(inst.B0), r), ncomb(len(inst.INS), r)
         P = plan["nparts"]
         pbits, shape = plan["pbits"], plan["shape"]
-        poolD = self.tables.pool(inst.B0, r, M, pow(inst.P0, -1, M))
+        multD = pow(inst.P0, -1, M)
+        poolD = self.tables.pool(inst.B0, r, M, multD)
         poolI = self.tables.pool(inst.INS, r, M, 1)
+        tailD = self.tables.tail(inst.B0, r, M, multD, poolD)
+        tailI = self.tables.tail(inst.INS, r, M, 1, poolI)
         screen = self.tables.screen(inst.P0, inst.B, 1e-6)
         capD, capI, chunk = plan["capD"], plan["capI"], plan["chunk"]
         Dbuf = self._buf("D", P * capD * 16)
@@ -199,7 +204,7 @@ class Solver:
         ck = _lib.check
         launches = 0
         self._mark(marks, "start")
-        ck(lib.cf_gen_part(dp(poolD), len(inst.B0), r, 0, nD, pbits, capD, dp(dcnt), dp(Dbuf),
+        ck(lib.cf_gen_part(dp(poolD), dp(tailD), len(inst.B0), r, 0, nD, pbits, capD, dp(dcnt), dp(Dbuf),
                            dp(misc) + 4, shape, sh), "cf_gen_part(D)")
         launches += 1
         self._mark(marks, "gen_D")
@@ -207,7 +212,7 @@ class Solver:
             cnt = min(chunk, nIt - lo)
             if lo:
                 icnt.zero_()
-            ck(lib.cf_gen_part(dp(poolI), len(inst.INS), r, lo, cnt, pbits, capI, dp(icnt), dp(Ibuf),
+            ck(lib.cf_gen_part(dp(poolI), dp(tailI), len(inst.INS), r, lo, cnt, pbits, capI, dp(icnt), dp(Ibuf),
                                dp(misc) + 4, shape, sh), "cf_gen_part(I)")
             self._mark(marks, "gen_I")
             ck(lib.cf_join_part(dp(Dbuf), dp(dcnt), capD, dp(Ibuf), dp(icnt), capI, pbits, plan["sbits"],

@@ -56,6 +56,22 @@ class DeviceTables:
         key = ("pool", tuple(int(p) for p in primes), r, M, int(mult) % M)
         return self.get(key, lambda: pool_table_host(primes, r, M, mult))
 
+    def tail(self, primes, r: int, M: int, mult: int, pool_dev):
+        """Device tail table (b-subset products) of a pool, built on the device once."""
+        import torch
+        key = ("tail", tuple(int(p) for p in primes), r, M, int(mult) % M)
+        t = self._cache.get(key)
+        if t is None:
+            lib = _lib.load()
+            nbytes = lib.cf_tail_bytes(len(primes), r)
+            t = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=self.device)
+            _lib.check(lib.cf_build_tail(pool_dev.data_ptr(), len(primes), r, t.data_ptr(), _lib.stream_handle()),
+                       "cf_build_tail")
+            if len(self._cache) >= self.max_entries:
+                self._cache.pop(next(iter(self._cache)))
+            self._cache[key] = t
+        return t
+
     def screen(self, P0: int, B: int, eps: float):
         key = ("screen", P0, B, eps)
         return self.get(key, lambda: screen_table_host(P0, B, eps))

@@ -99,6 +99,14 @@ int cf_screen_prepare(const uint32_t* limbsB, int nlimbs, double lgP0, double lg
 int cf_gen_subsets(const void* pool_dev, int n, int r, uint64_t lo, uint64_t count, int id_mode, int bits,
                    int canon, uint64_t* keys, uint64_t* ids, void* stream);
 
+/* Tail table of a pool (device, cf_tail_bytes(n, r) bytes): the products of all
+ * b-subsets of the pool, b = min(r, 2), in lexicographic order, 16 bytes each.
+ * Built once per pool by cf_build_tail; the generators split every r-subset into
+ * an (r-b)-prefix and a b-suffix read from this table.  Requires pool primes
+ * below 2^31 and 2^32 not dividing M. */
+size_t cf_tail_bytes(int n, int r);
+int cf_build_tail(const void* pool_dev, int n, int r, void* tail, void* stream);
+
 /* Partitioned generation for the solve path (pool primes below 2^31): the
  * records of ranks [lo, lo+count) (id = lexicographic rank) are scattered into
  * 2^pbits (pbits 0..12) residue partitions -- the top pbits bits of
@@ -112,8 +120,8 @@ int cf_gen_subsets(const void* pool_dev, int n, int r, uint64_t lo, uint64_t cou
  * + sort_side() as the producer of a joinable side. */
 int cf_gen_part_shapes(void);
 size_t cf_gen_part_smem_bytes(int n, int r, int pbits, int shape);
-int cf_gen_part(const void* pool_dev, int n, int r, uint64_t lo, uint64_t count, int pbits, uint32_t cap,
-                uint32_t* counts, void* out, uint32_t* err, int shape, void* stream);
+int cf_gen_part(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count, int pbits,
+                uint32_t cap, uint32_t* counts, void* out, uint32_t* err, int shape, void* stream);
 
 /* ---- join ---------------------------------------------------------------- */
 
