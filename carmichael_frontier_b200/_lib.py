@@ -69,6 +69,8 @@ SIGNATURES = [
     ("cf_check_pairs", C.c_int, [vp, vp, vp, C.c_int, vp, vp, u32, vp, vp, vp]),
     ("cf_sort_tmp_bytes", sz, [u64]),
     ("cf_sort_pairs", C.c_int, [vp, vp, u64, C.c_int, vp, sz, vp]),
+    ("cf_sort_pairs_noalloc_max", u64, []),
+    ("cf_sort_pairs_noalloc", C.c_int, [vp, vp, u64, C.c_int, vp]),
     ("cf_merge_run_bytes", sz, []),
     ("cf_merge_join_runs", C.c_int, [vp, u64, vp, u64, vp, u64, vp, vp, vp, vp]),
 ]

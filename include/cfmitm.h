@@ -155,6 +155,18 @@ size_t cf_sort_tmp_bytes(uint64_t n);
 int cf_sort_pairs(uint64_t* keys, uint64_t* ids, uint64_t n, int key_bits, void* tmp, size_t tmp_bytes,
                   void* stream);
 
+/* The same sort for callers that cannot allocate device memory (for example
+ * when all device memory belongs to another allocator): no workspace argument;
+ * the scratch is a fixed array inside this library's own device memory (3 MiB,
+ * held by every GPU that loads the library).  n is limited to
+ * cf_sort_pairs_noalloc_max() = 131072 records; larger n returns CF_EBADARG.
+ * The first call on a device looks up the array's address on that device
+ * (make it before any stream capture).  Calls share the array: device work of
+ * two calls must not overlap.  This entry point has no counterpart in the
+ * reference. */
+uint64_t cf_sort_pairs_noalloc_max(void);
+int cf_sort_pairs_noalloc(uint64_t* keys, uint64_t* ids, uint64_t n, int key_bits, void* stream);
+
 /* Equal-key runs between sorted Dk[nD] and sorted Ik[nI]: runs (24 bytes each,
  * {I row, first D position, count}), unordered, counted in the device u64
  * counters *nruns and *npairs (zeroed by the caller).  The count/emit core of
