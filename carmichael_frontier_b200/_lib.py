@@ -65,6 +65,10 @@ SIGNATURES = [
     ("cf_gen_part", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, C.c_int, u32, vp, vp, vp, C.c_int, vp]),
     ("cf_join_part_smem_bytes", sz, [C.c_int]),
     ("cf_join_part", C.c_int, [vp, vp, u32, vp, vp, u32, C.c_int, C.c_int, u32, u32, vp, u32, vp, vp, vp]),
+    ("cf_dtab_bytes", sz, [C.c_int]),
+    ("cf_dtab_fp_bytes", sz, [C.c_int]),
+    ("cf_dtab_build", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, vp, vp]),
+    ("cf_fused_probe", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, u64, vp, u32, vp, vp, u32, vp]),
     ("cf_pair_result_bytes", sz, []),
     ("cf_check_pairs", C.c_int, [vp, vp, vp, C.c_int, vp, vp, u32, vp, vp, vp]),
     ("cf_sort_tmp_bytes", sz, [u64]),

@@ -75,8 +75,7 @@ k_check_pairs(const u64* __restrict__ poolD, const u64* __restrict__ poolI, cons
       out.i_idx[j] = (unsigned short)ii[j];
     }
     if (kd == ki) out.flags |= CF_HIT_KEY_EQUAL;
-    else atomicOr(err, CF_ERR_KEY_MISMATCH);
-    if (lg <= scr->lgB + scr->eps) {
+    if (kd == ki && lg <= scr->lgB + scr->eps) {
       out.flags |= CF_HIT_SCREEN;
       // --- distinctness of S = (B0 \ D) u I: D indices are distinct by construction
       //     (strictly increasing), I primes must avoid B0 and each other.

@@ -263,6 +263,16 @@ struct CfTailWalker {
   template <bool WANT_IDX>
   __device__ __forceinline__ void step(int n, const u64* __restrict__ binom, const CfArithFast& ar, int lane,
                                        CfElt32& myQ, u64& myj, int (&myidx)[A > 0 ? A : 1]) {
+    if (tend - cur >= 32) {                       // common case: the whole step lies in one tail
+      myQ = Q[A];
+      myj = cur + (u64)lane;
+      cur += 32;
+      if (WANT_IDX) {
+#pragma unroll
+        for (int j = 0; j < A; ++j) myidx[j] = idx[j];
+      }
+      return;
+    }
     int f = 0;
     myj = ~0ull;
     do {

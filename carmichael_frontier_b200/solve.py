@@ -73,6 +73,9 @@ class Tuning:
     i_chunk_records: int = 1 << 31  # I-side records per generation/join chunk
     pair_capacity: int = 1 << 14    # initial candidate-pair buffer (grown on overflow)
     sigma: float = 6.0              # partition capacity = mean + sigma*sqrt(mean) + 16
+    strategy: str = "fused"         # "fused": D table + generate-and-probe; "partition": materialised join
+    dtab_load: float = 5.0          # fused: minimum average D records per 16-slot bucket (up to 2x this)
+    fused_grid: int = 0             # fused probe CTAs (0 = one per 4096 records)
 
 
 def _pow2ceil(x: int) -> int:
@@ -163,8 +166,12 @@ class Solver:
         while sbits < tu.max_sbits and (1 << (sbits - 1)) < cD:
             sbits += 1
         isplit = tu.isplit or max(1, min(16, (2 * 148 * 2) // max(1, nparts)))
+        # 2^bbits buckets of 16 slots: average load between dtab_load and 2*dtab_load, never above 12
+        bbits = max(4, int(math.floor(math.log2(max(nD / tu.dtab_load, 2.0)))),
+                    math.ceil(math.log2(max(nD / 12.0, 2.0))))
         return dict(pbits=pbits, nparts=nparts, capD=max(cD, 1), capI=max(cI, 1), chunk=max(chunk, 1), sbits=sbits,
-                    isplit=isplit, pairs=pairs or tu.pair_capacity, shape=tu.gen_shape)
+                    isplit=isplit, pairs=pairs or tu.pair_capacity, shape=tu.gen_shape, strategy=tu.strategy,
+                    bbits=bbits)
 
     # -- one solve -----------------------------------------------------------
     def _mark(self, marks, tag):
@@ -176,6 +183,53 @@ class Solver:
     def enqueue(self, inst: Instance, plan: dict, marks: list | None = None):
         """Queue the whole device pipeline for `inst` on the stream (no host sync).
         `marks` (optional list) receives (tag, CUDA event) pairs around every kernel."""
+        if plan.get("strategy", "fused") == "fused":
+            return self._enqueue_fused(inst, plan, marks)
+        return self._enqueue_partition(inst, plan, marks)
+
+    def _tables_for(self, inst: Instance):
+        M, r = inst.M, inst.r
+        multD = pow(inst.P0, -1, M)
+        poolD = self.tables.pool(inst.B0, r, M, multD)
+        poolI = self.tables.pool(inst.INS, r, M, 1)
+        tailD = self.tables.tail(inst.B0, r, M, multD, poolD)
+        tailI = self.tables.tail(inst.INS, r, M, 1, poolI)
+        screen = self.tables.screen(inst.P0, inst.B, 1e-6)
+        return poolD, poolI, tailD, tailI, screen
+
+    def _enqueue_fused(self, inst: Instance, plan: dict, marks: list | None):
+        """D table build, fused generate-and-probe of the I side, pair check."""
+        torch, lib = self.torch, self.lib
+        r = inst.r
+        nD, nIt = ncomb(len(inst.B0), r), ncomb(len(inst.INS), r)
+        poolD, poolI, tailD, tailI, screen = self._tables_for(inst)
+        bbits = plan["bbits"]
+        tab = self._buf("dtab", lib.cf_dtab_bytes(bbits))
+        ctr = self._buf("ctr", 64)
+        misc = ctr[:64].view(torch.int32)
+        maxp = plan["pairs"]
+        pairs = self._buf("pairs", maxp * 16)
+        res = self._buf("res", maxp * self.result_bytes)
+        sh = self._sh()
+        dp = _lib.ptr
+        ck = _lib.check
+        misc.zero_()
+        tab[: lib.cf_dtab_fp_bytes(bbits)].zero_()
+        tab[lib.cf_dtab_bytes(bbits) - 4 * (1 << bbits): lib.cf_dtab_bytes(bbits)].zero_()
+        self._mark(marks, "start")
+        ck(lib.cf_dtab_build(dp(poolD), dp(tailD), len(inst.B0), r, 0, nD, dp(tab), bbits, dp(misc) + 4, sh),
+           "cf_dtab_build")
+        self._mark(marks, "gen_D")
+        ck(lib.cf_fused_probe(dp(poolI), dp(tailI), len(inst.INS), r, 0, nIt, dp(tab), bbits, 0, dp(pairs), maxp,
+                              dp(misc), dp(misc) + 4, self.tuning.fused_grid, sh), "cf_fused_probe")
+        self._mark(marks, "probe")
+        ck(lib.cf_check_pairs(dp(poolD), dp(poolI), dp(screen), r, dp(pairs), dp(misc), maxp, dp(res),
+                              dp(misc) + 4, sh), "cf_check_pairs")
+        self._mark(marks, "check")
+        return dict(misc=misc, dcnt=None, icnt=None, res=res, nD=nD, nI=nIt, plan=plan, launches=3)
+
+    def _enqueue_partition(self, inst: Instance, plan: dict, marks: list | None):
+        """Partitioned generation of both sides and the shared-memory partition join."""
         torch, lib = self.torch, self.lib
         r, M = inst.r, inst.M
         nD, nIt = ncomb(len(inst.B0), r), ncomb(len(inst.INS), r)
@@ -232,11 +286,13 @@ class Solver:
         misc = h["misc"][:2].cpu().numpy().view(np.uint32)
         npairs, err = int(misc[0]), int(misc[1])
         plan = h["plan"]
+        if err & _lib.ERR_TABLE_FULL:
+            raise _lib.CfError(_lib.CF_EOVERFLOW, "solve", "D table full (internal error)")
         if err & (_lib.ERR_PART_OVERFLOW | _lib.ERR_PAIR_OVERFLOW):
-            dmax = int(h["dcnt"].max().item())
-            imax = int(h["icnt"].max().item())
             newp = dict(plan)
             if err & _lib.ERR_PART_OVERFLOW:
+                dmax = int(h["dcnt"].max().item())
+                imax = int(h["icnt"].max().item())
                 newp["capD"] = max(plan["capD"], dmax + 16)
                 newp["capI"] = max(plan["capI"], imax + 16)
             if err & _lib.ERR_PAIR_OVERFLOW:
@@ -255,11 +311,15 @@ class Solver:
         r = inst.r
         hits, screened, above, rejected, pairs = [], 0, 0, 0, []
         bset = inst.B0
+        fused = h["plan"].get("strategy") == "fused"
+        nres = 0
         for row in res:
             f = int(row["flags"])
             if not f & _lib.HIT_KEY_EQUAL:
-                rejected += 1
-                continue
+                if not fused:           # the partition join compares full keys: unequal residues are a bug
+                    rejected += 1
+                continue                # fused: a 32-bit fingerprint collision, not a pair
+            nres += 1
             pairs.append((tuple(bset[int(x)] for x in row["d_idx"][:r]),
                           tuple(inst.INS[int(x)] for x in row["i_idx"][:r])))
             if not f & _lib.HIT_SCREEN:
@@ -291,7 +351,7 @@ class Solver:
             hits.append(Hit(D, I, n, fac))
         hits.sort(key=lambda x: (x.n, x.D, x.I))
         pairs.sort()
-        return SolveResult(hits=hits, n_D=h["nD"], n_I=h["nI"], residue_pairs=len(res), screened=screened,
+        return SolveResult(hits=hits, n_D=h["nD"], n_I=h["nI"], residue_pairs=nres, screened=screened,
                            above_bound=above, rejected=rejected, plan=dict(h["plan"]), pairs=pairs)
 
     def solve_instance(self, inst: Instance, verify: bool = True, timed: bool = False,
@@ -302,6 +362,8 @@ class Solver:
         if nI == 0 or nD == 0:
             return SolveResult([], nD, nI, 0, 0, 0, 0)
         plan = self.plan(nD, nI)
+        if nD >= 1 << 32:                 # D ranks in the fused table are 32-bit
+            plan["strategy"] = "partition"
         for _attempt in range(6):
             ev0 = ev1 = None
             if timed:
@@ -320,6 +382,7 @@ class Solver:
                 out.launches = h["launches"]
                 return out
             plan = self.plan(nD, nI, newp["capD"], newp["capI"], newp["pairs"])
+            plan["strategy"] = newp.get("strategy", plan["strategy"])
         raise _lib.CfError(_lib.CF_EOVERFLOW, "solve", "capacities kept overflowing")
 
     def _torch_stream(self):
@@ -341,17 +404,18 @@ class Solver:
 _default_solvers: dict = {}
 
 
-def solve(M: int, Q, B0, r: int, B: int, device=None, verify: bool = True) -> SolveResult:
+def solve(M: int, Q, B0, r: int, B: int, device=None, verify: bool = True, strategy: str = "fused") -> SolveResult:
     """Every Carmichael hit S = (B0 \\ D) u I with |D| = |I| = r, prod(S) == 1 (mod M), prod(S) <= B.
 
     Q is the eligible pool Q(M) (primes q with (q-1) | M and q not dividing M);
-    INS = Q \\ B0.  Hits are certified on the host and returned ascending by n."""
+    INS = Q \\ B0.  Hits are certified on the host and returned ascending by n.
+    strategy: "fused" (D table + generate-and-probe) or "partition" (materialised join)."""
     import torch
     dev = torch.device(device if device is not None else "cuda")
-    key = (dev.type, dev.index)
+    key = (dev.type, dev.index, strategy)
     s = _default_solvers.get(key)
     if s is None:
-        s = _default_solvers[key] = Solver(dev)
+        s = _default_solvers[key] = Solver(dev, tuning=Tuning(strategy=strategy))
     return s.solve(M, Q, B0, r, B, verify=verify)
 
 

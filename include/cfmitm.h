@@ -138,6 +138,29 @@ int cf_join_part(const void* D, const uint32_t* dcount, uint32_t capD, const voi
                  uint32_t capI, int pbits, int sbits, uint32_t isplit, uint32_t grid, void* pairs,
                  uint32_t max_pairs, uint32_t* npairs, uint32_t* err, void* stream);
 
+/* Fused generate-and-probe join (the I side is never written to memory).
+ * D table: 2^bbits buckets of 16 slots, cf_dtab_bytes(bbits) bytes: first an
+ * array of 32-byte fingerprint sectors (16 16-bit fingerprints per bucket, the
+ * one sector a probe reads; cf_dtab_fp_bytes(bbits) bytes, L2-resident for
+ * r <= 5), then per slot a second 32-bit fingerprint and the D rank, then a
+ * 4-byte fill counter per bucket.  Before building, the caller zeroes the
+ * fingerprint array and the fill counters (the last 4 * 2^bbits bytes).
+ * cf_dtab_build inserts the D records of ranks [lo, lo+count), count < 2^32;
+ * cf_fused_probe generates the I records of ranks [lo, lo+count) in
+ * registers, probes the table and appends every {D rank, I rank} candidate
+ * whose fingerprints agree through *npairs (zeroed by the caller);
+ * cf_check_pairs then flags the pairs whose residues are equal
+ * (CF_HIT_KEY_EQUAL), which is the exact pair set.  Replaces join_sorted
+ * (gpu/mitm_gpu2.py:107-119) and the probe of src/mitm64.cpp:85-101 without
+ * materialising the I side. */
+size_t cf_dtab_bytes(int bbits);
+size_t cf_dtab_fp_bytes(int bbits);
+int cf_dtab_build(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count, void* tab,
+                  int bbits, uint32_t* err, void* stream);
+int cf_fused_probe(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count,
+                   const void* tab, int bbits, uint64_t d_rank0, void* pairs, uint32_t max_pairs,
+                   uint32_t* npairs, uint32_t* err, uint32_t grid, void* stream);
+
 /* Exact check of candidate pairs (lexicographic-rank ids): recomputed residues,
  * conservative fp64 log-size screen, exact size n <= B, Korselt, distinctness.
  * results[t] (cf_pair_result_bytes() each) for t < min(*npairs, max_pairs).

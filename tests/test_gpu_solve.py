@@ -11,9 +11,9 @@ from carmichael_frontier_b200.solve import Instance
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def solver(cuda):
-    return Solver(cuda)
+@pytest.fixture(scope="module", params=["fused", "partition"])
+def solver(cuda, request):
+    return Solver(cuda, tuning=Tuning(strategy=request.param))
 
 
 def as_lists(pairs):
@@ -49,9 +49,10 @@ def test_small_instances_vs_exhaustive(solver, seed):
         assert res.rejected == 0
 
 
-def test_small_modulus_many_pairs_grows_buffers(cuda):
+@pytest.mark.parametrize("strategy", ["fused", "partition"])
+def test_small_modulus_many_pairs_grows_buffers(cuda, strategy):
     # tiny M: residues collide massively, so partitions and the pair buffer overflow and are regrown
-    s = Solver(cuda, tuning=Tuning(d_per_part=64, pair_capacity=16, sigma=0.0))
+    s = Solver(cuda, tuning=Tuning(d_per_part=64, pair_capacity=16, sigma=0.0, strategy=strategy, dtab_load=11.5))
     M = 2 ** 5 * 3 ** 2 * 5 * 7 * 11 * 13
     Q = W.eligible_pool(M)
     B0 = Q[:20]
