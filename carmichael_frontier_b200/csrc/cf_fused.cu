@@ -29,11 +29,20 @@ constexpr size_t kBinomSmemMaxF = 24 * 1024;
 
 // Bucket and fingerprints of a residue, from its canonical odd part X (< m) and
 // 2-adic part x2 (< 2^a, a <= 32): the pair is the residue, so equal residues
-// give equal bucket and fingerprints.
-__device__ __forceinline__ u64 cf_fuse_h(u64 X, u32 x2) { return (X + ((u64)x2 << 32) * 0x2545F491u) * CF_HASH_MULT; }
-
-__device__ __forceinline__ u64 cf_fuse_g(u64 X, u32 x2) {
-  return (X ^ (X >> 31) ^ ((u64)x2 << 40)) * 0xD6E8FEB86659FD93ull;
+// give equal bucket and fingerprints.  The bucket and the 16-bit fingerprint
+// are the top bbits and the next 16 bits of one 64-bit multiplicative hash;
+// the 32-bit side fingerprint is an independent 32-bit fold of the residue.
+struct CfFuseKey {
+  u32 bucket, f16, f32;
+};
+__device__ __forceinline__ CfFuseKey cf_fuse_key(u64 X, u32 x2, int bbits) {
+  const u64 h = (X ^ ((u64)x2 << 32)) * CF_HASH_MULT;
+  CfFuseKey k;
+  k.bucket = (u32)(h >> (64 - bbits));
+  const u32 f = (u32)(h >> (48 - bbits)) & 0xffffu;
+  k.f16 = f ? f : 1u;                       // 0 marks an empty slot
+  k.f32 = (u32)X ^ ((u32)(X >> 32) * 0x85EBCA6Bu) ^ (x2 * 0xC2B2AE35u);
+  return k;
 }
 
 // Canonical odd part and 2-adic part of prefix product q times tail entry e.
@@ -54,20 +63,13 @@ struct DTab {
   int bbits;
 };
 
-__device__ __forceinline__ void fuse_fps(u64 X, u32 x2, u32& f16, u32& f32) {
-  const u64 g = cf_fuse_g(X, x2);
-  f16 = (u32)(g >> 48);
-  f16 = f16 ? f16 : 1u;                     // 0 marks an empty slot
-  f32 = (u32)g;
-}
-
 // Insert a residue (X, x2) with its rank; returns false if every bucket was full.
 // A slot is claimed with one atomicAdd on the bucket's fill counter; the claimed
 // 16-bit half is then set with atomicOr (its word is shared with a neighbour slot).
 __device__ __forceinline__ bool dtab_insert(const DTab& t, u64 X, u32 x2, u64 rank) {
-  u32 f16, f32;
-  fuse_fps(X, x2, f16, f32);
-  u64 b = cf_fuse_h(X, x2) >> (64 - t.bbits);
+  const CfFuseKey fk = cf_fuse_key(X, x2, t.bbits);
+  const u32 f16 = fk.f16, f32 = fk.f32;
+  u64 b = fk.bucket;
   for (u64 tries = 0; tries < t.nb; ++tries) {
     const u32 s = atomicAdd(&t.fill[b], 1u);
     if (s < 16u) {
@@ -115,14 +117,18 @@ __device__ __noinline__ void probe_slow(const DTab& t, u64 b, u32 f16, u32 f32, 
   }
 }
 
-// Fast test of one bucket: any 16-bit fingerprint equal to f16 (hit), or no empty slot (full).
+// Nonzero iff some 16-bit half of w is zero (SWAR test; exact, no false positives).
+__device__ __forceinline__ u32 cf_zero_half(u32 w) { return (w - 0x00010001u) & ~w & 0x80008000u; }
+
+// Fast test of one bucket: any 16-bit fingerprint equal to f16 (hit), or the
+// bucket is full.  Slots are claimed in order, so the bucket is full exactly
+// when its last slot (the high half of the last word) is occupied.
 __device__ __forceinline__ bool probe_fast(uint4 r0, uint4 r1, u32 f16) {
   const u32 ff = f16 * 0x10001u;
-  const u32 eq = __vcmpeq2(r0.x, ff) | __vcmpeq2(r0.y, ff) | __vcmpeq2(r0.z, ff) | __vcmpeq2(r0.w, ff) |
-                 __vcmpeq2(r1.x, ff) | __vcmpeq2(r1.y, ff) | __vcmpeq2(r1.z, ff) | __vcmpeq2(r1.w, ff);
-  const u32 z = __vcmpeq2(r0.x, 0u) | __vcmpeq2(r0.y, 0u) | __vcmpeq2(r0.z, 0u) | __vcmpeq2(r0.w, 0u) |
-                __vcmpeq2(r1.x, 0u) | __vcmpeq2(r1.y, 0u) | __vcmpeq2(r1.z, 0u) | __vcmpeq2(r1.w, 0u);
-  return (eq != 0u) | (z == 0u);
+  const u32 eq = cf_zero_half(r0.x ^ ff) | cf_zero_half(r0.y ^ ff) | cf_zero_half(r0.z ^ ff) |
+                 cf_zero_half(r0.w ^ ff) | cf_zero_half(r1.x ^ ff) | cf_zero_half(r1.y ^ ff) |
+                 cf_zero_half(r1.z ^ ff) | cf_zero_half(r1.w ^ ff);
+  return (eq != 0u) | ((r1.w >> 16) != 0u);
 }
 
 struct FuseSmem {
@@ -202,12 +208,10 @@ k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo
         if (MODE == 0) {
           bad |= !dtab_insert(tab, X, x2, rank_base + off);
         } else {
-          const u64 b = cf_fuse_h(X, x2) >> (64 - tab.bbits);
-          u32 f16, f32;
-          fuse_fps(X, x2, f16, f32);
-          const uint4* row = (const uint4*)(tab.fpw + b * 8);
-          if (probe_fast(__ldg(row), __ldg(row + 1), f16))
-            probe_slow(tab, b, f16, f32, rank_base + off, pairs, max_pairs, npairs, err);
+          const CfFuseKey fk = cf_fuse_key(X, x2, tab.bbits);
+          const uint4* row = (const uint4*)(tab.fpw + (u64)fk.bucket * 8);
+          if (probe_fast(__ldg(row), __ldg(row + 1), fk.f16))
+            probe_slow(tab, fk.bucket, fk.f16, fk.f32, rank_base + off, pairs, max_pairs, npairs, err);
         }
       }
     }
@@ -270,7 +274,7 @@ extern "C" size_t cf_dtab_fp_bytes(int bbits) {
 extern "C" int cf_dtab_build(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count, void* tab,
                              int bbits, u32* err, void* stream) {
   if (!pool_dev || !tail || !tab || !err || n < 1 || n > CF_MAX_POOL || r < 1 || r > CF_MAX_DISPATCH_R ||
-      bbits < 1 || bbits > 30) {
+      bbits < 1 || bbits > 28) {
     cf_set_error("cf_dtab_build: bad arguments%s", "");
     return CF_EBADARG;
   }
@@ -294,7 +298,7 @@ extern "C" int cf_fused_probe(const void* pool_dev, const void* tail, int n, int
                               const void* tab, int bbits, u64 d_rank0, void* pairs, u32 max_pairs, u32* npairs,
                               u32* err, u32 grid, void* stream) {
   if (!pool_dev || !tail || !tab || !npairs || !err || (max_pairs && !pairs) || n < 1 || n > CF_MAX_POOL ||
-      r < 1 || r > CF_MAX_DISPATCH_R || bbits < 1 || bbits > 30) {
+      r < 1 || r > CF_MAX_DISPATCH_R || bbits < 1 || bbits > 28) {
     cf_set_error("cf_fused_probe: bad arguments%s", "");
     return CF_EBADARG;
   }
