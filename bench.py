@@ -35,6 +35,7 @@ UNIT = "records/s"
 WORKLOAD = "k64_r5_single_modulus"
 SEED_POOL = 64          # candidate seeds for the step sequence
 BYTES_PER_RECORD = 32   # algorithmic: one 16-B {key,id} write + one 16-B read per record entering the join
+L2_RANDOM_SECTOR_READS = 2.0e11   # random 32-byte loads/s from an L2-resident table (cf_micro_l2_probe on B200)
 
 
 def parse_args():
@@ -309,14 +310,19 @@ def run_ours(args):
         peak, peak_src = 6650.0, "fallback"
     t_path = kt["gen_D"] + kt["gen_I"] + kt["join"] + kt["probe"]
     achieved = BYTES_PER_RECORD * recs / t_path / 1e9 if t_path > 0 else None
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tfile):
-        try:
-            tj = json.load(open(tfile))
-            traffic = tj["bytes_per_record"] * recs / len(timed)     # per step (one launch sequence)
-        except Exception:
-            traffic = None
+    traffic = None     # DRAM bytes per step of the join-path kernels, scaled from the committed ncu capture
+    tfile = os.path.join(ROOT, "profiles", "k_fused_k64_r5_seed0.md")
+    if args.strategy == "fused" and os.path.exists(tfile):
+        per = {}
+        for line in open(tfile):
+            if line.startswith("- traffic_bytes_per_"):
+                k, v = line[2:].split(":")
+                per[k.split()[0]] = float(v)
+        if "traffic_bytes_per_I_record" in per:
+            n_i_all = sum(math.comb(len(w.INS), w.r) for w in timed)
+            n_d_all = sum(math.comb(len(w.B0), w.r) for w in timed)
+            traffic = (per["traffic_bytes_per_I_record"] * n_i_all
+                       + per.get("traffic_bytes_per_D_record", 0.0) * n_d_all) / len(timed)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -352,6 +358,11 @@ def run_ours(args):
                          "peak_source": peak_src},
             "strategy": solver.tuning.strategy,
             "kernels": kern,
+            "l2_probe": ({"achieved_probes_per_s": sum(math.comb(len(w.INS), w.r) for w in timed) / kt["probe"],
+                          "ceiling_probes_per_s": L2_RANDOM_SECTOR_READS,
+                          "frac": sum(math.comb(len(w.INS), w.r) for w in timed) / kt["probe"] / L2_RANDOM_SECTOR_READS,
+                          "note": "one 32-byte L2 sector read per I record; ceiling = random 32-B loads/s measured on this B200"}
+                         if kt["probe"] > 0 else None),
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // max(1, len(timed)),
                     "d2h_bytes_per_step": d2h // max(1, len(timed)), "api": "carmichael_frontier_b200.solve"},

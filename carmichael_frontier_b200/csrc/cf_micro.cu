@@ -1,0 +1,60 @@
+// cf_micro.cu -- microbenchmarks that measure the ceilings the kernels are judged
+// against on the running GPU:
+//   cf_micro_l2_probe : random 32-byte reads from a table (L2-resident when it is
+//                       small): the ceiling of the fused probe, which reads one
+//                       32-byte fingerprint sector per record.
+//   cf_micro_mulhi    : 64-bit Montgomery products (two mul.hi.u64 and two
+//                       mul.lo.u64 each) per second, eight independent chains per
+//                       thread: the integer ceiling of residue generation.
+#include "cf_abi_internal.h"
+
+namespace {
+
+__global__ void __launch_bounds__(512)
+k_micro_l2(const uint4* __restrict__ tab, u64 mask, int iters, u64* __restrict__ sink) {
+  u64 x = (u64)(blockIdx.x * 512 + threadIdx.x) * 0x9E3779B97F4A7C15ull + 12345;
+  u32 acc = 0;
+  for (int i = 0; i < iters; ++i) {
+    x = x * 6364136223846793005ull + 1442695040888963407ull;
+    const u64 b = (x >> 20) & mask;
+    const uint4 v = __ldg(tab + b * 2), w = __ldg(tab + b * 2 + 1);
+    acc ^= v.x ^ w.w;
+  }
+  if (acc == 0x9E3779B9u) sink[0] = acc;      // keeps the loads live
+}
+
+__global__ void __launch_bounds__(256)
+k_micro_mul(int iters, u64 m, u64 minv, u64* __restrict__ sink) {
+  // eight independent chains per thread so that the pipe, not latency, is measured
+  u64 a[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = (u64)(blockIdx.x * 256 + threadIdx.x) * 0x9E3779B97F4A7C15ull + j;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = cf_redc_mul(a[j] & (m - 1), a[(j + 1) & 7] & (m - 1), m, minv);
+  }
+  u64 s = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s ^= a[j];
+  if (s == 0x1234) sink[0] = s;
+}
+
+}  // namespace
+
+extern "C" int cf_micro_l2_probe(const void* table, u64 bucket_mask, int iters, u32 blocks, u64* sink,
+                                 void* stream) {
+  if (!table || !sink || iters < 1 || blocks < 1) { cf_set_error("cf_micro_l2_probe: bad arguments%s", ""); return CF_EBADARG; }
+  k_micro_l2<<<blocks, 512, 0, (cudaStream_t)stream>>>((const uint4*)table, bucket_mask, iters, sink);
+  CF_LAUNCH_CHECK("cf_micro_l2_probe");
+  return CF_OK;
+}
+
+extern "C" int cf_micro_mulhi(int iters, u32 blocks, u64* sink, void* stream) {
+  if (!sink || iters < 1 || blocks < 1) { cf_set_error("cf_micro_mulhi: bad arguments%s", ""); return CF_EBADARG; }
+  const u64 m = (1ull << 61) - 1;               // odd modulus below 2^62
+  u64 minv = m;
+  for (int i = 0; i < 6; ++i) minv *= 2 - m * minv;
+  k_micro_mul<<<blocks, 256, 0, (cudaStream_t)stream>>>(iters, m, minv, sink);
+  CF_LAUNCH_CHECK("cf_micro_mulhi");
+  return CF_OK;
+}

@@ -1,0 +1,62 @@
+"""Measured ceilings on the running GPU (random L2 sector reads, 64-bit Montgomery products).
+
+    python -m carmichael_frontier_b200.micro
+prints one JSON line; bench.py quotes the L2 figure as the fused probe's ceiling.
+"""
+from __future__ import annotations
+
+import json
+
+from . import _lib
+
+
+def l2_random_reads(table_mb: int = 32, iters: int = 2048, reps: int = 3) -> float:
+    """Random 32-byte reads per second from a table of `table_mb` MiB."""
+    import torch
+    lib = _lib.load()
+    nb = (table_mb << 20) // 32
+    nb = 1 << (nb.bit_length() - 1)
+    tab = torch.randint(0, 1 << 30, (nb * 8,), dtype=torch.int32, device="cuda")
+    sink = torch.zeros(2, dtype=torch.int64, device="cuda")
+    blocks = torch.cuda.get_device_properties(0).multi_processor_count * 4
+    sh = torch.cuda.current_stream().cuda_stream
+    _lib.check(lib.cf_micro_l2_probe(tab.data_ptr(), nb - 1, 64, blocks, sink.data_ptr(), sh), "l2 probe")
+    best = 0.0
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.check(lib.cf_micro_l2_probe(tab.data_ptr(), nb - 1, iters, blocks, sink.data_ptr(), sh), "l2 probe")
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, blocks * 512 * iters / (e0.elapsed_time(e1) * 1e-3))
+    return best
+
+
+def montgomery_products(iters: int = 4096, reps: int = 3) -> float:
+    """64-bit Montgomery products per second."""
+    import torch
+    lib = _lib.load()
+    sink = torch.zeros(2, dtype=torch.int64, device="cuda")
+    blocks = torch.cuda.get_device_properties(0).multi_processor_count * 8
+    sh = torch.cuda.current_stream().cuda_stream
+    _lib.check(lib.cf_micro_mulhi(16, blocks, sink.data_ptr(), sh), "mulhi")
+    best = 0.0
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.check(lib.cf_micro_mulhi(iters, blocks, sink.data_ptr(), sh), "mulhi")
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, blocks * 256 * iters * 8 / (e0.elapsed_time(e1) * 1e-3))
+    return best
+
+
+def main() -> None:
+    out = {"l2_random_32B_reads_per_s": {mb: l2_random_reads(mb) for mb in (8, 32, 64)},
+           "hbm_random_32B_reads_per_s": l2_random_reads(4096, iters=256),
+           "montgomery64_products_per_s": montgomery_products()}
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()
