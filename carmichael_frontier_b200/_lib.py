@@ -67,10 +67,17 @@ SIGNATURES = [
     ("cf_join_part", C.c_int, [vp, vp, u32, vp, vp, u32, C.c_int, C.c_int, u32, u32, vp, u32, vp, vp, vp]),
     ("cf_dtab_bytes", sz, [C.c_int]),
     ("cf_dtab_fp_bytes", sz, [C.c_int]),
+    ("cf_dtab_bytes2", sz, [C.c_int, C.c_int]),
+    ("cf_dtab_build2", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, C.c_int, vp, vp]),
+    ("cf_fused_probe2", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, C.c_int, u64, vp, u32, vp, vp,
+                                  u32, vp]),
     ("cf_dtab_build", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, vp, vp]),
     ("cf_fused_probe", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, u64, vp, u32, vp, vp, u32, vp]),
     ("cf_pair_result_bytes", sz, []),
     ("cf_check_pairs", C.c_int, [vp, vp, vp, C.c_int, vp, vp, u32, vp, vp, vp]),
+    ("cf_batch_mod_bytes", sz, []),
+    ("cf_batch_max_r", C.c_int, []),
+    ("cf_batch_run", C.c_int, [C.c_int, vp, vp, u32, u32, vp, vp, vp, u32, vp, vp, vp, u32, vp]),
     ("cf_sort_tmp_bytes", sz, [u64]),
     ("cf_sort_pairs", C.c_int, [vp, vp, u64, C.c_int, vp, sz, vp]),
     ("cf_sort_pairs_noalloc_max", u64, []),

@@ -1,0 +1,168 @@
+// cf_dtab.cuh -- the D table of the fused join (shared by the single-modulus
+// kernels in cf_fused.cu and the batched portfolio kernels in cf_batch.cu).
+//
+// 2^bbits buckets of 16 slots.  A bucket's sixteen 16-bit fingerprints (0 =
+// empty) fill one 32-byte sector -- the only data a probe reads; a side array
+// holds, per slot, a second 32-bit fingerprint and the D rank (read only when
+// the 16-bit fingerprint matches); a fill counter per bucket hands out slots in
+// order, so "bucket full" is a test of the last slot, and a full bucket
+// continues into the next one.  An optional blocked Bloom filter is a first
+// level for tables too large for L2.
+#pragma once
+#include "cf_abi_internal.h"
+#include "cf_enum.cuh"
+
+constexpr size_t kBinomSmemMaxF = 24 * 1024;
+
+
+// Bucket and fingerprints of a residue, from its canonical odd part X (< m) and
+// 2-adic part x2 (< 2^a, a <= 32): the pair is the residue, so equal residues
+// give equal bucket and fingerprints.  The bucket and the 16-bit fingerprint
+// are the top bbits and the next 16 bits of one 64-bit multiplicative hash;
+// the 32-bit side fingerprint is an independent 32-bit fold of the residue.
+struct CfFuseKey {
+  u32 bucket, f16, f32;
+};
+__device__ __forceinline__ CfFuseKey cf_fuse_key(u64 X, u32 x2, int bbits) {
+  const u64 h = (X ^ ((u64)x2 << 32)) * CF_HASH_MULT;
+  CfFuseKey k;
+  k.bucket = (u32)(h >> (64 - bbits));
+  const u32 f = (u32)(h >> (48 - bbits)) & 0xffffu;
+  k.f16 = f ? f : 1u;                       // 0 marks an empty slot
+  k.f32 = (u32)X ^ ((u32)(X >> 32) * 0x85EBCA6Bu) ^ (x2 * 0xC2B2AE35u);
+  return k;
+}
+
+// Canonical odd part and 2-adic part of prefix product q times tail entry e.
+__device__ __forceinline__ void cf_fuse_res(CfElt32 q, const CfTailEnt& e, const CfMod32& md, u64 minv, u64& X,
+                                            u32& x2) {
+  X = cf_redc_mul(q.X, e.X, md.m, minv);            // q.X < 2m, e.X < m: canonical in [0, m)
+  x2 = ((u32)q.x2 * e.x2) & (u32)md.mask2;          // a <= 32 on this path
+}
+
+// D table: fp16[nb*16] (32 bytes per bucket), then side[nb*16] = {fp32, rank},
+// then the per-bucket fill counters used while building.
+struct DTab {
+  u32* fpw;       // fingerprint words: [nb * 8], two 16-bit fingerprints each
+  uint2* side;    // [nb * 16]: .x = 32-bit fingerprint, .y = D rank - rank0
+  u32* fill;      // [nb]: slots claimed so far (build only)
+  u32* bloom;     // optional first level: [2^fbits * 8] words (256-bit blocks), nullptr if off
+  u64 nb;         // buckets (power of two)
+  u64 rank0;      // first D rank of the build
+  int bbits;
+  int fbits;
+};
+
+// Blocked Bloom filter over the residues, for D tables too large for L2: a
+// 256-bit block (one 32-byte sector) per key, three bits set in it; a probe
+// that misses a bit skips the DRAM-resident table.  The block and bit indices
+// come from a second 64-bit hash, independent of the table's.
+struct CfBloomKey {
+  u32 block, w0, w1, w2, m0, m1, m2;
+};
+__device__ __forceinline__ CfBloomKey cf_bloom_key(u64 X, u32 x2, int fbits) {
+  const u64 g = (X * 0xC2B2AE3D27D4EB4Full) ^ ((u64)x2 * 0x165667B19E3779F9ull);
+  const u64 h = (g ^ (g >> 29)) * 0xD6E8FEB86659FD93ull;
+  CfBloomKey k;
+  k.block = (u32)(h >> (64 - fbits));
+  const u32 b0 = (u32)(h >> 8) & 255u, b1 = (u32)(h >> 16) & 255u, b2 = (u32)(h >> 24) & 255u;
+  k.w0 = b0 >> 5; k.m0 = 1u << (b0 & 31);
+  k.w1 = b1 >> 5; k.m1 = 1u << (b1 & 31);
+  k.w2 = b2 >> 5; k.m2 = 1u << (b2 & 31);
+  return k;
+}
+
+__device__ __forceinline__ u32 cf_word8(uint4 a, uint4 b, u32 w) {
+  const u32 v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  u32 r = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) r = (w == (u32)i) ? v[i] : r;
+  return r;
+}
+
+// Insert a residue (X, x2) with its rank; returns false if every bucket was full.
+// A slot is claimed with one atomicAdd on the bucket's fill counter; the claimed
+// 16-bit half is then set with atomicOr (its word is shared with a neighbour slot).
+__device__ __forceinline__ bool dtab_insert(const DTab& t, u64 X, u32 x2, u64 rank) {
+  if (t.bloom) {
+    const CfBloomKey bk = cf_bloom_key(X, x2, t.fbits);
+    u32* blk = t.bloom + (u64)bk.block * 8;
+    atomicOr(blk + bk.w0, bk.m0);
+    atomicOr(blk + bk.w1, bk.m1);
+    atomicOr(blk + bk.w2, bk.m2);
+  }
+  const CfFuseKey fk = cf_fuse_key(X, x2, t.bbits);
+  const u32 f16 = fk.f16, f32 = fk.f32;
+  u64 b = fk.bucket;
+  for (u64 tries = 0; tries < t.nb; ++tries) {
+    const u32 s = atomicAdd(&t.fill[b], 1u);
+    if (s < 16u) {
+      uint2 sd;
+      sd.x = f32;
+      sd.y = (u32)(rank - t.rank0);
+      t.side[b * 16 + s] = sd;
+      atomicOr(&t.fpw[b * 8 + (s >> 1)], f16 << (16 * (s & 1)));
+      return true;
+    }
+    b = (b + 1) & (t.nb - 1);
+  }
+  return false;
+}
+
+// Pair sink: candidates go to pairs[k] through the counter *npairs; in batched
+// runs the modulus index goes to mods[k] as well (mods == nullptr otherwise).
+struct CfPairSink {
+  CfPair* pairs;
+  u32* mods;
+  u32* npairs;
+  u32* err;
+  u32 max_pairs;
+  u32 mod;
+};
+
+__device__ __forceinline__ void emit_pair(u64 d, u64 i, const CfPairSink& o) {
+  const u32 k = atomicAdd(o.npairs, 1u);
+  if (k < o.max_pairs) {
+    CfPair pr;
+    pr.d_id = d;
+    pr.i_id = i;
+    o.pairs[k] = pr;
+    if (o.mods) o.mods[k] = o.mod;
+  } else {
+    atomicOr(o.err, CF_ERR_PAIR_OVERFLOW);
+  }
+}
+
+// Cold path: emit the matches of bucket b and continue through full buckets.
+static __device__ __noinline__ void probe_slow(const DTab& t, u64 b, u32 f16, u32 f32, u64 irank,
+                                               const CfPairSink& o) {
+  for (u64 tries = 0; tries < t.nb; ++tries) {
+    const u32* row = t.fpw + b * 8;
+    bool full = true;
+    for (int s = 0; s < 16; ++s) {
+      const u32 v = (row[s >> 1] >> (16 * (s & 1))) & 0xffffu;
+      full &= (v != 0u);
+      if (v == f16) {
+        const uint2 sd = t.side[b * 16 + s];
+        if (sd.x == f32) emit_pair(t.rank0 + sd.y, irank, o);
+      }
+    }
+    if (!full) return;
+    b = (b + 1) & (t.nb - 1);
+  }
+}
+
+// Nonzero iff some 16-bit half of w is zero (SWAR test; exact, no false positives).
+__device__ __forceinline__ u32 cf_zero_half(u32 w) { return (w - 0x00010001u) & ~w & 0x80008000u; }
+
+// Fast test of one bucket: any 16-bit fingerprint equal to f16 (hit), or the
+// bucket is full.  Slots are claimed in order, so the bucket is full exactly
+// when its last slot (the high half of the last word) is occupied.
+__device__ __forceinline__ bool probe_fast(uint4 r0, uint4 r1, u32 f16) {
+  const u32 ff = f16 * 0x10001u;
+  const u32 eq = cf_zero_half(r0.x ^ ff) | cf_zero_half(r0.y ^ ff) | cf_zero_half(r0.z ^ ff) |
+                 cf_zero_half(r0.w ^ ff) | cf_zero_half(r1.x ^ ff) | cf_zero_half(r1.y ^ ff) |
+                 cf_zero_half(r1.z ^ ff) | cf_zero_half(r1.w ^ ff);
+  return (eq != 0u) | ((r1.w >> 16) != 0u);
+}
+

@@ -90,9 +90,10 @@ __device__ __forceinline__ u64 cf_colex_rank(const int (&idx)[R], const u64* __r
 // Fast: primes < 2^31, lazy 32-bit-radix Montgomery (cf_redc32); key = CRT pair.
 struct CfArithFast {
   CfMod32 md;
-  const u32* p;
+  const u32* p;            // primes as u32 (shared memory), or nullptr to read p64
+  const u64* p64 = nullptr; // primes of the pool table (global memory)
   typedef CfElt32 E;
-  __device__ __forceinline__ E mul(E a, int i) const { return cf_mul32(a, p[i], md); }
+  __device__ __forceinline__ E mul(E a, int i) const { return cf_mul32(a, p ? p[i] : (u32)p64[i], md); }
   __device__ __forceinline__ u64 key(E a) const { return cf_key32(a, md); }
 };
 // Wide: any prime below 2^64 (reduced mod M on the host), 64-bit Montgomery keys.

@@ -18,118 +18,12 @@
 // equal -- exactly the pair set of the reference's join_sorted
 // (gpu/mitm_gpu2.py:107-119) and mitm64.cpp's probe (src/mitm64.cpp:85-101),
 // with all duplicates.
-#include "cf_abi_internal.h"
-#include "cf_enum.cuh"
+#include "cf_dtab.cuh"
 
 namespace {
 
 constexpr int kFuseBlock = 256;
 constexpr int kFuseSteps = 64;            // 32 x 64 = 2048 consecutive records per warp range
-constexpr size_t kBinomSmemMaxF = 24 * 1024;
-
-// Bucket and fingerprints of a residue, from its canonical odd part X (< m) and
-// 2-adic part x2 (< 2^a, a <= 32): the pair is the residue, so equal residues
-// give equal bucket and fingerprints.  The bucket and the 16-bit fingerprint
-// are the top bbits and the next 16 bits of one 64-bit multiplicative hash;
-// the 32-bit side fingerprint is an independent 32-bit fold of the residue.
-struct CfFuseKey {
-  u32 bucket, f16, f32;
-};
-__device__ __forceinline__ CfFuseKey cf_fuse_key(u64 X, u32 x2, int bbits) {
-  const u64 h = (X ^ ((u64)x2 << 32)) * CF_HASH_MULT;
-  CfFuseKey k;
-  k.bucket = (u32)(h >> (64 - bbits));
-  const u32 f = (u32)(h >> (48 - bbits)) & 0xffffu;
-  k.f16 = f ? f : 1u;                       // 0 marks an empty slot
-  k.f32 = (u32)X ^ ((u32)(X >> 32) * 0x85EBCA6Bu) ^ (x2 * 0xC2B2AE35u);
-  return k;
-}
-
-// Canonical odd part and 2-adic part of prefix product q times tail entry e.
-__device__ __forceinline__ void cf_fuse_res(CfElt32 q, const CfTailEnt& e, const CfMod32& md, u64 minv, u64& X,
-                                            u32& x2) {
-  X = cf_redc_mul(q.X, e.X, md.m, minv);            // q.X < 2m, e.X < m: canonical in [0, m)
-  x2 = ((u32)q.x2 * e.x2) & (u32)md.mask2;          // a <= 32 on this path
-}
-
-// D table: fp16[nb*16] (32 bytes per bucket), then side[nb*16] = {fp32, rank},
-// then the per-bucket fill counters used while building.
-struct DTab {
-  u32* fpw;       // fingerprint words: [nb * 8], two 16-bit fingerprints each
-  uint2* side;    // [nb * 16]: .x = 32-bit fingerprint, .y = D rank - rank0
-  u32* fill;      // [nb]: slots claimed so far (build only)
-  u64 nb;         // buckets (power of two)
-  u64 rank0;      // first D rank of the build
-  int bbits;
-};
-
-// Insert a residue (X, x2) with its rank; returns false if every bucket was full.
-// A slot is claimed with one atomicAdd on the bucket's fill counter; the claimed
-// 16-bit half is then set with atomicOr (its word is shared with a neighbour slot).
-__device__ __forceinline__ bool dtab_insert(const DTab& t, u64 X, u32 x2, u64 rank) {
-  const CfFuseKey fk = cf_fuse_key(X, x2, t.bbits);
-  const u32 f16 = fk.f16, f32 = fk.f32;
-  u64 b = fk.bucket;
-  for (u64 tries = 0; tries < t.nb; ++tries) {
-    const u32 s = atomicAdd(&t.fill[b], 1u);
-    if (s < 16u) {
-      uint2 sd;
-      sd.x = f32;
-      sd.y = (u32)(rank - t.rank0);
-      t.side[b * 16 + s] = sd;
-      atomicOr(&t.fpw[b * 8 + (s >> 1)], f16 << (16 * (s & 1)));
-      return true;
-    }
-    b = (b + 1) & (t.nb - 1);
-  }
-  return false;
-}
-
-__device__ __forceinline__ void emit_pair(u64 d, u64 i, CfPair* __restrict__ pairs, u32 max_pairs,
-                                          u32* __restrict__ npairs, u32* __restrict__ err) {
-  const u32 k = atomicAdd(npairs, 1u);
-  if (k < max_pairs) {
-    CfPair pr;
-    pr.d_id = d;
-    pr.i_id = i;
-    pairs[k] = pr;
-  } else {
-    atomicOr(err, CF_ERR_PAIR_OVERFLOW);
-  }
-}
-
-// Cold path: emit the matches of bucket b and continue through full buckets.
-__device__ __noinline__ void probe_slow(const DTab& t, u64 b, u32 f16, u32 f32, u64 irank, CfPair* __restrict__ pairs,
-                                        u32 max_pairs, u32* __restrict__ npairs, u32* __restrict__ err) {
-  for (u64 tries = 0; tries < t.nb; ++tries) {
-    const u32* row = t.fpw + b * 8;
-    bool full = true;
-    for (int s = 0; s < 16; ++s) {
-      const u32 v = (row[s >> 1] >> (16 * (s & 1))) & 0xffffu;
-      full &= (v != 0u);
-      if (v == f16) {
-        const uint2 sd = t.side[b * 16 + s];
-        if (sd.x == f32) emit_pair(t.rank0 + sd.y, irank, pairs, max_pairs, npairs, err);
-      }
-    }
-    if (!full) return;
-    b = (b + 1) & (t.nb - 1);
-  }
-}
-
-// Nonzero iff some 16-bit half of w is zero (SWAR test; exact, no false positives).
-__device__ __forceinline__ u32 cf_zero_half(u32 w) { return (w - 0x00010001u) & ~w & 0x80008000u; }
-
-// Fast test of one bucket: any 16-bit fingerprint equal to f16 (hit), or the
-// bucket is full.  Slots are claimed in order, so the bucket is full exactly
-// when its last slot (the high half of the last word) is occupied.
-__device__ __forceinline__ bool probe_fast(uint4 r0, uint4 r1, u32 f16) {
-  const u32 ff = f16 * 0x10001u;
-  const u32 eq = cf_zero_half(r0.x ^ ff) | cf_zero_half(r0.y ^ ff) | cf_zero_half(r0.z ^ ff) |
-                 cf_zero_half(r0.w ^ ff) | cf_zero_half(r1.x ^ ff) | cf_zero_half(r1.y ^ ff) |
-                 cf_zero_half(r1.z ^ ff) | cf_zero_half(r1.w ^ ff);
-  return (eq != 0u) | ((r1.w >> 16) != 0u);
-}
 
 struct FuseSmem {
   size_t p32, binom, total;
@@ -164,7 +58,7 @@ __device__ __forceinline__ const u64* fuse_setup(const u64* __restrict__ pool, u
 
 // MODE 0: insert every record of [lo, lo+count) into the D table.
 // MODE 1: probe every record of [lo, lo+count) against the D table.
-template <int R, int MODE>
+template <int R, int MODE, bool BLOOM>
 __global__ void __launch_bounds__(kFuseBlock)
 k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo, u64 count, DTab tab,
         CfPair* __restrict__ pairs, u32 max_pairs, u32* __restrict__ npairs, u32* __restrict__ err, u32 steps) {
@@ -187,6 +81,13 @@ k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo
   st.x2 = hd->x20;
   __syncthreads();
   const int lane = threadIdx.x & 31;
+  CfPairSink sink;
+  sink.pairs = pairs;
+  sink.mods = nullptr;
+  sink.npairs = npairs;
+  sink.err = err;
+  sink.max_pairs = max_pairs;
+  sink.mod = 0;
   const u64 per_warp = 32ull * steps;
   const u64 nwarps = (u64)gridDim.x * (kFuseBlock / 32);
   bool bad = false;
@@ -208,10 +109,18 @@ k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo
         if (MODE == 0) {
           bad |= !dtab_insert(tab, X, x2, rank_base + off);
         } else {
+          if (BLOOM) {
+            const CfBloomKey bk = cf_bloom_key(X, x2, tab.fbits);
+            const uint4* blk = (const uint4*)(tab.bloom + (u64)bk.block * 8);
+            const uint4 a = __ldg(blk), c = __ldg(blk + 1);
+            const bool in = (cf_word8(a, c, bk.w0) & bk.m0) && (cf_word8(a, c, bk.w1) & bk.m1) &&
+                            (cf_word8(a, c, bk.w2) & bk.m2);
+            if (!in) continue;
+          }
           const CfFuseKey fk = cf_fuse_key(X, x2, tab.bbits);
           const uint4* row = (const uint4*)(tab.fpw + (u64)fk.bucket * 8);
           if (probe_fast(__ldg(row), __ldg(row + 1), fk.f16))
-            probe_slow(tab, fk.bucket, fk.f16, fk.f32, rank_base + off, pairs, max_pairs, npairs, err);
+            probe_slow(tab, fk.bucket, fk.f16, fk.f32, rank_base + off, sink);
         }
       }
     }
@@ -223,7 +132,7 @@ template <int R, int MODE>
 int launch_fused(const u64* pool, const CfTailEnt* tail, int n, u64 lo, u64 count, const DTab& tab, CfPair* pairs,
                  u32 max_pairs, u32* npairs, u32* err, u32 grid, cudaStream_t st) {
   const size_t smem = fuse_layout(n, R).total;
-  auto kern = k_fused<R, MODE>;
+  auto kern = (MODE == 1 && tab.bloom) ? k_fused<R, MODE, true> : k_fused<R, MODE, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cf_cuda_status(e, "cf_fused: smem attribute");
   const u32 steps = MODE == 0 ? 8u : (u32)kFuseSteps;      // the build is atomic-latency-bound: more warps
@@ -243,12 +152,14 @@ void dispatch_fused(int mode, const u64* pool, const CfTailEnt* tail, int n, u64
                   : launch_fused<R, 1>(pool, tail, n, lo, count, tab, pairs, max_pairs, npairs, err, grid, st);
 }
 
-DTab make_tab(void* tab, int bbits, u64 rank0) {
+DTab make_tab(void* tab, int bbits, int fbits, u64 rank0) {
   DTab t;
   t.nb = 1ull << bbits;
   t.fpw = (u32*)tab;
   t.side = (uint2*)((unsigned char*)tab + t.nb * 32);
   t.fill = (u32*)((unsigned char*)tab + t.nb * 160);
+  t.fbits = fbits;
+  t.bloom = fbits ? (u32*)((unsigned char*)tab + t.nb * 164) : nullptr;
   t.rank0 = rank0;
   t.bbits = bbits;
   return t;
@@ -257,11 +168,14 @@ DTab make_tab(void* tab, int bbits, u64 rank0) {
 }  // namespace
 
 // Bytes of a D table with 2^bbits buckets (32 bytes of 16-bit fingerprints, 128
-// bytes of side data and a 4-byte fill counter each).
-extern "C" size_t cf_dtab_bytes(int bbits) {
-  if (bbits < 1 || bbits > 30) return 0;
-  return ((size_t)1 << bbits) * 164;
+// bytes of side data and a 4-byte fill counter each) and, when fbits > 0, a
+// Bloom filter of 2^fbits 32-byte blocks after it.
+extern "C" size_t cf_dtab_bytes2(int bbits, int fbits) {
+  if (bbits < 1 || bbits > 28 || fbits < 0 || fbits > 26) return 0;
+  return ((size_t)1 << bbits) * 164 + (fbits ? ((size_t)1 << fbits) * 32 : 0);
 }
+
+extern "C" size_t cf_dtab_bytes(int bbits) { return cf_dtab_bytes2(bbits, 0); }
 
 extern "C" size_t cf_dtab_fp_bytes(int bbits) {
   if (bbits < 1 || bbits > 30) return 0;
@@ -269,10 +183,11 @@ extern "C" size_t cf_dtab_fp_bytes(int bbits) {
 }
 
 // Build: insert the D-side records of ranks [lo, lo+count), count < 2^32.  The
-// caller zeroes the fingerprint array (the first cf_dtab_fp_bytes(bbits) bytes)
-// and the fill counters (the last 4 * 2^bbits bytes) first.
-extern "C" int cf_dtab_build(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count, void* tab,
-                             int bbits, u32* err, void* stream) {
+// caller zeroes the fingerprint array (the first cf_dtab_fp_bytes(bbits) bytes),
+// the fill counters (4 * 2^bbits bytes from offset 160 * 2^bbits) and the Bloom
+// filter (when fbits > 0) first.
+extern "C" int cf_dtab_build2(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count, void* tab,
+                              int bbits, int fbits, u32* err, void* stream) {
   if (!pool_dev || !tail || !tab || !err || n < 1 || n > CF_MAX_POOL || r < 1 || r > CF_MAX_DISPATCH_R ||
       bbits < 1 || bbits > 28) {
     cf_set_error("cf_dtab_build: bad arguments%s", "");
@@ -280,7 +195,8 @@ extern "C" int cf_dtab_build(const void* pool_dev, const void* tail, int n, int 
   }
   if (count == 0) return CF_OK;
   if (count >= (1ull << 32)) { cf_set_error("cf_dtab_build: at most 2^32-1 D records per table%s", ""); return CF_EBADARG; }
-  const DTab t = make_tab(tab, bbits, lo);
+  if (fbits < 0 || fbits > 26) { cf_set_error("cf_dtab_build: fbits must be 0..26%s", ""); return CF_EBADARG; }
+  const DTab t = make_tab(tab, bbits, fbits, lo);
   int rc = CF_OK;
   CF_DISPATCH_R(r, dispatch_fused, 0, (const u64*)pool_dev, (const CfTailEnt*)tail, n, lo, count, t, nullptr, 0u,
                 nullptr, err, 0u, (cudaStream_t)stream, &rc);
@@ -289,25 +205,38 @@ extern "C" int cf_dtab_build(const void* pool_dev, const void* tail, int n, int 
   return CF_OK;
 }
 
+extern "C" int cf_dtab_build(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count, void* tab,
+                             int bbits, u32* err, void* stream) {
+  return cf_dtab_build2(pool_dev, tail, n, r, lo, count, tab, bbits, 0, err, stream);
+}
+
 // Probe: generate the I-side records of ranks [lo, lo+count) in registers and
 // append every (D rank, I rank) candidate whose 32-bit fingerprints agree
 // through *npairs (zeroed by the caller); cf_check_pairs then keeps the pairs
 // whose residues are equal.  d_rank0: first D rank of the table's build.
 // grid: CTAs (0 = one per 4096 records).
-extern "C" int cf_fused_probe(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count,
-                              const void* tab, int bbits, u64 d_rank0, void* pairs, u32 max_pairs, u32* npairs,
-                              u32* err, u32 grid, void* stream) {
+extern "C" int cf_fused_probe2(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count,
+                               const void* tab, int bbits, int fbits, u64 d_rank0, void* pairs, u32 max_pairs,
+                               u32* npairs, u32* err, u32 grid, void* stream) {
   if (!pool_dev || !tail || !tab || !npairs || !err || (max_pairs && !pairs) || n < 1 || n > CF_MAX_POOL ||
       r < 1 || r > CF_MAX_DISPATCH_R || bbits < 1 || bbits > 28) {
     cf_set_error("cf_fused_probe: bad arguments%s", "");
     return CF_EBADARG;
   }
   if (count == 0) return CF_OK;
-  const DTab t = make_tab((void*)tab, bbits, d_rank0);
+  if (fbits < 0 || fbits > 26) { cf_set_error("cf_fused_probe: fbits must be 0..26%s", ""); return CF_EBADARG; }
+  const DTab t = make_tab((void*)tab, bbits, fbits, d_rank0);
   int rc = CF_OK;
   CF_DISPATCH_R(r, dispatch_fused, 1, (const u64*)pool_dev, (const CfTailEnt*)tail, n, lo, count, t,
                 (CfPair*)pairs, max_pairs, npairs, err, grid, (cudaStream_t)stream, &rc);
   if (rc != CF_OK) return rc;
   CF_LAUNCH_CHECK("cf_fused_probe");
   return CF_OK;
+}
+
+extern "C" int cf_fused_probe(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count,
+                              const void* tab, int bbits, u64 d_rank0, void* pairs, u32 max_pairs, u32* npairs,
+                              u32* err, u32 grid, void* stream) {
+  return cf_fused_probe2(pool_dev, tail, n, r, lo, count, tab, bbits, 0, d_rank0, pairs, max_pairs, npairs, err,
+                         grid, stream);
 }

@@ -1,0 +1,434 @@
+"""Batched portfolio: many moduli (uneven pool sizes, mixed radii) in persistent kernels.
+
+The reference solves one instance at a time: ``run_instance``
+(gpu/mitm_gpu_mstar_driver.py:184-286) generates, sorts and joins each side with
+the CuPy kernels of gpu/mitm_gpu2.py and is called per instance from the driver
+loop (:311).  Here a whole portfolio is split into batches whose D tables fit a
+memory budget, and each batch is four device operations on one stream:
+
+  zero   the fingerprint arrays, fill counters and Bloom filters of the batch
+  k_batch<0>     every modulus's D table      (persistent, device work queue)
+  k_batch<1>     every modulus's I window     (persistent, device work queue)
+  k_batch_check  every candidate pair, any radius
+
+followed by one synchronisation and host certification of the hits.  Tickets of
+the work queue are ordered by modulus, so the table being probed stays in L2
+while a modulus is worked on, and small moduli cost no launch of their own.
+The per-batch sequence is fixed, so ``run(..., graphs=True)`` captures it once
+per batch in a CUDA graph and replays it.
+
+Two per-modulus forms are kept for comparison:
+  run_plain        the reference's form on this GPU: mitm_gpu2 generate ->
+                   sort_side -> join_sorted per modulus (one modulus per launch
+                   sequence), host exact check of the pairs
+  run_per_modulus  this library's single-modulus fused solve, one modulus at a time
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .certify import verify_certificate
+from .solve import (RESULT_DTYPE, Hit, Instance, SolveResult, Solver, Tuning, dtab_shape, finish_rows)
+from .tables import ncomb, pool_table_host, screen_table_host
+
+MOD_DTYPE = np.dtype([
+    ("poolD", "<u8"), ("tailD", "<u8"), ("poolI", "<u8"), ("tailI", "<u8"), ("screen", "<u8"),
+    ("fpw", "<u8"), ("side", "<u8"), ("fill", "<u8"), ("bloom", "<u8"),
+    ("nD", "<u8"), ("i_lo", "<u8"), ("nI", "<u8"),
+    ("bbits", "<i4"), ("fbits", "<i4"), ("r", "<i4"), ("pad", "<i4")])
+
+_ALIGN = 256
+
+
+def _up(x: int, a: int = _ALIGN) -> int:
+    return (x + a - 1) // a * a
+
+
+@dataclass
+class BatchTuning:
+    """Launch shape of the batched kernels (chosen by autotune.tune_batch when tuned)."""
+    ticket: int = 8192                 # records per work-queue ticket (multiple of 32)
+    grid: int = 0                      # persistent CTAs per launch (0 = one resident wave)
+    mem_budget: int = 24 << 30         # D-table bytes of one batch
+    pair_capacity: int = 1 << 16       # initial candidate buffer (grown on overflow)
+    dtab: Tuning = field(default_factory=Tuning)   # D-table sizing (dtab_load, Bloom level)
+
+
+@dataclass
+class _Batch:
+    idx: list                          # portfolio positions of the moduli in this batch
+    mods: object = None                # device CfBatchMod[nmod]
+    tsD: object = None                 # device u64[nmod+1] ticket prefix sums, D sides
+    tsI: object = None                 # device u64[nmod+1] ticket prefix sums, I windows
+    zero_bytes: int = 0                # arena bytes zeroed before the build
+    arena_bytes: int = 0
+    records: int = 0
+    graph: object = None
+
+
+@dataclass
+class PreparedPortfolio:
+    instances: list
+    i_limit: int | None
+    nD: list
+    nI: list
+    shapes: list                       # (bbits, fbits) per modulus, None when not batched
+    batches: list
+    fallback: list                     # portfolio positions solved one at a time (r > max or nD >= 2^32)
+    trivial: dict                      # position -> SolveResult (r = 0 or an empty side)
+    tables: object = None              # device blob of pool and screen tables (kept alive)
+    tails: object = None               # device blob of tail tables (kept alive)
+    pairs_cap: int = 0
+
+    @property
+    def records(self) -> int:
+        return sum(self.nD[k] + self.nI[k] for k in range(len(self.instances)))
+
+
+class BatchSolver:
+    """Solves portfolios of moduli on one device and stream with the batched kernels."""
+
+    def __init__(self, device=None, stream=None, tuning: BatchTuning | None = None):
+        import torch
+        self.torch = torch
+        self.lib = _lib.load()
+        self.device = torch.device(device if device is not None else "cuda")
+        if self.device.type != "cuda":
+            raise RuntimeError("the batched join runs on a CUDA device only")
+        self.stream = stream
+        self.tuning = tuning or BatchTuning()
+        if self.tuning.ticket <= 0 or self.tuning.ticket % 32:
+            raise ValueError("ticket must be a positive multiple of 32")
+        assert self.lib.cf_batch_mod_bytes() == MOD_DTYPE.itemsize
+        self.max_r = self.lib.cf_batch_max_r()
+        self.result_bytes = self.lib.cf_pair_result_bytes()
+        self._bufs: dict = {}
+        self._single: Solver | None = None
+
+    # -- buffers -------------------------------------------------------------
+    def _buf(self, name: str, nbytes: int):
+        t = self._bufs.get(name)
+        if t is None or t.numel() < nbytes:
+            self._drop_graphs()
+            t = self.torch.empty(max(nbytes, 16), dtype=self.torch.uint8, device=self.device)
+            self._bufs[name] = t
+        return t
+
+    def _drop_graphs(self):
+        for prep in getattr(self, "_live", []):
+            for b in prep.batches:
+                b.graph = None
+
+    def _sh(self):
+        return _lib.stream_handle(self.stream)
+
+    def _torch_stream(self):
+        return self.stream if self.stream is not None else self.torch.cuda.current_stream(self.device)
+
+    # -- preparation ---------------------------------------------------------
+    def prepare(self, instances: list, i_limit: int | None = None) -> PreparedPortfolio:
+        """Host tables of every modulus, one upload, device tail tables, batch split."""
+        torch, lib = self.torch, self.lib
+        tu = self.tuning
+        insts = [w if isinstance(w, Instance) else Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in instances]
+        N = len(insts)
+        nD = [ncomb(len(x.B0), x.r) if x.r else 1 for x in insts]
+        nI = [ncomb(len(x.INS), x.r) if x.r else 1 for x in insts]
+        if i_limit is not None:
+            nI = [min(v, int(i_limit)) for v in nI]
+        shapes: list = [None] * N
+        trivial: dict = {}
+        fallback: list = []
+        batched: list = []
+        for k, x in enumerate(insts):
+            if x.r == 0 or nD[k] == 0 or nI[k] == 0:
+                trivial[k] = None
+            elif x.r > self.max_r or nD[k] >= 1 << 32:
+                fallback.append(k)
+            else:
+                shapes[k] = dtab_shape(nD[k], tu.dtab)
+                batched.append(k)
+        # host tables packed into one blob (pools and screens), uploaded once
+        host_parts, offs, off = [], {}, 0
+        for k in batched:
+            x = insts[k]
+            multD = pow(x.P0, -1, x.M)
+            for tag, arr in (("pD", pool_table_host(x.B0, x.r, x.M, multD)),
+                             ("pI", pool_table_host(x.INS, x.r, x.M, 1)),
+                             ("sc", screen_table_host(x.P0, x.B, 1e-6))):
+                offs[(k, tag)] = off
+                host_parts.append((off, arr))
+                off = _up(off + arr.nbytes)
+        blob_host = np.zeros(max(off, 16), dtype=np.uint8)
+        for o, arr in host_parts:
+            blob_host[o:o + arr.nbytes] = arr.view(np.uint8)
+        blob = torch.from_numpy(blob_host).to(self.device)
+        base = blob.data_ptr()
+        # tail tables, built on the device from the uploaded pools
+        toffs, toff = {}, 0
+        for k in batched:
+            x = insts[k]
+            for tag, n in (("tD", len(x.B0)), ("tI", len(x.INS))):
+                toffs[(k, tag)] = toff
+                toff = _up(toff + lib.cf_tail_bytes(n, x.r))
+        tails = torch.empty(max(toff, 16), dtype=torch.uint8, device=self.device)
+        tbase = tails.data_ptr()
+        sh = self._sh()
+        for k in batched:
+            x = insts[k]
+            _lib.check(lib.cf_build_tail(base + offs[(k, "pD")], len(x.B0), x.r, tbase + toffs[(k, "tD")], sh),
+                       "cf_build_tail(D)")
+            _lib.check(lib.cf_build_tail(base + offs[(k, "pI")], len(x.INS), x.r, tbase + toffs[(k, "tI")], sh),
+                       "cf_build_tail(I)")
+        # batches: consecutive moduli whose D tables fit the budget
+        batches, cur, cur_bytes = [], [], 0
+        for k in batched:
+            bb, fb = shapes[k]
+            nbytes = _up(36 << bb) + (_up(32 << fb) if fb else 0) + _up(128 << bb)
+            if cur and cur_bytes + nbytes > tu.mem_budget:
+                batches.append(_Batch(cur))
+                cur, cur_bytes = [], 0
+            cur.append(k)
+            cur_bytes += nbytes
+        if cur:
+            batches.append(_Batch(cur))
+        # descriptors with arena offsets (arena pointers are filled in at run time)
+        for b in batches:
+            zoff, soff_rel = 0, 0
+            rows = np.zeros(len(b.idx), dtype=MOD_DTYPE)
+            zl, sl = [], []
+            for j, k in enumerate(b.idx):
+                x = insts[k]
+                bb, fb = shapes[k]
+                zl.append(zoff)
+                zoff += _up(36 << bb) + (_up(32 << fb) if fb else 0)
+                sl.append(soff_rel)
+                soff_rel += _up(128 << bb)
+                rows[j]["poolD"] = base + offs[(k, "pD")]
+                rows[j]["poolI"] = base + offs[(k, "pI")]
+                rows[j]["screen"] = base + offs[(k, "sc")]
+                rows[j]["tailD"] = tbase + toffs[(k, "tD")]
+                rows[j]["tailI"] = tbase + toffs[(k, "tI")]
+                rows[j]["nD"] = nD[k]
+                rows[j]["i_lo"] = 0
+                rows[j]["nI"] = nI[k]
+                rows[j]["bbits"], rows[j]["fbits"], rows[j]["r"] = bb, fb, x.r
+            b.zero_bytes = zoff
+            b.arena_bytes = zoff + soff_rel
+            b.records = sum(nD[k] + nI[k] for k in b.idx)
+            b._rows, b._zl, b._sl = rows, zl, sl
+            t = tu.ticket
+            tsD = np.zeros(len(b.idx) + 1, dtype=np.uint64)
+            tsI = np.zeros(len(b.idx) + 1, dtype=np.uint64)
+            tsD[1:] = np.cumsum([-(-nD[k] // t) for k in b.idx])
+            tsI[1:] = np.cumsum([-(-nI[k] // t) for k in b.idx])
+            b.tsD = torch.from_numpy(tsD.view(np.int64)).to(self.device)
+            b.tsI = torch.from_numpy(tsI.view(np.int64)).to(self.device)
+        prep = PreparedPortfolio(insts, i_limit, nD, nI, shapes, batches, fallback, trivial, blob, tails,
+                                 tu.pair_capacity)
+        self._place(prep)
+        self._live = getattr(self, "_live", []) + [prep]
+        return prep
+
+    def _place(self, prep: PreparedPortfolio):
+        """Point every batch's descriptors into the shared arena and upload them."""
+        torch = self.torch
+        if not prep.batches:
+            return
+        need = max(b.arena_bytes for b in prep.batches)
+        arena = self._buf("arena", need)
+        abase = arena.data_ptr()
+        for b in prep.batches:
+            rows = b._rows.copy()
+            for j, k in enumerate(b.idx):
+                bb, fb = prep.shapes[k]
+                z = abase + b._zl[j]
+                rows[j]["fpw"] = z
+                rows[j]["fill"] = z + (32 << bb)
+                rows[j]["bloom"] = z + _up(36 << bb) if fb else 0
+                rows[j]["side"] = abase + b.zero_bytes + b._sl[j]
+            b.mods = torch.from_numpy(rows.view(np.uint8).copy()).to(self.device)
+            b._arena_ptr = abase
+
+    # -- running -------------------------------------------------------------
+    def _enqueue(self, b: _Batch, maxp: int):
+        lib, dp, ck = self.lib, _lib.ptr, _lib.check
+        arena = self._bufs["arena"]
+        misc = self._buf("misc", 64)
+        pairs = self._buf("pairs", maxp * 16)
+        pmod = self._buf("pmod", maxp * 4)
+        res = self._buf("res", maxp * self.result_bytes)
+        sh = self._sh()
+        tu = self.tuning
+        arena[: b.zero_bytes].zero_()
+        misc[:32].zero_()
+        m = dp(misc)
+        nmod = len(b.idx)
+        ck(lib.cf_batch_run(0, dp(b.mods), dp(b.tsD), nmod, tu.ticket, m, dp(pairs), dp(pmod), maxp, m + 16, m + 20,
+                            None, tu.grid, sh), "cf_batch_run(build)")
+        ck(lib.cf_batch_run(1, dp(b.mods), dp(b.tsI), nmod, tu.ticket, m + 8, dp(pairs), dp(pmod), maxp, m + 16,
+                            m + 20, None, tu.grid, sh), "cf_batch_run(probe)")
+        ck(lib.cf_batch_run(2, dp(b.mods), None, nmod, 0, None, dp(pairs), dp(pmod), maxp, m + 16, m + 20, dp(res),
+                            0, sh), "cf_batch_run(check)")
+
+    def _launch(self, b: _Batch, maxp: int, graphs: bool):
+        torch = self.torch
+        if not graphs:
+            self._enqueue(b, maxp)
+            return
+        if b.graph is None or b._graph_maxp != maxp or b._arena_ptr != self._bufs["arena"].data_ptr():
+            for nm, nb in (("misc", 64), ("pairs", maxp * 16), ("pmod", maxp * 4), ("res", maxp * self.result_bytes)):
+                self._buf(nm, nb)            # allocate outside the capture
+            g = torch.cuda.CUDAGraph()
+            s = torch.cuda.Stream(self.device)
+            s.wait_stream(self._torch_stream())
+            with torch.cuda.stream(s):
+                prev, self.stream = self.stream, s
+                try:
+                    with torch.cuda.graph(g, stream=s):
+                        self._enqueue(b, maxp)
+                finally:
+                    self.stream = prev
+            self._torch_stream().wait_stream(s)
+            b.graph, b._graph_maxp = g, maxp
+        with torch.cuda.stream(self._torch_stream()):
+            b.graph.replay()
+
+    def run(self, prep: PreparedPortfolio, verify: bool = True, graphs: bool = False,
+            marks: list | None = None) -> list[SolveResult]:
+        """Every result of the portfolio, in input order."""
+        torch = self.torch
+        out: list = [None] * len(prep.instances)
+        for k in prep.trivial:
+            out[k] = self._trivial(prep, k, verify)
+        for b in prep.batches:
+            if b._arena_ptr != self._bufs["arena"].data_ptr():
+                self._place(prep)
+            for _attempt in range(8):
+                maxp = prep.pairs_cap
+                self._launch(b, maxp, graphs)
+                if marks is not None:
+                    ev = torch.cuda.Event(enable_timing=True)
+                    ev.record(self._torch_stream())
+                    marks.append(("batch", ev))
+                self._torch_stream().synchronize()
+                misc = self._bufs["misc"][:32].cpu().numpy().view(np.uint32)
+                npairs, err = int(misc[4]), int(misc[5])
+                if err & _lib.ERR_PAIR_OVERFLOW:
+                    prep.pairs_cap = 1 << max(npairs + 16, 2 * maxp).bit_length()
+                    continue
+                if err & _lib.ERR_TABLE_FULL:
+                    raise _lib.CfError(_lib.CF_EOVERFLOW, "batch", "D table full (internal error)")
+                if err:
+                    raise _lib.CfError(_lib.CF_EBADARG, "batch", f"a batched kernel rejected its work (err {err:#x})")
+                break
+            else:
+                raise _lib.CfError(_lib.CF_EOVERFLOW, "batch", "pair buffer kept overflowing")
+            rows = np.frombuffer(self._bufs["res"][: npairs * self.result_bytes].cpu().numpy().tobytes(),
+                                 dtype=RESULT_DTYPE)
+            mods = self._bufs["pmod"][: npairs * 4].cpu().numpy().view(np.uint32)
+            order = np.argsort(mods, kind="stable")
+            rows, mods = rows[order], mods[order]
+            cuts = np.searchsorted(mods, np.arange(len(b.idx) + 1))
+            for j, k in enumerate(b.idx):
+                bb, fb = prep.shapes[k]
+                plan = dict(strategy="fused", batched=True, bbits=bb, fbits=fb, i_limit=prep.i_limit)
+                out[k] = finish_rows(prep.instances[k], rows[cuts[j]:cuts[j + 1]], prep.nD[k], prep.nI[k], plan,
+                                     verify)
+        if prep.fallback:
+            if self._single is None:
+                self._single = Solver(self.device, self.stream, self.tuning.dtab)
+            for k in prep.fallback:
+                out[k] = self._single.solve_instance(prep.instances[k], verify=verify, i_limit=prep.i_limit)
+        return out
+
+    def _trivial(self, prep: PreparedPortfolio, k: int, verify: bool) -> SolveResult:
+        x = prep.instances[k]
+        if x.r == 0:
+            if self._single is None:
+                self._single = Solver(self.device, self.stream, self.tuning.dtab)
+            return self._single._solve_r0(x)
+        return SolveResult([], prep.nD[k], prep.nI[k], 0, 0, 0, 0)
+
+    def solve(self, instances: list, i_limit: int | None = None, verify: bool = True,
+              graphs: bool = False) -> list[SolveResult]:
+        return self.run(self.prepare(instances, i_limit), verify=verify, graphs=graphs)
+
+    def release(self, prep: PreparedPortfolio):
+        """Drop a prepared portfolio's graphs and device tables."""
+        for b in prep.batches:
+            b.graph = None
+            b.mods = b.tsD = b.tsI = None
+        prep.tables = prep.tails = None
+        live = getattr(self, "_live", [])
+        self._live = [p for p in live if p is not prep]
+
+
+# -- per-modulus forms, for comparison ------------------------------------------
+
+def run_per_modulus(instances: list, i_limit: int | None = None, verify: bool = True, device=None,
+                    solver: Solver | None = None) -> list[SolveResult]:
+    """This library's single-modulus fused solve, one modulus at a time."""
+    s = solver or Solver(device)
+    out = []
+    for w in instances:
+        x = w if isinstance(w, Instance) else Instance.build(w.M, w.Q, w.B0, w.r, w.B)
+        out.append(s.solve_instance(x, verify=verify, i_limit=i_limit))
+    return out
+
+
+def run_plain(instances: list, i_limit: int | None = None, verify: bool = True, chunk: int = 1 << 27,
+              device=None) -> list[SolveResult]:
+    """The reference's per-modulus GPU form: generate -> sort_side -> join_sorted on each side
+    (gpu/mitm_gpu2.py:79-119 as driven by gpu/mitm_gpu_mstar_driver.py:184-286), keys
+    prod(D) and P0 * prod(I) mod M, exact check of every pair on the host."""
+    from . import mitm_gpu2 as G
+    out = []
+    for w in instances:
+        x = w if isinstance(w, Instance) else Instance.build(w.M, w.Q, w.B0, w.r, w.B)
+        r, M = x.r, x.M
+        nD = ncomb(len(x.B0), r)
+        nI = ncomb(len(x.INS), r)
+        if i_limit is not None:
+            nI = min(nI, int(i_limit))
+        if r == 0 or nD == 0 or nI == 0:
+            out.append(SolveResult([], nD, nI, 0, 0, 0, 0))
+            continue
+        bits = max(6, (max(len(x.B0), len(x.INS)) - 1).bit_length())
+        Dk, Did = G.sort_side(*G.generate(x.B0, r, M, 1, bits, device=device))
+        pairs = []
+        for lo in range(0, nI, chunk):
+            hi = min(nI, lo + chunk)
+            Ik, Iid = G.sort_side(*G.generate(x.INS, r, M, x.P0 % M, bits, lo, hi, device=device))
+            d_ids, i_ids = G.join_sorted(Dk, Did, Ik, Iid)
+            if d_ids.numel():
+                pairs += list(zip(G.decode_ids(d_ids, r, bits), G.decode_ids(i_ids, r, bits)))
+            del Ik, Iid
+        hits, above, rejected, plist = [], 0, 0, []
+        for di, ii in pairs:
+            D = tuple(x.B0[i] for i in di)
+            I = tuple(x.INS[i] for i in ii)
+            plist.append((D, I))
+            dset = set(D)
+            fac = tuple(sorted([p for p in x.B0 if p not in dset] + list(I)))
+            n = math.prod(fac)
+            if n > x.B:
+                above += 1
+                continue
+            ok = (n - 1) % M == 0
+            if ok and verify:
+                ok, n2, _ = verify_certificate(fac)
+                ok = ok and n2 == n
+            if ok:
+                hits.append(Hit(D, I, n, fac))
+            else:
+                rejected += 1
+        hits.sort(key=lambda h: (h.n, h.D, h.I))
+        plist.sort()
+        out.append(SolveResult(hits, nD, nI, len(plist), len(plist) - above, above, rejected,
+                               plan=dict(strategy="plain"), pairs=plist))
+    return out

@@ -75,7 +75,29 @@ class Tuning:
     sigma: float = 6.0              # partition capacity = mean + sigma*sqrt(mean) + 16
     strategy: str = "fused"         # "fused": D table + generate-and-probe; "partition": materialised join
     dtab_load: float = 5.0          # fused: minimum average D records per 16-slot bucket (up to 2x this)
-    fused_grid: int = 0             # fused probe CTAs (0 = one per 4096 records)
+    fused_grid: int = 0             # fused probe CTAs (0 = one per 16384 records)
+    l2_table_bytes: int = 48 << 20  # fingerprint arrays above this get a Bloom-filter first level
+    max_fbits: int = 21             # Bloom filter at most 2^21 blocks of 32 bytes (64 MB)
+
+
+def dtab_shape(nD: int, tu: Tuning) -> tuple[int, int]:
+    """(bbits, fbits) of the D table for nD records: 2^bbits buckets of 16 slots at an
+    average load between dtab_load and 2*dtab_load (never above 12), and a Bloom-filter
+    first level (about 8 bits per D record, at most 2^max_fbits blocks of 32 bytes) when
+    the fingerprint array would not stay in L2."""
+    bbits = max(4, int(math.floor(math.log2(max(nD / tu.dtab_load, 2.0)))),
+                math.ceil(math.log2(max(nD / 12.0, 2.0))))
+    fbits = 0
+    if (1 << bbits) * 32 > tu.l2_table_bytes:
+        fbits = min(tu.max_fbits, max(4, math.ceil(math.log2(max(nD / 32.0, 2.0)))))
+    return bbits, fbits
+
+
+def _i_window(inst: "Instance", plan: dict) -> int:
+    """I ranks joined: [0, C(|INS|, r)) or its prefix [0, plan["i_limit"])."""
+    nI = ncomb(len(inst.INS), inst.r)
+    lim = plan.get("i_limit")
+    return nI if lim is None else min(nI, int(lim))
 
 
 def _pow2ceil(x: int) -> int:
@@ -123,6 +145,58 @@ class Instance:
         return Instance(M, base, ins, r, B, P0)
 
 
+def finish_rows(inst: Instance, res: np.ndarray, nD: int, nI: int, plan: dict, verify: bool) -> SolveResult:
+    """SolveResult of one modulus from its checked candidate rows (RESULT_DTYPE).
+
+    Rows without CF_HIT_KEY_EQUAL are fingerprint collisions of the fused join and
+    are dropped; for the partition join, which compares full keys, they count as
+    rejected.  Every hit is re-derived and, with verify, certified on the host."""
+    r = inst.r
+    hits, screened, above, rejected, pairs = [], 0, 0, 0, []
+    bset = inst.B0
+    fused = plan.get("strategy") == "fused"
+    nres = 0
+    for row in res:
+        f = int(row["flags"])
+        if not f & _lib.HIT_KEY_EQUAL:
+            if not fused:
+                rejected += 1
+            continue
+        nres += 1
+        di = [int(x) for x in row["d_idx"][:r]]
+        ii = [int(x) for x in row["i_idx"][:r]]
+        D = tuple(bset[i] for i in di)
+        I = tuple(inst.INS[i] for i in ii)
+        pairs.append((D, I))
+        if not f & _lib.HIT_SCREEN:
+            above += 1
+            continue
+        screened += 1
+        if not f & _lib.HIT_SIZE_EXACT:
+            above += 1
+            continue
+        if (f & ALL_FLAGS) != ALL_FLAGS:
+            rejected += 1
+            continue
+        dset = set(D)
+        fac = tuple(sorted([p for p in bset if p not in dset] + list(I)))
+        n = 1
+        for p in fac:
+            n *= p
+        ok = n <= inst.B and (n - 1) % inst.M == 0
+        if verify and ok:
+            ok, n2, _why = verify_certificate(fac)
+            ok = ok and n2 == n
+        if not ok:
+            rejected += 1
+            continue
+        hits.append(Hit(D, I, n, fac))
+    hits.sort(key=lambda x: (x.n, x.D, x.I))
+    pairs.sort()
+    return SolveResult(hits=hits, n_D=nD, n_I=nI, residue_pairs=nres, screened=screened,
+                       above_bound=above, rejected=rejected, plan=dict(plan), pairs=pairs)
+
+
 class Solver:
     """Reusable device state for repeated solves on one device and stream."""
 
@@ -166,12 +240,10 @@ class Solver:
         while sbits < tu.max_sbits and (1 << (sbits - 1)) < cD:
             sbits += 1
         isplit = tu.isplit or max(1, min(16, (2 * 148 * 2) // max(1, nparts)))
-        # 2^bbits buckets of 16 slots: average load between dtab_load and 2*dtab_load, never above 12
-        bbits = max(4, int(math.floor(math.log2(max(nD / tu.dtab_load, 2.0)))),
-                    math.ceil(math.log2(max(nD / 12.0, 2.0))))
+        bbits, fbits = dtab_shape(nD, tu)
         return dict(pbits=pbits, nparts=nparts, capD=max(cD, 1), capI=max(cI, 1), chunk=max(chunk, 1), sbits=sbits,
                     isplit=isplit, pairs=pairs or tu.pair_capacity, shape=tu.gen_shape, strategy=tu.strategy,
-                    bbits=bbits)
+                    bbits=bbits, fbits=fbits)
 
     # -- one solve -----------------------------------------------------------
     def _mark(self, marks, tag):
@@ -201,10 +273,11 @@ class Solver:
         """D table build, fused generate-and-probe of the I side, pair check."""
         torch, lib = self.torch, self.lib
         r = inst.r
-        nD, nIt = ncomb(len(inst.B0), r), ncomb(len(inst.INS), r)
+        nD, nIt = ncomb(len(inst.B0), r), _i_window(inst, plan)
         poolD, poolI, tailD, tailI, screen = self._tables_for(inst)
-        bbits = plan["bbits"]
-        tab = self._buf("dtab", lib.cf_dtab_bytes(bbits))
+        bbits, fbits = plan["bbits"], plan.get("fbits", 0)
+        tbytes = lib.cf_dtab_bytes2(bbits, fbits)
+        tab = self._buf("dtab", tbytes)
         ctr = self._buf("ctr", 64)
         misc = ctr[:64].view(torch.int32)
         maxp = plan["pairs"]
@@ -214,14 +287,15 @@ class Solver:
         dp = _lib.ptr
         ck = _lib.check
         misc.zero_()
-        tab[: lib.cf_dtab_fp_bytes(bbits)].zero_()
-        tab[lib.cf_dtab_bytes(bbits) - 4 * (1 << bbits): lib.cf_dtab_bytes(bbits)].zero_()
+        nb = 1 << bbits
+        tab[: 32 * nb].zero_()                     # fingerprint sectors
+        tab[160 * nb: tbytes].zero_()              # fill counters and Bloom filter
         self._mark(marks, "start")
-        ck(lib.cf_dtab_build(dp(poolD), dp(tailD), len(inst.B0), r, 0, nD, dp(tab), bbits, dp(misc) + 4, sh),
-           "cf_dtab_build")
+        ck(lib.cf_dtab_build2(dp(poolD), dp(tailD), len(inst.B0), r, 0, nD, dp(tab), bbits, fbits, dp(misc) + 4,
+                              sh), "cf_dtab_build")
         self._mark(marks, "gen_D")
-        ck(lib.cf_fused_probe(dp(poolI), dp(tailI), len(inst.INS), r, 0, nIt, dp(tab), bbits, 0, dp(pairs), maxp,
-                              dp(misc), dp(misc) + 4, self.tuning.fused_grid, sh), "cf_fused_probe")
+        ck(lib.cf_fused_probe2(dp(poolI), dp(tailI), len(inst.INS), r, 0, nIt, dp(tab), bbits, fbits, 0, dp(pairs),
+                               maxp, dp(misc), dp(misc) + 4, self.tuning.fused_grid, sh), "cf_fused_probe")
         self._mark(marks, "probe")
         ck(lib.cf_check_pairs(dp(poolD), dp(poolI), dp(screen), r, dp(pairs), dp(misc), maxp, dp(res),
                               dp(misc) + 4, sh), "cf_check_pairs")
@@ -232,7 +306,7 @@ class Solver:
         """Partitioned generation of both sides and the shared-memory partition join."""
         torch, lib = self.torch, self.lib
         r, M = inst.r, inst.M
-        nD, nIt = ncomb(len(inst.B0), r), ncomb(len(inst.INS), r)
+        nD, nIt = ncomb(len(inst.B0), r), _i_window(inst, plan)
         P = plan["nparts"]
         pbits, shape = plan["pbits"], plan["shape"]
         multD = pow(inst.P0, -1, M)
@@ -308,60 +382,21 @@ class Solver:
         return self._finish(inst, h, res, verify), None
 
     def _finish(self, inst: Instance, h: dict, res: np.ndarray, verify: bool) -> SolveResult:
-        r = inst.r
-        hits, screened, above, rejected, pairs = [], 0, 0, 0, []
-        bset = inst.B0
-        fused = h["plan"].get("strategy") == "fused"
-        nres = 0
-        for row in res:
-            f = int(row["flags"])
-            if not f & _lib.HIT_KEY_EQUAL:
-                if not fused:           # the partition join compares full keys: unequal residues are a bug
-                    rejected += 1
-                continue                # fused: a 32-bit fingerprint collision, not a pair
-            nres += 1
-            pairs.append((tuple(bset[int(x)] for x in row["d_idx"][:r]),
-                          tuple(inst.INS[int(x)] for x in row["i_idx"][:r])))
-            if not f & _lib.HIT_SCREEN:
-                above += 1
-                continue
-            screened += 1
-            if not f & _lib.HIT_SIZE_EXACT:
-                above += 1
-                continue
-            if (f & ALL_FLAGS) != ALL_FLAGS:
-                rejected += 1
-                continue
-            di = [int(x) for x in row["d_idx"][:r]]
-            ii = [int(x) for x in row["i_idx"][:r]]
-            D = tuple(bset[i] for i in di)
-            I = tuple(inst.INS[i] for i in ii)
-            dset = set(D)
-            fac = tuple(sorted([p for p in bset if p not in dset] + list(I)))
-            n = 1
-            for p in fac:
-                n *= p
-            ok = n <= inst.B and (n - 1) % inst.M == 0
-            if verify and ok:
-                ok, n2, _why = verify_certificate(fac)
-                ok = ok and n2 == n
-            if not ok:
-                rejected += 1
-                continue
-            hits.append(Hit(D, I, n, fac))
-        hits.sort(key=lambda x: (x.n, x.D, x.I))
-        pairs.sort()
-        return SolveResult(hits=hits, n_D=h["nD"], n_I=h["nI"], residue_pairs=nres, screened=screened,
-                           above_bound=above, rejected=rejected, plan=dict(h["plan"]), pairs=pairs)
+        return finish_rows(inst, res, h["nD"], h["nI"], h["plan"], verify)
 
     def solve_instance(self, inst: Instance, verify: bool = True, timed: bool = False,
-                       marks: list | None = None) -> SolveResult:
+                       marks: list | None = None, i_limit: int | None = None) -> SolveResult:
+        """Join one instance.  i_limit: join only the I ranks [0, i_limit) (a bounded
+        sample of the instance; every pair with such an I rank is found)."""
         if inst.r == 0:
             return self._solve_r0(inst)
         nD, nI = ncomb(len(inst.B0), inst.r), ncomb(len(inst.INS), inst.r)
+        if i_limit is not None:
+            nI = min(nI, int(i_limit))
         if nI == 0 or nD == 0:
             return SolveResult([], nD, nI, 0, 0, 0, 0)
         plan = self.plan(nD, nI)
+        plan["i_limit"] = i_limit
         if nD >= 1 << 32:                 # D ranks in the fused table are 32-bit
             plan["strategy"] = "partition"
         for _attempt in range(6):
@@ -383,6 +418,7 @@ class Solver:
                 return out
             plan = self.plan(nD, nI, newp["capD"], newp["capI"], newp["pairs"])
             plan["strategy"] = newp.get("strategy", plan["strategy"])
+            plan["i_limit"] = i_limit
         raise _lib.CfError(_lib.CF_EOVERFLOW, "solve", "capacities kept overflowing")
 
     def _torch_stream(self):

@@ -47,8 +47,20 @@ def test_bad_arguments_fail_loudly_without_gpu():
     assert b"table buffer too small" in lib.cf_last_error_string() or b"M < 2^62" in lib.cf_last_error_string()
     assert lib.cf_gen_subsets(None, 3, 2, 0, 1, 0, 8, 1, None, None, None) == _lib.CF_EBADARG
     assert lib.cf_join_part(None, None, 1, None, None, 1, 1, 2, 1, 0, None, 0, None, None, None) == _lib.CF_EBADARG
+    assert lib.cf_batch_run(0, None, None, 1, 64, None, None, None, 0, None, None, None, 0, None) == _lib.CF_EBADARG
     with pytest.raises(_lib.CfError):
         _lib.check(lib.cf_gen_subsets(None, 3, 2, 0, 1, 0, 8, 1, None, None, None), "probe")
+
+
+def test_batch_descriptor_layout():
+    from carmichael_frontier_b200.portfolio import MOD_DTYPE
+    lib = _lib.load()
+    assert lib.cf_batch_mod_bytes() == MOD_DTYPE.itemsize == 112
+    assert lib.cf_batch_max_r() == 8
+    # a ticket that is not a multiple of 32 is rejected before any device call
+    one = np.zeros(8, dtype=np.uint64)
+    assert lib.cf_batch_run(0, one.ctypes.data, one.ctypes.data, 1, 48, one.ctypes.data, None, None, 0,
+                            one.ctypes.data, one.ctypes.data, None, 0, None) == _lib.CF_EBADARG
 
 
 def _hostkey(M, v):

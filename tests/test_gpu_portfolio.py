@@ -1,0 +1,110 @@
+"""Batched portfolio: the persistent work-queue kernels against per-modulus solves,
+the reference's mitm64 pair sets and the exhaustive oracle."""
+import math
+import random
+
+import pytest
+
+import oracle as O
+from carmichael_frontier_b200 import Solver, workloads as W
+from carmichael_frontier_b200.portfolio import BatchSolver, BatchTuning, run_per_modulus, run_plain
+from carmichael_frontier_b200.solve import Instance
+
+pytestmark = pytest.mark.gpu
+
+
+def as_lists(pairs):
+    return sorted([list(D), list(I)] for D, I in pairs)
+
+
+def summary(res):
+    return (res.n_D, res.n_I, res.residue_pairs, res.above_bound, res.rejected, as_lists(res.pairs),
+            [(h.D, h.I, h.n) for h in res.hits])
+
+
+def small_portfolio(seed, count):
+    """Moduli with small pools, radii 1..4, bounds cutting the pair sets."""
+    rng = random.Random(seed)
+    out = []
+    for j in range(count):
+        M = W.draw_modulus(500 + 31 * seed + j)
+        Q = W.eligible_pool(M, 5518)
+        k = rng.randint(10, 22)
+        r = rng.randint(1, 4)
+        Qs = Q[: k + rng.randint(r, 40)]
+        B0 = Qs[:k]
+        B = W.product(B0) * 10 ** rng.randint(0, 14)
+        out.append(Instance.build(M, Qs, B0, r, B))
+    return out
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_batched_small_vs_exhaustive(cuda, seed):
+    insts = small_portfolio(seed, 24)
+    res = BatchSolver(cuda).solve(insts)
+    for x, got in zip(insts, res):
+        pairs, hits = O.solve_exhaustive(x.M, x.B0 + x.INS, x.B0, x.r, x.B)
+        assert as_lists(got.pairs) == as_lists(pairs)
+        assert [(h.D, h.I, h.n) for h in got.hits] == [(tuple(D), tuple(I), n) for D, I, n in hits]
+        assert got.rejected == 0
+
+
+def test_batched_config2_matches_reference_mitm64(cuda, golden):
+    # five full-size k=64 r=5 moduli in one batch: the reference's own pair sets
+    insts = [Instance.build(g["M"], g["Q"], g["B0"], g["r"], int(g["B"])) for g in golden["config2"]]
+    res = BatchSolver(cuda).solve(insts)
+    for g, got in zip(golden["config2"], res):
+        assert got.n_D == g["d_leaves"] and got.n_I == g["i_leaves"]
+        assert got.residue_pairs == g["matches"]
+        assert as_lists(got.pairs) == g["pairs"]
+        assert sorted([list(h.D), list(h.I), str(h.n)] for h in got.hits) == g["hits"]
+
+
+def test_batched_portfolio_sample_equals_per_modulus_and_plain(cuda):
+    # the first moduli of the seeded 1024-modulus portfolio (radii 4..6, pools 120..400),
+    # I side limited to a rank prefix; all three forms must agree exactly
+    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config3(12)]
+    lim = 1 << 20
+    got = BatchSolver(cuda).solve(insts, i_limit=lim)
+    one = run_per_modulus(insts, i_limit=lim, solver=Solver(cuda))
+    plain = run_plain(insts, i_limit=lim, device=cuda)
+    for a, b, c in zip(got, one, plain):
+        assert summary(a) == summary(b)
+        assert (a.residue_pairs, as_lists(a.pairs), [h.n for h in a.hits]) == \
+               (c.residue_pairs, as_lists(c.pairs), [h.n for h in c.hits])
+        assert a.above_bound == c.above_bound
+
+
+def test_batched_split_budget_graphs_and_overflow(cuda):
+    # many small batches (tiny budget), a pair buffer of 16 that must grow, CUDA-graph replay
+    M = 2 ** 5 * 3 ** 2 * 5 * 7 * 11 * 13          # tiny modulus: residues collide massively
+    Q = W.eligible_pool(M)
+    insts = [Instance.build(M, Q, Q[:20], 3, 1 << 2040)] + small_portfolio(7, 10)
+    ref = [summary(x) for x in BatchSolver(cuda).solve(insts)]
+    bs = BatchSolver(cuda, tuning=BatchTuning(mem_budget=4096, pair_capacity=16, ticket=64))
+    prep = bs.prepare(insts)
+    assert len(prep.batches) > 3
+    for graphs in (False, True, True):
+        assert [summary(x) for x in bs.run(prep, graphs=graphs)] == ref
+    pairs, _ = O.solve_exhaustive(M, Q, Q[:20], 3, 1 << 2040)
+    assert len(pairs) > 200 and as_lists(bs.run(prep)[0].pairs) == as_lists(pairs)
+
+
+def test_batched_edge_cases(cuda):
+    # r = 0, an empty I side, a radius above the batched kernels' maximum (solved one at a time)
+    M = 21621600
+    Q = W.eligible_pool(M)
+    B0 = Q[:29]
+    insts = [Instance.build(M, Q, B0, 0, 10 ** 200),
+             Instance.build(M, Q[:30], B0, 2, 10 ** 200),          # |INS| = 1 < r: no I records
+             Instance.build(M, Q[:40], Q[:12], 9, 1 << 2040),      # r = 9: per-modulus fallback
+             Instance.build(M, Q, B0, 2, W.product(B0) * 10 ** 8)]
+    bs = BatchSolver(cuda)
+    res = bs.solve(insts)
+    assert res[1].n_I == 0 and res[1].residue_pairs == 0
+    prep = bs.prepare(insts)
+    assert prep.fallback == [2]
+    one = run_per_modulus(insts, solver=Solver(cuda))
+    for a, b in zip(res, one):
+        assert summary(a) == summary(b)
+    assert len(res[3].hits) == 2

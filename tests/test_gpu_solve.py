@@ -94,3 +94,13 @@ def test_edge_cases(solver):
         solver.solve(w.M * 2 ** 40, w.Q, w.B0, 2, w.B)   # M >= 2^62
     with pytest.raises(ValueError):
         solver.solve(w.M, w.Q + (13,), w.B0, 2, w.B)   # 13 divides M
+
+
+@pytest.mark.parametrize("idx", [1, 4])
+def test_config2_with_bloom_first_level(cuda, golden, idx):
+    # force the Bloom-filter first level (normally only for D tables larger than L2)
+    g = golden["config2"][idx]
+    s = Solver(cuda, tuning=Tuning(strategy="fused", l2_table_bytes=0, max_fbits=18))
+    res = s.solve(g["M"], g["Q"], g["B0"], g["r"], int(g["B"]))
+    assert res.plan["fbits"] > 0
+    assert as_lists(res.pairs) == g["pairs"]
