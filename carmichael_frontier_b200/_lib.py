@@ -69,8 +69,8 @@ SIGNATURES = [
     ("cf_dtab_fp_bytes", sz, [C.c_int]),
     ("cf_dtab_bytes2", sz, [C.c_int, C.c_int]),
     ("cf_dtab_build2", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, C.c_int, vp, vp]),
-    ("cf_fused_probe2", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, C.c_int, u64, vp, u32, vp, vp,
-                                  u32, vp]),
+    ("cf_fused_probe2", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, C.c_int, u64, C.c_int, vp, u32,
+                                  vp, vp, u32, vp]),
     ("cf_dtab_build", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, vp, vp]),
     ("cf_fused_probe", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, u64, vp, u32, vp, vp, u32, vp]),
     ("cf_pair_result_bytes", sz, []),

@@ -26,7 +26,8 @@ constexpr int kBatchMaxR = 8;
 
 // One modulus of a batch.  fpw/fill/bloom are zeroed by the caller before the
 // build; side needs no initialisation.  D ranks are [0, nD); I ranks
-// [i_lo, i_lo + nI).
+// [i_lo, i_lo + nI).  swap = 0: the table holds the D side and the I window
+// probes; swap = 1: the table holds the I window and the D side probes.
 struct CfBatchMod {
   const u64* poolD;
   const CfTailEnt* tailD;
@@ -39,15 +40,16 @@ struct CfBatchMod {
   u32* bloom;        // 2^fbits blocks of 32 B, or null
   u64 nD, i_lo, nI;
   int bbits, fbits;
-  int r, pad;
+  int r, swap;
 };
 
 template <int R, int MODE>
 __device__ __forceinline__ bool batch_ticket(const CfBatchMod& md, u32 mod, u64 first, u32 left, int lane,
                                              const CfPairSink& sink0) {
   constexpr int B = R < 2 ? R : 2;
-  const u64* pool = MODE == 0 ? md.poolD : md.poolI;
-  const CfTailEnt* tail = MODE == 0 ? md.tailD : md.tailI;
+  const bool d_side = (MODE == 0) == (md.swap == 0);     // this ticket walks the D side
+  const u64* pool = d_side ? md.poolD : md.poolI;
+  const CfTailEnt* tail = d_side ? md.tailD : md.tailI;
   const CfPoolHdr* hd = (const CfPoolHdr*)pool;
   if (!hd->fast32 || hd->tail_b != (u64)B) return false;
   const int n = (int)hd->n;
@@ -66,11 +68,12 @@ __device__ __forceinline__ bool batch_ticket(const CfBatchMod& md, u32 mod, u64 
   tab.side = md.side;
   tab.fill = md.fill;
   tab.bloom = md.bloom;
-  tab.rank0 = 0;
+  tab.rank0 = md.swap ? md.i_lo : 0;
   tab.bbits = md.bbits;
   tab.fbits = md.fbits;
   CfPairSink sink = sink0;
   sink.mod = mod;
+  sink.swap = (u32)md.swap;
   CfTailWalker<R, B> w;
   w.init(first, n, binom, ar, st, hd->tail_n);
   const u64 rank_base = first + (u64)lane;
@@ -119,6 +122,7 @@ k_batch(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart /*[n
   sink.err = err;
   sink.max_pairs = max_pairs;
   sink.mod = 0;
+  sink.swap = 0;
   bool ok = true, badarg = false;
   for (;;) {
     u64 t = 0;
@@ -131,11 +135,12 @@ k_batch(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart /*[n
       if (tstart[mid] <= t) lo = mid; else hi = mid;
     }
     const CfBatchMod& md = mods[lo];
-    const u64 n_side = MODE == 0 ? md.nD : md.nI;
+    const bool d_side = (MODE == 0) == (md.swap == 0);
+    const u64 n_side = d_side ? md.nD : md.nI;
     const u64 first = (t - tstart[lo]) * (u64)ticket;
     if (first >= n_side) continue;
     const u32 left = (u32)((n_side - first) < ticket ? (n_side - first) : ticket);
-    const u64 rank0 = first + (MODE == 0 ? 0 : md.i_lo);
+    const u64 rank0 = first + (d_side ? 0 : md.i_lo);
     bool good;
     switch (md.r) {
       case 1: good = batch_ticket<1, MODE>(md, lo, rank0, left, lane, sink); break;
@@ -180,11 +185,12 @@ k_batch_check(const CfBatchMod* __restrict__ mods, const CfPair* __restrict__ pa
 extern "C" size_t cf_batch_mod_bytes(void) { return sizeof(CfBatchMod); }
 extern "C" int cf_batch_max_r(void) { return kBatchMaxR; }
 
-// mode 0: build the D tables of every modulus; mode 1: probe every I window;
-// mode 2: check every candidate pair.
+// mode 0: build the table of every modulus (from its smaller side); mode 1:
+// probe it with the other side; mode 2: check every candidate pair.
 //   mods    device array of nmod CfBatchMod descriptors (radius 1..8 each)
 //   tstart  device array of nmod+1 ticket prefix sums: tstart[m+1]-tstart[m] =
-//           ceil(nD/ticket) for mode 0, ceil(nI/ticket) for mode 1
+//           ceil(records of the table's side / ticket) for mode 0, of the
+//           probing side for mode 1
 //   ticket  records per ticket, a multiple of 32 (modes 0 and 1)
 //   queue   device u64, zeroed before each of modes 0 and 1
 //   pairs, pmod  candidate (D rank, I rank) pairs and their modulus indices,

@@ -41,14 +41,15 @@ __device__ __forceinline__ void cf_fuse_res(CfElt32 q, const CfTailEnt& e, const
 }
 
 // D table: fp16[nb*16] (32 bytes per bucket), then side[nb*16] = {fp32, rank},
-// then the per-bucket fill counters used while building.
+// then the per-bucket fill counters used while building.  "D table" names the
+// structure; it holds whichever side of the join is smaller.
 struct DTab {
   u32* fpw;       // fingerprint words: [nb * 8], two 16-bit fingerprints each
-  uint2* side;    // [nb * 16]: .x = 32-bit fingerprint, .y = D rank - rank0
+  uint2* side;    // [nb * 16]: .x = 32-bit fingerprint, .y = rank - rank0
   u32* fill;      // [nb]: slots claimed so far (build only)
   u32* bloom;     // optional first level: [2^fbits * 8] words (256-bit blocks), nullptr if off
   u64 nb;         // buckets (power of two)
-  u64 rank0;      // first D rank of the build
+  u64 rank0;      // first rank of the build
   int bbits;
   int fbits;
 };
@@ -111,6 +112,8 @@ __device__ __forceinline__ bool dtab_insert(const DTab& t, u64 X, u32 x2, u64 ra
 
 // Pair sink: candidates go to pairs[k] through the counter *npairs; in batched
 // runs the modulus index goes to mods[k] as well (mods == nullptr otherwise).
+// The table holds the smaller side: the D side (swap = 0) or the I side (swap =
+// 1, the D side probes); pairs are always stored as {D rank, I rank}.
 struct CfPairSink {
   CfPair* pairs;
   u32* mods;
@@ -118,14 +121,15 @@ struct CfPairSink {
   u32* err;
   u32 max_pairs;
   u32 mod;
+  u32 swap;
 };
 
-__device__ __forceinline__ void emit_pair(u64 d, u64 i, const CfPairSink& o) {
+__device__ __forceinline__ void emit_pair(u64 stored, u64 probing, const CfPairSink& o) {
   const u32 k = atomicAdd(o.npairs, 1u);
   if (k < o.max_pairs) {
     CfPair pr;
-    pr.d_id = d;
-    pr.i_id = i;
+    pr.d_id = o.swap ? probing : stored;
+    pr.i_id = o.swap ? stored : probing;
     o.pairs[k] = pr;
     if (o.mods) o.mods[k] = o.mod;
   } else {

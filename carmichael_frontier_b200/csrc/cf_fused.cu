@@ -61,7 +61,8 @@ __device__ __forceinline__ const u64* fuse_setup(const u64* __restrict__ pool, u
 template <int R, int MODE, bool BLOOM>
 __global__ void __launch_bounds__(kFuseBlock)
 k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo, u64 count, DTab tab,
-        CfPair* __restrict__ pairs, u32 max_pairs, u32* __restrict__ npairs, u32* __restrict__ err, u32 steps) {
+        CfPair* __restrict__ pairs, u32 max_pairs, u32* __restrict__ npairs, u32* __restrict__ err, u32 steps,
+        u32 swap) {
   constexpr int B = R < 2 ? R : 2;
   extern __shared__ __align__(16) unsigned char smem[];
   const CfPoolHdr* hd = (const CfPoolHdr*)pool;
@@ -88,6 +89,7 @@ k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo
   sink.err = err;
   sink.max_pairs = max_pairs;
   sink.mod = 0;
+  sink.swap = swap;
   const u64 per_warp = 32ull * steps;
   const u64 nwarps = (u64)gridDim.x * (kFuseBlock / 32);
   bool bad = false;
@@ -130,7 +132,7 @@ k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo
 
 template <int R, int MODE>
 int launch_fused(const u64* pool, const CfTailEnt* tail, int n, u64 lo, u64 count, const DTab& tab, CfPair* pairs,
-                 u32 max_pairs, u32* npairs, u32* err, u32 grid, cudaStream_t st) {
+                 u32 max_pairs, u32* npairs, u32* err, u32 grid, u32 swap, cudaStream_t st) {
   const size_t smem = fuse_layout(n, R).total;
   auto kern = (MODE == 1 && tab.bloom) ? k_fused<R, MODE, true> : k_fused<R, MODE, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -141,15 +143,17 @@ int launch_fused(const u64* pool, const CfTailEnt* tail, int n, u64 lo, u64 coun
   if (grid && g > grid) g = grid;
   if (g == 0) g = 1;
   if (g > 0x7fffffffull) g = 0x7fffffffull;
-  kern<<<(unsigned)g, kFuseBlock, smem, st>>>(pool, tail, lo, count, tab, pairs, max_pairs, npairs, err, steps);
+  kern<<<(unsigned)g, kFuseBlock, smem, st>>>(pool, tail, lo, count, tab, pairs, max_pairs, npairs, err, steps,
+                                              swap);
   return CF_OK;
 }
 
 template <int R>
 void dispatch_fused(int mode, const u64* pool, const CfTailEnt* tail, int n, u64 lo, u64 count, const DTab& tab,
-                    CfPair* pairs, u32 max_pairs, u32* npairs, u32* err, u32 grid, cudaStream_t st, int* rc) {
-  *rc = mode == 0 ? launch_fused<R, 0>(pool, tail, n, lo, count, tab, pairs, max_pairs, npairs, err, grid, st)
-                  : launch_fused<R, 1>(pool, tail, n, lo, count, tab, pairs, max_pairs, npairs, err, grid, st);
+                    CfPair* pairs, u32 max_pairs, u32* npairs, u32* err, u32 grid, u32 swap, cudaStream_t st,
+                    int* rc) {
+  *rc = mode == 0 ? launch_fused<R, 0>(pool, tail, n, lo, count, tab, pairs, max_pairs, npairs, err, grid, 0, st)
+                  : launch_fused<R, 1>(pool, tail, n, lo, count, tab, pairs, max_pairs, npairs, err, grid, swap, st);
 }
 
 DTab make_tab(void* tab, int bbits, int fbits, u64 rank0) {
@@ -199,7 +203,7 @@ extern "C" int cf_dtab_build2(const void* pool_dev, const void* tail, int n, int
   const DTab t = make_tab(tab, bbits, fbits, lo);
   int rc = CF_OK;
   CF_DISPATCH_R(r, dispatch_fused, 0, (const u64*)pool_dev, (const CfTailEnt*)tail, n, lo, count, t, nullptr, 0u,
-                nullptr, err, 0u, (cudaStream_t)stream, &rc);
+                nullptr, err, 0u, 0u, (cudaStream_t)stream, &rc);
   if (rc != CF_OK) return rc;
   CF_LAUNCH_CHECK("cf_dtab_build");
   return CF_OK;
@@ -210,25 +214,27 @@ extern "C" int cf_dtab_build(const void* pool_dev, const void* tail, int n, int 
   return cf_dtab_build2(pool_dev, tail, n, r, lo, count, tab, bbits, 0, err, stream);
 }
 
-// Probe: generate the I-side records of ranks [lo, lo+count) in registers and
-// append every (D rank, I rank) candidate whose 32-bit fingerprints agree
-// through *npairs (zeroed by the caller); cf_check_pairs then keeps the pairs
-// whose residues are equal.  d_rank0: first D rank of the table's build.
-// grid: CTAs (0 = one per 4096 records).
+// Probe: generate the records of ranks [lo, lo+count) of the probing side in
+// registers and append every candidate whose 32-bit fingerprints agree through
+// *npairs (zeroed by the caller); cf_check_pairs then keeps the pairs whose
+// residues are equal.  tab_rank0: first rank of the table's build.  swap = 0:
+// the table holds D records and the I side probes; swap = 1: the table holds I
+// records and the D side probes (build on the smaller side).  Pairs are stored
+// as {D rank, I rank} either way.  grid: CTAs (0 = one per 16384 records).
 extern "C" int cf_fused_probe2(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count,
-                               const void* tab, int bbits, int fbits, u64 d_rank0, void* pairs, u32 max_pairs,
-                               u32* npairs, u32* err, u32 grid, void* stream) {
+                               const void* tab, int bbits, int fbits, u64 tab_rank0, int swap, void* pairs,
+                               u32 max_pairs, u32* npairs, u32* err, u32 grid, void* stream) {
   if (!pool_dev || !tail || !tab || !npairs || !err || (max_pairs && !pairs) || n < 1 || n > CF_MAX_POOL ||
-      r < 1 || r > CF_MAX_DISPATCH_R || bbits < 1 || bbits > 28) {
+      r < 1 || r > CF_MAX_DISPATCH_R || bbits < 1 || bbits > 28 || (swap != 0 && swap != 1)) {
     cf_set_error("cf_fused_probe: bad arguments%s", "");
     return CF_EBADARG;
   }
   if (count == 0) return CF_OK;
   if (fbits < 0 || fbits > 26) { cf_set_error("cf_fused_probe: fbits must be 0..26%s", ""); return CF_EBADARG; }
-  const DTab t = make_tab((void*)tab, bbits, fbits, d_rank0);
+  const DTab t = make_tab((void*)tab, bbits, fbits, tab_rank0);
   int rc = CF_OK;
   CF_DISPATCH_R(r, dispatch_fused, 1, (const u64*)pool_dev, (const CfTailEnt*)tail, n, lo, count, t,
-                (CfPair*)pairs, max_pairs, npairs, err, grid, (cudaStream_t)stream, &rc);
+                (CfPair*)pairs, max_pairs, npairs, err, grid, (u32)swap, (cudaStream_t)stream, &rc);
   if (rc != CF_OK) return rc;
   CF_LAUNCH_CHECK("cf_fused_probe");
   return CF_OK;
@@ -237,6 +243,6 @@ extern "C" int cf_fused_probe2(const void* pool_dev, const void* tail, int n, in
 extern "C" int cf_fused_probe(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count,
                               const void* tab, int bbits, u64 d_rank0, void* pairs, u32 max_pairs, u32* npairs,
                               u32* err, u32 grid, void* stream) {
-  return cf_fused_probe2(pool_dev, tail, n, r, lo, count, tab, bbits, 0, d_rank0, pairs, max_pairs, npairs, err,
+  return cf_fused_probe2(pool_dev, tail, n, r, lo, count, tab, bbits, 0, d_rank0, 0, pairs, max_pairs, npairs, err,
                          grid, stream);
 }

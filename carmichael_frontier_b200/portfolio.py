@@ -3,12 +3,12 @@
 The reference solves one instance at a time: ``run_instance``
 (gpu/mitm_gpu_mstar_driver.py:184-286) generates, sorts and joins each side with
 the CuPy kernels of gpu/mitm_gpu2.py and is called per instance from the driver
-loop (:311).  Here a whole portfolio is split into batches whose D tables fit a
+loop (:311).  Here a whole portfolio is split into batches whose tables fit a
 memory budget, and each batch is four device operations on one stream:
 
   zero   the fingerprint arrays, fill counters and Bloom filters of the batch
-  k_batch<0>     every modulus's D table      (persistent, device work queue)
-  k_batch<1>     every modulus's I window     (persistent, device work queue)
+  k_batch<0>     every modulus's table from its smaller side   (persistent, device work queue)
+  k_batch<1>     probes of every table by the other side       (persistent, device work queue)
   k_batch_check  every candidate pair, any radius
 
 followed by one synchronisation and host certification of the hits.  Tickets of
@@ -39,7 +39,7 @@ MOD_DTYPE = np.dtype([
     ("poolD", "<u8"), ("tailD", "<u8"), ("poolI", "<u8"), ("tailI", "<u8"), ("screen", "<u8"),
     ("fpw", "<u8"), ("side", "<u8"), ("fill", "<u8"), ("bloom", "<u8"),
     ("nD", "<u8"), ("i_lo", "<u8"), ("nI", "<u8"),
-    ("bbits", "<i4"), ("fbits", "<i4"), ("r", "<i4"), ("pad", "<i4")])
+    ("bbits", "<i4"), ("fbits", "<i4"), ("r", "<i4"), ("swap", "<i4")])
 
 _ALIGN = 256
 
@@ -62,8 +62,8 @@ class BatchTuning:
 class _Batch:
     idx: list                          # portfolio positions of the moduli in this batch
     mods: object = None                # device CfBatchMod[nmod]
-    tsD: object = None                 # device u64[nmod+1] ticket prefix sums, D sides
-    tsI: object = None                 # device u64[nmod+1] ticket prefix sums, I windows
+    tsD: object = None                 # device u64[nmod+1] ticket prefix sums, table sides (build)
+    tsI: object = None                 # device u64[nmod+1] ticket prefix sums, probing sides
     zero_bytes: int = 0                # arena bytes zeroed before the build
     arena_bytes: int = 0
     records: int = 0
@@ -78,7 +78,7 @@ class PreparedPortfolio:
     nI: list
     shapes: list                       # (bbits, fbits) per modulus, None when not batched
     batches: list
-    fallback: list                     # portfolio positions solved one at a time (r > max or nD >= 2^32)
+    fallback: list                     # portfolio positions solved one at a time (r > max or both sides >= 2^32)
     trivial: dict                      # position -> SolveResult (r = 0 or an empty side)
     tables: object = None              # device blob of pool and screen tables (kept alive)
     tails: object = None               # device blob of tail tables (kept alive)
@@ -147,10 +147,10 @@ class BatchSolver:
         for k, x in enumerate(insts):
             if x.r == 0 or nD[k] == 0 or nI[k] == 0:
                 trivial[k] = None
-            elif x.r > self.max_r or nD[k] >= 1 << 32:
+            elif x.r > self.max_r or min(nD[k], nI[k]) >= 1 << 32:
                 fallback.append(k)
             else:
-                shapes[k] = dtab_shape(nD[k], tu.dtab)
+                shapes[k] = dtab_shape(min(nD[k], nI[k]), tu.dtab)     # the table holds the smaller side
                 batched.append(k)
         # host tables packed into one blob (pools and screens), uploaded once
         host_parts, offs, off = [], {}, 0
@@ -217,6 +217,7 @@ class BatchSolver:
                 rows[j]["i_lo"] = 0
                 rows[j]["nI"] = nI[k]
                 rows[j]["bbits"], rows[j]["fbits"], rows[j]["r"] = bb, fb, x.r
+                rows[j]["swap"] = int(nI[k] < nD[k])
             b.zero_bytes = zoff
             b.arena_bytes = zoff + soff_rel
             b.records = sum(nD[k] + nI[k] for k in b.idx)
@@ -224,8 +225,9 @@ class BatchSolver:
             t = tu.ticket
             tsD = np.zeros(len(b.idx) + 1, dtype=np.uint64)
             tsI = np.zeros(len(b.idx) + 1, dtype=np.uint64)
-            tsD[1:] = np.cumsum([-(-nD[k] // t) for k in b.idx])
-            tsI[1:] = np.cumsum([-(-nI[k] // t) for k in b.idx])
+            # mode 0 walks the table's (smaller) side, mode 1 the probing side
+            tsD[1:] = np.cumsum([-(-min(nD[k], nI[k]) // t) for k in b.idx])
+            tsI[1:] = np.cumsum([-(-max(nD[k], nI[k]) // t) for k in b.idx])
             b.tsD = torch.from_numpy(tsD.view(np.int64)).to(self.device)
             b.tsI = torch.from_numpy(tsI.view(np.int64)).to(self.device)
         prep = PreparedPortfolio(insts, i_limit, nD, nI, shapes, batches, fallback, trivial, blob, tails,

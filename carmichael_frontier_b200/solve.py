@@ -240,10 +240,10 @@ class Solver:
         while sbits < tu.max_sbits and (1 << (sbits - 1)) < cD:
             sbits += 1
         isplit = tu.isplit or max(1, min(16, (2 * 148 * 2) // max(1, nparts)))
-        bbits, fbits = dtab_shape(nD, tu)
+        bbits, fbits = dtab_shape(min(nD, nI), tu)     # the table holds the smaller side
         return dict(pbits=pbits, nparts=nparts, capD=max(cD, 1), capI=max(cI, 1), chunk=max(chunk, 1), sbits=sbits,
                     isplit=isplit, pairs=pairs or tu.pair_capacity, shape=tu.gen_shape, strategy=tu.strategy,
-                    bbits=bbits, fbits=fbits)
+                    bbits=bbits, fbits=fbits, swap=nI < nD)
 
     # -- one solve -----------------------------------------------------------
     def _mark(self, marks, tag):
@@ -290,11 +290,17 @@ class Solver:
         nb = 1 << bbits
         tab[: 32 * nb].zero_()                     # fingerprint sectors
         tab[160 * nb: tbytes].zero_()              # fill counters and Bloom filter
+        # build on the smaller side (swap: the table holds the I window and the D side probes)
+        swap = bool(plan.get("swap")) and nIt < nD
+        sideD = (dp(poolD), dp(tailD), len(inst.B0), nD)
+        sideI = (dp(poolI), dp(tailI), len(inst.INS), nIt)
+        bpool, btail, bn, bcount = sideI if swap else sideD
+        ppool, ptail, pn, pcount = sideD if swap else sideI
         self._mark(marks, "start")
-        ck(lib.cf_dtab_build2(dp(poolD), dp(tailD), len(inst.B0), r, 0, nD, dp(tab), bbits, fbits, dp(misc) + 4,
-                              sh), "cf_dtab_build")
+        ck(lib.cf_dtab_build2(bpool, btail, bn, r, 0, bcount, dp(tab), bbits, fbits, dp(misc) + 4, sh),
+           "cf_dtab_build")
         self._mark(marks, "gen_D")
-        ck(lib.cf_fused_probe2(dp(poolI), dp(tailI), len(inst.INS), r, 0, nIt, dp(tab), bbits, fbits, 0, dp(pairs),
+        ck(lib.cf_fused_probe2(ppool, ptail, pn, r, 0, pcount, dp(tab), bbits, fbits, 0, int(swap), dp(pairs),
                                maxp, dp(misc), dp(misc) + 4, self.tuning.fused_grid, sh), "cf_fused_probe")
         self._mark(marks, "probe")
         ck(lib.cf_check_pairs(dp(poolD), dp(poolI), dp(screen), r, dp(pairs), dp(misc), maxp, dp(res),
@@ -397,7 +403,7 @@ class Solver:
             return SolveResult([], nD, nI, 0, 0, 0, 0)
         plan = self.plan(nD, nI)
         plan["i_limit"] = i_limit
-        if nD >= 1 << 32:                 # D ranks in the fused table are 32-bit
+        if min(nD, nI) >= 1 << 32:        # ranks in the fused table are 32-bit
             plan["strategy"] = "partition"
         for _attempt in range(6):
             ev0 = ev1 = None

@@ -155,16 +155,20 @@ int cf_join_part(const void* D, const uint32_t* dcount, uint32_t capD, const voi
  * materialising the I side. */
 size_t cf_dtab_bytes(int bbits);
 size_t cf_dtab_fp_bytes(int bbits);
-/* Variants with an optional first level for D tables larger than L2: a blocked
- * Bloom filter of 2^fbits 32-byte blocks (3 bits per D record; fbits 0 = none)
+/* Variants with an optional first level for tables larger than L2: a blocked
+ * Bloom filter of 2^fbits 32-byte blocks (3 bits per record; fbits 0 = none)
  * placed after the table (cf_dtab_bytes2(bbits, fbits) bytes in all; the caller
- * zeroes the filter with the fingerprint array and fill counters). */
+ * zeroes the filter with the fingerprint array and fill counters), and the
+ * choice of the side the table holds: the table can be built from either
+ * side's pool (cf_dtab_build2 does not care); swap = 1 tells the probe that the
+ * table holds I records and the D side is probing, so that pairs are still
+ * stored as {D rank, I rank}.  A hash join builds on its smaller side. */
 size_t cf_dtab_bytes2(int bbits, int fbits);
 int cf_dtab_build2(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count, void* tab,
                    int bbits, int fbits, uint32_t* err, void* stream);
 int cf_fused_probe2(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count,
-                    const void* tab, int bbits, int fbits, uint64_t d_rank0, void* pairs, uint32_t max_pairs,
-                    uint32_t* npairs, uint32_t* err, uint32_t grid, void* stream);
+                    const void* tab, int bbits, int fbits, uint64_t tab_rank0, int swap, void* pairs,
+                    uint32_t max_pairs, uint32_t* npairs, uint32_t* err, uint32_t grid, void* stream);
 int cf_dtab_build(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count, void* tab,
                   int bbits, uint32_t* err, void* stream);
 int cf_fused_probe(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count,
@@ -186,12 +190,14 @@ int cf_check_pairs(const void* poolD, const void* poolI, const void* screen, int
  * mode 1 probes every modulus's I-rank window, mode 2 checks every candidate.
  * mods: device array of nmod descriptors of cf_batch_mod_bytes() bytes each
  *   {poolD, tailD, poolI, tailI, screen, fpw, side, fill, bloom (8-byte
- *    pointers); nD, i_lo, nI (u64); bbits, fbits, r, pad (i32)}
+ *    pointers); nD, i_lo, nI (u64); bbits, fbits, r, swap (i32)}
  * with the D-table areas laid out as cf_dtab_build2's (fingerprints 32 B, side
  * 128 B, fill 4 B per bucket; Bloom filter 32 B per block) but placed by the
- * caller; fpw, fill and bloom are zeroed before mode 0.  tstart: device
- * u64[nmod+1] prefix sums of ceil(side records / ticket) (D sides for mode 0,
- * I windows for mode 1); queue: device u64 zeroed before modes 0 and 1;
+ * caller; fpw, fill and bloom are zeroed before mode 0.  swap = 0: the table
+ * holds the D side and the I window probes; swap = 1: the table holds the I
+ * window and the D side probes.  tstart: device u64[nmod+1] prefix sums of
+ * ceil(side records / ticket) (the table's side for mode 0, the probing side
+ * for mode 1); queue: device u64 zeroed before modes 0 and 1;
  * candidates go to pairs/pmod (pair, modulus index) through *npairs, and mode 2
  * writes one result per pair as cf_check_pairs does.  The reference solves one
  * instance at a time (run_instance, gpu/mitm_gpu_mstar_driver.py:184-286,
