@@ -75,6 +75,14 @@ SIGNATURES = [
     ("cf_fused_probe", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, u64, vp, u32, vp, vp, u32, vp]),
     ("cf_pair_result_bytes", sz, []),
     ("cf_check_pairs", C.c_int, [vp, vp, vp, C.c_int, vp, vp, u32, vp, vp, vp]),
+    ("cf_scan_tmp_bytes", sz, [u64]),
+    ("cf_scan_u64", C.c_int, [vp, u64, vp, vp, sz, vp]),
+    ("cf_bgen_count", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, u64, vp, vp, vp, vp, C.c_int, C.c_int, C.c_int,
+                                C.c_int, vp, vp, vp]),
+    ("cf_bgen_expand", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, u64, vp, vp, vp, vp, vp, vp, vp, vp, C.c_int,
+                                 C.c_int, u64, u64, vp, vp, vp, vp, vp, vp]),
+    ("cf_rec_build", C.c_int, [vp, u64, vp, C.c_int, C.c_int, vp, vp]),
+    ("cf_rec_probe", C.c_int, [vp, u64, vp, C.c_int, C.c_int, C.c_int, vp, u32, vp, vp, vp]),
     ("cf_batch_mod_bytes", sz, []),
     ("cf_batch_max_r", C.c_int, []),
     ("cf_batch_run", C.c_int, [C.c_int, vp, vp, u32, u32, vp, vp, vp, u32, vp, vp, vp, u32, vp]),

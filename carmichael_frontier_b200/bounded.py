@@ -1,0 +1,238 @@
+"""Product-bounded record producers on the GPU: the filtered I side (igen / idump) and
+the Dmin-filtered D side (ddump), exact integer bounds, reference record order.
+
+  generate_I  every r-subset I of the ascending pool with prod(I) < Icap and at most
+              hmax primes above `split`: key = P0 * prod(I) mod M, id = colex rank
+              (gpu/igen_gpu.py:1-21, src/mitm64_idump_stream2.cpp with IDUMP_RANK=1)
+  generate_D  every r-subset D of the ascending base with prod(D) >= Dmin:
+              key = prod(D) mod M, id = 6-bit packed indices or a 64-bit mask
+              (src/mitm64_ddump.cpp:29-44)
+
+The kernels (csrc/cf_bgen.cu) expand the enumeration tree one level at a time; the
+exact bound tables that make every level one contiguous child range per node are
+built here with Python integers, like the reference's quotient table
+(gpu/igen_gpu.py:92-101).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import _lib
+from .tables import DeviceTables, key_of
+
+U128 = 1 << 128
+
+
+def quotient_table(INS, r: int, Icap: int) -> list[int]:
+    """H[t*n + x] = floor((Icap-1) / (a_x ... a_{x+t})) for x + t < n (0 otherwise), 0 <= t < r."""
+    n = len(INS)
+    top = Icap - 1
+    H = [0] * (r * n)
+    for t in range(r):
+        if t >= n:
+            break
+        w = math.prod(INS[:t + 1])
+        for x in range(n - t):
+            if x:
+                w = w // INS[x - 1] * INS[x + t]
+            H[t * n + x] = top // w
+    return H
+
+
+def dmin_table(B, r: int, Dmin: int) -> list[int]:
+    """G[t*n + x] = ceil(Dmin / (b_x b_{x-1} ... b_{x-t})) for x >= t (unused otherwise), 0 <= t < r."""
+    n = len(B)
+    G = [U128 - 1] * (r * n)
+    for t in range(r):
+        for x in range(t, n):
+            w = math.prod(B[x - t:x + 1])
+            G[t * n + x] = -(-Dmin // w) if Dmin > 0 else 0
+    return G
+
+
+def _cat_u64(parts):
+    """Concatenate torch uint64 tensors (through int64 views: torch has no uint64 cat on CUDA)."""
+    import torch
+    if len(parts) == 1:
+        return parts[0]
+    return torch.cat([p.view(torch.int64) for p in parts]).view(torch.uint64)
+
+
+def _u128_pairs(vals) -> np.ndarray:
+    a = np.zeros(2 * len(vals), dtype=np.uint64)
+    m = (1 << 64) - 1
+    for i, v in enumerate(vals):
+        v = min(int(v), U128 - 1)
+        a[2 * i] = v & m
+        a[2 * i + 1] = v >> 64
+    return a
+
+
+class BoundedGenerator:
+    """Level-by-level bounded enumeration on one device (torch tensors as buffers)."""
+
+    def __init__(self, device=None, max_nodes: int = 1 << 27):
+        import torch
+        self.torch = torch
+        self.lib = _lib.load()
+        self.device = torch.device(device if device is not None else "cuda")
+        if self.device.type != "cuda":
+            raise RuntimeError("bounded generation runs on a CUDA device only")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.tables = DeviceTables(self.device)
+        self.max_nodes = max_nodes
+        self.launches = 0
+
+    # -- primitives -----------------------------------------------------------
+    def _scan(self, cnt, F: int):
+        torch = self.torch
+        offs = torch.empty(F + 1, dtype=torch.int64, device=self.device)
+        nb = self.lib.cf_scan_tmp_bytes(F)
+        tmp = torch.empty(max(nb, 16), dtype=torch.uint8, device=self.device)
+        _lib.check(self.lib.cf_scan_u64(_lib.ptr(cnt), F, _lib.ptr(offs), _lib.ptr(tmp), nb, _lib.stream_handle()),
+                   "cf_scan_u64")
+        self.launches += 2
+        return offs
+
+    def _frontier(self, side: int, pool, bounds, n: int, r: int, split_idx: int, hmax: int, bitmask: int,
+                  xa: int, xb: int, M: int, mult: int):
+        """Nodes at depth r-1 of the block of first indices [xa, xb), their child
+        offsets and first child indices; None if a level exceeds max_nodes."""
+        torch, lib, dp = self.torch, self.lib, _lib.ptr
+        dev = self.device
+        root = np.array([key_of(M, mult % M)], dtype=np.uint64).view(np.int64)    # key form of the multiplier
+        key = torch.from_numpy(root).to(dev)
+        alo = torch.ones(1, dtype=torch.int64, device=dev)
+        ahi = torch.zeros(1, dtype=torch.int64, device=dev)
+        ids = torch.zeros(1, dtype=torch.int64, device=dev)
+        meta = torch.full((1,), 0xFFFF, dtype=torch.int32, device=dev)
+        F = 1
+        sh = _lib.stream_handle()
+        for d in range(r):
+            cnt = torch.empty(F, dtype=torch.int64, device=dev)
+            xs = torch.empty(F, dtype=torch.int32, device=dev)
+            _lib.check(lib.cf_bgen_count(side, d, r, n, F, dp(alo), dp(ahi), dp(meta), dp(bounds), split_idx, hmax,
+                                         xa, xb, dp(cnt), dp(xs), sh), "cf_bgen_count")
+            self.launches += 1
+            offs = self._scan(cnt, F)
+            total = int(offs[F].item())
+            if d == r - 1:
+                return dict(F=F, key=key, alo=alo, ahi=ahi, ids=ids, meta=meta, offs=offs, xs=xs, total=total)
+            if total == 0:
+                return dict(F=0, total=0)
+            if total > self.max_nodes:
+                return None
+            nkey = torch.empty(total, dtype=torch.int64, device=dev)
+            nalo = torch.empty(total, dtype=torch.int64, device=dev)
+            nahi = torch.empty(total, dtype=torch.int64, device=dev)
+            nids = torch.empty(total, dtype=torch.int64, device=dev)
+            nmeta = torch.empty(total, dtype=torch.int32, device=dev)
+            _lib.check(lib.cf_bgen_expand(side, d, r, n, F, dp(pool), dp(key), dp(alo), dp(ahi), dp(ids), dp(meta),
+                                          dp(offs), dp(xs), split_idx, bitmask, 0, total, dp(nkey), dp(nalo),
+                                          dp(nahi), dp(nids), dp(nmeta), sh), "cf_bgen_expand")
+            self.launches += 1
+            key, alo, ahi, ids, meta, F = nkey, nalo, nahi, nids, nmeta, total
+        raise AssertionError("unreachable")
+
+    def _blocks(self, side, pool, bounds, n, r, split_idx, hmax, bitmask, xa, xb, M, mult):
+        """Depth-(r-1) frontiers covering first indices [xa, xb), in record order."""
+        fr = self._frontier(side, pool, bounds, n, r, split_idx, hmax, bitmask, xa, xb, M, mult)
+        if fr is not None:
+            return [fr]
+        if xb - xa <= 1:
+            raise _lib.CfError(_lib.CF_ENOMEM, "bounded", "one first index has more partial subsets than max_nodes")
+        mid = (xa + xb) // 2
+        lo = self._blocks(side, pool, bounds, n, r, split_idx, hmax, bitmask, xa, mid, M, mult)
+        hi = self._blocks(side, pool, bounds, n, r, split_idx, hmax, bitmask, mid, xb, M, mult)
+        # I side enumerates first indices ascending, D side descending
+        return lo + hi if side == 0 else hi + lo
+
+    def _records(self, side, pool, bounds, n, r, split_idx, hmax, bitmask, max_records, M, mult):
+        torch, lib, dp = self.torch, self.lib, _lib.ptr
+        sh = _lib.stream_handle()
+        for fr in self._blocks(side, pool, bounds, n, r, split_idx, hmax, bitmask, 0, n, M, mult):
+            total = fr["total"]
+            c0 = 0
+            while c0 < total:
+                cc = min(max_records, total - c0)
+                keys = torch.empty(cc, dtype=torch.uint64, device=self.device)
+                ids = torch.empty(cc, dtype=torch.uint64, device=self.device)
+                _lib.check(lib.cf_bgen_expand(side, r - 1, r, n, fr["F"], dp(pool), dp(fr["key"]), dp(fr["alo"]),
+                                              dp(fr["ahi"]), dp(fr["ids"]), dp(fr["meta"]), dp(fr["offs"]),
+                                              dp(fr["xs"]), split_idx, bitmask, c0, cc, dp(keys), None, None,
+                                              dp(ids), None, sh), "cf_bgen_expand(records)")
+                self.launches += 1
+                yield keys, ids
+                c0 += cc
+
+    # -- the two producers ------------------------------------------------------
+    def generate_I(self, INS, r: int, M: int, P0: int, Icap: int, split=None, hmax=None,
+                   max_records: int = 200_000_000):
+        """Yields (keys, ids) torch uint64 chunks of the filtered I side; returns the total."""
+        INS = [int(p) for p in INS]
+        n = len(INS)
+        assert 1 <= r <= 16 and n <= 1024 and 2 <= M < (1 << 62)
+        assert all(INS[i] < INS[i + 1] for i in range(n - 1)), "INS must be strictly ascending"
+        assert Icap - 1 < U128, "Icap needs more than 128 bits"
+        if Icap <= 1 or n < r:
+            return 0
+        assert math.comb(n, r) < 1 << 64, "rank ids would overflow u64"
+        split_idx = n if split is None else next((i for i, p in enumerate(INS) if p > split), n)
+        hmax = r if hmax is None else int(hmax)
+        pool = self.tables.pool(INS, r, M, P0 % M)
+        bounds = self.tables.get(("igenH", tuple(INS), r, Icap),
+                                 lambda: _u128_pairs(quotient_table(INS, r, Icap)).view(np.uint8))
+        total = 0
+        for keys, ids in self._records(0, pool, bounds, n, r, split_idx, hmax, 0, max_records, M, P0):
+            total += keys.numel()
+            yield keys, ids
+        return total
+
+    def generate_D(self, B, r: int, M: int, Dmin: int, bitmask: int = 0, max_records: int = 1 << 62):
+        """(keys, ids, count) of the Dmin-filtered D side (torch uint64), ddump's order.
+        bitmask: 0 = 6-bit packed ids (a mask when r > 10), 1 = 64-bit index mask (both
+        for bases of at most 64 primes, as the dumper), 2 = colex rank (any base)."""
+        torch = self.torch
+        B = [int(p) for p in B]
+        n = len(B)
+        mode = int(bitmask)
+        if mode == 0 and r > 10:
+            mode = 1
+        assert mode in (0, 1, 2) and 1 <= r <= 16 and 2 <= M < (1 << 62)
+        assert n <= (1024 if mode == 2 else 64), "packed and mask ids need a base of at most 64 primes"
+        assert all(B[i] < B[i + 1] for i in range(n - 1)), "the base must be strictly ascending"
+        if mode == 2:
+            assert math.comb(n, r) < 1 << 64, "rank ids would overflow u64"
+        empty = (torch.empty(0, dtype=torch.uint64, device=self.device),) * 2 + (0,)
+        if n < r or Dmin >= U128:
+            return empty
+        assert math.prod(B[-r:]) < U128, "products of r base primes must stay below 2^128"
+        pool = self.tables.pool(B, r, M, 1)
+        bounds = self.tables.get(("ddumpG", tuple(B), r, Dmin),
+                                 lambda: _u128_pairs(dmin_table(B, r, max(int(Dmin), 0))).view(np.uint8))
+        ks, is_ = [], []
+        for k, i in self._records(1, pool, bounds, n, r, n, r, mode, max_records, M, 1):
+            ks.append(k)
+            is_.append(i)
+        if not ks:
+            return empty
+        k = _cat_u64(ks)
+        i = _cat_u64(is_)
+        return k, i, int(k.numel())
+
+
+_gens: dict = {}
+
+
+def generator(device=None) -> BoundedGenerator:
+    import torch
+    d = torch.device(device if device is not None else "cuda")
+    if d.index is None:
+        d = torch.device("cuda", torch.cuda.current_device())
+    g = _gens.get(d)
+    if g is None:
+        g = _gens[d] = BoundedGenerator(d)
+    return g

@@ -73,7 +73,9 @@ class Tuning:
     i_chunk_records: int = 1 << 31  # I-side records per generation/join chunk
     pair_capacity: int = 1 << 14    # initial candidate-pair buffer (grown on overflow)
     sigma: float = 6.0              # partition capacity = mean + sigma*sqrt(mean) + 16
-    strategy: str = "fused"         # "fused": D table + generate-and-probe; "partition": materialised join
+    strategy: str = "fused"         # "fused": table + generate-and-probe; "partition": materialised join;
+                                    # "bounded": size-bound-pruned sides + record join; "auto": bounded
+                                    # where the bound prunes, else fused
     dtab_load: float = 5.0          # fused: minimum average D records per 16-slot bucket (up to 2x this)
     fused_grid: int = 0             # fused probe CTAs (0 = one per 16384 records)
     l2_table_bytes: int = 48 << 20  # fingerprint arrays above this get a Bloom-filter first level
@@ -211,6 +213,7 @@ class Solver:
         self.tuning = tuning or Tuning()
         self.tables = DeviceTables(self.device)
         self._bufs: dict[str, object] = {}
+        self._bounded = None
         self.result_bytes = self.lib.cf_pair_result_bytes()
         assert self.result_bytes == RESULT_DTYPE.itemsize
 
@@ -396,6 +399,13 @@ class Solver:
         sample of the instance; every pair with such an I rank is found)."""
         if inst.r == 0:
             return self._solve_r0(inst)
+        st = self.tuning.strategy
+        if i_limit is None and (st == "bounded" or st == "auto"):
+            from . import bsolve
+            if bsolve.applicable(inst) and (st == "bounded" or bsolve.prunes(inst)):
+                if self._bounded is None:
+                    self._bounded = bsolve.BoundedSolve(self)
+                return self._bounded.solve(inst, verify)
         nD, nI = ncomb(len(inst.B0), inst.r), ncomb(len(inst.INS), inst.r)
         if i_limit is not None:
             nI = min(nI, int(i_limit))
@@ -451,7 +461,9 @@ def solve(M: int, Q, B0, r: int, B: int, device=None, verify: bool = True, strat
 
     Q is the eligible pool Q(M) (primes q with (q-1) | M and q not dividing M);
     INS = Q \\ B0.  Hits are certified on the host and returned ascending by n.
-    strategy: "fused" (D table + generate-and-probe) or "partition" (materialised join)."""
+    strategy: "fused" (table + generate-and-probe), "partition" (materialised join), "bounded"
+    (both sides pruned by the size bound, then a record join) or "auto" (bounded where the
+    bound prunes, else fused).  Every strategy returns the same hits."""
     import torch
     dev = torch.device(device if device is not None else "cuda")
     key = (dev.type, dev.index, strategy)

@@ -183,6 +183,47 @@ size_t cf_pair_result_bytes(void);
 int cf_check_pairs(const void* poolD, const void* poolI, const void* screen, int r, const void* pairs,
                    const uint32_t* npairs, uint32_t max_pairs, void* results, uint32_t* err, void* stream);
 
+/* ---- product-bounded producers (filtered I side, Dmin-filtered D side) ---- */
+
+/* Level-by-level expansion of the bounded enumeration tree.  A frontier node is
+ * {key (key form), exact product (alo, ahi), partial id, meta = last index |
+ * count of large primes << 16}; the root is {key(mult), 1, 0, 0xffff}.
+ * bounds: r x n u128 values as (lo, hi) u64 pairs, row t = positions left after
+ * the chosen index:
+ *   side 0 (I, ascending, id = colex rank): H[t][x] = floor((Icap-1) /
+ *     (a_x ... a_{x+t})), child x kept iff product <= H[t][x]; indices >=
+ *     split_idx count as large, at most hmax of them.  The records of
+ *     src/mitm64_idump_stream2.cpp (IDUMP_RANK=1) and gpu/igen_gpu.py:26-76
+ *     (its igen kernel, count and write passes), in the same lexicographic order.
+ *   side 1 (D, descending; bitmask 0: 6-bit packed ids, 1: index mask, both
+ *     for n <= 64; 2: colex rank, any n): G[t][x] = ceil(Dmin / (b_x b_{x-1}
+ *     ... b_{x-t})), child x kept iff product >= G[t][x].  The records of
+ *     src/mitm64_ddump.cpp:29-44, same order.
+ * cf_bgen_count writes each node's child count and first child index;
+ * cf_scan_u64 turns counts into offsets (offs[F] = total); cf_bgen_expand writes
+ * children [c0, c0+cc): nodes for d < r-1, records {canonical key, id} for
+ * d = r-1.  First indices can be restricted to [xa, xb) at depth 0. */
+size_t cf_scan_tmp_bytes(uint64_t n);
+int cf_scan_u64(const uint64_t* in, uint64_t n, uint64_t* out, void* tmp, size_t tmp_bytes, void* stream);
+int cf_bgen_count(int side, int d, int r, int n, uint64_t F, const uint64_t* alo, const uint64_t* ahi,
+                  const uint32_t* meta, const uint64_t* bounds, int split_idx, int hmax, int xa, int xb,
+                  uint64_t* cnt, uint32_t* xs, void* stream);
+int cf_bgen_expand(int side, int d, int r, int n, uint64_t F, const void* pool, const uint64_t* key,
+                   const uint64_t* alo, const uint64_t* ahi, const uint64_t* id, const uint32_t* meta,
+                   const uint64_t* offs, const uint32_t* xs, int split_idx, int bitmask, uint64_t c0, uint64_t cc,
+                   uint64_t* okey, uint64_t* oalo, uint64_t* oahi, uint64_t* oid, uint32_t* ometa, void* stream);
+
+/* Hash join of two materialised sides of {canonical key} records (the bounded
+ * producers' output): cf_rec_build inserts the smaller side's keys into a table
+ * of cf_dtab_bytes2(bbits, fbits) bytes (zeroed as for cf_dtab_build2);
+ * cf_rec_probe probes it with the other side and appends every candidate
+ * {D position, I position} (swap = 1 when the table holds the I side); the
+ * caller drops the rare candidates whose keys differ.  Replaces sort_side +
+ * join_sorted on the filtered sides (gpu/mitm_gpu_mstar_driver.py:241-262). */
+int cf_rec_build(const uint64_t* keys, uint64_t n, void* tab, int bbits, int fbits, uint32_t* err, void* stream);
+int cf_rec_probe(const uint64_t* keys, uint64_t n, const void* tab, int bbits, int fbits, int swap, void* pairs,
+                 uint32_t max_pairs, uint32_t* npairs, uint32_t* err, void* stream);
+
 /* ---- batched portfolio --------------------------------------------------- */
 
 /* Many moduli (radius 1..cf_batch_max_r() each, mixed) joined by persistent
