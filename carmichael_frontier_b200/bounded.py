@@ -98,9 +98,12 @@ class BoundedGenerator:
         return offs
 
     def _frontier(self, side: int, pool, bounds, n: int, r: int, split_idx: int, hmax: int, bitmask: int,
-                  xa: int, xb: int, M: int, mult: int):
+                  xa: int, xb: int, M: int, mult: int, limit: int | None = -1):
         """Nodes at depth r-1 of the block of first indices [xa, xb), their child
-        offsets and first child indices; None if a level exceeds max_nodes."""
+        offsets and first child indices; None if a level exceeds the node limit
+        (max_nodes by default; None = no limit)."""
+        if limit == -1:
+            limit = self.max_nodes
         torch, lib, dp = self.torch, self.lib, _lib.ptr
         dev = self.device
         root = np.array([key_of(M, mult % M)], dtype=np.uint64).view(np.int64)    # key form of the multiplier
@@ -123,7 +126,7 @@ class BoundedGenerator:
                 return dict(F=F, key=key, alo=alo, ahi=ahi, ids=ids, meta=meta, offs=offs, xs=xs, total=total)
             if total == 0:
                 return dict(F=0, total=0)
-            if total > self.max_nodes:
+            if limit is not None and total > limit:
                 return None
             nkey = torch.empty(total, dtype=torch.int64, device=dev)
             nalo = torch.empty(total, dtype=torch.int64, device=dev)
@@ -138,17 +141,21 @@ class BoundedGenerator:
         raise AssertionError("unreachable")
 
     def _blocks(self, side, pool, bounds, n, r, split_idx, hmax, bitmask, xa, xb, M, mult):
-        """Depth-(r-1) frontiers covering first indices [xa, xb), in record order."""
+        """Yields the depth-(r-1) frontiers covering first indices [xa, xb), in record
+        order; a block whose frontier exceeds max_nodes is halved."""
         fr = self._frontier(side, pool, bounds, n, r, split_idx, hmax, bitmask, xa, xb, M, mult)
         if fr is not None:
-            return [fr]
+            yield fr
+            return
         if xb - xa <= 1:
-            raise _lib.CfError(_lib.CF_ENOMEM, "bounded", "one first index has more partial subsets than max_nodes")
+            # a single first index cannot be split further: expand it whole
+            yield self._frontier(side, pool, bounds, n, r, split_idx, hmax, bitmask, xa, xb, M, mult, None)
+            return
         mid = (xa + xb) // 2
-        lo = self._blocks(side, pool, bounds, n, r, split_idx, hmax, bitmask, xa, mid, M, mult)
-        hi = self._blocks(side, pool, bounds, n, r, split_idx, hmax, bitmask, mid, xb, M, mult)
         # I side enumerates first indices ascending, D side descending
-        return lo + hi if side == 0 else hi + lo
+        halves = ((xa, mid), (mid, xb)) if side == 0 else ((mid, xb), (xa, mid))
+        for a, b in halves:
+            yield from self._blocks(side, pool, bounds, n, r, split_idx, hmax, bitmask, a, b, M, mult)
 
     def _records(self, side, pool, bounds, n, r, split_idx, hmax, bitmask, max_records, M, mult):
         torch, lib, dp = self.torch, self.lib, _lib.ptr
@@ -169,22 +176,38 @@ class BoundedGenerator:
                 c0 += cc
 
     # -- the two producers ------------------------------------------------------
-    def generate_I(self, INS, r: int, M: int, P0: int, Icap: int, split=None, hmax=None,
-                   max_records: int = 200_000_000):
-        """Yields (keys, ids) torch uint64 chunks of the filtered I side; returns the total."""
+    def _setup_I(self, INS, r, M, P0, Icap, split, hmax):
         INS = [int(p) for p in INS]
         n = len(INS)
         assert 1 <= r <= 16 and n <= 1024 and 2 <= M < (1 << 62)
         assert all(INS[i] < INS[i + 1] for i in range(n - 1)), "INS must be strictly ascending"
         assert Icap - 1 < U128, "Icap needs more than 128 bits"
         if Icap <= 1 or n < r:
-            return 0
+            return None
         assert math.comb(n, r) < 1 << 64, "rank ids would overflow u64"
         split_idx = n if split is None else next((i for i, p in enumerate(INS) if p > split), n)
         hmax = r if hmax is None else int(hmax)
         pool = self.tables.pool(INS, r, M, P0 % M)
         bounds = self.tables.get(("igenH", tuple(INS), r, Icap),
                                  lambda: _u128_pairs(quotient_table(INS, r, Icap)).view(np.uint8))
+        return INS, n, split_idx, hmax, pool, bounds
+
+    def frontiers_I(self, INS, r: int, M: int, P0: int, Icap: int, split=None, hmax=None):
+        """(pool, iterator of depth-(r-1) frontiers) of the filtered I side: the leaves
+        are not written, for cf_bgen_probe.  (None, []) when the side is empty."""
+        st = self._setup_I(INS, r, M, P0, Icap, split, hmax)
+        if st is None:
+            return None, iter(())
+        INS, n, split_idx, hmax, pool, bounds = st
+        return pool, self._blocks(0, pool, bounds, n, r, split_idx, hmax, 0, 0, n, M, P0)
+
+    def generate_I(self, INS, r: int, M: int, P0: int, Icap: int, split=None, hmax=None,
+                   max_records: int = 200_000_000):
+        """Yields (keys, ids) torch uint64 chunks of the filtered I side; returns the total."""
+        st = self._setup_I(INS, r, M, P0, Icap, split, hmax)
+        if st is None:
+            return 0
+        INS, n, split_idx, hmax, pool, bounds = st
         total = 0
         for keys, ids in self._records(0, pool, bounds, n, r, split_idx, hmax, 0, max_records, M, P0):
             total += keys.numel()

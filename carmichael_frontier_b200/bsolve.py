@@ -9,9 +9,10 @@ smallest insertion primes this gives the reference driver's two filters
     prod(D) >= Dmin = ceil(P0 * Imin / B)
 
 The filtered sides come from the bounded producers (csrc/cf_bgen.cu: the igen /
-idump and ddump records), are joined by the record hash join (csrc/cf_rec_join.cu,
-table on the smaller side), and every equal-key pair is checked exactly on the
-host (prod(S) <= B, prod(S) == 1 mod M, certificate), as run_instance does
+idump and ddump records) and are joined through the record table of
+csrc/cf_rec_join.cu -- built on the D records with the I leaves probing it as
+they are generated (csrc/cf_bgen_probe.cu), or built on the I records when those
+are fewer -- and every equal-key pair is checked exactly on the host (prod(S) <= B, prod(S) == 1 mod M, certificate), as run_instance does
 (:241-262).  The hit set equals the unpruned join's: pruning removes only
 subsets that no hit can contain.  Where the bound prunes hard (B = prod(B0) *
 10^4, the serving workload) the sides are a tiny fraction of C(n, r).
@@ -23,7 +24,7 @@ import math
 import numpy as np
 
 from . import _lib
-from .bounded import U128, _cat_u64
+from .bounded import U128
 from .certify import verify_certificate
 from .tables import unrank_colex
 
@@ -58,93 +59,134 @@ def prunes(inst) -> bool:
 
 
 class BoundedSolve:
-    """Solves one instance with the bounded producers and the record hash join."""
+    """Solves one instance with the bounded producers and a record-table join.
+
+    The D side (Dmin filter) is materialised.  The I side (Icap filter) is expanded
+    to its last level; when its leaves outnumber the D records they are never
+    written: cf_bgen_probe computes each leaf and probes a table of the D records.
+    Otherwise the I leaves are written and the table is built on them."""
+
+    LEAF_CHUNK = 1 << 30          # I leaves per probe launch
 
     def __init__(self, solver):
         from .bounded import BoundedGenerator
         self.s = solver
         self.torch = solver.torch
         self.lib = solver.lib
-        self.gen = BoundedGenerator(solver.device)
+        self.gen = BoundedGenerator(solver.device, max_nodes=solver.tuning.max_nodes)
 
-    def generate(self, inst, i_chunk: int = 1 << 28):
-        """Filtered sides on the device: (Dk, Did, [(Ik, Iid), ...], nD, nI, caps)."""
-        Icap, Dmin = caps(inst)
-        Dk, Did, nD = self.gen.generate_D(inst.B0, inst.r, inst.M, Dmin, bitmask=2)
-        chunks = list(self.gen.generate_I(inst.INS, inst.r, inst.M, inst.P0, Icap, max_records=i_chunk))
-        nI = sum(int(k.numel()) for k, _ in chunks)
-        return Dk, Did, chunks, nD, nI, (Icap, Dmin)
-
-    def solve(self, inst, verify: bool = True):
-        from .solve import Hit, SolveResult, dtab_shape
-        torch, lib, dp, ck = self.torch, self.lib, _lib.ptr, _lib.check
-        r = inst.r
-        Dk, Did, chunks, nD, nI, (Icap, Dmin) = self.generate(inst)
-        plan = dict(strategy="bounded", Icap=Icap, Dmin=Dmin)
-        if nD == 0 or nI == 0:
-            return SolveResult([], nD, nI, 0, 0, 0, 0, plan=plan)
-        # the table holds the smaller side (the I side only when it is one chunk)
-        swap = len(chunks) == 1 and nI < nD
-        if (nI if swap else nD) >= RANK_LIMIT:
+    def _table(self, keys, n: int, plan: dict):
+        from .solve import dtab_shape
+        torch, lib, dp = self.torch, self.lib, _lib.ptr
+        if n >= RANK_LIMIT:
             raise _lib.CfError(_lib.CF_EOVERFLOW, "bounded", "table side has 2^32 records or more")
-        build = chunks[0][0] if swap else Dk
-        nb = nI if swap else nD
-        bbits, fbits = dtab_shape(nb, self.s.tuning)
-        plan.update(bbits=bbits, fbits=fbits, swap=swap)
+        bbits, fbits = dtab_shape(n, self.s.tuning)
+        plan.update(bbits=bbits, fbits=fbits)
         tbytes = lib.cf_dtab_bytes2(bbits, fbits)
         tab = self.s._buf("btab", tbytes)
-        ctr = self.s._buf("bctr", 64)
-        misc = ctr[:64].view(torch.int32)
-        sh = self.s._sh()
         nbk = 1 << bbits
         tab[: 32 * nbk].zero_()
         tab[160 * nbk: tbytes].zero_()
-        misc.zero_()
-        ck(lib.cf_rec_build(dp(build), nb, dp(tab), bbits, fbits, dp(misc) + 4, sh), "cf_rec_build")
-        probes = [(Dk, 0)] if swap else []
-        if not swap:
-            off = 0
-            for k, _ in chunks:
-                probes.append((k, off))
-                off += int(k.numel())
+        self.misc.zero_()
+        _lib.check(lib.cf_rec_build(dp(keys), n, dp(tab), bbits, fbits, dp(self.misc) + 4, self.s._sh()),
+                   "cf_rec_build")
+        return tab, bbits, fbits
+
+    def _probe(self, launch, maxp: int):
+        """Run one probe launch (a function of (pairs, max_pairs)), regrowing the pair
+        buffer on overflow; returns (candidate array [k, 2] u64, max_pairs)."""
+        while True:
+            pairs = self.s._buf("bpairs", maxp * 16)
+            self.misc[0].zero_()
+            launch(pairs, maxp)
+            m = self.misc[:2].cpu().numpy().view(np.uint32)
+            npairs, err = int(m[0]), int(m[1])
+            if err & _lib.ERR_TABLE_FULL:
+                raise _lib.CfError(_lib.CF_EOVERFLOW, "bounded", "join table full (internal error)")
+            if err & _lib.ERR_PAIR_OVERFLOW:
+                self.misc[1].zero_()
+                maxp = max(2 * maxp, npairs + 16)
+                continue
+            if err:
+                raise _lib.CfError(_lib.CF_EBADARG, "bounded", f"record join failed (err {err:#x})")
+            pv = pairs[: npairs * 16].cpu().numpy().view(np.uint64).reshape(npairs, 2).copy() if npairs else None
+            return pv, maxp
+
+    def solve(self, inst, verify: bool = True):
+        from .solve import SolveResult
+        torch, lib, dp = self.torch, self.lib, _lib.ptr
+        r, M = inst.r, inst.M
+        Icap, Dmin = caps(inst)
+        plan = dict(strategy="bounded", Icap=Icap, Dmin=Dmin)
+        self.misc = self.s._buf("bctr", 64)[:64].view(torch.int32)
+        sh = self.s._sh()
+        Dk, Did, nD = self.gen.generate_D(inst.B0, r, M, Dmin, bitmask=2)
+        poolI, blocks = self.gen.frontiers_I(inst.INS, r, M, inst.P0, Icap)
+        blocks = iter(blocks)
+        first = next(blocks, None)
+        if nD == 0 or first is None:
+            nI = sum(b["total"] for b in ([first] if first else []) + list(blocks))
+            return SolveResult([], nD, nI, 0, 0, 0, 0, plan=plan)
+        second = next(blocks, None)
         maxp = self.s.tuning.pair_capacity
-        found = []
-        for keys, off in probes:
-            while True:
-                pairs = self.s._buf("bpairs", maxp * 16)
-                misc[0].zero_()
-                ck(lib.cf_rec_probe(dp(keys), keys.numel(), dp(tab), bbits, fbits, int(swap), dp(pairs), maxp,
-                                    dp(misc), dp(misc) + 4, sh), "cf_rec_probe")
-                m = misc[:2].cpu().numpy().view(np.uint32)
-                npairs, err = int(m[0]), int(m[1])
-                if err & _lib.ERR_TABLE_FULL:
-                    raise _lib.CfError(_lib.CF_EOVERFLOW, "bounded", "join table full (internal error)")
-                if err & _lib.ERR_PAIR_OVERFLOW:
-                    misc[1].zero_()
-                    maxp = max(2 * maxp, npairs + 16)
-                    continue
-                if err:
-                    raise _lib.CfError(_lib.CF_EBADARG, "bounded", f"record join failed (err {err:#x})")
-                if npairs:
-                    pv = pairs[: npairs * 16].cpu().numpy().view(np.uint64).reshape(npairs, 2).copy()
-                    pv[:, 1] += np.uint64(off)        # I positions of a probing chunk start at its offset
-                    found.append(pv)
-                break
-        Ik_all = _cat_u64([k for k, _ in chunks])
-        Iid_all = _cat_u64([i for _, i in chunks])
+        cands = []                         # (D position, I colex id) arrays
+        nI = 0
+        if second is None and first["total"] < nD:
+            # one small I block: write its leaves and build the table on them
+            nI = first["total"]
+            plan["table"] = "I"
+            if nI:
+                Ik = torch.empty(nI, dtype=torch.uint64, device=self.s.device)
+                Iid = torch.empty(nI, dtype=torch.uint64, device=self.s.device)
+                fr = first
+                _lib.check(lib.cf_bgen_expand(0, r - 1, r, len(inst.INS), fr["F"], dp(poolI), dp(fr["key"]),
+                                              dp(fr["alo"]), dp(fr["ahi"]), dp(fr["ids"]), dp(fr["meta"]),
+                                              dp(fr["offs"]), dp(fr["xs"]), len(inst.INS), 0, 0, nI, dp(Ik), None,
+                                              None, dp(Iid), None, sh), "cf_bgen_expand(records)")
+                tab, bb, fb = self._table(Ik, nI, plan)
+                pv, maxp = self._probe(lambda pairs, mp: _lib.check(
+                    lib.cf_rec_probe(dp(Dk), nD, dp(tab), bb, fb, 1, dp(pairs), mp, dp(self.misc),
+                                     dp(self.misc) + 4, sh), "cf_rec_probe"), maxp)
+                if pv is not None:
+                    iid = Iid.view(torch.int64)[torch.from_numpy(pv[:, 1].astype(np.int64)).to(self.s.device)]
+                    pv[:, 1] = iid.cpu().numpy().view(np.uint64)
+                    cands.append(pv)
+        else:
+            # the table holds the D records; every I leaf probes it without being written
+            plan["table"] = "D"
+            tab, bb, fb = self._table(Dk, nD, plan)
+            chain = [first] + ([second] if second is not None else [])
+            for fr in _chain(chain, blocks):
+                total = fr["total"]
+                nI += total
+                for c0 in range(0, total, self.LEAF_CHUNK):
+                    cc = min(self.LEAF_CHUNK, total - c0)
+                    pv, maxp = self._probe(lambda pairs, mp, fr=fr, c0=c0, cc=cc: _lib.check(
+                        lib.cf_bgen_probe(r, len(inst.INS), fr["F"], dp(poolI), dp(fr["key"]), dp(fr["ids"]),
+                                          dp(fr["offs"]), dp(fr["xs"]), c0, cc, dp(tab), bb, fb, dp(pairs), mp,
+                                          dp(self.misc), dp(self.misc) + 4, sh), "cf_bgen_probe"), maxp)
+                    if pv is not None:
+                        cands.append(pv)
+        return self._finish(inst, Dk, Did, cands, nD, nI, plan, verify)
+
+    def _finish(self, inst, Dk, Did, cands, nD, nI, plan, verify):
+        from .solve import Hit, SolveResult
+        torch = self.torch
+        r, M = inst.r, inst.M
         hits, pairs_out, above, rejected, screened = [], [], 0, 0, 0
-        if found:
-            pv = np.concatenate(found)
+        if cands:
+            pv = np.concatenate(cands)
             dpos = torch.from_numpy(pv[:, 0].astype(np.int64)).to(self.s.device)
-            ipos = torch.from_numpy(pv[:, 1].astype(np.int64)).to(self.s.device)
             dk = Dk.view(torch.int64)[dpos].cpu().numpy().view(np.uint64)
-            ik = Ik_all.view(torch.int64)[ipos].cpu().numpy().view(np.uint64)
             di = Did.view(torch.int64)[dpos].cpu().numpy().view(np.uint64)
-            ii = Iid_all.view(torch.int64)[ipos].cpu().numpy().view(np.uint64)
             B0, INS = inst.B0, inst.INS
-            for j in np.nonzero(dk == ik)[0]:
+            P0m = inst.P0 % M
+            for j in range(len(pv)):
+                ii = unrank_colex(int(pv[j, 1]), r, len(INS))
+                I = tuple(INS[x] for x in ii)
+                if (P0m * math.prod(I)) % M != int(dk[j]):
+                    continue                   # fingerprint collision, not an equal-residue pair
                 D = tuple(B0[x] for x in unrank_colex(int(di[j]), r, len(B0)))
-                I = tuple(INS[x] for x in unrank_colex(int(ii[j]), r, len(INS)))
                 pairs_out.append((D, I))
                 dset = set(D)
                 fac = tuple(sorted([p for p in B0 if p not in dset] + list(I)))
@@ -153,7 +195,7 @@ class BoundedSolve:
                     above += 1
                     continue
                 screened += 1
-                ok = (n - 1) % inst.M == 0
+                ok = (n - 1) % M == 0
                 if ok and verify:
                     ok, n2, _ = verify_certificate(fac)
                     ok = ok and n2 == n
@@ -165,3 +207,8 @@ class BoundedSolve:
         pairs_out.sort()
         return SolveResult(hits, nD, nI, len(pairs_out), screened, above, rejected, plan=plan, pairs=pairs_out,
                            launches=self.gen.launches)
+
+
+def _chain(head, rest):
+    yield from head
+    yield from rest

@@ -80,6 +80,7 @@ class Tuning:
     fused_grid: int = 0             # fused probe CTAs (0 = one per 16384 records)
     l2_table_bytes: int = 48 << 20  # fingerprint arrays above this get a Bloom-filter first level
     max_fbits: int = 21             # Bloom filter at most 2^21 blocks of 32 bytes (64 MB)
+    max_nodes: int = 1 << 27        # bounded strategy: frontier nodes per block of first indices
 
 
 def dtab_shape(nD: int, tu: Tuning) -> tuple[int, int]:

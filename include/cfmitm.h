@@ -224,6 +224,16 @@ int cf_rec_build(const uint64_t* keys, uint64_t n, void* tab, int bbits, int fbi
 int cf_rec_probe(const uint64_t* keys, uint64_t n, const void* tab, int bbits, int fbits, int swap, void* pairs,
                  uint32_t max_pairs, uint32_t* npairs, uint32_t* err, void* stream);
 
+/* The last level of the bounded I side fused with the probe of a cf_rec_build
+ * table of D records: the leaves [c0, c0+cc) of a depth-(r-1) I frontier (the
+ * node arrays, offsets and first child indices of cf_bgen_count / cf_scan_u64)
+ * are computed in registers and probed, never written; candidates are
+ * {D position, I colex id}.  Replaces the igen chunks x sorted D chunks join of
+ * gpu/mitm_gpu_mstar_driver.py:241-262 when the I side is the large one. */
+int cf_bgen_probe(int r, int n, uint64_t F, const void* pool, const uint64_t* key, const uint64_t* id,
+                  const uint64_t* offs, const uint32_t* xs, uint64_t c0, uint64_t cc, const void* tab, int bbits,
+                  int fbits, void* pairs, uint32_t max_pairs, uint32_t* npairs, uint32_t* err, void* stream);
+
 /* ---- batched portfolio --------------------------------------------------- */
 
 /* Many moduli (radius 1..cf_batch_max_r() each, mixed) joined by persistent

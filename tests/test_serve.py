@@ -1,0 +1,85 @@
+"""Serving loop host logic on the CPU: footprint upper bounds and admission."""
+import itertools
+import math
+import random
+import threading
+import time
+import types
+
+from carmichael_frontier_b200 import serve, workloads as W
+from carmichael_frontier_b200.serve import Server, count_ge_upper, count_lt_upper
+
+
+def test_count_bounds_are_upper_bounds():
+    rng = random.Random(3)
+    for _ in range(30):
+        M = W.draw_modulus(rng.randrange(10 ** 6))
+        P = W.eligible_pool(M, 10 ** 5)[: rng.randint(6, 22)]
+        r = rng.randint(1, min(5, len(P)))
+        prods = [math.prod(c) for c in itertools.combinations(P, r)]
+        lo = rng.choice(prods)
+        hi = rng.choice(prods)
+        ge = sum(1 for x in prods if x >= lo)
+        lt = sum(1 for x in prods if x < hi)
+        ub_ge, ub_lt = count_ge_upper(P, r, lo), count_lt_upper(P, r, hi)
+        assert ge <= ub_ge <= math.comb(len(P), r)
+        assert lt <= ub_lt <= math.comb(len(P), r)
+
+
+def _fake_server(budget, slots, log):
+    active = []
+    lock = threading.Lock()
+
+    def solve(state, inst):
+        with lock:
+            active.append(inst)
+            log.append(("start", inst.rid, [a.rid for a in active], sum(a.need for a in active)))
+        time.sleep(inst.dt)
+        with lock:
+            active.remove(inst)
+        return types.SimpleNamespace(hits=[], rid=inst.rid)
+
+    return Server(slots=slots, budget=budget, solve_fn=solve).start()
+
+
+def test_admission_respects_budget_and_runs_oversize_alone():
+    rng = random.Random(1)
+    log = []
+    srv = _fake_server(budget=100, slots=4, log=log)
+    reqs = [types.SimpleNamespace(rid=i, need=rng.choice([10, 30, 60, 150]), dt=rng.uniform(0.001, 0.01))
+            for i in range(60)]
+    ts = [srv.submit(q) for q in reqs]
+    for t in ts:
+        assert t.done.wait(20)
+    srv.stop()
+    assert all(t.error is None and t.result.rid == t.inst.rid for t in ts)
+    for _tag, rid, running, used in log:
+        need = reqs[rid].need
+        if need > 100:
+            assert running == [rid]            # larger than the budget: alone
+        else:
+            assert used <= 100 and len(running) <= 4
+    assert max(len(e[2]) for e in log) > 1      # requests did overlap
+    assert srv.adm.peak <= 100 and srv.adm.used == 0
+
+
+def test_no_starvation_of_large_requests():
+    log = []
+    srv = _fake_server(budget=100, slots=4, log=log)
+    big = types.SimpleNamespace(rid=0, need=90, dt=0.001)
+    smalls = [types.SimpleNamespace(rid=i, need=20, dt=0.02) for i in range(1, 40)]
+    ts = [srv.submit(smalls[0]), srv.submit(big)] + [srv.submit(q) for q in smalls[1:]]
+    for t in ts:
+        assert t.done.wait(30)
+    srv.stop()
+    order = [e[1] for e in log]
+    assert order.index(0) <= srv.adm.max_bypass + 2
+
+
+def test_poisson_stats_shape():
+    srv = _fake_server(budget=1000, slots=2, log=[])
+    reqs = [types.SimpleNamespace(rid=i, need=1, dt=0.002) for i in range(20)]
+    st, ts = serve.run_poisson(srv, reqs, rate=500.0, seed=2)
+    srv.stop()
+    assert st["requests"] == 20 and st["errors"] == 0
+    assert st["p50_ms"] <= st["p99_ms"] and st["throughput_rps"] > 0
