@@ -49,6 +49,14 @@ def parse_args():
     ap.add_argument("--strategy", choices=("fused", "partition"), default="fused")
     ap.add_argument("--case", type=int, default=None,
                     help="profile a single seeded modulus (every step solves config-2 seed CASE)")
+    ap.add_argument("--workload", choices=("single", "portfolio", "serving"), default="single",
+                    help="single: the headline k=64 r=5 line; portfolio / serving: their own lines")
+    ap.add_argument("--moduli", type=int, default=1024)
+    ap.add_argument("--i-limit", type=int, default=1 << 24)
+    ap.add_argument("--plain-moduli", type=int, default=128)
+    ap.add_argument("--requests", type=int, default=120)
+    ap.add_argument("--loads", default="3,5,8", help="offered requests/s of the serving runs")
+    ap.add_argument("--slots", type=int, default=4)
     return ap.parse_args()
 
 
@@ -334,8 +342,11 @@ def run_ours(args):
 
     if rank == 0:
         kern = {k: {"ms_total": 1e3 * v} for k, v in kt.items()}
+        # the table is built on the smaller side and probed by the larger one
+        n_build = sum(min(math.comb(len(w.B0), w.r), math.comb(len(w.INS), w.r)) for w in timed)
+        n_probe = sum(max(math.comb(len(w.B0), w.r), math.comb(len(w.INS), w.r)) for w in timed)
         if kt["probe"] > 0:
-            kern["probe"]["records_per_s"] = sum(math.comb(len(w.INS), w.r) for w in timed) / kt["probe"]
+            kern["probe"]["records_per_s"] = n_probe / kt["probe"]
         n_d = sum(math.comb(len(w.B0), w.r) for w in timed)
         n_i = sum(math.comb(len(w.INS), w.r) for w in timed)
         if kt["gen_I"] > 0:
@@ -343,7 +354,7 @@ def run_ours(args):
         if kt["join"] > 0:
             kern["join"]["GB_s"] = 16 * (n_i + n_d) / kt["join"] / 1e9
         if kt["gen_D"] > 0:
-            kern["gen_D"]["GB_s"] = 16 * n_d / kt["gen_D"] / 1e9
+            kern["gen_D"]["GB_s"] = 16 * (n_build if args.strategy == "fused" else n_d) / kt["gen_D"] / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
@@ -358,10 +369,11 @@ def run_ours(args):
                          "peak_source": peak_src},
             "strategy": solver.tuning.strategy,
             "kernels": kern,
-            "l2_probe": ({"achieved_probes_per_s": sum(math.comb(len(w.INS), w.r) for w in timed) / kt["probe"],
+            "l2_probe": ({"achieved_probes_per_s": n_probe / kt["probe"],
                           "ceiling_probes_per_s": L2_RANDOM_SECTOR_READS,
-                          "frac": sum(math.comb(len(w.INS), w.r) for w in timed) / kt["probe"] / L2_RANDOM_SECTOR_READS,
-                          "note": "one 32-byte L2 sector read per I record; ceiling = random 32-B loads/s measured on this B200"}
+                          "frac": n_probe / kt["probe"] / L2_RANDOM_SECTOR_READS,
+                          "note": "one 32-byte L2 sector read per probing record; ceiling = random 32-B loads/s "
+                                  "measured on this B200"}
                          if kt["probe"] > 0 else None),
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // max(1, len(timed)),
@@ -376,10 +388,155 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ portfolio (batched vs per-modulus)
+def run_portfolio(args):
+    """Seeded 1024-modulus portfolio (k=64, pools 120..400, r in {4,5,6}, B=10^148); every
+    modulus joined over its full D side and the first --i-limit I ranks (a bounded sample:
+    the unpruned I sides total ~1e14 records).  Forms: batched persistent kernels (CUDA
+    graphs replayed), this library's per-modulus fused solve, and the reference's
+    per-modulus mitm_gpu2 form (generate / sort_side / join_sorted) on the first
+    --plain-moduli moduli."""
+    import torch
+    from carmichael_frontier_b200 import Solver, workloads as W
+    from carmichael_frontier_b200.portfolio import BatchSolver, run_per_modulus, run_plain
+    from carmichael_frontier_b200.solve import Instance
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    lim = args.i_limit
+    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config3(args.moduli)]
+    bs = BatchSolver(dev)
+    t0 = time.perf_counter()
+    prep = bs.prepare(insts, lim)
+    torch.cuda.synchronize(dev)
+    t_prep = time.perf_counter() - t0
+    recs = prep.records
+    clocks = ClockSampler(gpu_uuid(torch, dev))
+    clocks.start()
+    for _ in range(args.warmup):
+        ref = bs.run(prep, graphs=True)
+    torch.cuda.synchronize(dev)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        res = bs.run(prep, graphs=True)
+        torch.cuda.synchronize(dev)
+        times.append(time.perf_counter() - t0)
+    t_b = statistics.median(times)
+    one = Solver(dev)
+    run_per_modulus(insts[:4], i_limit=lim, solver=one)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    per = run_per_modulus(insts, i_limit=lim, solver=one)
+    torch.cuda.synchronize(dev)
+    t_p = time.perf_counter() - t0
+    npl = min(args.plain_moduli, len(insts))
+    run_plain(insts[:1], i_limit=1 << 16, device=dev)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    plain = run_plain(insts[:npl], i_limit=lim, device=dev)
+    torch.cuda.synchronize(dev)
+    t_pl = time.perf_counter() - t0
+    clk = clocks.stop()
+    rec_pl = sum(prep.nD[k] + prep.nI[k] for k in range(npl))
+    same = [(a.residue_pairs, a.pairs, [h.n for h in a.hits]) for a in res] == \
+           [(a.residue_pairs, a.pairs, [h.n for h in a.hits]) for a in per]
+    same_plain = [(a.residue_pairs, sorted(a.pairs), [h.n for h in a.hits]) for a in res[:npl]] == \
+                 [(a.residue_pairs, sorted(a.pairs), [h.n for h in a.hits]) for a in plain]
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            w0 = W.config3(1)[0]
+            n, dt, kind, cores, sample = run_cpu_engine(w0, os.cpu_count() or 1, args.cpu_seconds)
+            cpu = {"value": n / dt, "unit": "records/s", "cores": cores, "kind": kind, "sample": sample,
+                   "moduli_per_s_equiv": (n / dt) / (recs / len(insts))}
+        except Exception as e:
+            cpu = {"value": None, "unit": "records/s", "sample": f"failed: {e}"}
+    line = {"metric": "portfolio moduli solved/s (batched persistent kernels)", "value": len(insts) / t_b,
+            "unit": "moduli/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_b, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64", "data": "synthetic (seeded moduli)",
+            "config": {"workload": "portfolio_1024_k64_r456", "moduli": len(insts), "i_limit": lim,
+                       "records": recs, "batches": len(prep.batches), "prepare_s": t_prep,
+                       "sample": f"full D sides, I ranks [0, {lim}) per modulus"},
+            "forms": {
+                "batched": {"moduli_per_s": len(insts) / t_b, "records_per_s": recs / t_b, "s": t_b,
+                            "graphs": True, "launches_per_batch": 4},
+                "per_modulus_fused": {"moduli_per_s": len(insts) / t_p, "records_per_s": recs / t_p, "s": t_p,
+                                      "same_results": same},
+                "plain_mitm_gpu2": {"moduli": npl, "moduli_per_s": npl / t_pl, "records_per_s": rec_pl / t_pl,
+                                    "s": t_pl, "same_results": same_plain},
+            },
+            "speedup_vs_plain_records": (recs / t_b) / (rec_pl / t_pl),
+            "hits": sum(len(x.hits) for x in res), "residue_pairs": sum(x.residue_pairs for x in res),
+            "cpu_baseline": cpu,
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                       "samples": clk["samples"]}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ serving (continuous batching)
+def run_serving(args):
+    """The first --requests requests of the seeded serving stream (k = 64..100, pools 80..320,
+    r = 3..6, B = prod(B0) * 10^4), Poisson arrivals at three offered loads, served by the
+    continuous-batching loop; the serial form (one request at a time) at the same loads."""
+    import torch
+    from carmichael_frontier_b200 import Solver, Tuning, serve, workloads as W
+    from carmichael_frontier_b200.solve import Instance
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config5_requests(args.requests)]
+    warm = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config5_requests(8, seed=1)]
+    alone = Solver(dev, tuning=Tuning(strategy="auto", max_nodes=1 << 22))
+    for x in warm:
+        alone.solve_instance(x)
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(gpu_uuid(torch, dev))
+    clocks.start()
+    loads = [float(x) for x in args.loads.split(",")]
+    out = {"continuous": [], "serial": []}
+    for rate in loads:
+        srv = serve.Server(dev, slots=args.slots, strategy="auto").start()
+        st, _ = serve.run_poisson(srv, insts, rate=rate, seed=7)
+        srv.stop()
+        out["continuous"].append(st)
+        torch.cuda.empty_cache()
+
+        def one(x):
+            r = alone.solve_instance(x)
+            torch.cuda.synchronize(dev)
+            alone._bufs.clear()
+            return r
+        st2, _ = serve.run_serial(one, insts, rate=rate, seed=7)
+        out["serial"].append(st2)
+    clk = clocks.stop()
+    mid = out["continuous"][len(loads) // 2]
+    line = {"metric": "serving p50/p99 solve latency (ms) and requests/s", "value": mid["p99_ms"], "unit": "ms (p99)",
+            "n_gpus": 1, "steps": len(insts), "warmup": len(warm), "ms_per_step": mid["mean_ms"],
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded request stream)",
+            "config": {"workload": "serving_k64-100_r3-6", "requests": len(insts), "slots": args.slots,
+                       "offered_rps": loads, "arrivals": "Poisson, seed 7",
+                       "sample": f"first {len(insts)} of the 10,000-request stream"},
+            "continuous": out["continuous"], "serial": out["serial"],
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                       "samples": clk["samples"]}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "portfolio":
+        run_portfolio(args)
+    elif args.workload == "serving":
+        run_serving(args)
     else:
         run_ours(args)
 

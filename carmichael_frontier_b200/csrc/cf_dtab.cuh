@@ -4,9 +4,10 @@
 // 2^bbits buckets of 16 slots.  A bucket's sixteen 16-bit fingerprints (0 =
 // empty) fill one 32-byte sector -- the only data a probe reads; a side array
 // holds, per slot, a second 32-bit fingerprint and the D rank (read only when
-// the 16-bit fingerprint matches); a fill counter per bucket hands out slots in
-// order, so "bucket full" is a test of the last slot, and a full bucket
-// continues into the next one.  An optional blocked Bloom filter is a first
+// the 16-bit fingerprint matches); slots are claimed in order by compare-and-swap
+// on the fingerprint words, so "bucket full" is a test of the last slot, and a
+// full bucket continues into the next one.  (The per-bucket fill counters of the
+// layout are no longer used by the build.)  An optional blocked Bloom filter is a first
 // level for tables too large for L2.
 #pragma once
 #include "cf_abi_internal.h"
@@ -82,8 +83,13 @@ __device__ __forceinline__ u32 cf_word8(uint4 a, uint4 b, u32 w) {
 }
 
 // Insert a residue (X, x2) with its rank; returns false if every bucket was full.
-// A slot is claimed with one atomicAdd on the bucket's fill counter; the claimed
-// 16-bit half is then set with atomicOr (its word is shared with a neighbour slot).
+// A slot is claimed with one compare-and-swap on the fingerprint word holding the
+// bucket's first empty 16-bit half: slots are only ever set, and a claim always
+// takes the first empty slot it sees, so the occupied slots of a bucket are a
+// prefix and "bucket full" is "last slot occupied".  A failed swap means another
+// thread filled that word first; the claim retries with the value it returned
+// (at most 16 slots per bucket, so the retries are bounded).  The side entry is
+// written after the claim; probes run only after the build has completed.
 __device__ __forceinline__ bool dtab_insert(const DTab& t, u64 X, u32 x2, u64 rank) {
   if (t.bloom) {
     const CfBloomKey bk = cf_bloom_key(X, x2, t.fbits);
@@ -96,14 +102,36 @@ __device__ __forceinline__ bool dtab_insert(const DTab& t, u64 X, u32 x2, u64 ra
   const u32 f16 = fk.f16, f32 = fk.f32;
   u64 b = fk.bucket;
   for (u64 tries = 0; tries < t.nb; ++tries) {
-    const u32 s = atomicAdd(&t.fill[b], 1u);
-    if (s < 16u) {
-      uint2 sd;
-      sd.x = f32;
-      sd.y = (u32)(rank - t.rank0);
-      t.side[b * 16 + s] = sd;
-      atomicOr(&t.fpw[b * 8 + (s >> 1)], f16 << (16 * (s & 1)));
-      return true;
+    u32* row = t.fpw + b * 8;
+    const uint4 r0 = __ldcg((const uint4*)row), r1 = __ldcg((const uint4*)row + 1);
+    const u32 w8[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+    int w = 0;                                     // first word with an empty half
+#pragma unroll
+    for (int i = 7; i >= 0; --i)
+      if ((w8[i] & 0xffff0000u) == 0u) w = i;
+    if ((w8[7] & 0xffff0000u) != 0u) w = 8;        // last slot occupied: bucket full
+    u32 cur = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) cur = (w == i) ? w8[i] : cur;
+    // each pass either claims a slot, sees one more slot filled by another thread,
+    // or moves to the next word: at most 16 + 8 passes per bucket
+    for (int spin = 0; w < 8 && spin < 32; ++spin) {
+      if ((cur & 0xffff0000u) != 0u) {             // this word is full: move to the next one
+        ++w;
+        cur = (w < 8) ? __ldcg(&row[w]) : 0u;
+        continue;
+      }
+      const bool lo_free = (cur & 0xffffu) == 0u;
+      const u32 nv = lo_free ? (cur | f16) : (cur | (f16 << 16));
+      const u32 prev = atomicCAS(&row[w], cur, nv);
+      if (prev == cur) {
+        uint2 sd;
+        sd.x = f32;
+        sd.y = (u32)(rank - t.rank0);
+        t.side[b * 16 + 2 * w + (lo_free ? 0 : 1)] = sd;
+        return true;
+      }
+      cur = prev;
     }
     b = (b + 1) & (t.nb - 1);
   }

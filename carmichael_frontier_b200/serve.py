@@ -100,8 +100,10 @@ def footprint(inst: Instance, tu: Tuning) -> dict:
         nD = count_ge_upper(inst.B0, r, Dmin)
         nI = count_lt_upper(inst.INS, r, Icap)
         frontier = 40 * min(max_nodes, max(nD, nI))           # one frontier block of nodes
-        # table on the I leaves (written) or on the D records (I leaves probed): either may be chosen
-        side = max(16 * nI + _dtab_bytes(nI, tu), _dtab_bytes(nD, tu))
+        # table on the I leaves (written only when they are fewer than the D records, so at
+        # most min(nI, nD) of them) or on the D records (I leaves probed, never written)
+        m = min(nI, nD)
+        side = max(16 * m + _dtab_bytes(m, tu), _dtab_bytes(nD, tu))
         return dict(bytes=fixed + 16 * nD + frontier * 2 + side, strategy="bounded", nD=nD, nI=nI)
     small = min(math.comb(nB, r), math.comb(nI_full, r))
     tails = 16 * (math.comb(nB, 2) + math.comb(nI_full, 2))

@@ -78,7 +78,7 @@ class Tuning:
                                     # where the bound prunes, else fused
     dtab_load: float = 5.0          # fused: minimum average D records per 16-slot bucket (up to 2x this)
     fused_grid: int = 0             # fused probe CTAs (0 = one per 16384 records)
-    l2_table_bytes: int = 48 << 20  # fingerprint arrays above this get a Bloom-filter first level
+    l2_table_bytes: int = 72 << 20  # fingerprint arrays above this get a Bloom-filter first level
     max_fbits: int = 21             # Bloom filter at most 2^21 blocks of 32 bytes (64 MB)
     max_nodes: int = 1 << 27        # bounded strategy: frontier nodes per block of first indices
 
@@ -87,12 +87,15 @@ def dtab_shape(nD: int, tu: Tuning) -> tuple[int, int]:
     """(bbits, fbits) of the D table for nD records: 2^bbits buckets of 16 slots at an
     average load between dtab_load and 2*dtab_load (never above 12), and a Bloom-filter
     first level (about 8 bits per D record, at most 2^max_fbits blocks of 32 bytes) when
-    the fingerprint array would not stay in L2."""
+    the fingerprint array would not stay in L2 -- and none when that cap leaves fewer than
+    6 bits per record."""
     bbits = max(4, int(math.floor(math.log2(max(nD / tu.dtab_load, 2.0)))),
                 math.ceil(math.log2(max(nD / 12.0, 2.0))))
     fbits = 0
     if (1 << bbits) * 32 > tu.l2_table_bytes:
         fbits = min(tu.max_fbits, max(4, math.ceil(math.log2(max(nD / 32.0, 2.0)))))
+        if (256 << fbits) < 6 * nD:      # under 6 filter bits per record the filter passes nearly everything
+            fbits = 0
     return bbits, fbits
 
 
