@@ -234,6 +234,20 @@ int cf_bgen_probe(int r, int n, uint64_t F, const void* pool, const uint64_t* ke
                   const uint64_t* offs, const uint32_t* xs, uint64_t c0, uint64_t cc, const void* tab, int bbits,
                   int fbits, void* pairs, uint32_t max_pairs, uint32_t* npairs, uint32_t* err, void* stream);
 
+/* ---- streamed (out-of-core) join --------------------------------------------- */
+
+/* Range partitioning of canonical {key, id} records (key < M) for sides larger than
+ * HBM: partition p = floor(key * 2^pbits / M) (1 <= pbits <= 12), so equal residues
+ * meet in the same partition and partitions can be joined one at a time.
+ * cf_part_hist adds the partition sizes of keys[0..n) to counts[2^pbits];
+ * cf_part_scatter writes each record to out[cursor[p]++] (cursor = the partitions'
+ * start offsets from a cf_part_hist of the same keys; order inside a partition is
+ * not kept).  Replaces the reference's D chunks x I chunks streaming
+ * (gpu/mitm_gpu_mstar_driver.py:100-118, 241-262) for sides that do not fit. */
+int cf_part_hist(const uint64_t* keys, uint64_t n, uint64_t M, int pbits, uint64_t* counts, void* stream);
+int cf_part_scatter(const uint64_t* keys, const uint64_t* ids, uint64_t n, uint64_t M, int pbits, uint64_t* cursor,
+                    uint64_t* okeys, uint64_t* oids, void* stream);
+
 /* ---- batched portfolio --------------------------------------------------- */
 
 /* Many moduli (radius 1..cf_batch_max_r() each, mixed) joined by persistent
