@@ -49,8 +49,9 @@ def parse_args():
     ap.add_argument("--strategy", choices=("fused", "partition"), default="fused")
     ap.add_argument("--case", type=int, default=None,
                     help="profile a single seeded modulus (every step solves config-2 seed CASE)")
-    ap.add_argument("--workload", choices=("single", "portfolio", "serving"), default="single",
-                    help="single: the headline k=64 r=5 line; portfolio / serving: their own lines")
+    ap.add_argument("--workload", choices=("single", "portfolio", "serving", "large"), default="single",
+                    help="single: the headline k=64 r=5 line; portfolio / serving / large: their own lines")
+    ap.add_argument("--stream-i-limit", type=int, default=1 << 29)
     ap.add_argument("--moduli", type=int, default=1024)
     ap.add_argument("--i-limit", type=int, default=1 << 24)
     ap.add_argument("--plain-moduli", type=int, default=128)
@@ -529,6 +530,65 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ large radius (r = 7, pool 160)
+def run_large(args):
+    """k=64, one seeded modulus, pool capped at 160 primes, r = 7: D = C(64,7) = 6.2e8,
+    I = C(96,7) = 1.19e10 records (191 GB as 16-byte records).  Two forms:
+    fused   the whole instance: table on the D side, every I record generated and probed
+            in registers (nothing materialised, fits in HBM);
+    streamed both sides spilled as 16-byte records to pinned host memory, partitioned by the
+            top 8 bits of the residue, streamed back partition by partition and joined --
+            on the I ranks [0, --stream-i-limit) (a bounded sample: the full I side is 191 GB
+            of host memory)."""
+    import torch
+    from carmichael_frontier_b200 import Solver, Tuning, workloads as W
+    from carmichael_frontier_b200.solve import Instance
+    from carmichael_frontier_b200.streamed import streamed_solve
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    w = W.config4()
+    inst = Instance.build(w.M, w.Q, w.B0, w.r, w.B)
+    s = Solver(dev, tuning=Tuning(strategy="fused"))
+    clocks = ClockSampler(gpu_uuid(torch, dev))
+    clocks.start()
+    res = s.solve_instance(inst, timed=True)           # warm-up: tables and buffers
+    times = []
+    for _ in range(max(1, args.steps)):
+        marks = []
+        r1 = s.solve_instance(inst, timed=True, marks=marks)
+        times.append(r1.device_ms / 1e3)
+    t_f = statistics.median(times)
+    kt = {}
+    for (t0, a), (tag, b) in zip(marks, marks[1:]):
+        kt[tag] = kt.get(tag, 0.0) + a.elapsed_time(b) / 1e3
+    lim = args.stream_i_limit
+    torch.cuda.empty_cache()
+    sres, st = streamed_solve(inst, pbits=8, i_limit=lim, device=dev)
+    clk = clocks.stop()
+    n_sample = sres.n_D + sres.n_I
+    line = {"metric": "large-radius join records/s (k=64, pool 160, r=7)", "value": r1.records / t_f,
+            "unit": "records/s", "n_gpus": 1, "steps": len(times), "warmup": 1, "ms_per_step": 1e3 * t_f,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded modulus)",
+            "config": {"workload": "k64_pool160_r7", "modulus": w.name, "n_D": r1.n_D, "n_I": r1.n_I,
+                       "materialised_I_bytes": 16 * r1.n_I},
+            "fused": {"records_per_s": r1.records / t_f, "s": t_f, "plan": {k: r1.plan.get(k) for k in
+                                                                            ("bbits", "fbits", "swap")},
+                      "kernel_s": kt, "residue_pairs": r1.residue_pairs, "hits": len(r1.hits)},
+            "streamed": {"i_limit": lim, "records": n_sample, "records_per_s": n_sample / (st["spill_s"] + st["join_s"]),
+                         "spill_s": st["spill_s"], "join_s": st["join_s"], "host_bytes": st["host_bytes"],
+                         "pin_alloc_s": st["pin_alloc_s"],
+                         "d2h_GB_s": st["d2h_bytes"] / st["spill_s"] / 1e9,
+                         "h2d_GB_s": st["h2d_bytes"] / st["join_s"] / 1e9,
+                         "residue_pairs": sres.residue_pairs, "launches": sres.launches},
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                       "samples": clk["samples"]}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -537,6 +597,8 @@ def main():
         run_portfolio(args)
     elif args.workload == "serving":
         run_serving(args)
+    elif args.workload == "large":
+        run_large(args)
     else:
         run_ours(args)
 

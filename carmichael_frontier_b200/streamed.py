@@ -93,9 +93,18 @@ class StreamedJoin:
                    "cf_gen_subsets")
         self.launches += 1
 
-    def spill(self, primes, r: int, M: int, mult: int, lo: int = 0, hi: int | None = None) -> HostSide:
+    def host_buffers(self, n: int):
+        """Pinned host arrays for n records (keys, ids): allocate once, reuse across spills
+        (pinning host memory runs at a few GB/s, far slower than the copies)."""
+        import torch
+        return (torch.empty(max(n, 1), dtype=torch.int64, pin_memory=True),
+                torch.empty(max(n, 1), dtype=torch.int64, pin_memory=True))
+
+    def spill(self, primes, r: int, M: int, mult: int, lo: int = 0, hi: int | None = None,
+              out=None) -> HostSide:
         """Generate the records of ranks [lo, hi) on the device and leave them, grouped by
-        residue range, in pinned host memory."""
+        residue range, in pinned host memory (`out`: arrays from host_buffers, else
+        allocated here)."""
         torch, lib, dp = self.torch, self.lib, _lib.ptr
         n = len(primes)
         total = ncomb(n, r) if hi is None else hi
@@ -117,8 +126,10 @@ class StreamedJoin:
         cnts = counts.cpu().numpy()
         off = np.zeros(P + 1, dtype=np.int64)
         off[1:] = np.cumsum(cnts)
-        hk = torch.empty(max(N, 1), dtype=torch.int64, pin_memory=True)
-        hi_ = torch.empty(max(N, 1), dtype=torch.int64, pin_memory=True)
+        if out is not None and out[0].numel() >= N and out[1].numel() >= N:
+            hk, hi_ = out
+        else:
+            hk, hi_ = self.host_buffers(N)
         # pass 2: generate, partition on the device, copy each partition slice to its host
         # offset on the copy stream; two staging sets, so chunk k+1 is generated and
         # partitioned while chunk k is copied out
@@ -272,9 +283,11 @@ def streamed_solve(inst, pbits: int = 8, i_limit: int | None = None, device=None
     nI = ncomb(len(inst.INS), r)
     if i_limit is not None:
         nI = min(nI, int(i_limit))
+    ta = time.perf_counter()
+    dbuf, ibuf = sj.host_buffers(nD), sj.host_buffers(nI)
     t0 = time.perf_counter()
-    D = sj.spill(inst.B0, r, M, 1)
-    I = sj.spill(inst.INS, r, M, inst.P0 % M, 0, nI)
+    D = sj.spill(inst.B0, r, M, 1, out=dbuf)
+    I = sj.spill(inst.INS, r, M, inst.P0 % M, 0, nI, out=ibuf)
     t1 = time.perf_counter()
     cand = sj.join(D, I)
     t2 = time.perf_counter()
@@ -300,6 +313,6 @@ def streamed_solve(inst, pbits: int = 8, i_limit: int | None = None, device=None
     pairs.sort()
     res = SolveResult(hits, nD, nI, len(pairs), len(pairs) - above, above, 0,
                       plan=dict(strategy="streamed", pbits=pbits), pairs=pairs, launches=sj.launches)
-    stats = dict(spill_s=t1 - t0, join_s=t2 - t1, h2d_bytes=sj.h2d_bytes, d2h_bytes=sj.d2h_bytes,
+    stats = dict(spill_s=t1 - t0, join_s=t2 - t1, pin_alloc_s=t0 - ta, h2d_bytes=sj.h2d_bytes, d2h_bytes=sj.d2h_bytes,
                  host_bytes=16 * (D.n + I.n))
     return res, stats
