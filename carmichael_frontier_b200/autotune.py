@@ -1,10 +1,14 @@
-"""Autotuner for the partitioned join's launch parameters.
+"""Autotuners for the launch parameters.
 
-Chooses, per workload class (radius and side sizes), the partition count
-(through the D records per partition), the generator's launch shape (threads
-per CTA x subsets per thread) and the join's CTAs per partition, by timing
-complete device solves with CUDA events on a representative instance.  The
-results are cached in memory and can be saved to / loaded from a JSON file.
+``tune``: per workload class (radius and side sizes) of the partitioned join,
+the partition count (through the D records per partition), the generator's
+launch shape (threads per CTA x subsets per thread) and the join's CTAs per
+partition, by timing complete device solves with CUDA events on a
+representative instance; results cached in memory and optionally in a JSON file.
+
+``tune_batch``: for the batched portfolio kernels, the work-queue ticket size
+(records a warp takes per queue pop) and the persistent grid, by timing whole
+batch runs of a prepared portfolio.
 """
 from __future__ import annotations
 
@@ -60,6 +64,45 @@ def tune(inst: Instance, device=None, reps: int = 3, shapes=None, d_per_part=D_P
             best = (ms, tu)
     if best is None:
         raise RuntimeError("no launch configuration ran")
+    return best[1], rows
+
+
+TICKETS = (2048, 8192, 32768)
+GRID_PER_SM = (0, 2, 4)                 # 0 = one resident wave (the occupancy limit)
+
+
+def tune_batch(prep, device=None, reps: int = 3, tickets=TICKETS, grids=GRID_PER_SM, base=None,
+               verbose: bool = False):
+    """Fastest (ticket, grid) for a prepared portfolio: returns (BatchTuning, rows).  Each
+    candidate re-prepares the portfolio's ticket tables and times `reps` whole runs."""
+    import time
+
+    import torch
+
+    from .portfolio import BatchSolver, BatchTuning
+    sms = torch.cuda.get_device_properties(torch.device(device if device is not None else "cuda")).multi_processor_count
+    rows, best = [], None
+    base = base or BatchTuning()
+    for ticket, g in itertools.product(tickets, grids):
+        tu = BatchTuning(ticket=ticket, grid=g * sms, mem_budget=base.mem_budget, pair_capacity=base.pair_capacity,
+                         dtab=base.dtab)
+        bs = BatchSolver(device, tuning=tu)
+        p2 = bs.prepare(prep.instances, prep.i_limit)
+        bs.run(p2, verify=False)
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            bs.run(p2, verify=False)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        ms = 1e3 * sorted(ts)[len(ts) // 2]
+        rows.append(dict(ticket=ticket, grid=g * sms, ms=ms))
+        if verbose:
+            print(f"  ticket={ticket} grid={g * sms}: {ms:.2f} ms", flush=True)
+        if best is None or ms < best[0]:
+            best = (ms, tu)
+        bs.release(p2)
     return best[1], rows
 
 

@@ -108,3 +108,14 @@ def test_batched_edge_cases(cuda):
     for a, b in zip(res, one):
         assert summary(a) == summary(b)
     assert len(res[3].hits) == 2
+
+
+def test_batch_autotuner_keeps_results(cuda):
+    from carmichael_frontier_b200.autotune import tune_batch
+    insts = small_portfolio(11, 16)
+    bs = BatchSolver(cuda)
+    prep = bs.prepare(insts)
+    ref = [summary(x) for x in bs.run(prep)]
+    tu, rows = tune_batch(prep, cuda, reps=1, tickets=(64, 8192), grids=(0, 2))
+    assert len(rows) == 4 and all(r["ms"] > 0 for r in rows)
+    assert [summary(x) for x in BatchSolver(cuda, tuning=tu).solve(insts)] == ref
