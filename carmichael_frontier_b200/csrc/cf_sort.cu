@@ -22,8 +22,8 @@
 namespace {
 
 constexpr int kSortBlock = 512;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortBlock * kSortItems;  // 8192
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortBlock * kSortItems;  // 4096
 constexpr int kRadix = 256;
 constexpr int kWarps = kSortBlock / 32;
 constexpr u64 kFlagAgg = 1ull << 62;
@@ -73,8 +73,9 @@ __device__ __forceinline__ u32 lanemask_lt() {
 
 constexpr size_t kPassSmem = (size_t)kSortTile * 8 + (size_t)kSortTile + (size_t)kWarps * kRadix * 4;
 
-// One onesweep pass over the digit at bit `shift`.
-__global__ void __launch_bounds__(kSortBlock)
+// One onesweep pass over the digit at bit `shift`.  Two CTAs per SM: each item's
+// digit (9 bits, 0x100 = no item) rides in the top bits of its local offset.
+__global__ void __launch_bounds__(kSortBlock, 2)
 k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __restrict__ kout,
             u64* __restrict__ iout, u64 n, int shift, const u64* __restrict__ gexcl /*[256]*/,
             u64* __restrict__ status /*[tiles][256]*/, u32* __restrict__ ticket, u32* __restrict__ err) {
@@ -95,8 +96,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
   const u64 base = (u64)tile * kSortTile;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   u64 key[kSortItems];
-  u32 loc[kSortItems];
-  u32 dig[kSortItems];
+  u32 loc[kSortItems];                      // local offset (low 16 bits) | digit << 16
   const u32 lt = lanemask_lt();
   u32* wc = s_wc + wid * kRadix;
 #pragma unroll
@@ -105,7 +105,6 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
     const bool valid = e < n;
     key[it] = valid ? kin[e] : 0ull;
     const u32 d = valid ? (u32)((key[it] >> shift) & 0xff) : 0x100u;
-    dig[it] = d;
     const u32 peers = __match_any_sync(0xffffffffu, d);
     u32 cnt = 0;
     if (valid) cnt = wc[d];
@@ -113,7 +112,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
     const u32 r = __popc(peers & lt);
     if (valid && r == 0) wc[d] = cnt + __popc(peers);
     __syncwarp();
-    loc[it] = cnt + r;
+    loc[it] = (cnt + r) | (d << 16);
   }
   __syncthreads();
   if (threadIdx.x < kRadix) {                 // per digit: exclusive over warps, tile total
@@ -166,10 +165,12 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
   __syncthreads();
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
-    if (dig[it] < 0x100u) {
-      loc[it] += s_doff[dig[it]] + wc[dig[it]];
-      s_buf[loc[it]] = key[it];
-      s_dj[loc[it]] = (unsigned char)dig[it];
+    const u32 d = loc[it] >> 16;
+    if (d < 0x100u) {
+      const u32 l = (loc[it] & 0xffffu) + s_doff[d] + wc[d];
+      loc[it] = l | (d << 16);
+      s_buf[l] = key[it];
+      s_dj[l] = (unsigned char)d;
     }
   }
   __syncthreads();
@@ -182,9 +183,9 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
   __syncthreads();
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
-    if (dig[it] < 0x100u) {
+    if ((loc[it] >> 16) < 0x100u) {
       const u64 e = base + (u64)wid * 32 * kSortItems + (u64)it * 32 + lane;
-      s_buf[loc[it]] = iin[e];
+      s_buf[loc[it] & 0xffffu] = iin[e];
     }
   }
   __syncthreads();

@@ -1,7 +1,9 @@
-"""Measured ceilings on the running GPU (random L2 sector reads, 64-bit Montgomery products).
+"""Measured ceilings on the running GPU (random L2 sector reads, 64-bit Montgomery products)
+and the rate of the LSD radix sort (the materialised join's sort_side).
 
-    python -m carmichael_frontier_b200.micro
-prints one JSON line; bench.py quotes the L2 figure as the fused probe's ceiling.
+    python -m carmichael_frontier_b200.micro            # ceilings, one JSON line
+    python -m carmichael_frontier_b200.micro sort N     # cf_sort_pairs on N random 62-bit keys
+bench.py quotes the L2 figure as the fused probe's ceiling.
 """
 from __future__ import annotations
 
@@ -51,7 +53,39 @@ def montgomery_products(iters: int = 4096, reps: int = 3) -> float:
     return best
 
 
+def sort_rate(n: int, key_bits: int = 62, reps: int = 3) -> dict:
+    """cf_sort_pairs on n random (key, id) records: records/s and the HBM bytes per second
+    of its passes (each 8-bit digit pass reads and writes 16 bytes per record)."""
+    import torch
+    lib = _lib.load()
+    g = torch.Generator(device="cuda").manual_seed(7)
+    k0 = torch.randint(0, 1 << key_bits, (n,), dtype=torch.int64, device="cuda", generator=g)
+    keys, ids = torch.empty_like(k0), torch.arange(n, dtype=torch.int64, device="cuda")
+    nb = lib.cf_sort_tmp_bytes(n)
+    tmp = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    sh = torch.cuda.current_stream().cuda_stream
+    best = None
+    for _ in range(reps + 1):
+        keys.copy_(k0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.check(lib.cf_sort_pairs(keys.data_ptr(), ids.data_ptr(), n, key_bits, tmp.data_ptr(), nb, sh), "sort")
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3
+        best = t if best is None else min(best, t)
+    assert bool((keys[1:] >= keys[:-1]).all())
+    passes = (key_bits + 7) // 8
+    return {"n": n, "s": best, "records_per_s": n / best, "passes": passes,
+            "GB_s": (32 * passes + 8) * n / best / 1e9}     # passes + one histogram read of the keys
+
+
 def main() -> None:
+    import sys
+    if len(sys.argv) > 2 and sys.argv[1] == "sort":
+        print(json.dumps(sort_rate(int(sys.argv[2]))))
+        return
     out = {"l2_random_32B_reads_per_s": {mb: l2_random_reads(mb) for mb in (8, 32, 64)},
            "hbm_random_32B_reads_per_s": l2_random_reads(4096, iters=256),
            "montgomery64_products_per_s": montgomery_products()}
