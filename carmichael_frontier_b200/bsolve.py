@@ -112,21 +112,31 @@ class BoundedSolve:
             pv = pairs[: npairs * 16].cpu().numpy().view(np.uint64).reshape(npairs, 2).copy() if npairs else None
             return pv, maxp
 
+    def join(self, B0, INS, r: int, M: int, P0: int, Icap: int, Dmin: int, split=None, hmax=None):
+        """Equal-residue pairs of the filtered sides: D = r-subsets of B0 with prod >= Dmin,
+        I = r-subsets of INS with prod < Icap and at most hmax primes above split.
+        Returns (pairs as (D index tuple, I index tuple), nD, nI, plan)."""
+        inst = _Sides(list(B0), list(INS), r, M, P0)
+        return self._join(inst, Icap, Dmin, split, hmax)
+
     def solve(self, inst, verify: bool = True):
-        from .solve import SolveResult
+        Icap, Dmin = caps(inst)
+        pairs, nD, nI, plan = self._join(inst, Icap, Dmin, None, None)
+        return self._finish(inst, pairs, nD, nI, plan, verify)
+
+    def _join(self, inst, Icap, Dmin, split, hmax):
         torch, lib, dp = self.torch, self.lib, _lib.ptr
         r, M = inst.r, inst.M
-        Icap, Dmin = caps(inst)
         plan = dict(strategy="bounded", Icap=Icap, Dmin=Dmin)
         self.misc = self.s._buf("bctr", 64)[:64].view(torch.int32)
         sh = self.s._sh()
         Dk, Did, nD = self.gen.generate_D(inst.B0, r, M, Dmin, bitmask=2)
-        poolI, blocks = self.gen.frontiers_I(inst.INS, r, M, inst.P0, Icap)
+        poolI, blocks = self.gen.frontiers_I(inst.INS, r, M, inst.P0, Icap, split, hmax)
         blocks = iter(blocks)
         first = next(blocks, None)
         if nD == 0 or first is None:
             nI = sum(b["total"] for b in ([first] if first else []) + list(blocks))
-            return SolveResult([], nD, nI, 0, 0, 0, 0, plan=plan)
+            return [], nD, nI, plan
         second = next(blocks, None)
         maxp = self.s.tuning.pair_capacity
         cands = []                         # (D position, I colex id) arrays
@@ -167,26 +177,29 @@ class BoundedSolve:
                                           dp(self.misc), dp(self.misc) + 4, sh), "cf_bgen_probe"), maxp)
                     if pv is not None:
                         cands.append(pv)
-        return self._finish(inst, Dk, Did, cands, nD, nI, plan, verify)
-
-    def _finish(self, inst, Dk, Did, cands, nD, nI, plan, verify):
-        from .solve import Hit, SolveResult
-        torch = self.torch
-        r, M = inst.r, inst.M
-        hits, pairs_out, above, rejected, screened = [], [], 0, 0, 0
+        pairs = []
         if cands:
             pv = np.concatenate(cands)
             dpos = torch.from_numpy(pv[:, 0].astype(np.int64)).to(self.s.device)
             dk = Dk.view(torch.int64)[dpos].cpu().numpy().view(np.uint64)
             di = Did.view(torch.int64)[dpos].cpu().numpy().view(np.uint64)
-            B0, INS = inst.B0, inst.INS
             P0m = inst.P0 % M
             for j in range(len(pv)):
-                ii = unrank_colex(int(pv[j, 1]), r, len(INS))
-                I = tuple(INS[x] for x in ii)
-                if (P0m * math.prod(I)) % M != int(dk[j]):
+                ii = unrank_colex(int(pv[j, 1]), r, len(inst.INS))
+                if (P0m * math.prod(inst.INS[x] for x in ii)) % M != int(dk[j]):
                     continue                   # fingerprint collision, not an equal-residue pair
-                D = tuple(B0[x] for x in unrank_colex(int(di[j]), r, len(B0)))
+                pairs.append((unrank_colex(int(di[j]), r, len(inst.B0)), ii))
+        return pairs, nD, nI, plan
+
+    def _finish(self, inst, pairs, nD, nI, plan, verify):
+        from .solve import Hit, SolveResult
+        r, M = inst.r, inst.M
+        hits, pairs_out, above, rejected, screened = [], [], 0, 0, 0
+        if pairs:
+            B0, INS = inst.B0, inst.INS
+            for di_, ii_ in pairs:
+                D = tuple(B0[x] for x in di_)
+                I = tuple(INS[x] for x in ii_)
                 pairs_out.append((D, I))
                 dset = set(D)
                 fac = tuple(sorted([p for p in B0 if p not in dset] + list(I)))
@@ -207,6 +220,13 @@ class BoundedSolve:
         pairs_out.sort()
         return SolveResult(hits, nD, nI, len(pairs_out), screened, above, rejected, plan=plan, pairs=pairs_out,
                            launches=self.gen.launches)
+
+
+class _Sides:
+    """The fields of an instance the join needs (base, insertion pool, radius, modulus, P0)."""
+
+    def __init__(self, B0, INS, r, M, P0):
+        self.B0, self.INS, self.r, self.M, self.P0 = B0, INS, r, M, P0
 
 
 def _chain(head, rest):

@@ -1,0 +1,123 @@
+"""Drop-in instance functions for the reference's GPU driver (gpu/mitm_gpu_mstar_driver.py).
+
+The driver's control plane -- pool construction, bases, radius loop, h-strata
+(hmax_for), checkpoints, the incumbent and its oracle -- stays the reference's.
+What it calls per instance is replaced:
+
+  build_D(B0, M, r, Dmin)        -> (sorted D chunks, nD)          (:100-118)
+  run_instance(tag, B0, INS, r, hmax, ...) -> bool                  (:184-286)
+
+``run_instance`` applies the driver's exact bounds for the current incumbent U
+(Icap exclusive, Dmin, the per-radius insertion cap), joins the filtered sides
+on the GPU (csrc/cf_bgen.cu producers, a record table of the D side probed by
+the I leaves in registers), re-checks every pair in exact integers as the driver
+does (n = P0 * prod(I) / prod(D) < U), hands each completion below U to the
+driver's ``consider`` and logs the driver's instance line -- the format
+gpu/verify_family_coverage.py reads (" r=<r> ", "dfilter", no "INCOMPLETE").
+"""
+from __future__ import annotations
+
+import math
+import time
+
+from .bounded import generator
+from .tables import unrank_colex
+
+
+def instance_bounds(B0, INS, r: int, U: int):
+    """The driver's bounds for radius r below U (gpu/mitm_gpu_mstar_driver.py:188-205):
+    (Icap exclusive, Dmin, cap_r, affordable INS)."""
+    B0s = sorted(B0)
+    P0 = math.prod(B0)
+    topI = math.prod(INS[-r:])
+    ptb = math.prod(B0s[-r:])
+    Icap = max(1, min(topI + 1, (U * ptb) // P0 + 1))
+    Imin = math.prod(INS[:r])
+    Dmin = (P0 * Imin) // U + 1
+    Imin1 = math.prod(INS[:r - 1])
+    cap_r = (Icap - 1) // Imin1
+    return Icap, Dmin, cap_r, [q for q in INS if q <= cap_r]
+
+
+def build_D(B0, M: int, r: int, Dmin=None, nchunks: int = 1, device=None):
+    """Sorted D-side chunks [(keys, ids), ...] and the record count: the r-subsets of the
+    64-prime base with prod >= Dmin (every subset when Dmin is None), keys prod(D) mod M,
+    ids 6-bit packed indices (an index mask for r > 10), as src/mitm64_ddump emits them;
+    sorted with the drop-in sort_side.  The reference splits D into NCHUNKS_D pieces."""
+    import torch
+
+    from . import mitm_gpu2 as G
+    g = generator(device)
+    k, i, nD = g.generate_D(sorted(B0), r, M, 0 if Dmin is None else int(Dmin), bitmask=1 if r > 10 else 0)
+    if nD == 0:
+        return [], 0
+    chunks = []
+    step = -(-nD // max(1, nchunks))
+    for a in range(0, nD, step):
+        chunks.append(G.sort_side(k[a:a + step], i[a:a + step]))
+    del k, i
+    torch.cuda.empty_cache()
+    return chunks, nD
+
+
+def run_instance(tag, B0, INS, r: int, hmax: int, M: int, U: int, split: int, consider, log,
+                 state: dict | None = None, solver=None) -> bool:
+    """One exchange instance below the bound U, as the driver's run_instance: returns True
+    when the instance is complete.  consider(key, factors, label) receives every completion
+    below U (the driver's incumbent update and oracle); log(str) writes the instance line."""
+    from .solve import Solver, Tuning
+    B0s = sorted(B0)
+    B0set = set(B0)
+    P0 = math.prod(B0)
+    Icap, Dmin, cap_r, INS_aff = instance_bounds(B0, INS, r, U)
+    st = state if state is not None else {}
+    if len(INS_aff) < r:
+        log(f"  {tag} r={r}: affordable pool has {len(INS_aff)} < r primes (cap_r={cap_r}); nothing to search")
+        st["instances"] = st.get("instances", 0) + 1
+        return True
+    s = solver or Solver(tuning=Tuning(strategy="bounded"))
+    if s._bounded is None:
+        from .bsolve import BoundedSolve
+        s._bounded = BoundedSolve(s)
+    t0 = time.time()
+    pairs_idx, nD, nI, plan = s._bounded.join(B0s, INS_aff, r, M, P0, Icap, Dmin, split, hmax)
+    dt = time.time() - t0
+    below = nb = 0
+    rmin = None
+    for di, ii in pairs_idx:
+        D = [B0s[x] for x in di]
+        I = [INS_aff[x] for x in ii]
+        prodD, prodI = math.prod(D), math.prod(I)
+        if prodI >= Icap or (P0 * prodI) % prodD:
+            continue
+        n = P0 * prodI // prodD
+        if n >= U:
+            continue
+        below += 1
+        fac = sorted((B0set - set(D)) | set(I))
+        if consider((M, tag, r, hmax), fac, f"mstar_{tag}_r{r}_h<={hmax}_b200"):
+            nb += 1
+        if rmin is None or n < rmin:
+            rmin = n
+    st["instances"] = st.get("instances", 0) + 1
+    st["pairs_total"] = st.get("pairs_total", 0) + len(pairs_idx)
+    st["completions_below_U"] = st.get("completions_below_U", 0) + below
+    gb = 0.0
+    try:
+        import torch
+        f, tot = torch.cuda.mem_get_info()
+        gb = (tot - f) / 2 ** 30
+    except Exception:
+        pass
+    log(f"  {tag} r={r} h<={hmax} |INS|={len(INS_aff)} dfilter rank b200: D {nD:,} {0.0:.1f}s | I {nI:,} rec "
+        f"{dt:.1f}s pairs={len(pairs_idx)} below_U={below} min_digits={len(str(rmin)) if rmin else None} "
+        f"improved={nb} | GPU {gb:.1f}GB")
+    return True
+
+
+def decode_pair(B0, INS, r: int, d_colex: int, i_colex: int):
+    """(D primes, I primes) of a pair of colex ids (the ids the bounded producers emit)."""
+    B0s = sorted(B0)
+    return (tuple(B0s[x] for x in unrank_colex(d_colex, r, len(B0s))),
+            tuple(INS[x] for x in unrank_colex(i_colex, r, len(INS))))
+
