@@ -41,6 +41,14 @@ struct CfBatchMod {
   u64 nD, i_lo, nI;
   int bbits, fbits;
   int r, swap;
+  // partitioned build (pcap > 0): the table side's records are first scattered
+  // into 2^max(0, bbits - kPlb) bucket ranges, then each range is built in
+  // shared memory and written out whole
+  u32* pkw;          // [nparts * pcap]: bucket within the range << 16 | 16-bit fingerprint
+  uint2* psd;        // [nparts * pcap]: side entries {32-bit fingerprint, rank - rank0}
+  u32* pcnt;         // [nparts]: records scattered into each range (zeroed by the caller)
+  u32 pcap;          // records a range holds (0: this modulus uses the in-place build)
+  u32 pad_;
 };
 
 template <int R, int MODE>
@@ -159,6 +167,283 @@ k_batch(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart /*[n
   if (badarg) atomicOr(err, CF_ERR_BAD_ARG);
 }
 
+// ---------------------------------------------------------------------------
+// Partitioned table build.  Building a table larger than L2 by compare-and-swap
+// in place costs a random DRAM read and write of a fingerprint sector and of a
+// side-entry sector per record.  Instead:
+//   k_bscatter  generates the table side in tiles of kScTile records, ranks each
+//               tile's records by bucket range (2^kPlb buckets) in shared
+//               memory, reserves each range's space with one atomic per tile
+//               and writes the records there (the writes of one range land in
+//               consecutive addresses, so L2 merges them into whole sectors);
+//   k_bplace    takes one bucket range per CTA, claims its records' slots in
+//               shared memory with the same rule as dtab_claim, and writes the
+//               range's fingerprint rows and side entries out in order;
+//   k_bfix      inserts the rare records that ran past the end of their range
+//               (every bucket from theirs to the range's last one full) into
+//               the finished table with dtab_claim, continuing in the next range.
+// The result is a table the probe reads exactly like one built in place: every
+// record sits in the first non-full bucket at or after its own.
+// ---------------------------------------------------------------------------
+constexpr int kPlb = 10;
+constexpr u32 kPartBuckets = 1u << kPlb;
+constexpr int kScBlock = 512;
+constexpr int kScTile = 8192;                 // records per scatter ticket (16 per thread)
+constexpr int kScWarpRecs = kScTile / (kScBlock / 32);
+constexpr u32 kScMaxParts = 4096;             // bucket ranges per modulus (bbits <= kPlb + 12)
+constexpr size_t kScSmem = (size_t)kScTile * 16 + (size_t)kScMaxParts * 4;
+constexpr int kPlBlock = 1024;
+constexpr size_t kPlSmem = (size_t)kPartBuckets * (32 + 128);
+
+struct CfOvf {
+  u32 mod, bucket, f16, f32, rank, pad;
+};
+
+template <int R>
+__device__ __forceinline__ bool scatter_gen(const CfBatchMod& md, u64 first, u32 count, u64* s_pk, uint2* s_sd,
+                                            u32* s_h) {
+  constexpr int B = R < 2 ? R : 2;
+  const bool d_side = md.swap == 0;              // the table holds the smaller side
+  const u64* pool = d_side ? md.poolD : md.poolI;
+  const CfTailEnt* tail = d_side ? md.tailD : md.tailI;
+  const CfPoolHdr* hd = (const CfPoolHdr*)pool;
+  if (!hd->fast32 || hd->tail_b != (u64)B) return false;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const u32 wbeg = (u32)wid * kScWarpRecs;
+  if (wbeg >= count) return true;
+  const u32 wcnt = min((u32)kScWarpRecs, count - wbeg);
+  const int n = (int)hd->n;
+  const u64* binom = pool + cf_pool_off_binom(n);
+  CfArithFast ar;
+  ar.md = cf_mod32_from_hdr(hd);
+  ar.p = nullptr;
+  ar.p64 = pool + cf_pool_off_prime(n);
+  const u64 minv = hd->minv;
+  CfElt32 st;
+  st.X = hd->X0s;
+  st.x2 = hd->x20;
+  const u64 rank0 = d_side ? 0 : md.i_lo;        // enumeration rank of the side's first record
+  CfTailWalker<R, B> w;
+  w.init(rank0 + first + wbeg, n, binom, ar, st, hd->tail_n);
+  const u32 pmask = md.bbits > kPlb ? ~0u : 0u;
+  for (u32 off = 0; off < wcnt; off += 32) {     // uniform across the warp
+    CfElt32 q = st;
+    u64 j;
+    int unused[R - B > 0 ? R - B : 1];
+    w.template step<false>(n, binom, ar, lane, q, j, unused);
+    if (off + (u32)lane < wcnt) {
+      u64 X;
+      u32 x2;
+      cf_fuse_res(q, tail[j], ar.md, minv, X, x2);
+      if (md.bloom) {
+        const CfBloomKey bk = cf_bloom_key(X, x2, md.fbits);
+        u32* blk = md.bloom + (u64)bk.block * 8;
+        atomicOr(blk + bk.w0, bk.m0);
+        atomicOr(blk + bk.w1, bk.m1);
+        atomicOr(blk + bk.w2, bk.m2);
+      }
+      const CfFuseKey fk = cf_fuse_key(X, x2, md.bbits);
+      const u32 p = (fk.bucket >> kPlb) & pmask;
+      const u32 bl = fk.bucket & (kPartBuckets - 1u);
+      const u32 pos = atomicAdd(&s_h[p], 1u);
+      const u32 i = wbeg + off + (u32)lane;
+      s_pk[i] = (u64)((bl << 16) | fk.f16) | ((u64)p << 32) | ((u64)pos << 48);
+      s_sd[i] = make_uint2(fk.f32, (u32)(first + i));
+    }
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(kScBlock, 1)
+k_bscatter(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart, u32 nmod,
+           unsigned long long* __restrict__ queue, u32* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  u64* s_pk = (u64*)smem;                        // [kScTile] range-local key | range << 32 | rank in range << 48
+  uint2* s_sd = (uint2*)(s_pk + kScTile);        // [kScTile] side entries
+  u32* s_h = (u32*)(s_sd + kScTile);             // [kScMaxParts] tile counts, then global offsets
+  __shared__ u64 s_t;
+  const u64 total = tstart[nmod];
+  bool ok = true;
+  for (;;) {
+    if (threadIdx.x == 0) s_t = atomicAdd(queue, 1ull);
+    __syncthreads();
+    const u64 t = s_t;
+    if (t >= total) break;
+    u32 lo = 0, hi = nmod;                       // the modulus with tstart[lo] <= t < tstart[lo + 1]
+    while (hi - lo > 1) {
+      const u32 mid = (lo + hi) >> 1;
+      if (tstart[mid] <= t) lo = mid; else hi = mid;
+    }
+    const CfBatchMod& md = mods[lo];
+    const u64 n_side = md.swap ? md.nI : md.nD;
+    const u64 first = (t - tstart[lo]) * (u64)kScTile;
+    const u32 nparts = md.bbits > kPlb ? 1u << (md.bbits - kPlb) : 1u;
+    const bool good = first < n_side && nparts <= kScMaxParts && md.pcap > 0;
+    const u32 count = good ? (u32)min((u64)kScTile, n_side - first) : 0u;
+    for (u32 p = threadIdx.x; p < nparts && good; p += kScBlock) s_h[p] = 0;
+    __syncthreads();
+    if (good) {
+      bool g = true;
+      switch (md.r) {
+        case 1: g = scatter_gen<1>(md, first, count, s_pk, s_sd, s_h); break;
+        case 2: g = scatter_gen<2>(md, first, count, s_pk, s_sd, s_h); break;
+        case 3: g = scatter_gen<3>(md, first, count, s_pk, s_sd, s_h); break;
+        case 4: g = scatter_gen<4>(md, first, count, s_pk, s_sd, s_h); break;
+        case 5: g = scatter_gen<5>(md, first, count, s_pk, s_sd, s_h); break;
+        case 6: g = scatter_gen<6>(md, first, count, s_pk, s_sd, s_h); break;
+        case 7: g = scatter_gen<7>(md, first, count, s_pk, s_sd, s_h); break;
+        case 8: g = scatter_gen<8>(md, first, count, s_pk, s_sd, s_h); break;
+        default: g = false; break;
+      }
+      ok &= g;
+    } else if (first < n_side) {
+      ok = false;
+    }
+    __syncthreads();
+    for (u32 p = threadIdx.x; p < nparts && good; p += kScBlock) {
+      const u32 c = s_h[p];
+      if (c) s_h[p] = atomicAdd(&md.pcnt[p], c);
+    }
+    __syncthreads();
+    for (u32 i = threadIdx.x; i < count; i += kScBlock) {
+      const u64 pk = s_pk[i];
+      const u32 p = (u32)(pk >> 32) & 0xffffu;
+      const u32 g = s_h[p] + (u32)(pk >> 48);
+      if (g < md.pcap) {
+        const u64 at = (u64)p * md.pcap + g;
+        md.pkw[at] = (u32)pk;
+        md.psd[at] = s_sd[i];
+      } else {
+        atomicOr(err, CF_ERR_PART_OVERFLOW);
+      }
+    }
+    __syncthreads();
+  }
+  if (!ok) atomicOr(err, CF_ERR_BAD_ARG);
+}
+
+// Claim a slot in the shared-memory rows of one bucket range, with dtab_claim's
+// rule; returns false when the claim ran past the range's last bucket (only
+// when the range is not the whole table; a whole table wraps around).
+__device__ __forceinline__ bool place_claim(u32* s_fp, uint2* s_side, u32 nbp, bool whole, u32 b, u32 f16,
+                                            uint2 sd) {
+  for (u32 tries = 0; tries < nbp; ++tries) {
+    volatile u32* row = s_fp + b * 8;
+    int w = 8;
+    u32 cur = 0;
+#pragma unroll
+    for (int i = 7; i >= 0; --i) {
+      const u32 v = row[i];
+      if ((v & 0xffff0000u) == 0u) { w = i; cur = v; }
+    }
+    for (int spin = 0; w < 8 && spin < 32; ++spin) {
+      if ((cur & 0xffff0000u) != 0u) {
+        ++w;
+        cur = (w < 8) ? row[w] : 0u;
+        continue;
+      }
+      const bool lo_free = (cur & 0xffffu) == 0u;
+      const u32 nv = lo_free ? (cur | f16) : (cur | (f16 << 16));
+      const u32 prev = atomicCAS(s_fp + b * 8 + w, cur, nv);
+      if (prev == cur) {
+        s_side[b * 16 + 2 * w + (lo_free ? 0 : 1)] = sd;
+        return true;
+      }
+      cur = prev;
+    }
+    if (++b == nbp) {
+      if (!whole) return false;
+      b = 0;
+    }
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(kPlBlock, 1)
+k_bplace(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart, u32 nmod,
+         unsigned long long* __restrict__ queue, CfOvf* __restrict__ ovf, u32 ovf_cap, u32* __restrict__ novf,
+         u32* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  u32* s_fp = (u32*)smem;                                    // [kPartBuckets * 8]
+  uint2* s_side = (uint2*)(s_fp + kPartBuckets * 8);         // [kPartBuckets * 16]
+  __shared__ u64 s_t;
+  const u64 total = tstart[nmod];
+  for (;;) {
+    if (threadIdx.x == 0) s_t = atomicAdd(queue, 1ull);
+    __syncthreads();
+    const u64 t = s_t;
+    if (t >= total) break;
+    u32 lo = 0, hi = nmod;
+    while (hi - lo > 1) {
+      const u32 mid = (lo + hi) >> 1;
+      if (tstart[mid] <= t) lo = mid; else hi = mid;
+    }
+    const CfBatchMod& md = mods[lo];
+    const u32 p = (u32)(t - tstart[lo]);
+    const u64 nb = 1ull << md.bbits;
+    const u32 nbp = nb < kPartBuckets ? (u32)nb : kPartBuckets;
+    const u64 b0 = (u64)p * nbp;
+    const bool whole = nbp == nb;
+    for (u32 i = threadIdx.x; i < nbp * 8; i += kPlBlock) s_fp[i] = 0;
+    __syncthreads();
+    const u32 cnt = min(md.pcnt[p], md.pcap);
+    const u32* kw = md.pkw + (u64)p * md.pcap;
+    const uint2* sd = md.psd + (u64)p * md.pcap;
+    for (u32 i = threadIdx.x; i < cnt; i += kPlBlock) {
+      const u32 k = kw[i];
+      const uint2 e = sd[i];
+      const u32 b = (k >> 16) & (nbp - 1u);
+      if (!place_claim(s_fp, s_side, nbp, whole, b, k & 0xffffu, e)) {
+        if (whole) {
+          atomicOr(err, CF_ERR_TABLE_FULL);
+          continue;
+        }
+        const u32 o = atomicAdd(novf, 1u);
+        if (o < ovf_cap) {
+          CfOvf v;
+          v.mod = lo;
+          v.bucket = (u32)((b0 + nbp) & (nb - 1));
+          v.f16 = k & 0xffffu;
+          v.f32 = e.x;
+          v.rank = e.y;
+          v.pad = 0;
+          ovf[o] = v;
+        } else {
+          atomicOr(err, CF_ERR_TABLE_FULL);
+        }
+      }
+    }
+    __syncthreads();
+    uint4* gfp = (uint4*)(md.fpw + b0 * 8);
+    const uint4* sfp = (const uint4*)s_fp;
+    for (u32 i = threadIdx.x; i < nbp * 2; i += kPlBlock) gfp[i] = sfp[i];
+    uint4* gsd = (uint4*)(md.side + b0 * 16);
+    const uint4* ssd = (const uint4*)s_side;
+    for (u32 i = threadIdx.x; i < nbp * 8; i += kPlBlock) gsd[i] = ssd[i];
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256)
+k_bfix(const CfBatchMod* __restrict__ mods, const CfOvf* __restrict__ ovf, const u32* __restrict__ novf, u32 ovf_cap,
+       u32* __restrict__ err) {
+  const u32 n = min(*novf, ovf_cap);
+  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const CfOvf v = ovf[i];
+    const CfBatchMod& md = mods[v.mod];
+    DTab tab;
+    tab.nb = 1ull << md.bbits;
+    tab.fpw = md.fpw;
+    tab.side = md.side;
+    tab.fill = md.fill;
+    tab.bloom = md.bloom;
+    tab.rank0 = 0;
+    tab.bbits = md.bbits;
+    tab.fbits = md.fbits;
+    if (!dtab_claim(tab, v.bucket, v.f16, make_uint2(v.f32, v.rank))) atomicOr(err, CF_ERR_TABLE_FULL);
+  }
+}
+
 __global__ void __launch_bounds__(128)
 k_batch_check(const CfBatchMod* __restrict__ mods, const CfPair* __restrict__ pairs, const u32* __restrict__ pmod,
               const u32* __restrict__ npairs, u32 max_pairs, CfPairResult* __restrict__ res) {
@@ -238,5 +523,49 @@ extern "C" int cf_batch_run(int mode, const void* mods, const u64* tstart, u32 n
     k_batch<1><<<grid, kBatchBlock, 0, st>>>((const CfBatchMod*)mods, tstart, nmod, ticket,
                                              (unsigned long long*)queue, (CfPair*)pairs, pmod, max_pairs, npairs, err);
   CF_LAUNCH_CHECK("cf_batch_run");
+  return CF_OK;
+}
+
+extern "C" u32 cf_batch_part_buckets(void) { return kPartBuckets; }
+extern "C" u32 cf_batch_part_tile(void) { return kScTile; }
+extern "C" u32 cf_batch_part_max_ranges(void) { return kScMaxParts; }
+extern "C" size_t cf_batch_ovf_bytes(void) { return sizeof(CfOvf); }
+
+// Partitioned table build of the moduli whose descriptor has pcap > 0.
+//   phase 0: scatter (tstart: nmod+1 prefix sums of ceil(table-side records /
+//            cf_batch_part_tile()), 0 for moduli built in place)
+//   phase 1: place (tstart: prefix sums of the bucket ranges per modulus,
+//            2^max(0, bbits - log2 cf_batch_part_buckets()), 0 for in-place moduli)
+//   phase 2: insert the records that ran past their range (tstart unused)
+// queue: a device u64 zeroed before each of phases 0 and 1; ovf: ovf_cap entries of
+// cf_batch_ovf_bytes(), *novf zeroed before phase 1.  Errors go to *err:
+// CF_ERR_PART_OVERFLOW when a range received more than pcap records (the caller
+// rebuilds in place), CF_ERR_TABLE_FULL when the overflow list ran out.
+extern "C" int cf_batch_part(int phase, const void* mods, const u64* tstart, u32 nmod, void* queue, void* ovf,
+                             u32 ovf_cap, u32* novf, u32* err, u32 grid, void* stream) {
+  if (phase < 0 || phase > 2 || !mods || nmod == 0 || !err || (phase < 2 && (!tstart || !queue)) ||
+      (phase > 0 && (!novf || (ovf_cap && !ovf)))) {
+    cf_set_error("cf_batch_part: bad arguments%s", "");
+    return CF_EBADARG;
+  }
+  const cudaStream_t st = (cudaStream_t)stream;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (phase == 0) {
+    cudaError_t e = cudaFuncSetAttribute(k_bscatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScSmem);
+    if (e != cudaSuccess) return cf_cuda_status(e, "cf_batch_part: smem attribute");
+    k_bscatter<<<grid ? grid : (u32)sms, kScBlock, kScSmem, st>>>((const CfBatchMod*)mods, tstart, nmod,
+                                                                 (unsigned long long*)queue, err);
+  } else if (phase == 1) {
+    cudaError_t e = cudaFuncSetAttribute(k_bplace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlSmem);
+    if (e != cudaSuccess) return cf_cuda_status(e, "cf_batch_part: smem attribute");
+    k_bplace<<<grid ? grid : (u32)sms, kPlBlock, kPlSmem, st>>>((const CfBatchMod*)mods, tstart, nmod,
+                                                               (unsigned long long*)queue, (CfOvf*)ovf, ovf_cap,
+                                                               novf, err);
+  } else {
+    k_bfix<<<32, 256, 0, st>>>((const CfBatchMod*)mods, (const CfOvf*)ovf, novf, ovf_cap, err);
+  }
+  CF_LAUNCH_CHECK("cf_batch_part");
   return CF_OK;
 }

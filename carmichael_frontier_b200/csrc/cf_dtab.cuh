@@ -82,7 +82,8 @@ __device__ __forceinline__ u32 cf_word8(uint4 a, uint4 b, u32 w) {
   return r;
 }
 
-// Insert a residue (X, x2) with its rank; returns false if every bucket was full.
+// Claim a slot for (f16, side entry sd) in bucket b or, when b is full, in the
+// first non-full bucket after it; returns false if every bucket was full.
 // A slot is claimed with one compare-and-swap on the fingerprint word holding the
 // bucket's first empty 16-bit half: slots are only ever set, and a claim always
 // takes the first empty slot it sees, so the occupied slots of a bucket are a
@@ -90,17 +91,7 @@ __device__ __forceinline__ u32 cf_word8(uint4 a, uint4 b, u32 w) {
 // thread filled that word first; the claim retries with the value it returned
 // (at most 16 slots per bucket, so the retries are bounded).  The side entry is
 // written after the claim; probes run only after the build has completed.
-__device__ __forceinline__ bool dtab_insert(const DTab& t, u64 X, u32 x2, u64 rank) {
-  if (t.bloom) {
-    const CfBloomKey bk = cf_bloom_key(X, x2, t.fbits);
-    u32* blk = t.bloom + (u64)bk.block * 8;
-    atomicOr(blk + bk.w0, bk.m0);
-    atomicOr(blk + bk.w1, bk.m1);
-    atomicOr(blk + bk.w2, bk.m2);
-  }
-  const CfFuseKey fk = cf_fuse_key(X, x2, t.bbits);
-  const u32 f16 = fk.f16, f32 = fk.f32;
-  u64 b = fk.bucket;
+__device__ __forceinline__ bool dtab_claim(const DTab& t, u64 b, u32 f16, uint2 sd) {
   for (u64 tries = 0; tries < t.nb; ++tries) {
     u32* row = t.fpw + b * 8;
     const uint4 r0 = __ldcg((const uint4*)row), r1 = __ldcg((const uint4*)row + 1);
@@ -125,9 +116,6 @@ __device__ __forceinline__ bool dtab_insert(const DTab& t, u64 X, u32 x2, u64 ra
       const u32 nv = lo_free ? (cur | f16) : (cur | (f16 << 16));
       const u32 prev = atomicCAS(&row[w], cur, nv);
       if (prev == cur) {
-        uint2 sd;
-        sd.x = f32;
-        sd.y = (u32)(rank - t.rank0);
         t.side[b * 16 + 2 * w + (lo_free ? 0 : 1)] = sd;
         return true;
       }
@@ -136,6 +124,19 @@ __device__ __forceinline__ bool dtab_insert(const DTab& t, u64 X, u32 x2, u64 ra
     b = (b + 1) & (t.nb - 1);
   }
   return false;
+}
+
+// Insert a residue (X, x2) with its rank; returns false if every bucket was full.
+__device__ __forceinline__ bool dtab_insert(const DTab& t, u64 X, u32 x2, u64 rank) {
+  if (t.bloom) {
+    const CfBloomKey bk = cf_bloom_key(X, x2, t.fbits);
+    u32* blk = t.bloom + (u64)bk.block * 8;
+    atomicOr(blk + bk.w0, bk.m0);
+    atomicOr(blk + bk.w1, bk.m1);
+    atomicOr(blk + bk.w2, bk.m2);
+  }
+  const CfFuseKey fk = cf_fuse_key(X, x2, t.bbits);
+  return dtab_claim(t, fk.bucket, fk.f16, make_uint2(fk.f32, (u32)(rank - t.rank0)));
 }
 
 // Pair sink: candidates go to pairs[k] through the counter *npairs; in batched

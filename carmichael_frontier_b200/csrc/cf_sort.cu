@@ -71,57 +71,165 @@ __device__ __forceinline__ u32 lanemask_lt() {
   return m;
 }
 
-constexpr size_t kPassSmem = (size_t)kSortTile * 8 + (size_t)kSortTile + (size_t)kWarps * kRadix * 4;
+// Bulk (TMA) copies of a tile into shared memory, completed on an mbarrier.
+__device__ __forceinline__ u32 smem_addr(const void* p) { return (u32)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(u64* bar, u32 count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(u64* bar, u32 bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// global -> shared, `bytes` a multiple of 16, both addresses 16-byte aligned
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, u32 bytes, u64* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+// Bounded wait for phase `parity` of an mbarrier; false if the limit ran out.
+__device__ __forceinline__ bool mbar_wait(u64* bar, u32 parity, u32 limit) {
+  const u32 a = smem_addr(bar);
+  for (u32 i = 0; i < limit; ++i) {
+    u32 done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
 
-// One onesweep pass over the digit at bit `shift`.  Two CTAs per SM: each item's
-// digit (9 bits, 0x100 = no item) rides in the top bits of its local offset.
+// Write a staged tile (staged element j has digit s_dj[j]) to its global places,
+// kSortItems elements per thread with their shared-memory loads issued together.
+__device__ __forceinline__ void write_tile(const u64* s_v, const unsigned char* s_dj, const u64* s_gbase,
+                                           const u32* s_doff, u64* __restrict__ out, int tv) {
+  u32 d[kSortItems];
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    const int j = threadIdx.x + k * kSortBlock;
+    d[k] = j < tv ? s_dj[j] : 0u;
+  }
+  u64 dst[kSortItems], v[kSortItems];
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    const int j = threadIdx.x + k * kSortBlock;
+    dst[k] = s_gbase[d[k]] + (u64)(j - (int)s_doff[d[k]]);
+    v[k] = s_v[j < tv ? j : 0];
+  }
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k)
+    if (threadIdx.x + k * kSortBlock < tv) out[dst[k]] = v[k];
+}
+
+constexpr int kLookWin = 8;           // predecessor tiles read per look-back round trip
+constexpr u32 kMbarLimit = 1u << 22;  // try_wait rounds (each suspends for a while) before giving up
+constexpr size_t kPassSmem = (size_t)kSortTile * 16 + (size_t)kSortTile + (size_t)kWarps * kRadix * 4;
+
+// One onesweep pass over the digit at bit `shift`.  Two CTAs per SM.  BULK: the
+// tile's keys and ids are brought into shared memory by two bulk copies at the
+// start (every pointer 16-byte aligned), so the id load overlaps the ranking;
+// otherwise by plain coalesced loads.  Each item's digit (9 bits, 0x100 = no
+// item) rides in the top bits of its local offset.
+template <bool BULK>
 __global__ void __launch_bounds__(kSortBlock, 2)
 k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __restrict__ kout,
             u64* __restrict__ iout, u64 n, int shift, const u64* __restrict__ gexcl /*[256]*/,
             u64* __restrict__ status /*[tiles][256]*/, u32* __restrict__ ticket, u32* __restrict__ err) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  u64* s_buf = (u64*)smem;                                   // kSortTile words (keys, then ids)
-  unsigned char* s_dj = smem + (size_t)kSortTile * 8;        // digit of staged element j
+  extern __shared__ __align__(128) unsigned char smem[];
+  u64* s_kin = (u64*)smem;                                   // tile keys; later the staging area
+  u64* s_iin = s_kin + kSortTile;                            // tile ids
+  unsigned char* s_dj = (unsigned char*)(s_iin + kSortTile); // digit of staged element j
   u32* s_wc = (u32*)(s_dj + kSortTile);                      // [kWarps][256] warp digit counts
+  __shared__ __align__(8) u64 s_bar[2];
   __shared__ u32 s_tile;
   __shared__ u32 s_dcnt[kRadix];
   __shared__ u32 s_doff[kRadix];
   __shared__ u64 s_gbase[kRadix];
   __shared__ u32 s_scan[kWarps];
 
-  if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
-  for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortBlock) s_wc[i] = 0;
+  if (threadIdx.x == 0) {
+    s_tile = atomicAdd(ticket, 1u);
+    if (BULK) {
+      mbar_init(&s_bar[0], 1);
+      mbar_init(&s_bar[1], 1);
+      mbar_fence_init();
+    }
+  }
   __syncthreads();
   const u32 tile = s_tile;
   const u64 base = (u64)tile * kSortTile;
+  const u64 left = n - base;
+  const int tv = (int)(left < (u64)kSortTile ? left : (u64)kSortTile);
+  if (BULK) {
+    if (threadIdx.x == 0) {
+      const u32 bytes = (u32)(tv & ~1) * 8u;   // whole 16-byte units; an odd last record is loaded below
+      mbar_expect_tx(&s_bar[0], bytes);
+      if (bytes) bulk_g2s(s_kin, kin + base, bytes, &s_bar[0]);
+      mbar_expect_tx(&s_bar[1], bytes);
+      if (bytes) bulk_g2s(s_iin, iin + base, bytes, &s_bar[1]);
+      if (tv & 1) {
+        s_kin[tv - 1] = kin[base + tv - 1];
+        s_iin[tv - 1] = iin[base + tv - 1];
+      }
+    }
+  } else {
+    for (int j = threadIdx.x; j < tv; j += kSortBlock) {
+      s_kin[j] = kin[base + j];
+      s_iin[j] = iin[base + j];
+    }
+  }
+  for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortBlock) s_wc[i] = 0;
+  __syncthreads();
+  if (BULK && !mbar_wait(&s_bar[0], 0, kMbarLimit)) {
+    atomicOr(err, CF_ERR_SPIN_LIMIT);
+    mbar_wait(&s_bar[0], 0, kMbarLimit);
+  }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   u64 key[kSortItems];
   u32 loc[kSortItems];                      // local offset (low 16 bits) | digit << 16
+  u32 peers[kSortItems];
   const u32 lt = lanemask_lt();
   u32* wc = s_wc + wid * kRadix;
+  // the keys and their peer masks first (independent of one another), then the
+  // per-item counter chain of this warp, so the loads overlap
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
-    const u64 e = base + (u64)wid * 32 * kSortItems + (u64)it * 32 + lane;
-    const bool valid = e < n;
-    key[it] = valid ? kin[e] : 0ull;
-    const u32 d = valid ? (u32)((key[it] >> shift) & 0xff) : 0x100u;
-    const u32 peers = __match_any_sync(0xffffffffu, d);
+    const int e = wid * 32 * kSortItems + it * 32 + lane;
+    key[it] = e < tv ? s_kin[e] : 0ull;
+  }
+#pragma unroll
+  for (int it = 0; it < kSortItems; ++it) {
+    const int e = wid * 32 * kSortItems + it * 32 + lane;
+    const u32 d = e < tv ? (u32)((key[it] >> shift) & 0xff) : 0x100u;
+    loc[it] = d << 16;
+    peers[it] = __match_any_sync(0xffffffffu, d);
+  }
+#pragma unroll
+  for (int it = 0; it < kSortItems; ++it) {
+    const u32 d = loc[it] >> 16;
+    const bool valid = d < 0x100u;
     u32 cnt = 0;
     if (valid) cnt = wc[d];
     __syncwarp();
-    const u32 r = __popc(peers & lt);
-    if (valid && r == 0) wc[d] = cnt + __popc(peers);
+    const u32 r = __popc(peers[it] & lt);
+    if (valid && r == 0) wc[d] = cnt + __popc(peers[it]);
     __syncwarp();
-    loc[it] = (cnt + r) | (d << 16);
+    loc[it] |= cnt + r;
   }
   __syncthreads();
   if (threadIdx.x < kRadix) {                 // per digit: exclusive over warps, tile total
     const int d = threadIdx.x;
+    u32 v[kWarps];
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) v[w] = s_wc[w * kRadix + d];
     u32 run = 0;
+#pragma unroll
     for (int w = 0; w < kWarps; ++w) {
-      const u32 v = s_wc[w * kRadix + d];
       s_wc[w * kRadix + d] = run;
-      run += v;
+      run += v[w];
     }
     s_dcnt[d] = run;
     const u64 pub = (tile == 0) ? (kFlagInc | (u64)run) : (kFlagAgg | (u64)run);
@@ -143,19 +251,30 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
     for (int w = 0; w < wid; ++w) add += s_scan[w];
     s_doff[d] += add;
     u64 excl = 0;
-    if (tile > 0) {                           // decoupled look-back, bounded
+    if (tile > 0) {
+      // decoupled look-back, kLookWin predecessors per round trip, bounded.  Tile 0
+      // always publishes an inclusive prefix, so the walk ends at tile 0 at the latest.
       int j = (int)tile - 1;
       u32 spins = 0;
-      while (j >= 0) {
-        const u64 v = ((volatile u64*)status)[(u64)j * kRadix + d];
-        const u64 f = v & ~kValMask;
-        if (f == 0) {
-          if (++spins > kSpinLimit) { atomicOr(err, CF_ERR_SPIN_LIMIT); break; }
-          continue;
+      for (;;) {
+        u64 v[kLookWin];
+#pragma unroll
+        for (int w = 0; w < kLookWin; ++w)
+          v[w] = (j - w >= 0) ? ((volatile const u64*)status)[(u64)(j - w) * kRadix + d] : kFlagInc;
+        int used = 0;
+        bool stop = false, stall = false;
+#pragma unroll
+        for (int w = 0; w < kLookWin; ++w) {
+          if (stop || stall) continue;
+          const u64 f = v[w] & ~kValMask;
+          if (f == 0) { stall = true; continue; }
+          excl += v[w] & kValMask;
+          ++used;
+          if (f == kFlagInc) stop = true;
         }
-        excl += v & kValMask;
-        if (f == kFlagInc) break;
-        --j;
+        if (stop) break;
+        j -= used;
+        if (used == 0 && ++spins > kSpinLimit) { atomicOr(err, CF_ERR_SPIN_LIMIT); break; }
       }
       __threadfence();
       ((volatile u64*)status)[(u64)tile * kRadix + d] = kFlagInc | (excl + s_dcnt[d]);
@@ -163,36 +282,44 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
     s_gbase[d] = gexcl[d] + excl;
   }
   __syncthreads();
+  {
+    u32 add[kSortItems];
 #pragma unroll
-  for (int it = 0; it < kSortItems; ++it) {
-    const u32 d = loc[it] >> 16;
-    if (d < 0x100u) {
-      const u32 l = (loc[it] & 0xffffu) + s_doff[d] + wc[d];
-      loc[it] = l | (d << 16);
-      s_buf[l] = key[it];
-      s_dj[l] = (unsigned char)d;
+    for (int it = 0; it < kSortItems; ++it) {
+      const u32 d = loc[it] >> 16;
+      add[it] = d < 0x100u ? s_doff[d] + wc[d] : 0u;
+    }
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it) {
+      const u32 d = loc[it] >> 16;
+      if (d < 0x100u) {
+        const u32 l = (loc[it] & 0xffffu) + add[it];
+        loc[it] = l | (d << 16);
+        s_kin[l] = key[it];
+        s_dj[l] = (unsigned char)d;
+      }
     }
   }
   __syncthreads();
-  const u64 left = n - base;
-  const int tv = (int)(left < (u64)kSortTile ? left : (u64)kSortTile);
-  for (int j = threadIdx.x; j < tv; j += kSortBlock) {
-    const u32 d = s_dj[j];
-    kout[s_gbase[d] + (u64)(j - (int)s_doff[d])] = s_buf[j];
+  write_tile(s_kin, s_dj, s_gbase, s_doff, kout, tv);
+  if (BULK && !mbar_wait(&s_bar[1], 0, kMbarLimit)) {
+    atomicOr(err, CF_ERR_SPIN_LIMIT);
+    mbar_wait(&s_bar[1], 0, kMbarLimit);
   }
   __syncthreads();
+  {
+    u64 idv[kSortItems];
 #pragma unroll
-  for (int it = 0; it < kSortItems; ++it) {
-    if ((loc[it] >> 16) < 0x100u) {
-      const u64 e = base + (u64)wid * 32 * kSortItems + (u64)it * 32 + lane;
-      s_buf[loc[it] & 0xffffu] = iin[e];
+    for (int it = 0; it < kSortItems; ++it) {
+      const int e = wid * 32 * kSortItems + it * 32 + lane;
+      idv[it] = (loc[it] >> 16) < 0x100u ? s_iin[e] : 0ull;
     }
+#pragma unroll
+    for (int it = 0; it < kSortItems; ++it)
+      if ((loc[it] >> 16) < 0x100u) s_kin[loc[it] & 0xffffu] = idv[it];
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < tv; j += kSortBlock) {
-    const u32 d = s_dj[j];
-    iout[s_gbase[d] + (u64)(j - (int)s_doff[d])] = s_buf[j];
-  }
+  write_tile(s_kin, s_dj, s_gbase, s_doff, iout, tv);
 }
 
 // ---------------------------------------------------------------------------
@@ -289,7 +416,9 @@ extern "C" int cf_sort_pairs(u64* keys, u64* ids, u64 n, int key_bits, void* tmp
   e = cudaMemcpyAsync(hh, hist, sizeof hh, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: histogram read");
-  e = cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPassSmem);
+  e = cudaFuncSetAttribute(k_sort_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPassSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sort_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPassSmem);
   if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: smem attribute");
   u64 *ka = keys, *ia = ids, *kb = k2, *ib = i2;
   int done = 0;
@@ -297,8 +426,15 @@ extern "C" int cf_sort_pairs(u64* keys, u64* ids, u64 n, int key_bits, void* tmp
     bool trivial = false;
     for (int d = 0; d < kRadix; ++d) if (hh[p * kRadix + d] == n) trivial = true;
     if (trivial) continue;
-    k_sort_pass<<<(unsigned)tiles, kSortBlock, kPassSmem, st>>>(ka, ia, kb, ib, n, 8 * p, excl + p * kRadix,
-                                                                 status + (u64)p * tiles * kRadix, tickets + p, errw);
+    // bulk copies read 16-byte units from 16-byte boundaries: every tile starts at
+    // a multiple of 4096 records, so aligned source arrays suffice
+    const bool bulk = ((((uintptr_t)ka) | ((uintptr_t)ia)) & 15u) == 0;
+    if (bulk)
+      k_sort_pass<true><<<(unsigned)tiles, kSortBlock, kPassSmem, st>>>(
+          ka, ia, kb, ib, n, 8 * p, excl + p * kRadix, status + (u64)p * tiles * kRadix, tickets + p, errw);
+    else
+      k_sort_pass<false><<<(unsigned)tiles, kSortBlock, kPassSmem, st>>>(
+          ka, ia, kb, ib, n, 8 * p, excl + p * kRadix, status + (u64)p * tiles * kRadix, tickets + p, errw);
     CF_LAUNCH_CHECK("cf_sort_pairs: pass");
     u64* t = ka; ka = kb; kb = t;
     t = ia; ia = ib; ib = t;

@@ -39,13 +39,19 @@ MOD_DTYPE = np.dtype([
     ("poolD", "<u8"), ("tailD", "<u8"), ("poolI", "<u8"), ("tailI", "<u8"), ("screen", "<u8"),
     ("fpw", "<u8"), ("side", "<u8"), ("fill", "<u8"), ("bloom", "<u8"),
     ("nD", "<u8"), ("i_lo", "<u8"), ("nI", "<u8"),
-    ("bbits", "<i4"), ("fbits", "<i4"), ("r", "<i4"), ("swap", "<i4")])
+    ("bbits", "<i4"), ("fbits", "<i4"), ("r", "<i4"), ("swap", "<i4"),
+    ("pkw", "<u8"), ("psd", "<u8"), ("pcnt", "<u8"), ("pcap", "<u4"), ("pad_", "<u4")])
 
 _ALIGN = 256
 
 
 def _up(x: int, a: int = _ALIGN) -> int:
     return (x + a - 1) // a * a
+
+
+def tu_ovf_bytes(solver) -> int:
+    """Bytes of the overflow list of the partitioned build."""
+    return max(64, solver.tuning.ovf_capacity * solver.lib.cf_batch_ovf_bytes())
 
 
 @dataclass
@@ -56,6 +62,10 @@ class BatchTuning:
     mem_budget: int = 24 << 30         # D-table bytes of one batch
     pair_capacity: int = 1 << 16       # initial candidate buffer (grown on overflow)
     dtab: Tuning = field(default_factory=Tuning)   # D-table sizing (dtab_load, Bloom level)
+    part_build: bool = True            # partitioned table build for tables above part_min_buckets
+    part_min_buckets: int = 1 << 16    # smaller tables (L2-resident) are built in place
+    part_sigma: float = 8.0            # bucket-range capacity = mean + sigma*sqrt(mean) + 32
+    ovf_capacity: int = 1 << 16        # records that ran past their bucket range (per batch)
 
 
 @dataclass
@@ -64,6 +74,11 @@ class _Batch:
     mods: object = None                # device CfBatchMod[nmod]
     tsD: object = None                 # device u64[nmod+1] ticket prefix sums, table sides (build)
     tsI: object = None                 # device u64[nmod+1] ticket prefix sums, probing sides
+    tsD_all: object = None             # table-side tickets with every modulus built in place
+    tsS: object = None                 # scatter tickets of the partitioned build (0 for in-place moduli)
+    tsP: object = None                 # bucket ranges of the partitioned build (0 for in-place moduli)
+    n_part: int = 0                    # moduli of this batch with the partitioned build
+    use_part: bool = True              # False after a bucket range overflowed: build in place
     zero_bytes: int = 0                # arena bytes zeroed before the build
     arena_bytes: int = 0
     records: int = 0
@@ -184,11 +199,25 @@ class BatchSolver:
                        "cf_build_tail(D)")
             _lib.check(lib.cf_build_tail(base + offs[(k, "pI")], len(x.INS), x.r, tbase + toffs[(k, "tI")], sh),
                        "cf_build_tail(I)")
+        # partitioned build: (ranges, range capacity) per modulus, None when built in place
+        lib_pb = lib.cf_batch_part_buckets()
+        plb = lib_pb.bit_length() - 1
+        part: dict = {}
+        for k in batched:
+            bb, _fb = shapes[k]
+            nparts = 1 << max(0, bb - plb)
+            if tu.part_build and (1 << bb) >= tu.part_min_buckets and nparts <= lib.cf_batch_part_max_ranges():
+                mean = min(nD[k], nI[k]) / nparts
+                cap = int(math.ceil(mean + tu.part_sigma * math.sqrt(mean) + 32))
+                part[k] = (nparts, (cap + 3) // 4 * 4)
         # batches: consecutive moduli whose D tables fit the budget
         batches, cur, cur_bytes = [], [], 0
         for k in batched:
             bb, fb = shapes[k]
             nbytes = _up(36 << bb) + (_up(32 << fb) if fb else 0) + _up(128 << bb)
+            if k in part:
+                npt, cap = part[k]
+                nbytes += _up(npt * 4) + _up(npt * cap * 4) + _up(npt * cap * 8)
             if cur and cur_bytes + nbytes > tu.mem_budget:
                 batches.append(_Batch(cur))
                 cur, cur_bytes = [], 0
@@ -198,16 +227,23 @@ class BatchSolver:
             batches.append(_Batch(cur))
         # descriptors with arena offsets (arena pointers are filled in at run time)
         for b in batches:
-            zoff, soff_rel = 0, 0
+            zoff, soff_rel, poff_rel = 0, 0, 0
             rows = np.zeros(len(b.idx), dtype=MOD_DTYPE)
-            zl, sl = [], []
+            zl, sl, pl = [], [], []
             for j, k in enumerate(b.idx):
                 x = insts[k]
                 bb, fb = shapes[k]
                 zl.append(zoff)
                 zoff += _up(36 << bb) + (_up(32 << fb) if fb else 0)
+                if k in part:                      # range counters sit in the zeroed region
+                    zoff += _up(part[k][0] * 4)
                 sl.append(soff_rel)
                 soff_rel += _up(128 << bb)
+                pl.append(poff_rel)
+                if k in part:
+                    npt, cap = part[k]
+                    poff_rel += _up(npt * cap * 4) + _up(npt * cap * 8)
+                    rows[j]["pcap"] = cap
                 rows[j]["poolD"] = base + offs[(k, "pD")]
                 rows[j]["poolI"] = base + offs[(k, "pI")]
                 rows[j]["screen"] = base + offs[(k, "sc")]
@@ -219,17 +255,27 @@ class BatchSolver:
                 rows[j]["bbits"], rows[j]["fbits"], rows[j]["r"] = bb, fb, x.r
                 rows[j]["swap"] = int(nI[k] < nD[k])
             b.zero_bytes = zoff
-            b.arena_bytes = zoff + soff_rel
+            b.arena_bytes = zoff + soff_rel + poff_rel
             b.records = sum(nD[k] + nI[k] for k in b.idx)
-            b._rows, b._zl, b._sl = rows, zl, sl
+            b._rows, b._zl, b._sl, b._pl = rows, zl, sl, pl
+            b._side_bytes = soff_rel
+            b._part = {j: part[k] for j, k in enumerate(b.idx) if k in part}
+            b.n_part = len(b._part)
             t = tu.ticket
-            tsD = np.zeros(len(b.idx) + 1, dtype=np.uint64)
-            tsI = np.zeros(len(b.idx) + 1, dtype=np.uint64)
-            # mode 0 walks the table's (smaller) side, mode 1 the probing side
-            tsD[1:] = np.cumsum([-(-min(nD[k], nI[k]) // t) for k in b.idx])
-            tsI[1:] = np.cumsum([-(-max(nD[k], nI[k]) // t) for k in b.idx])
-            b.tsD = torch.from_numpy(tsD.view(np.int64)).to(self.device)
-            b.tsI = torch.from_numpy(tsI.view(np.int64)).to(self.device)
+            tile = lib.cf_batch_part_tile()
+
+            def _prefix(vals):
+                a = np.zeros(len(b.idx) + 1, dtype=np.uint64)
+                a[1:] = np.cumsum(vals)
+                return torch.from_numpy(a.view(np.int64)).to(self.device)
+            # mode 0 walks the table's (smaller) side, mode 1 the probing side; the
+            # partitioned build takes the table sides of the moduli in b._part
+            build = [-(-min(nD[k], nI[k]) // t) for k in b.idx]
+            b.tsD_all = _prefix(build)
+            b.tsD = _prefix([0 if j in b._part else v for j, v in enumerate(build)])
+            b.tsI = _prefix([-(-max(nD[k], nI[k]) // t) for k in b.idx])
+            b.tsS = _prefix([-(-min(nD[k], nI[k]) // tile) if j in b._part else 0 for j, k in enumerate(b.idx)])
+            b.tsP = _prefix([b._part[j][0] if j in b._part else 0 for j in range(len(b.idx))])
         prep = PreparedPortfolio(insts, i_limit, nD, nI, shapes, batches, fallback, trivial, blob, tails,
                                  tu.pair_capacity)
         self._place(prep)
@@ -253,6 +299,12 @@ class BatchSolver:
                 rows[j]["fill"] = z + (32 << bb)
                 rows[j]["bloom"] = z + _up(36 << bb) if fb else 0
                 rows[j]["side"] = abase + b.zero_bytes + b._sl[j]
+                if j in b._part:
+                    npt, cap = b._part[j]
+                    rows[j]["pcnt"] = z + _up(36 << bb) + (_up(32 << fb) if fb else 0)
+                    pk = abase + b.zero_bytes + b._side_bytes + b._pl[j]
+                    rows[j]["pkw"] = pk
+                    rows[j]["psd"] = pk + _up(npt * cap * 4)
             b.mods = torch.from_numpy(rows.view(np.uint8).copy()).to(self.device)
             b._arena_ptr = abase
 
@@ -261,17 +313,29 @@ class BatchSolver:
         lib, dp, ck = self.lib, _lib.ptr, _lib.check
         arena = self._bufs["arena"]
         misc = self._buf("misc", 64)
+        ovf = self._buf("ovf", tu_ovf_bytes(self))
         pairs = self._buf("pairs", maxp * 16)
         pmod = self._buf("pmod", maxp * 4)
         res = self._buf("res", maxp * self.result_bytes)
         sh = self._sh()
         tu = self.tuning
         arena[: b.zero_bytes].zero_()
-        misc[:32].zero_()
+        misc.zero_()
+        # misc: +0 build queue, +8 probe queue, +16 npairs, +20 err, +24 overflow count,
+        # +32 scatter queue, +40 range queue (partitioned build)
         m = dp(misc)
         nmod = len(b.idx)
-        ck(lib.cf_batch_run(0, dp(b.mods), dp(b.tsD), nmod, tu.ticket, m, dp(pairs), dp(pmod), maxp, m + 16, m + 20,
-                            None, tu.grid, sh), "cf_batch_run(build)")
+        part = b.use_part and b.n_part > 0
+        if part:
+            oc = self.tuning.ovf_capacity
+            ck(lib.cf_batch_part(0, dp(b.mods), dp(b.tsS), nmod, m + 32, None, 0, m + 24, m + 20, 0, sh),
+               "cf_batch_part(scatter)")
+            ck(lib.cf_batch_part(1, dp(b.mods), dp(b.tsP), nmod, m + 40, dp(ovf), oc, m + 24, m + 20, 0, sh),
+               "cf_batch_part(place)")
+            ck(lib.cf_batch_part(2, dp(b.mods), None, nmod, None, dp(ovf), oc, m + 24, m + 20, 0, sh),
+               "cf_batch_part(fix)")
+        ck(lib.cf_batch_run(0, dp(b.mods), dp(b.tsD if part else b.tsD_all), nmod, tu.ticket, m, dp(pairs), dp(pmod),
+                            maxp, m + 16, m + 20, None, tu.grid, sh), "cf_batch_run(build)")
         ck(lib.cf_batch_run(1, dp(b.mods), dp(b.tsI), nmod, tu.ticket, m + 8, dp(pairs), dp(pmod), maxp, m + 16,
                             m + 20, None, tu.grid, sh), "cf_batch_run(probe)")
         ck(lib.cf_batch_run(2, dp(b.mods), None, nmod, 0, None, dp(pairs), dp(pmod), maxp, m + 16, m + 20, dp(res),
@@ -283,7 +347,8 @@ class BatchSolver:
             self._enqueue(b, maxp)
             return
         if b.graph is None or b._graph_maxp != maxp or b._arena_ptr != self._bufs["arena"].data_ptr():
-            for nm, nb in (("misc", 64), ("pairs", maxp * 16), ("pmod", maxp * 4), ("res", maxp * self.result_bytes)):
+            for nm, nb in (("misc", 64), ("ovf", tu_ovf_bytes(self)), ("pairs", maxp * 16), ("pmod", maxp * 4),
+                           ("res", maxp * self.result_bytes)):
                 self._buf(nm, nb)            # allocate outside the capture
             g = torch.cuda.CUDAGraph()
             s = torch.cuda.Stream(self.device)
@@ -320,6 +385,9 @@ class BatchSolver:
                 self._torch_stream().synchronize()
                 misc = self._bufs["misc"][:32].cpu().numpy().view(np.uint32)
                 npairs, err = int(misc[4]), int(misc[5])
+                if err & _lib.ERR_PART_OVERFLOW and b.use_part and b.n_part:
+                    b.use_part, b.graph = False, None       # a bucket range overflowed: build in place
+                    continue
                 if err & _lib.ERR_PAIR_OVERFLOW:
                     prep.pairs_cap = 1 << max(npairs + 16, 2 * maxp).bit_length()
                     continue
@@ -364,7 +432,7 @@ class BatchSolver:
         """Drop a prepared portfolio's graphs and device tables."""
         for b in prep.batches:
             b.graph = None
-            b.mods = b.tsD = b.tsI = None
+            b.mods = b.tsD = b.tsI = b.tsD_all = b.tsS = b.tsP = None
         prep.tables = prep.tails = None
         live = getattr(self, "_live", [])
         self._live = [p for p in live if p is not prep]

@@ -55,12 +55,28 @@ def test_bad_arguments_fail_loudly_without_gpu():
 def test_batch_descriptor_layout():
     from carmichael_frontier_b200.portfolio import MOD_DTYPE
     lib = _lib.load()
-    assert lib.cf_batch_mod_bytes() == MOD_DTYPE.itemsize == 112
+    assert lib.cf_batch_mod_bytes() == MOD_DTYPE.itemsize == 144
     assert lib.cf_batch_max_r() == 8
     # a ticket that is not a multiple of 32 is rejected before any device call
     one = np.zeros(8, dtype=np.uint64)
     assert lib.cf_batch_run(0, one.ctypes.data, one.ctypes.data, 1, 48, one.ctypes.data, None, None, 0,
                             one.ctypes.data, one.ctypes.data, None, 0, None) == _lib.CF_EBADARG
+
+
+def test_batch_partitioned_build_constants_and_arguments():
+    lib = _lib.load()
+    assert lib.cf_batch_part_buckets() == 1024
+    assert lib.cf_batch_part_tile() == 8192
+    assert lib.cf_batch_part_max_ranges() == 4096
+    assert lib.cf_batch_ovf_bytes() == 24
+    one = np.zeros(8, dtype=np.uint64)
+    p = one.ctypes.data
+    # bad phase, missing queue or tickets, missing overflow counter: rejected before any device call
+    assert lib.cf_batch_part(3, p, p, 1, p, p, 1, p, p, 0, None) == _lib.CF_EBADARG
+    assert lib.cf_batch_part(0, p, None, 1, p, None, 0, None, p, 0, None) == _lib.CF_EBADARG
+    assert lib.cf_batch_part(1, p, p, 1, None, p, 1, p, p, 0, None) == _lib.CF_EBADARG
+    assert lib.cf_batch_part(2, p, None, 1, None, p, 1, None, p, 0, None) == _lib.CF_EBADARG
+    assert lib.cf_batch_part(0, p, p, 0, p, None, 0, None, p, 0, None) == _lib.CF_EBADARG
 
 
 def _hostkey(M, v):

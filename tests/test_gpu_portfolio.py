@@ -119,3 +119,35 @@ def test_batch_autotuner_keeps_results(cuda):
     tu, rows = tune_batch(prep, cuda, reps=1, tickets=(64, 8192), grids=(0, 2))
     assert len(rows) == 4 and all(r["ms"] > 0 for r in rows)
     assert [summary(x) for x in BatchSolver(cuda, tuning=tu).solve(insts)] == ref
+
+
+def test_batched_partitioned_build_matches_in_place(cuda):
+    # tables at 12 records per 16-slot bucket (about one bucket in ten overflows, some of
+    # them at the end of a 1024-bucket range), tiny whole-table ranges, and the in-place build
+    from carmichael_frontier_b200.solve import Tuning
+    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config3(6)]
+    insts += small_portfolio(3, 8)
+    lim = 12 << 17
+    dense = Tuning(dtab_load=12.0)
+    part = BatchSolver(cuda, tuning=BatchTuning(dtab=dense, part_min_buckets=16))
+    prep = part.prepare(insts, i_limit=lim)
+    assert sum(b.n_part for b in prep.batches) >= 10
+    got = part.run(prep)
+    assert all(b.use_part for b in prep.batches)
+    inplace = BatchSolver(cuda, tuning=BatchTuning(dtab=dense, part_build=False)).solve(insts, i_limit=lim)
+    one = run_per_modulus(insts, i_limit=lim, solver=Solver(cuda))
+    for a, b, c in zip(got, inplace, one):
+        assert summary(a) == summary(b) == summary(c)
+
+
+def test_batched_partitioned_range_overflow_falls_back(cuda):
+    # bucket ranges given less room than they receive: the batch is rebuilt in place
+    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config3(3)]
+    lim = 1 << 19
+    bs = BatchSolver(cuda, tuning=BatchTuning(part_sigma=-6.0, part_min_buckets=16))
+    prep = bs.prepare(insts, i_limit=lim)
+    got = bs.run(prep, graphs=True)
+    assert not any(b.use_part for b in prep.batches if b.n_part)
+    ref = BatchSolver(cuda, tuning=BatchTuning(part_build=False)).solve(insts, i_limit=lim)
+    for a, b in zip(got, ref):
+        assert summary(a) == summary(b)
