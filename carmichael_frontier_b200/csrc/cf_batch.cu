@@ -42,13 +42,13 @@ struct CfBatchMod {
   int bbits, fbits;
   int r, swap;
   // partitioned build (pcap > 0): the table side's records are first scattered
-  // into 2^max(0, bbits - kPlb) bucket ranges, then each range is built in
+  // into 2^max(0, bbits - plb) bucket ranges, then each range is built in
   // shared memory and written out whole
   u32* pkw;          // [nparts * pcap]: bucket within the range << 16 | 16-bit fingerprint
   uint2* psd;        // [nparts * pcap]: side entries {32-bit fingerprint, rank - rank0}
   u32* pcnt;         // [nparts]: records scattered into each range (zeroed by the caller)
   u32 pcap;          // records a range holds (0: this modulus uses the in-place build)
-  u32 pad_;
+  u32 plb;           // log2 buckets per range (kPlbMin..kPlbMax)
 };
 
 template <int R, int MODE>
@@ -106,10 +106,7 @@ __device__ __forceinline__ bool batch_ticket(const CfBatchMod& md, u32 mod, u64 
                           (cf_word8(a, c, bk.w2) & bk.m2);
           if (!in) continue;
         }
-        const CfFuseKey fk = cf_fuse_key(X, x2, tab.bbits);
-        const uint4* row = (const uint4*)(tab.fpw + (u64)fk.bucket * 8);
-        if (probe_fast(__ldg(row), __ldg(row + 1), fk.f16))
-          probe_slow(tab, fk.bucket, fk.f16, fk.f32, rank_base + off, sink);
+        dtab_probe(tab, cf_fuse_key(X, x2, tab.bbits), rank_base + off, sink);
       }
     }
   }
@@ -172,7 +169,7 @@ k_batch(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart /*[n
 // in place costs a random DRAM read and write of a fingerprint sector and of a
 // side-entry sector per record.  Instead:
 //   k_bscatter  generates the table side in tiles of kScTile records, ranks each
-//               tile's records by bucket range (2^kPlb buckets) in shared
+//               tile's records by bucket range (2^plb buckets) in shared
 //               memory, reserves each range's space with one atomic per tile
 //               and writes the records there (the writes of one range land in
 //               consecutive addresses, so L2 merges them into whole sectors);
@@ -185,23 +182,30 @@ k_batch(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart /*[n
 // The result is a table the probe reads exactly like one built in place: every
 // record sits in the first non-full bucket at or after its own.
 // ---------------------------------------------------------------------------
-constexpr int kPlb = 10;
-constexpr u32 kPartBuckets = 1u << kPlb;
-constexpr int kScBlock = 512;
-constexpr int kScTile = 8192;                 // records per scatter ticket (16 per thread)
+constexpr int kPlbMin = 9;                    // 512-bucket ranges: 80 KB, two CTAs per SM
+constexpr int kPlbMax = 10;                   // 1024-bucket ranges: 160 KB, one CTA per SM
+constexpr int kScBlock = 256;
+constexpr int kScMinBlocks = 3;               // CTAs per SM (64 KB of shared memory each)
+constexpr int kScTile = 4096;                 // records per scatter ticket (16 per thread)
 constexpr int kScWarpRecs = kScTile / (kScBlock / 32);
-constexpr u32 kScMaxParts = 4096;             // bucket ranges per modulus (bbits <= kPlb + 12)
-constexpr size_t kScSmem = (size_t)kScTile * 16 + (size_t)kScMaxParts * 4;
-constexpr int kPlBlock = 1024;
-constexpr size_t kPlSmem = (size_t)kPartBuckets * (32 + 128);
+constexpr u32 kScMaxParts = 4096;             // bucket ranges per modulus (bbits <= plb + 12)
+constexpr size_t kScSmem = (size_t)kScTile * 12 + (size_t)kScMaxParts * 4;
+constexpr int kPlItems = 8;                   // records a thread loads before claiming (more loop if needed)
+template <int PLB>
+struct PlaceShape {
+  static constexpr int kBlock = PLB == kPlbMax ? 1024 : 512;
+  static constexpr int kMinBlocks = PLB == kPlbMax ? 1 : 2;
+  static constexpr u32 kBuckets = 1u << PLB;
+  static constexpr size_t kSmem = (size_t)kBuckets * (32 + 128 + 4);
+};
 
 struct CfOvf {
   u32 mod, bucket, f16, f32, rank, pad;
 };
 
 template <int R>
-__device__ __forceinline__ bool scatter_gen(const CfBatchMod& md, u64 first, u32 count, u64* s_pk, uint2* s_sd,
-                                            u32* s_h) {
+__device__ __forceinline__ bool scatter_gen(const CfBatchMod& md, u64 first, u32 count, u32* s_kw, u32* s_pp,
+                                            u32* s_f32, u32* s_h) {
   constexpr int B = R < 2 ? R : 2;
   const bool d_side = md.swap == 0;              // the table holds the smaller side
   const u64* pool = d_side ? md.poolD : md.poolI;
@@ -225,7 +229,8 @@ __device__ __forceinline__ bool scatter_gen(const CfBatchMod& md, u64 first, u32
   const u64 rank0 = d_side ? 0 : md.i_lo;        // enumeration rank of the side's first record
   CfTailWalker<R, B> w;
   w.init(rank0 + first + wbeg, n, binom, ar, st, hd->tail_n);
-  const u32 pmask = md.bbits > kPlb ? ~0u : 0u;
+  const int plb = (int)md.plb;
+  const u32 pmask = md.bbits > plb ? ~0u : 0u;
   for (u32 off = 0; off < wcnt; off += 32) {     // uniform across the warp
     CfElt32 q = st;
     u64 j;
@@ -243,24 +248,26 @@ __device__ __forceinline__ bool scatter_gen(const CfBatchMod& md, u64 first, u32
         atomicOr(blk + bk.w2, bk.m2);
       }
       const CfFuseKey fk = cf_fuse_key(X, x2, md.bbits);
-      const u32 p = (fk.bucket >> kPlb) & pmask;
-      const u32 bl = fk.bucket & (kPartBuckets - 1u);
+      const u32 p = (fk.bucket >> plb) & pmask;
+      const u32 bl = fk.bucket & ((1u << plb) - 1u);
       const u32 pos = atomicAdd(&s_h[p], 1u);
       const u32 i = wbeg + off + (u32)lane;
-      s_pk[i] = (u64)((bl << 16) | fk.f16) | ((u64)p << 32) | ((u64)pos << 48);
-      s_sd[i] = make_uint2(fk.f32, (u32)(first + i));
+      s_kw[i] = (bl << 16) | fk.f16;
+      s_pp[i] = (p << 12) | pos;
+      s_f32[i] = fk.f32;
     }
   }
   return true;
 }
 
-__global__ void __launch_bounds__(kScBlock, 1)
+__global__ void __launch_bounds__(kScBlock, kScMinBlocks)
 k_bscatter(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart, u32 nmod,
            unsigned long long* __restrict__ queue, u32* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem[];
-  u64* s_pk = (u64*)smem;                        // [kScTile] range-local key | range << 32 | rank in range << 48
-  uint2* s_sd = (uint2*)(s_pk + kScTile);        // [kScTile] side entries
-  u32* s_h = (u32*)(s_sd + kScTile);             // [kScMaxParts] tile counts, then global offsets
+  u32* s_kw = (u32*)smem;                        // [kScTile] bucket within the range << 16 | 16-bit fingerprint
+  u32* s_pp = s_kw + kScTile;                    // [kScTile] range << 12 | place among the tile's records of it
+  u32* s_f32 = s_pp + kScTile;                   // [kScTile] 32-bit fingerprint (the side entry's rank is first + i)
+  u32* s_h = s_f32 + kScTile;                    // [kScMaxParts] tile counts, then global offsets
   __shared__ u64 s_t;
   const u64 total = tstart[nmod];
   bool ok = true;
@@ -277,22 +284,23 @@ k_bscatter(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart, 
     const CfBatchMod& md = mods[lo];
     const u64 n_side = md.swap ? md.nI : md.nD;
     const u64 first = (t - tstart[lo]) * (u64)kScTile;
-    const u32 nparts = md.bbits > kPlb ? 1u << (md.bbits - kPlb) : 1u;
-    const bool good = first < n_side && nparts <= kScMaxParts && md.pcap > 0;
+    const bool plb_ok = md.plb >= (u32)kPlbMin && md.plb <= (u32)kPlbMax;
+    const u32 nparts = plb_ok && md.bbits > (int)md.plb ? 1u << (md.bbits - (int)md.plb) : 1u;
+    const bool good = first < n_side && nparts <= kScMaxParts && md.pcap > 0 && plb_ok;
     const u32 count = good ? (u32)min((u64)kScTile, n_side - first) : 0u;
     for (u32 p = threadIdx.x; p < nparts && good; p += kScBlock) s_h[p] = 0;
     __syncthreads();
     if (good) {
       bool g = true;
       switch (md.r) {
-        case 1: g = scatter_gen<1>(md, first, count, s_pk, s_sd, s_h); break;
-        case 2: g = scatter_gen<2>(md, first, count, s_pk, s_sd, s_h); break;
-        case 3: g = scatter_gen<3>(md, first, count, s_pk, s_sd, s_h); break;
-        case 4: g = scatter_gen<4>(md, first, count, s_pk, s_sd, s_h); break;
-        case 5: g = scatter_gen<5>(md, first, count, s_pk, s_sd, s_h); break;
-        case 6: g = scatter_gen<6>(md, first, count, s_pk, s_sd, s_h); break;
-        case 7: g = scatter_gen<7>(md, first, count, s_pk, s_sd, s_h); break;
-        case 8: g = scatter_gen<8>(md, first, count, s_pk, s_sd, s_h); break;
+        case 1: g = scatter_gen<1>(md, first, count, s_kw, s_pp, s_f32, s_h); break;
+        case 2: g = scatter_gen<2>(md, first, count, s_kw, s_pp, s_f32, s_h); break;
+        case 3: g = scatter_gen<3>(md, first, count, s_kw, s_pp, s_f32, s_h); break;
+        case 4: g = scatter_gen<4>(md, first, count, s_kw, s_pp, s_f32, s_h); break;
+        case 5: g = scatter_gen<5>(md, first, count, s_kw, s_pp, s_f32, s_h); break;
+        case 6: g = scatter_gen<6>(md, first, count, s_kw, s_pp, s_f32, s_h); break;
+        case 7: g = scatter_gen<7>(md, first, count, s_kw, s_pp, s_f32, s_h); break;
+        case 8: g = scatter_gen<8>(md, first, count, s_kw, s_pp, s_f32, s_h); break;
         default: g = false; break;
       }
       ok &= g;
@@ -300,56 +308,56 @@ k_bscatter(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart, 
       ok = false;
     }
     __syncthreads();
-    for (u32 p = threadIdx.x; p < nparts && good; p += kScBlock) {
-      const u32 c = s_h[p];
-      if (c) s_h[p] = atomicAdd(&md.pcnt[p], c);
+    // reserve each range's space: a thread's (up to 16) atomics are issued together
+    for (u32 p0 = 0; p0 < nparts && good; p0 += kScBlock * 16) {
+      u32 c[16], g[16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const u32 p = p0 + threadIdx.x + (u32)k * kScBlock;
+        c[k] = p < nparts ? s_h[p] : 0u;
+      }
+#pragma unroll
+      for (int k = 0; k < 16; ++k) g[k] = c[k] ? atomicAdd(&md.pcnt[p0 + threadIdx.x + (u32)k * kScBlock], c[k]) : 0u;
+#pragma unroll
+      for (int k = 0; k < 16; ++k)
+        if (c[k]) s_h[p0 + threadIdx.x + (u32)k * kScBlock] = g[k];
     }
     __syncthreads();
+    bool over = false;
+#pragma unroll 4
     for (u32 i = threadIdx.x; i < count; i += kScBlock) {
-      const u64 pk = s_pk[i];
-      const u32 p = (u32)(pk >> 32) & 0xffffu;
-      const u32 g = s_h[p] + (u32)(pk >> 48);
+      const u32 pp = s_pp[i];
+      const u32 p = pp >> 12;
+      const u32 g = s_h[p] + (pp & 0xfffu);
       if (g < md.pcap) {
         const u64 at = (u64)p * md.pcap + g;
-        md.pkw[at] = (u32)pk;
-        md.psd[at] = s_sd[i];
+        md.pkw[at] = s_kw[i];
+        md.psd[at] = make_uint2(s_f32[i], (u32)(first + i));
       } else {
-        atomicOr(err, CF_ERR_PART_OVERFLOW);
+        over = true;
       }
     }
+    if (over) atomicOr(err, CF_ERR_PART_OVERFLOW);
     __syncthreads();
   }
   if (!ok) atomicOr(err, CF_ERR_BAD_ARG);
 }
 
-// Claim a slot in the shared-memory rows of one bucket range, with dtab_claim's
-// rule; returns false when the claim ran past the range's last bucket (only
-// when the range is not the whole table; a whole table wraps around).
-__device__ __forceinline__ bool place_claim(u32* s_fp, uint2* s_side, u32 nbp, bool whole, u32 b, u32 f16,
-                                            uint2 sd) {
+// Claim a slot in the shared-memory rows of one bucket range.  The range is
+// private to this CTA, so a per-bucket fill counter hands out slots 0, 1, 2, ...
+// in claim order (one shared atomic per claim): the occupied slots of a bucket
+// are a prefix, a bucket is full after 16 claims and later claims continue in the
+// next bucket -- the layout dtab_claim produces.  Returns false when the claim
+// ran past the range's last bucket (only when the range is not the whole table;
+// a whole table wraps around).
+__device__ __forceinline__ bool place_claim(unsigned short* s_fp16, uint2* s_side, u32* s_fill, u32 nbp, bool whole,
+                                            u32 b, u32 f16, uint2 sd) {
   for (u32 tries = 0; tries < nbp; ++tries) {
-    volatile u32* row = s_fp + b * 8;
-    int w = 8;
-    u32 cur = 0;
-#pragma unroll
-    for (int i = 7; i >= 0; --i) {
-      const u32 v = row[i];
-      if ((v & 0xffff0000u) == 0u) { w = i; cur = v; }
-    }
-    for (int spin = 0; w < 8 && spin < 32; ++spin) {
-      if ((cur & 0xffff0000u) != 0u) {
-        ++w;
-        cur = (w < 8) ? row[w] : 0u;
-        continue;
-      }
-      const bool lo_free = (cur & 0xffffu) == 0u;
-      const u32 nv = lo_free ? (cur | f16) : (cur | (f16 << 16));
-      const u32 prev = atomicCAS(s_fp + b * 8 + w, cur, nv);
-      if (prev == cur) {
-        s_side[b * 16 + 2 * w + (lo_free ? 0 : 1)] = sd;
-        return true;
-      }
-      cur = prev;
+    const u32 slot = atomicAdd(&s_fill[b], 1u);
+    if (slot < 16u) {
+      s_fp16[b * 16 + slot] = (unsigned short)f16;
+      s_side[b * 16 + slot] = sd;
+      return true;
     }
     if (++b == nbp) {
       if (!whole) return false;
@@ -359,13 +367,17 @@ __device__ __forceinline__ bool place_claim(u32* s_fp, uint2* s_side, u32 nbp, b
   return false;
 }
 
-__global__ void __launch_bounds__(kPlBlock, 1)
+template <int PLB>
+__global__ void __launch_bounds__(PlaceShape<PLB>::kBlock, PlaceShape<PLB>::kMinBlocks)
 k_bplace(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart, u32 nmod,
          unsigned long long* __restrict__ queue, CfOvf* __restrict__ ovf, u32 ovf_cap, u32* __restrict__ novf,
          u32* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int kPlBlock = PlaceShape<PLB>::kBlock;
+  constexpr u32 kPartBuckets = PlaceShape<PLB>::kBuckets;
   u32* s_fp = (u32*)smem;                                    // [kPartBuckets * 8]
   uint2* s_side = (uint2*)(s_fp + kPartBuckets * 8);         // [kPartBuckets * 16]
+  u32* s_fill = (u32*)(s_side + kPartBuckets * 16);          // [kPartBuckets] slots claimed
   __shared__ u64 s_t;
   const u64 total = tstart[nmod];
   for (;;) {
@@ -380,20 +392,37 @@ k_bplace(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart, u3
     }
     const CfBatchMod& md = mods[lo];
     const u32 p = (u32)(t - tstart[lo]);
+    if (md.plb != (u32)PLB) {                    // the launch's range size must be the modulus's
+      if (threadIdx.x == 0) atomicOr(err, CF_ERR_BAD_ARG);
+      __syncthreads();
+      continue;
+    }
     const u64 nb = 1ull << md.bbits;
     const u32 nbp = nb < kPartBuckets ? (u32)nb : kPartBuckets;
     const u64 b0 = (u64)p * nbp;
     const bool whole = nbp == nb;
     for (u32 i = threadIdx.x; i < nbp * 8; i += kPlBlock) s_fp[i] = 0;
+    for (u32 i = threadIdx.x; i < nbp; i += kPlBlock) s_fill[i] = 0;
     __syncthreads();
     const u32 cnt = min(md.pcnt[p], md.pcap);
     const u32* kw = md.pkw + (u64)p * md.pcap;
     const uint2* sd = md.psd + (u64)p * md.pcap;
-    for (u32 i = threadIdx.x; i < cnt; i += kPlBlock) {
-      const u32 k = kw[i];
-      const uint2 e = sd[i];
+    for (u32 i0 = 0; i0 < cnt; i0 += kPlBlock * kPlItems) {
+     u32 kk[kPlItems];
+     uint2 ee[kPlItems];
+#pragma unroll
+     for (int q = 0; q < kPlItems; ++q) {        // this thread's records, loads issued together
+       const u32 i = i0 + threadIdx.x + (u32)q * kPlBlock;
+       kk[q] = i < cnt ? __ldcs(kw + i) : 0u;
+       ee[q] = i < cnt ? __ldcs(sd + i) : make_uint2(0u, 0u);
+     }
+#pragma unroll
+     for (int q = 0; q < kPlItems; ++q) {
+      if (i0 + threadIdx.x + (u32)q * kPlBlock >= cnt) continue;
+      const u32 k = kk[q];
+      const uint2 e = ee[q];
       const u32 b = (k >> 16) & (nbp - 1u);
-      if (!place_claim(s_fp, s_side, nbp, whole, b, k & 0xffffu, e)) {
+      if (!place_claim((unsigned short*)s_fp, s_side, s_fill, nbp, whole, b, k & 0xffffu, e)) {
         if (whole) {
           atomicOr(err, CF_ERR_TABLE_FULL);
           continue;
@@ -412,6 +441,7 @@ k_bplace(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart, u3
           atomicOr(err, CF_ERR_TABLE_FULL);
         }
       }
+     }
     }
     __syncthreads();
     uint4* gfp = (uint4*)(md.fpw + b0 * 8);
@@ -526,7 +556,7 @@ extern "C" int cf_batch_run(int mode, const void* mods, const u64* tstart, u32 n
   return CF_OK;
 }
 
-extern "C" u32 cf_batch_part_buckets(void) { return kPartBuckets; }
+extern "C" u32 cf_batch_part_buckets(int lb) { return lb >= kPlbMin && lb <= kPlbMax ? 1u << lb : 0u; }
 extern "C" u32 cf_batch_part_tile(void) { return kScTile; }
 extern "C" u32 cf_batch_part_max_ranges(void) { return kScMaxParts; }
 extern "C" size_t cf_batch_ovf_bytes(void) { return sizeof(CfOvf); }
@@ -542,9 +572,9 @@ extern "C" size_t cf_batch_ovf_bytes(void) { return sizeof(CfOvf); }
 // CF_ERR_PART_OVERFLOW when a range received more than pcap records (the caller
 // rebuilds in place), CF_ERR_TABLE_FULL when the overflow list ran out.
 extern "C" int cf_batch_part(int phase, const void* mods, const u64* tstart, u32 nmod, void* queue, void* ovf,
-                             u32 ovf_cap, u32* novf, u32* err, u32 grid, void* stream) {
+                             u32 ovf_cap, u32* novf, u32* err, int part_lb, u32 grid, void* stream) {
   if (phase < 0 || phase > 2 || !mods || nmod == 0 || !err || (phase < 2 && (!tstart || !queue)) ||
-      (phase > 0 && (!novf || (ovf_cap && !ovf)))) {
+      (phase > 0 && (!novf || (ovf_cap && !ovf))) || (phase == 1 && (part_lb < kPlbMin || part_lb > kPlbMax))) {
     cf_set_error("cf_batch_part: bad arguments%s", "");
     return CF_EBADARG;
   }
@@ -555,14 +585,23 @@ extern "C" int cf_batch_part(int phase, const void* mods, const u64* tstart, u32
   if (phase == 0) {
     cudaError_t e = cudaFuncSetAttribute(k_bscatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScSmem);
     if (e != cudaSuccess) return cf_cuda_status(e, "cf_batch_part: smem attribute");
-    k_bscatter<<<grid ? grid : (u32)sms, kScBlock, kScSmem, st>>>((const CfBatchMod*)mods, tstart, nmod,
+    k_bscatter<<<grid ? grid : (u32)sms * kScMinBlocks, kScBlock, kScSmem, st>>>((const CfBatchMod*)mods, tstart, nmod,
                                                                  (unsigned long long*)queue, err);
   } else if (phase == 1) {
-    cudaError_t e = cudaFuncSetAttribute(k_bplace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlSmem);
-    if (e != cudaSuccess) return cf_cuda_status(e, "cf_batch_part: smem attribute");
-    k_bplace<<<grid ? grid : (u32)sms, kPlBlock, kPlSmem, st>>>((const CfBatchMod*)mods, tstart, nmod,
-                                                               (unsigned long long*)queue, (CfOvf*)ovf, ovf_cap,
-                                                               novf, err);
+    cudaError_t e;
+    if (part_lb == kPlbMax) {
+      using S = PlaceShape<kPlbMax>;
+      e = cudaFuncSetAttribute(k_bplace<kPlbMax>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem);
+      if (e != cudaSuccess) return cf_cuda_status(e, "cf_batch_part: smem attribute");
+      k_bplace<kPlbMax><<<grid ? grid : (u32)sms * S::kMinBlocks, S::kBlock, S::kSmem, st>>>(
+          (const CfBatchMod*)mods, tstart, nmod, (unsigned long long*)queue, (CfOvf*)ovf, ovf_cap, novf, err);
+    } else {
+      using S = PlaceShape<kPlbMin>;
+      e = cudaFuncSetAttribute(k_bplace<kPlbMin>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem);
+      if (e != cudaSuccess) return cf_cuda_status(e, "cf_batch_part: smem attribute");
+      k_bplace<kPlbMin><<<grid ? grid : (u32)sms * S::kMinBlocks, S::kBlock, S::kSmem, st>>>(
+          (const CfBatchMod*)mods, tstart, nmod, (unsigned long long*)queue, (CfOvf*)ovf, ovf_cap, novf, err);
+    }
   } else {
     k_bfix<<<32, 256, 0, st>>>((const CfBatchMod*)mods, (const CfOvf*)ovf, novf, ovf_cap, err);
   }

@@ -48,9 +48,7 @@ k_bgen_probe(int r, int n, u64 F, const u64* __restrict__ pool, const u64* __res
       if (!((cf_word8(u, v, bk.w0) & bk.m0) && (cf_word8(u, v, bk.w1) & bk.m1) && (cf_word8(u, v, bk.w2) & bk.m2)))
         continue;
     }
-    const CfFuseKey fk = cf_fuse_key(X, 0u, tab.bbits);
-    const uint4* row = (const uint4*)(tab.fpw + (u64)fk.bucket * 8);
-    if (probe_fast(__ldg(row), __ldg(row + 1), fk.f16)) probe_slow(tab, fk.bucket, fk.f16, fk.f32, iid, sink);
+    dtab_probe(tab, cf_fuse_key(X, 0u, tab.bbits), iid, sink);
   }
 }
 

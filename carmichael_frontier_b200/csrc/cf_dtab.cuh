@@ -188,14 +188,37 @@ static __device__ __noinline__ void probe_slow(const DTab& t, u64 b, u32 f16, u3
 // Nonzero iff some 16-bit half of w is zero (SWAR test; exact, no false positives).
 __device__ __forceinline__ u32 cf_zero_half(u32 w) { return (w - 0x00010001u) & ~w & 0x80008000u; }
 
-// Fast test of one bucket: any 16-bit fingerprint equal to f16 (hit), or the
-// bucket is full.  Slots are claimed in order, so the bucket is full exactly
-// when its last slot (the high half of the last word) is occupied.
-__device__ __forceinline__ bool probe_fast(uint4 r0, uint4 r1, u32 f16) {
+// Any 16-bit fingerprint of a bucket's row equal to f16 (SWAR over the eight
+// words).  Slots are claimed in order, so the bucket is full exactly when its
+// last slot (the high half of the last word) is occupied.
+__device__ __forceinline__ bool probe_match(uint4 r0, uint4 r1, u32 f16) {
   const u32 ff = f16 * 0x10001u;
   const u32 eq = cf_zero_half(r0.x ^ ff) | cf_zero_half(r0.y ^ ff) | cf_zero_half(r0.z ^ ff) |
                  cf_zero_half(r0.w ^ ff) | cf_zero_half(r1.x ^ ff) | cf_zero_half(r1.y ^ ff) |
                  cf_zero_half(r1.z ^ ff) | cf_zero_half(r1.w ^ ff);
-  return (eq != 0u) | ((r1.w >> 16) != 0u);
+  return eq != 0u;
+}
+
+// Probe the table for one residue.  The bucket's fingerprint row is tested in
+// registers and, while that bucket is full, so are the rows after it (a full
+// bucket is common at 8-12 records per bucket, and sending it to the cold path
+// would hold up the whole warp); only a 16-bit fingerprint match, or a chain
+// longer than kProbeHops rows, takes the cold path, which emits the matches of
+// the chain from that bucket on.
+constexpr int kProbeHops = 4;
+__device__ __forceinline__ void dtab_probe(const DTab& t, const CfFuseKey& fk, u64 rank, const CfPairSink& o) {
+  u64 b = fk.bucket;
+#pragma unroll 1
+  for (int hop = 0;; ++hop) {
+    const uint4* row = (const uint4*)(t.fpw + b * 8);
+    const uint4 r0 = __ldg(row), r1 = __ldg(row + 1);
+    const bool full = (r1.w >> 16) != 0u;
+    if (probe_match(r0, r1, fk.f16) || (full && hop == kProbeHops - 1)) {
+      probe_slow(t, b, fk.f16, fk.f32, rank, o);
+      return;
+    }
+    if (!full) return;
+    b = (b + 1) & (t.nb - 1);
+  }
 }
 

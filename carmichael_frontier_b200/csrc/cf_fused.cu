@@ -119,10 +119,7 @@ k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo
                             (cf_word8(a, c, bk.w2) & bk.m2);
             if (!in) continue;
           }
-          const CfFuseKey fk = cf_fuse_key(X, x2, tab.bbits);
-          const uint4* row = (const uint4*)(tab.fpw + (u64)fk.bucket * 8);
-          if (probe_fast(__ldg(row), __ldg(row + 1), fk.f16))
-            probe_slow(tab, fk.bucket, fk.f16, fk.f32, rank_base + off, sink);
+          dtab_probe(tab, cf_fuse_key(X, x2, tab.bbits), rank_base + off, sink);
         }
       }
     }

@@ -45,9 +45,7 @@ k_rec_probe(const u64* __restrict__ keys, u64 n, DTab tab, CfPairSink sink) {
       if (!((cf_word8(a, c, bk.w0) & bk.m0) && (cf_word8(a, c, bk.w1) & bk.m1) && (cf_word8(a, c, bk.w2) & bk.m2)))
         continue;
     }
-    const CfFuseKey fk = cf_fuse_key(X, 0u, tab.bbits);
-    const uint4* row = (const uint4*)(tab.fpw + (u64)fk.bucket * 8);
-    if (probe_fast(__ldg(row), __ldg(row + 1), fk.f16)) probe_slow(tab, fk.bucket, fk.f16, fk.f32, i, sink);
+    dtab_probe(tab, cf_fuse_key(X, 0u, tab.bbits), i, sink);
   }
 }
 

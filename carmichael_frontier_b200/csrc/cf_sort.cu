@@ -65,6 +65,21 @@ __global__ void k_sort_hist_scan(const u64* __restrict__ hist, u64* __restrict__
   }
 }
 
+// Lanes of this warp whose BITS-bit value (the 8-bit digit; a ninth bit marks
+// "no item" in a partial tile) equals this lane's, from one ballot per bit (the
+// vote unit issues these at full rate, where a match-any instruction is far slower).
+template <int BITS>
+__device__ __forceinline__ u32 peer_mask(u32 d) {
+  u32 m = 0xffffffffu;
+#pragma unroll
+  for (int b = 0; b < BITS; ++b) {
+    const u32 bit = (d >> b) & 1u;
+    const u32 v = __ballot_sync(0xffffffffu, bit);
+    m &= bit ? v : ~v;
+  }
+  return m;
+}
+
 __device__ __forceinline__ u32 lanemask_lt() {
   u32 m;
   asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -105,7 +120,7 @@ __device__ __forceinline__ bool mbar_wait(u64* bar, u32 parity, u32 limit) {
 // Write a staged tile (staged element j has digit s_dj[j]) to its global places,
 // kSortItems elements per thread with their shared-memory loads issued together.
 __device__ __forceinline__ void write_tile(const u64* s_v, const unsigned char* s_dj, const u64* s_gbase,
-                                           const u32* s_doff, u64* __restrict__ out, int tv) {
+                                           u64* __restrict__ out, int tv) {
   u32 d[kSortItems];
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
@@ -116,7 +131,7 @@ __device__ __forceinline__ void write_tile(const u64* s_v, const unsigned char* 
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
     const int j = threadIdx.x + k * kSortBlock;
-    dst[k] = s_gbase[d[k]] + (u64)(j - (int)s_doff[d[k]]);
+    dst[k] = s_gbase[d[k]] + (u64)j;
     v[k] = s_v[j < tv ? j : 0];
   }
 #pragma unroll
@@ -147,7 +162,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
   __shared__ u32 s_tile;
   __shared__ u32 s_dcnt[kRadix];
   __shared__ u32 s_doff[kRadix];
-  __shared__ u64 s_gbase[kRadix];
+  __shared__ u64 s_gbase[kRadix];   // global position of staged element j of digit d: s_gbase[d] + j
   __shared__ u32 s_scan[kWarps];
 
   if (threadIdx.x == 0) {
@@ -205,7 +220,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
     const int e = wid * 32 * kSortItems + it * 32 + lane;
     const u32 d = e < tv ? (u32)((key[it] >> shift) & 0xff) : 0x100u;
     loc[it] = d << 16;
-    peers[it] = __match_any_sync(0xffffffffu, d);
+    peers[it] = tv == kSortTile ? peer_mask<8>(d) : peer_mask<9>(d);
   }
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
@@ -232,8 +247,9 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
       run += v[w];
     }
     s_dcnt[d] = run;
+    // flag and count share one 64-bit word and readers read nothing else that this
+    // tile writes, so the status store needs no fence before it
     const u64 pub = (tile == 0) ? (kFlagInc | (u64)run) : (kFlagAgg | (u64)run);
-    __threadfence();
     ((volatile u64*)status)[(u64)tile * kRadix + d] = pub;
     u32 incl = run;
 #pragma unroll
@@ -274,12 +290,14 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
         }
         if (stop) break;
         j -= used;
-        if (used == 0 && ++spins > kSpinLimit) { atomicOr(err, CF_ERR_SPIN_LIMIT); break; }
+        if (used == 0) {                       // predecessor not published yet: back off briefly
+          if (++spins > kSpinLimit) { atomicOr(err, CF_ERR_SPIN_LIMIT); break; }
+          __nanosleep(64);
+        }
       }
-      __threadfence();
       ((volatile u64*)status)[(u64)tile * kRadix + d] = kFlagInc | (excl + s_dcnt[d]);
     }
-    s_gbase[d] = gexcl[d] + excl;
+    s_gbase[d] = gexcl[d] + excl - s_doff[d];   // wraps mod 2^64; j >= s_doff[d] brings it back
   }
   __syncthreads();
   {
@@ -301,7 +319,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
     }
   }
   __syncthreads();
-  write_tile(s_kin, s_dj, s_gbase, s_doff, kout, tv);
+  write_tile(s_kin, s_dj, s_gbase, kout, tv);
   if (BULK && !mbar_wait(&s_bar[1], 0, kMbarLimit)) {
     atomicOr(err, CF_ERR_SPIN_LIMIT);
     mbar_wait(&s_bar[1], 0, kMbarLimit);
@@ -319,7 +337,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
       if ((loc[it] >> 16) < 0x100u) s_kin[loc[it] & 0xffffu] = idv[it];
   }
   __syncthreads();
-  write_tile(s_kin, s_dj, s_gbase, s_doff, iout, tv);
+  write_tile(s_kin, s_dj, s_gbase, iout, tv);
 }
 
 // ---------------------------------------------------------------------------

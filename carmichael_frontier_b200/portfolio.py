@@ -40,7 +40,7 @@ MOD_DTYPE = np.dtype([
     ("fpw", "<u8"), ("side", "<u8"), ("fill", "<u8"), ("bloom", "<u8"),
     ("nD", "<u8"), ("i_lo", "<u8"), ("nI", "<u8"),
     ("bbits", "<i4"), ("fbits", "<i4"), ("r", "<i4"), ("swap", "<i4"),
-    ("pkw", "<u8"), ("psd", "<u8"), ("pcnt", "<u8"), ("pcap", "<u4"), ("pad_", "<u4")])
+    ("pkw", "<u8"), ("psd", "<u8"), ("pcnt", "<u8"), ("pcap", "<u4"), ("plb", "<u4")])
 
 _ALIGN = 256
 
@@ -64,6 +64,7 @@ class BatchTuning:
     dtab: Tuning = field(default_factory=Tuning)   # D-table sizing (dtab_load, Bloom level)
     part_build: bool = True            # partitioned table build for tables above part_min_buckets
     part_min_buckets: int = 1 << 16    # smaller tables (L2-resident) are built in place
+    part_lb: int = 10                  # log2 buckets per range of the partitioned build (9 or 10)
     part_sigma: float = 8.0            # bucket-range capacity = mean + sigma*sqrt(mean) + 32
     ovf_capacity: int = 1 << 16        # records that ran past their bucket range (per batch)
 
@@ -200,8 +201,9 @@ class BatchSolver:
             _lib.check(lib.cf_build_tail(base + offs[(k, "pI")], len(x.INS), x.r, tbase + toffs[(k, "tI")], sh),
                        "cf_build_tail(I)")
         # partitioned build: (ranges, range capacity) per modulus, None when built in place
-        lib_pb = lib.cf_batch_part_buckets()
-        plb = lib_pb.bit_length() - 1
+        plb = tu.part_lb
+        if not lib.cf_batch_part_buckets(plb):
+            raise ValueError(f"part_lb {plb} is not supported by the partitioned build")
         part: dict = {}
         for k in batched:
             bb, _fb = shapes[k]
@@ -244,6 +246,7 @@ class BatchSolver:
                     npt, cap = part[k]
                     poff_rel += _up(npt * cap * 4) + _up(npt * cap * 8)
                     rows[j]["pcap"] = cap
+                    rows[j]["plb"] = plb
                 rows[j]["poolD"] = base + offs[(k, "pD")]
                 rows[j]["poolI"] = base + offs[(k, "pI")]
                 rows[j]["screen"] = base + offs[(k, "sc")]
@@ -328,11 +331,12 @@ class BatchSolver:
         part = b.use_part and b.n_part > 0
         if part:
             oc = self.tuning.ovf_capacity
-            ck(lib.cf_batch_part(0, dp(b.mods), dp(b.tsS), nmod, m + 32, None, 0, m + 24, m + 20, 0, sh),
+            lb = self.tuning.part_lb
+            ck(lib.cf_batch_part(0, dp(b.mods), dp(b.tsS), nmod, m + 32, None, 0, m + 24, m + 20, lb, 0, sh),
                "cf_batch_part(scatter)")
-            ck(lib.cf_batch_part(1, dp(b.mods), dp(b.tsP), nmod, m + 40, dp(ovf), oc, m + 24, m + 20, 0, sh),
+            ck(lib.cf_batch_part(1, dp(b.mods), dp(b.tsP), nmod, m + 40, dp(ovf), oc, m + 24, m + 20, lb, 0, sh),
                "cf_batch_part(place)")
-            ck(lib.cf_batch_part(2, dp(b.mods), None, nmod, None, dp(ovf), oc, m + 24, m + 20, 0, sh),
+            ck(lib.cf_batch_part(2, dp(b.mods), None, nmod, None, dp(ovf), oc, m + 24, m + 20, lb, 0, sh),
                "cf_batch_part(fix)")
         ck(lib.cf_batch_run(0, dp(b.mods), dp(b.tsD if part else b.tsD_all), nmod, tu.ticket, m, dp(pairs), dp(pmod),
                             maxp, m + 16, m + 20, None, tu.grid, sh), "cf_batch_run(build)")

@@ -256,7 +256,7 @@ int cf_part_scatter(const uint64_t* keys, const uint64_t* ids, uint64_t n, uint6
  * mods: device array of nmod descriptors of cf_batch_mod_bytes() bytes each
  *   {poolD, tailD, poolI, tailI, screen, fpw, side, fill, bloom (8-byte
  *    pointers); nD, i_lo, nI (u64); bbits, fbits, r, swap (i32);
- *    pkw, psd, pcnt (8-byte pointers); pcap, pad (u32)} -- the last five
+ *    pkw, psd, pcnt (8-byte pointers); pcap, plb (u32)} -- the last five
  *    describe the partitioned build below (pcap = 0: built by mode 0)
  * with the D-table areas laid out as cf_dtab_build2's (fingerprints 32 B, side
  * 128 B, fill 4 B per bucket; Bloom filter 32 B per block) but placed by the
@@ -277,14 +277,16 @@ int cf_batch_run(int mode, const void* mods, const uint64_t* tstart, uint32_t nm
 
 /* Partitioned table build for the batch (moduli with pcap > 0), in place of
  * mode 0 for tables larger than L2: phase 0 generates each table side and
- * scatters its records into bucket ranges of cf_batch_part_buckets() buckets
+ * scatters its records into bucket ranges of 2^plb buckets (plb 9 or 10, the
+ * same for every modulus of one phase-1 launch, given as part_lb; 0 from
+ * cf_batch_part_buckets(lb) means lb is not supported)
  * (pkw: range-local bucket << 16 | 16-bit fingerprint, psd: side entry; pcap
  * records per range, counts in pcnt, zeroed by the caller); phase 1 builds each
  * range in shared memory and writes its fingerprint rows and side entries out
  * whole; phase 2 inserts the few records that ran past the end of their range.
  * tstart: phase 0, prefix sums of ceil(table-side records / cf_batch_part_tile());
- * phase 1, prefix sums of the ranges per modulus (2^max(0, bbits - log2
- * cf_batch_part_buckets()), at most cf_batch_part_max_ranges()); 0 for moduli
+ * phase 1, prefix sums of the ranges per modulus (2^max(0, bbits - plb), at most
+ * cf_batch_part_max_ranges()); 0 for moduli
  * built by mode 0.  queue: device u64 zeroed before phases 0 and 1; ovf:
  * ovf_cap entries of cf_batch_ovf_bytes(), *novf zeroed before phase 1.
  * CF_ERR_PART_OVERFLOW in *err: a range received more than pcap records and
@@ -292,12 +294,12 @@ int cf_batch_run(int mode, const void* mods, const uint64_t* tstart, uint32_t nm
  * (same slots rule), so mode 1 probes it unchanged.  Replaces, like mode 0, the
  * D-side table build of the reference's join (recD, src/mitm64.cpp:51-73;
  * sort_side of the D chunk, gpu/mitm_gpu2.py:101-104). */
-uint32_t cf_batch_part_buckets(void);
+uint32_t cf_batch_part_buckets(int lb);
 uint32_t cf_batch_part_tile(void);
 uint32_t cf_batch_part_max_ranges(void);
 size_t cf_batch_ovf_bytes(void);
 int cf_batch_part(int phase, const void* mods, const uint64_t* tstart, uint32_t nmod, void* queue, void* ovf,
-                  uint32_t ovf_cap, uint32_t* novf, uint32_t* err, uint32_t grid, void* stream);
+                  uint32_t ovf_cap, uint32_t* novf, uint32_t* err, int part_lb, uint32_t grid, void* stream);
 
 /* ---- sorted-side drop-ins ------------------------------------------------ */
 

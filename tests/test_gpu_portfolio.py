@@ -123,21 +123,22 @@ def test_batch_autotuner_keeps_results(cuda):
 
 def test_batched_partitioned_build_matches_in_place(cuda):
     # tables at 12 records per 16-slot bucket (about one bucket in ten overflows, some of
-    # them at the end of a 1024-bucket range), tiny whole-table ranges, and the in-place build
+    # them at the end of a bucket range), tiny whole-table ranges, both range sizes, and the in-place build
     from carmichael_frontier_b200.solve import Tuning
     insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config3(6)]
     insts += small_portfolio(3, 8)
     lim = 12 << 17
     dense = Tuning(dtab_load=12.0)
-    part = BatchSolver(cuda, tuning=BatchTuning(dtab=dense, part_min_buckets=16))
-    prep = part.prepare(insts, i_limit=lim)
-    assert sum(b.n_part for b in prep.batches) >= 10
-    got = part.run(prep)
-    assert all(b.use_part for b in prep.batches)
     inplace = BatchSolver(cuda, tuning=BatchTuning(dtab=dense, part_build=False)).solve(insts, i_limit=lim)
     one = run_per_modulus(insts, i_limit=lim, solver=Solver(cuda))
-    for a, b, c in zip(got, inplace, one):
-        assert summary(a) == summary(b) == summary(c)
+    for lb in (9, 10):
+        part = BatchSolver(cuda, tuning=BatchTuning(dtab=dense, part_min_buckets=16, part_lb=lb))
+        prep = part.prepare(insts, i_limit=lim)
+        assert sum(b.n_part for b in prep.batches) >= 10
+        got = part.run(prep)
+        assert all(b.use_part for b in prep.batches)
+        for a, b, c in zip(got, inplace, one):
+            assert summary(a) == summary(b) == summary(c)
 
 
 def test_batched_partitioned_range_overflow_falls_back(cuda):
