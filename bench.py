@@ -301,6 +301,8 @@ def run_ours(args):
         n_b0, n_ins = len(w.B0), len(w.INS)
         lib = _lib.load()
         h2d += lib.cf_pool_bytes(n_b0, w.r) + lib.cf_pool_bytes(n_ins, w.r) + lib.cf_screen_bytes()
+        h2d += getattr(s, "h2d_desc_bytes", 0)   # table-build descriptor of the partitioned build
+        s.h2d_desc_bytes = 0
         d2h += 8 + res.residue_pairs * lib.cf_pair_result_bytes()
     f1.record(stream)
     torch.cuda.synchronize(dev)

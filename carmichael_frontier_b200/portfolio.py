@@ -32,15 +32,9 @@ import numpy as np
 
 from . import _lib
 from .certify import verify_certificate
-from .solve import (RESULT_DTYPE, Hit, Instance, SolveResult, Solver, Tuning, dtab_shape, finish_rows)
+from .solve import (MOD_DTYPE, RESULT_DTYPE, Hit, Instance, SolveResult, Solver, Tuning, dtab_shape, finish_rows,
+                    part_shape)
 from .tables import ncomb, pool_table_host, screen_table_host
-
-MOD_DTYPE = np.dtype([
-    ("poolD", "<u8"), ("tailD", "<u8"), ("poolI", "<u8"), ("tailI", "<u8"), ("screen", "<u8"),
-    ("fpw", "<u8"), ("side", "<u8"), ("fill", "<u8"), ("bloom", "<u8"),
-    ("nD", "<u8"), ("i_lo", "<u8"), ("nI", "<u8"),
-    ("bbits", "<i4"), ("fbits", "<i4"), ("r", "<i4"), ("swap", "<i4"),
-    ("pkw", "<u8"), ("psd", "<u8"), ("pcnt", "<u8"), ("pcap", "<u4"), ("plb", "<u4")])
 
 _ALIGN = 256
 
@@ -207,11 +201,10 @@ class BatchSolver:
         part: dict = {}
         for k in batched:
             bb, _fb = shapes[k]
-            nparts = 1 << max(0, bb - plb)
-            if tu.part_build and (1 << bb) >= tu.part_min_buckets and nparts <= lib.cf_batch_part_max_ranges():
-                mean = min(nD[k], nI[k]) / nparts
-                cap = int(math.ceil(mean + tu.part_sigma * math.sqrt(mean) + 32))
-                part[k] = (nparts, (cap + 3) // 4 * 4)
+            if tu.part_build and (1 << bb) >= tu.part_min_buckets:
+                ps = part_shape(min(nD[k], nI[k]), bb, plb, tu.part_sigma, lib.cf_batch_part_max_ranges())
+                if ps is not None:
+                    part[k] = ps
         # batches: consecutive moduli whose D tables fit the budget
         batches, cur, cur_bytes = [], [], 0
         for k in batched:

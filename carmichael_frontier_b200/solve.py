@@ -31,6 +31,26 @@ from .certify import verify_certificate
 from .tables import DeviceTables, ncomb, unrank_lex
 
 RESULT_DTYPE = np.dtype([("flags", "<u4"), ("r", "<u4"), ("d_idx", "<u2", (16,)), ("i_idx", "<u2", (16,))])
+
+# One modulus of the batched kernels (CfBatchMod, cf_batch_mod_bytes() bytes); the
+# single-modulus solve uses a one-row array of it for the partitioned table build.
+MOD_DTYPE = np.dtype([
+    ("poolD", "<u8"), ("tailD", "<u8"), ("poolI", "<u8"), ("tailI", "<u8"), ("screen", "<u8"),
+    ("fpw", "<u8"), ("side", "<u8"), ("fill", "<u8"), ("bloom", "<u8"),
+    ("nD", "<u8"), ("i_lo", "<u8"), ("nI", "<u8"),
+    ("bbits", "<i4"), ("fbits", "<i4"), ("r", "<i4"), ("swap", "<i4"),
+    ("pkw", "<u8"), ("psd", "<u8"), ("pcnt", "<u8"), ("pcap", "<u4"), ("plb", "<u4")])
+
+
+def part_shape(n_build: int, bbits: int, lb: int, sigma: float, max_ranges: int) -> tuple[int, int] | None:
+    """(bucket ranges, records per range) of the partitioned table build of n_build
+    records into 2^bbits buckets, or None when the table has too many ranges."""
+    nparts = 1 << max(0, bbits - lb)
+    if nparts > max_ranges:
+        return None
+    mean = n_build / nparts
+    cap = int(math.ceil(mean + sigma * math.sqrt(mean) + 32))
+    return nparts, (cap + 3) // 4 * 4
 ALL_FLAGS = (_lib.HIT_KEY_EQUAL | _lib.HIT_SCREEN | _lib.HIT_SIZE_EXACT | _lib.HIT_KORSELT | _lib.HIT_DISJOINT)
 
 
@@ -81,6 +101,10 @@ class Tuning:
     l2_table_bytes: int = 72 << 20  # fingerprint arrays above this get a Bloom-filter first level
     max_fbits: int = 21             # Bloom filter at most 2^21 blocks of 32 bytes (64 MB)
     max_nodes: int = 1 << 27        # bounded strategy: frontier nodes per block of first indices
+    part_build: bool = True         # fused: partitioned table build for tables of part_min_buckets or more
+    part_min_buckets: int = 1 << 21 # smaller tables stay in L2 while built alone: built in place
+    part_lb: int = 10               # log2 buckets per range of the partitioned build (9 or 10)
+    part_sigma: float = 8.0         # bucket-range capacity = mean + sigma*sqrt(mean) + 32
 
 
 def dtab_shape(nD: int, tu: Tuning) -> tuple[int, int]:
@@ -303,9 +327,16 @@ class Solver:
         sideI = (dp(poolI), dp(tailI), len(inst.INS), nIt)
         bpool, btail, bn, bcount = sideI if swap else sideD
         ppool, ptail, pn, pcount = sideD if swap else sideI
+        tu = self.tuning
+        pshape = None
+        if tu.part_build and not plan.get("no_part") and nb >= tu.part_min_buckets and r <= lib.cf_batch_max_r():
+            pshape = part_shape(bcount, bbits, tu.part_lb, tu.part_sigma, lib.cf_batch_part_max_ranges())
         self._mark(marks, "start")
-        ck(lib.cf_dtab_build2(bpool, btail, bn, r, 0, bcount, dp(tab), bbits, fbits, dp(misc) + 4, sh),
-           "cf_dtab_build")
+        if pshape is not None:
+            self._part_build(inst, plan, pshape, (poolD, poolI, tailD, tailI, screen), tab, nD, nIt, swap, misc)
+        else:
+            ck(lib.cf_dtab_build2(bpool, btail, bn, r, 0, bcount, dp(tab), bbits, fbits, dp(misc) + 4, sh),
+               "cf_dtab_build")
         self._mark(marks, "gen_D")
         ck(lib.cf_fused_probe2(ppool, ptail, pn, r, 0, pcount, dp(tab), bbits, fbits, 0, int(swap), dp(pairs),
                                maxp, dp(misc), dp(misc) + 4, self.tuning.fused_grid, sh), "cf_fused_probe")
@@ -314,6 +345,58 @@ class Solver:
                               dp(misc) + 4, sh), "cf_check_pairs")
         self._mark(marks, "check")
         return dict(misc=misc, dcnt=None, icnt=None, res=res, nD=nD, nI=nIt, plan=plan, launches=3)
+
+    def _part_build(self, inst: Instance, plan: dict, pshape: tuple, tables: tuple, tab, nD: int, nIt: int,
+                    swap: bool, misc):
+        """Partitioned table build (scatter by bucket range, shared-memory range build,
+        overflow fix-up) through a one-modulus descriptor of the batched kernels."""
+        torch, lib = self.torch, self.lib
+        dp, ck, sh = _lib.ptr, _lib.check, self._sh()
+        poolD, poolI, tailD, tailI, screen = tables
+        bbits, fbits = plan["bbits"], plan.get("fbits", 0)
+        nb = 1 << bbits
+        nparts, cap = pshape
+        n_build = nIt if swap else nD
+        tile = lib.cf_batch_part_tile()
+        # scratch: range counters, then the records of every range (4 + 8 bytes each)
+        ocap = 1 << 12
+        obytes = ocap * lib.cf_batch_ovf_bytes()
+        up = lambda x: (x + 255) // 256 * 256
+        scr = self._buf("pscratch", up(nparts * 4) + up(64) + up(obytes) + up(nparts * cap * 4) + nparts * cap * 8)
+        base = dp(scr)
+        pcnt, pmisc = base, base + up(nparts * 4)
+        ovf = pmisc + up(64)
+        pkw = ovf + up(obytes)
+        psd = pkw + up(nparts * cap * 4)
+        row = np.zeros(1, dtype=MOD_DTYPE)
+        row["poolD"], row["tailD"], row["poolI"], row["tailI"] = dp(poolD), dp(tailD), dp(poolI), dp(tailI)
+        row["screen"] = dp(screen)
+        t0 = dp(tab)
+        row["fpw"], row["side"], row["fill"] = t0, t0 + 32 * nb, t0 + 160 * nb
+        row["bloom"] = t0 + 164 * nb if fbits else 0
+        row["nD"], row["i_lo"], row["nI"] = nD, 0, nIt
+        row["bbits"], row["fbits"], row["r"], row["swap"] = bbits, fbits, inst.r, int(swap)
+        row["pkw"], row["psd"], row["pcnt"], row["pcap"], row["plb"] = pkw, psd, pcnt, cap, self.tuning.part_lb
+        host = np.zeros(MOD_DTYPE.itemsize // 8 + 4, dtype=np.uint64)
+        host[: MOD_DTYPE.itemsize // 8] = row.view(np.uint64)
+        k = MOD_DTYPE.itemsize // 8
+        host[k:k + 4] = (0, -(-n_build // tile), 0, nparts)        # scatter and range ticket prefix sums
+        # pinned staging, rewritten only after the previous solve has been collected
+        if getattr(self, "_pdesc_host", None) is None or self._pdesc_host.numel() < host.nbytes:
+            self._pdesc_host = torch.empty(host.nbytes, dtype=torch.uint8, pin_memory=True)
+        self._pdesc_host[: host.nbytes].numpy()[:] = host.view(np.uint8)
+        hdev = self._buf("pdesc", host.nbytes)
+        with torch.cuda.stream(self._torch_stream()):
+            hdev[: host.nbytes].copy_(self._pdesc_host[: host.nbytes], non_blocking=True)
+        self.h2d_desc_bytes = getattr(self, "h2d_desc_bytes", 0) + host.nbytes
+        mods, tsS, tsP = dp(hdev), dp(hdev) + 8 * k, dp(hdev) + 8 * k + 16
+        scr[: up(nparts * 4) + 64].zero_()
+        err = dp(misc) + 4
+        lb = self.tuning.part_lb
+        ck(lib.cf_batch_part(0, mods, tsS, 1, pmisc, None, 0, pmisc + 24, err, lb, 0, sh), "cf_batch_part(scatter)")
+        ck(lib.cf_batch_part(1, mods, tsP, 1, pmisc + 8, ovf, ocap, pmisc + 24, err, lb, 0, sh),
+           "cf_batch_part(place)")
+        ck(lib.cf_batch_part(2, mods, None, 1, None, ovf, ocap, pmisc + 24, err, lb, 0, sh), "cf_batch_part(fix)")
 
     def _enqueue_partition(self, inst: Instance, plan: dict, marks: list | None):
         """Partitioned generation of both sides and the shared-memory partition join."""
@@ -377,7 +460,9 @@ class Solver:
             raise _lib.CfError(_lib.CF_EOVERFLOW, "solve", "D table full (internal error)")
         if err & (_lib.ERR_PART_OVERFLOW | _lib.ERR_PAIR_OVERFLOW):
             newp = dict(plan)
-            if err & _lib.ERR_PART_OVERFLOW:
+            if err & _lib.ERR_PART_OVERFLOW and h["dcnt"] is None:
+                newp["no_part"] = True          # fused: a bucket range of the table build overflowed
+            elif err & _lib.ERR_PART_OVERFLOW:
                 dmax = int(h["dcnt"].max().item())
                 imax = int(h["icnt"].max().item())
                 newp["capD"] = max(plan["capD"], dmax + 16)
@@ -439,6 +524,7 @@ class Solver:
             plan = self.plan(nD, nI, newp["capD"], newp["capI"], newp["pairs"])
             plan["strategy"] = newp.get("strategy", plan["strategy"])
             plan["i_limit"] = i_limit
+            plan["no_part"] = newp.get("no_part", False)
         raise _lib.CfError(_lib.CF_EOVERFLOW, "solve", "capacities kept overflowing")
 
     def _torch_stream(self):

@@ -104,3 +104,21 @@ def test_config2_with_bloom_first_level(cuda, golden, idx):
     res = s.solve(g["M"], g["Q"], g["B0"], g["r"], int(g["B"]))
     assert res.plan["fbits"] > 0
     assert as_lists(res.pairs) == g["pairs"]
+
+
+def _pair_summary(res):
+    return (res.n_D, res.n_I, res.residue_pairs, sorted(res.pairs), [(h.D, h.I, h.n) for h in res.hits])
+
+
+def test_partitioned_table_build_matches_in_place(cuda, golden):
+    # the fused solve's table built by range scatter + shared-memory range builds (default),
+    # by the in-place build, and with range capacities too small (rebuilt in place on overflow)
+    insts = [Instance.build(g["M"], g["Q"], g["B0"], g["r"], int(g["B"])) for g in golden["config2"][:2]]
+    insts.append(Instance.build(*(lambda w: (w.M, w.Q, w.B0, w.r, w.B))(W.config3(2)[1])))
+    lim = 1 << 21
+    ref = [_pair_summary(Solver(cuda, tuning=Tuning(part_build=False)).solve_instance(x, i_limit=lim))
+           for x in insts]
+    for tu in (Tuning(part_min_buckets=16), Tuning(part_min_buckets=16, part_lb=9),
+               Tuning(part_min_buckets=16, part_sigma=-6.0), Tuning(part_min_buckets=16, dtab_load=12.0)):
+        s = Solver(cuda, tuning=tu)
+        assert [_pair_summary(s.solve_instance(x, i_limit=lim)) for x in insts] == ref
