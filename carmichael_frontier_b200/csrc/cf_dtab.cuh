@@ -206,12 +206,29 @@ __device__ __forceinline__ bool probe_match(uint4 r0, uint4 r1, u32 f16) {
 // longer than kProbeHops rows, takes the cold path, which emits the matches of
 // the chain from that bucket on.
 constexpr int kProbeHops = 4;
+
+// One bucket's 32-byte fingerprint row.  With a 32-byte aligned table it is one
+// 256-bit load that bypasses L1 (a random row has no reuse there, and one request
+// per probe instead of two halves the L1 traffic that bounds the probe);
+// otherwise two 128-bit loads.
+__device__ __forceinline__ void dtab_row(const u32* row, bool wide, uint4& r0, uint4& r1) {
+  if (wide) {
+    asm("ld.global.nc.L1::no_allocate.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(r0.x), "=r"(r0.y), "=r"(r0.z), "=r"(r0.w), "=r"(r1.x), "=r"(r1.y), "=r"(r1.z), "=r"(r1.w)
+        : "l"(row));
+  } else {
+    r0 = __ldg((const uint4*)row);
+    r1 = __ldg((const uint4*)row + 1);
+  }
+}
+
 __device__ __forceinline__ void dtab_probe(const DTab& t, const CfFuseKey& fk, u64 rank, const CfPairSink& o) {
   u64 b = fk.bucket;
+  const bool wide = ((uintptr_t)t.fpw & 31u) == 0u;
 #pragma unroll 1
   for (int hop = 0;; ++hop) {
-    const uint4* row = (const uint4*)(t.fpw + b * 8);
-    const uint4 r0 = __ldg(row), r1 = __ldg(row + 1);
+    uint4 r0, r1;
+    dtab_row(t.fpw + b * 8, wide, r0, r1);
     const bool full = (r1.w >> 16) != 0u;
     if (probe_match(r0, r1, fk.f16) || (full && hop == kProbeHops - 1)) {
       probe_slow(t, b, fk.f16, fk.f32, rank, o);
