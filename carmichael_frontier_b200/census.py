@@ -1,0 +1,231 @@
+"""Census producers: which moduli a 64-factor search must run, and their batched portfolios.
+
+The exchange join searches one family lambda(n) | M at a time; the census decides which moduli those
+are.  For an incumbent U (a Carmichael number with 64 prime factors) and M = lambda(U), every
+Carmichael n with 64 factors, n < U and lambda(n) | M has lambda(n) = D for some divisor D of M, all
+its primes in Q(D) = {q prime : (q-1) | D, q does not divide D} and n = 1 (mod D).  A divisor can carry
+such an n only if the 64 smallest primes of Q(D) multiply to less than U (a "survivor"); for a
+survivor every qualifying 64-subset uses primes q <= cap(D) = (U-1) // T63(D) only (T63 = product of
+the 63 smallest) and differs from the 64 smallest in at most rmax(D) places.  This restates the
+reference's divisor-family census (gpu/divisor_family_census.py:45-78: the survivor test, cap, rmax
+and the count s of the incumbent's primes that D forces out).  ``family_run`` then runs the rows as
+gpu/run_mstar_family.py:66-94 does (the 64 smallest primes at r = 0, then radii 1..rmax over the
+capped pool, bound n < U, through the driver drop-in's bounded GPU join), and ``family_instances``
+hands them to the batched portfolio or the serving loop as instances.
+
+The pools are built for all divisors at once: the candidate primes are q = d + 1 for the divisors d of
+M (so (q-1) | M), each candidate's divisor exponent vector is compared with every divisor's, and q
+divides D only when q is a prime of M present in D.  The reference factors and enumerates divisors of
+each D separately; the rows are the same (pinned against the reference's own census output).
+
+CPU work by nature (integer set arithmetic and 500-digit products, a few seconds per incumbent): it
+supplies the moduli; the joins run on the GPU.
+"""
+from __future__ import annotations
+
+import itertools
+import math
+
+import numpy as np
+
+SIEVE_BOUND = 2_000_000          # pool primes are taken below this; a row whose cap reaches it is rejected
+
+
+def _sieve(n: int) -> np.ndarray:
+    s = np.ones(n + 1, dtype=bool)
+    s[:2] = False
+    for i in range(2, math.isqrt(n) + 1):
+        if s[i]:
+            s[i * i::i] = False
+    return s
+
+
+_SIEVE: dict = {}
+
+
+def _is_prime_table(bound: int) -> np.ndarray:
+    t = _SIEVE.get(bound)
+    if t is None:
+        t = _SIEVE[bound] = _sieve(bound)
+    return t
+
+
+def factorize(m: int) -> dict[int, int]:
+    """Prime factorisation of m by trial division (the moduli here are products of small primes)."""
+    if m < 1:
+        raise ValueError("m must be positive")
+    f: dict[int, int] = {}
+    d = 2
+    while d * d <= m:
+        while m % d == 0:
+            f[d] = f.get(d, 0) + 1
+            m //= d
+        d += 1 if d == 2 else 2
+    if m > 1:
+        f[m] = f.get(m, 0) + 1
+    return f
+
+
+def carmichael_lambda(primes) -> int:
+    """lambda(n) of a squarefree n given by its primes: lcm of (p - 1)."""
+    return math.lcm(*[int(p) - 1 for p in primes])
+
+
+class DivisorLattice:
+    """Divisors of M as exponent vectors, and the eligible pool Q(D) of every divisor D."""
+
+    def __init__(self, M: int, sieve_bound: int = SIEVE_BOUND):
+        self.M = int(M)
+        self.fm = factorize(self.M)
+        self.primes = sorted(self.fm)
+        ranges = [range(self.fm[p] + 1) for p in self.primes]
+        vecs = list(itertools.product(*ranges))
+        self.E = np.asarray(vecs, dtype=np.int16).reshape(len(vecs), len(self.primes))
+        self.values = [math.prod(p ** e for p, e in zip(self.primes, v)) for v in vecs]
+        isp = _is_prime_table(sieve_bound)
+        cand = [j for j, d in enumerate(self.values) if 3 <= d + 1 <= sieve_bound and isp[d + 1]]
+        self.cq = np.asarray([self.values[j] + 1 for j in cand], dtype=np.int64)     # candidate primes
+        self.cE = self.E[cand]                                                        # exponents of q - 1
+        # q divides D only for q a prime factor of M whose exponent in D is at least 1
+        self.cidx = np.asarray([self.primes.index(int(q)) if int(q) in self.fm else -1 for q in self.cq],
+                               dtype=np.int64)
+        order = np.argsort(self.cq)
+        self.cq, self.cE, self.cidx = self.cq[order], self.cE[order], self.cidx[order]
+
+    def pool(self, j: int) -> list[int]:
+        """Q(D) below the sieve bound, ascending, for the divisor with index j."""
+        e = self.E[j]
+        ok = (self.cE <= e).all(axis=1)
+        inM = self.cidx >= 0
+        divides = np.zeros(len(self.cq), dtype=bool)
+        divides[inM] = e[self.cidx[inM]] >= 1
+        return [int(q) for q in self.cq[ok & ~divides]]
+
+
+def census_row(D: int, P: list[int], U: int, U_factors, k: int = 64, sieve_bound: int = SIEVE_BOUND):
+    """The census row of divisor D with pool P (ascending), or None when D cannot carry a k-factor
+    Carmichael number below U."""
+    if len(P) < k:
+        # every omitted prime exceeds the sieve bound: bound any completion from below
+        lb = math.prod(P) * (sieve_bound + 1) ** (k - len(P))
+        if lb < U:
+            raise ValueError(f"D={D}: {len(P)} eligible primes below the sieve bound and a completion could "
+                             "stay below U; raise the sieve bound")
+        return None
+    Tk = math.prod(P[:k])
+    if Tk >= U:
+        return None
+    cap = (U - 1) // (Tk // P[k - 1])
+    if cap >= sieve_bound:
+        raise ValueError(f"D={D}: cap {cap} reaches the sieve bound; raise it")
+    Pc = [q for q in P if q <= cap]
+    rmax = 0
+    for r in range(1, k + 1):
+        if k + r > len(Pc):
+            break
+        num = Tk * math.prod(Pc[k:k + r])
+        den = math.prod(P[k - r:k])
+        if num // den < U:
+            rmax = r
+        else:
+            break
+    s = sum(1 for p in U_factors if D % (int(p) - 1) != 0)
+    return {"D": D, "s": s, "pool": len(P), "cap": cap, "pool_capped": len(Pc), "rmax": rmax,
+            "digits_T64": len(str(Tk))}
+
+
+def divisor_family(U: int, U_factors, M: int | None = None, k: int = 64,
+                   sieve_bound: int = SIEVE_BOUND) -> tuple[dict, list[dict]]:
+    """Survivor rows of every divisor D of M = lambda(U) (the incumbent's own family), in divisor order.
+    Returns (factorisation of M, rows)."""
+    U = int(U)
+    if M is None:
+        M = carmichael_lambda(U_factors)
+    lat = DivisorLattice(M, sieve_bound)
+    order = sorted(range(len(lat.values)), key=lambda j: lat.values[j])
+    rows = []
+    for j in order:
+        row = census_row(lat.values[j], lat.pool(j), U, U_factors, k, sieve_bound)
+        if row is not None:
+            rows.append(row)
+    return dict(lat.fm), rows
+
+
+def family_instances(rows, U: int, r_min: int = 1, r_max: int | None = None, k: int = 64,
+                     sieve_bound: int = SIEVE_BOUND, with_base: bool = True):
+    """(row, radius, Instance) for every survivor row: radius 0 (the k smallest primes themselves, when
+    with_base) and radii r_min..min(rmax, r_max), each over the full capped pool with bound n < U -- the
+    per-family runs of gpu/run_mstar_family.py:66-94, here as one portfolio.  Rows whose modulus is 2^62
+    or more are skipped (keys are u64 residues), as the reference marks moduli of 2^64 and more
+    unsupported."""
+    from .solve import Instance
+    out = []
+    for row in rows:
+        D, cap, rmax = int(row["D"]), int(row["cap"]), int(row["rmax"])
+        if D >= 1 << 62:
+            continue
+        P = DivisorLattice(D, sieve_bound).pool(_top_index(D))
+        Pc = [q for q in P if q <= cap]
+        if len(Pc) != int(row["pool_capped"]):
+            raise ValueError(f"D={D}: capped pool has {len(Pc)} primes, the row says {row['pool_capped']}")
+        base = Pc[:k]
+        hi = min(rmax, 10 if r_max is None else r_max, 10)      # instances hold radii up to 10
+        radii = ([0] if with_base else []) + list(range(max(1, r_min), hi + 1))
+        for r in radii:
+            out.append((row, r, Instance.build(D, Pc, base, r, U - 1)))
+    return out
+
+
+def _top_index(D: int) -> int:
+    """Index of D itself among the divisors of D (the last exponent vector of the lattice)."""
+    fm = factorize(D)
+    return math.prod(e + 1 for e in fm.values()) - 1
+
+
+def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: int = 4000, k: int = 64,
+               sieve_bound: int = SIEVE_BOUND, consider=None, log=None, solver=None) -> dict:
+    """Run every survivor row as gpu/run_mstar_family.py:66-94 drives the reference's GPU driver: the
+    k smallest primes of the capped pool checked as a Carmichael number below U (radius 0), then each
+    radius r_min..min(rmax, r_max) at the driver's h-stratum bound, through ``driver.run_instance`` (the
+    driver's Icap/Dmin/affordable-pool bounds, product-bounded producers and record join on the GPU).
+    Radii whose bounds need more than 128-bit products are reported as skipped.
+
+    Returns {D: {"base_carmichael", "base_below_U", "instances": [per-radius counts], "skipped": [r]}};
+    consider(key, factors, label) receives every completion below U (defaults to collecting them)."""
+    from . import bsolve, driver
+    from .certify import verify_certificate
+    from .solve import Instance, Solver, Tuning
+    hits = []
+    if consider is None:
+        consider = lambda key, fac, label: hits.append((key, tuple(fac), label)) or True
+    log = log or (lambda s: None)
+    solver = solver or Solver(tuning=Tuning(strategy="bounded"))
+    out = {}
+    for row in rows:
+        D, cap, rmax = int(row["D"]), int(row["cap"]), int(row["rmax"])
+        if D >= 1 << 62:
+            out[D] = {"unsupported": "modulus of 2^62 or more (u64 residue keys)"}
+            continue
+        P = DivisorLattice(D, sieve_bound).pool(_top_index(D))
+        Pc = [q for q in P if q <= cap]
+        base, INS = Pc[:k], Pc[k:]
+        ok, n, _ = verify_certificate(base)
+        rec = {"base_carmichael": bool(ok), "base_below_U": bool(ok and n < U), "instances": [], "skipped": []}
+        if ok and n < U:
+            consider((D, "ksmall", 0, 0), base, "census_base")
+        hi = rmax if r_max is None else min(rmax, r_max)
+        for r in range(max(1, r_min), hi + 1):
+            h = driver.hmax_for(base, INS, r, U, split)
+            if h < 0:
+                continue
+            if r > 10 or not bsolve.applicable(Instance.build(D, Pc, base, r, U - 1)):
+                rec["skipped"].append(r)
+                continue
+            st: dict = {}
+            driver.run_instance("ksmall", base, INS, r, h, D, U, split, consider, log, st, solver)
+            rec["instances"].append(st["last"])
+        out[D] = rec
+    if hits:
+        out["completions"] = hits
+    return out
+

@@ -39,6 +39,24 @@ def instance_bounds(B0, INS, r: int, U: int):
     return Icap, Dmin, cap_r, [q for q in INS if q <= cap_r]
 
 
+def hmax_for(B0, INS, r: int, U: int, split: int = 4000) -> int:
+    """The driver's h-stratum bound (gpu/mitm_gpu_mstar_driver.py:84-98): the largest number h of
+    insertion primes above `split` with which an r-exchange could still come in below U (the
+    cheapest such product, P0 times the r-h smallest small primes and the h smallest large ones,
+    below U times the largest removable D product); -1 when no stratum can."""
+    small = [p for p in INS if p <= split]
+    large = [p for p in INS if p > split]
+    PB = math.prod(B0)
+    Dmax = math.prod(sorted(B0)[-r:])
+    best = -1
+    for h in range(0, r + 1):
+        if h > len(large) or r - h > len(small):
+            continue
+        if PB * math.prod(small[:r - h]) * math.prod(large[:h]) < U * Dmax:
+            best = h
+    return best
+
+
 def build_D(B0, M: int, r: int, Dmin=None, nchunks: int = 1, device=None):
     """Sorted D-side chunks [(keys, ids), ...] and the record count: the r-subsets of the
     64-prime base with prod >= Dmin (every subset when Dmin is None), keys prod(D) mod M,
@@ -74,6 +92,7 @@ def run_instance(tag, B0, INS, r: int, hmax: int, M: int, U: int, split: int, co
     if len(INS_aff) < r:
         log(f"  {tag} r={r}: affordable pool has {len(INS_aff)} < r primes (cap_r={cap_r}); nothing to search")
         st["instances"] = st.get("instances", 0) + 1
+        st["last"] = dict(r=r, hmax=hmax, ins=len(INS_aff), nD=0, nI=0, pairs=0, below_U=0)
         return True
     s = solver or Solver(tuning=Tuning(strategy="bounded"))
     if s._bounded is None:
@@ -100,6 +119,7 @@ def run_instance(tag, B0, INS, r: int, hmax: int, M: int, U: int, split: int, co
         if rmin is None or n < rmin:
             rmin = n
     st["instances"] = st.get("instances", 0) + 1
+    st["last"] = dict(r=r, hmax=hmax, ins=len(INS_aff), nD=nD, nI=nI, pairs=len(pairs_idx), below_U=below)
     st["pairs_total"] = st.get("pairs_total", 0) + len(pairs_idx)
     st["completions_below_U"] = st.get("completions_below_U", 0) + below
     gb = 0.0

@@ -1,0 +1,72 @@
+"""Golden rows of the divisor-family census and of its family runs (run here, where the reference
+tree exists).
+
+Runs the reference's own census (gpu/divisor_family_census.py, imported from the reference tree) for
+the incumbent of results_k64_best_global.json, checks that it reproduces the survivor rows the
+reference committed in gpu/divisor_family_lambdaJ.json, and writes them with the incumbent's size and
+primes to tests/golden/census_lambdaJ.json.  It also reads the reference's run records of that family
+(gpu/records/lambdaN_U524394558743/D<D>.log, one per survivor, written by gpu/run_mstar_family.py
+through gpu/mitm_gpu_mstar_driver.py) and keeps, per survivor, the base check and every instance line
+(radius, affordable insertion primes, D and I record counts after the bounds, residue pairs,
+completions below U).
+"""
+import glob
+import importlib.util
+import json
+import math
+import os
+import re
+import sys
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "census_lambdaJ.json")
+
+
+def main():
+    spec = importlib.util.spec_from_file_location("dfc", os.path.join(REF, "gpu", "divisor_family_census.py"))
+    dfc = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(dfc)
+    inc = json.load(open(os.path.join(REF, "results_k64_best_global.json")))
+    committed = json.load(open(os.path.join(REF, "gpu", "divisor_family_lambdaJ.json")))
+    U = int(inc["n"])
+    F = sorted(int(p) for p in inc["factors"])
+    M = math.lcm(*[p - 1 for p in F])
+    fm, rows = dfc.census(U, M, F)
+    key = lambda r: r["D"]
+    assert sorted(rows, key=key) == sorted(committed["survivors"], key=key), "reference census != its output"
+    runs = read_records(os.path.join(REF, "gpu", "records", "lambdaN_U524394558743"), U)
+    assert sorted(runs) == sorted(str(r["D"]) for r in rows), "records do not cover the survivors"
+    json.dump({"U": str(U), "factors": F, "lambda": str(M),
+               "lambda_factorization": {str(k): v for k, v in fm.items()},
+               "survivors": sorted(rows, key=key), "runs": runs}, open(OUT, "w"), indent=0)
+    print("wrote", OUT, len(rows), "rows", sum(len(v["instances"]) for v in runs.values()), "instances")
+
+
+INST = re.compile(r" r=(\d+) h<=(\d+) \|INS\|=(\d+)(?:/(\d+))? (host-exact|dfilter)[^:]*: D ([\d,]+).*?\| I ([\d,]+) "
+                  r"rec .*?pairs=(\d+) below_U=(\d+)")
+HEAD = re.compile(r"\[runner\] family=(\w+) D=(\d+) U=(\d+) pool=(\d+) cap=(\d+) rmax=(\d+)")
+BASE = re.compile(r"\[runner\] r=0 base=ksmall\((\d+) primes, largest (\d+)\) carmichael=(\w+) below_U=(\w+)")
+
+
+def read_records(folder, U):
+    runs = {}
+    for f in sorted(glob.glob(os.path.join(folder, "D*.log"))):
+        txt = open(f).read()
+        assert "INCOMPLETE" not in txt, f
+        h, b = HEAD.search(txt), BASE.search(txt)
+        assert int(h.group(3)) == U
+        inst = []
+        for line in txt.splitlines():
+            m = INST.search(line)
+            if m:
+                inst.append({"r": int(m.group(1)), "hmax": int(m.group(2)), "ins": int(m.group(3)),
+                             "nD": int(m.group(6).replace(",", "")), "nI": int(m.group(7).replace(",", "")),
+                             "pairs": int(m.group(8)), "below_U": int(m.group(9))})
+        runs[h.group(2)] = {"pool": int(h.group(4)), "cap": int(h.group(5)), "rmax": int(h.group(6)),
+                            "base_largest": int(b.group(2)), "base_carmichael": b.group(3) == "True",
+                            "base_below_U": b.group(4) == "True", "instances": inst}
+    return runs
+
+
+if __name__ == "__main__":
+    main()
