@@ -81,7 +81,12 @@ class DivisorLattice:
         ranges = [range(self.fm[p] + 1) for p in self.primes]
         vecs = list(itertools.product(*ranges))
         self.E = np.asarray(vecs, dtype=np.int16).reshape(len(vecs), len(self.primes))
-        self.values = [math.prod(p ** e for p, e in zip(self.primes, v)) for v in vecs]
+        values = [1]                      # same order as the exponent vectors (last prime fastest)
+        for p in self.primes:
+            pw = [p ** k for k in range(self.fm[p] + 1)]
+            values = [v * w for v in values for w in pw]
+        self.values = values
+        self.index = {v: j for j, v in enumerate(values)}
         isp = _is_prime_table(sieve_bound)
         cand = [j for j, d in enumerate(self.values) if 3 <= d + 1 <= sieve_bound and isp[d + 1]]
         self.cq = np.asarray([self.values[j] + 1 for j in cand], dtype=np.int64)     # candidate primes
@@ -160,11 +165,12 @@ def family_instances(rows, U: int, r_min: int = 1, r_max: int | None = None, k: 
     unsupported."""
     from .solve import Instance
     out = []
+    pools = _Pools([int(r["D"]) for r in rows if int(r["D"]) < 1 << 62], sieve_bound)
     for row in rows:
         D, cap, rmax = int(row["D"]), int(row["cap"]), int(row["rmax"])
         if D >= 1 << 62:
             continue
-        P = DivisorLattice(D, sieve_bound).pool(_top_index(D))
+        P = pools(D)
         Pc = [q for q in P if q <= cap]
         if len(Pc) != int(row["pool_capped"]):
             raise ValueError(f"D={D}: capped pool has {len(Pc)} primes, the row says {row['pool_capped']}")
@@ -180,6 +186,23 @@ def _top_index(D: int) -> int:
     """Index of D itself among the divisors of D (the last exponent vector of the lattice)."""
     fm = factorize(D)
     return math.prod(e + 1 for e in fm.values()) - 1
+
+
+class _Pools:
+    """Eligible pools of the rows' moduli from one lattice of their lcm (every row of one family
+    divides lambda), or one lattice per modulus when the lcm has too many divisors."""
+
+    def __init__(self, Ds, sieve_bound: int, max_divisors: int = 1 << 20):
+        self.sieve_bound = sieve_bound
+        self.lat = None
+        L = math.lcm(*[int(D) for D in Ds]) if Ds else 1
+        if math.prod(e + 1 for e in factorize(L).values()) <= max_divisors:
+            self.lat = DivisorLattice(L, sieve_bound)
+
+    def __call__(self, D: int) -> list[int]:
+        if self.lat is not None:
+            return self.lat.pool(self.lat.index[int(D)])
+        return DivisorLattice(D, self.sieve_bound).pool(_top_index(D))
 
 
 def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: int = 4000, k: int = 64,
@@ -201,12 +224,13 @@ def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: in
     log = log or (lambda s: None)
     solver = solver or Solver(tuning=Tuning(strategy="bounded"))
     out = {}
+    pools = _Pools([int(r["D"]) for r in rows if int(r["D"]) < 1 << 62], sieve_bound)
     for row in rows:
         D, cap, rmax = int(row["D"]), int(row["cap"]), int(row["rmax"])
         if D >= 1 << 62:
             out[D] = {"unsupported": "modulus of 2^62 or more (u64 residue keys)"}
             continue
-        P = DivisorLattice(D, sieve_bound).pool(_top_index(D))
+        P = pools(D)
         Pc = [q for q in P if q <= cap]
         base, INS = Pc[:k], Pc[k:]
         ok, n, _ = verify_certificate(base)

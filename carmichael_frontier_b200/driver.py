@@ -123,10 +123,9 @@ def run_instance(tag, B0, INS, r: int, hmax: int, M: int, U: int, split: int, co
     st["pairs_total"] = st.get("pairs_total", 0) + len(pairs_idx)
     st["completions_below_U"] = st.get("completions_below_U", 0) + below
     gb = 0.0
-    try:
+    try:                                   # device memory held by this process's allocator (no driver query)
         import torch
-        f, tot = torch.cuda.mem_get_info()
-        gb = (tot - f) / 2 ** 30
+        gb = torch.cuda.memory_reserved() / 2 ** 30
     except Exception:
         pass
     log(f"  {tag} r={r} h<={hmax} |INS|={len(INS_aff)} dfilter rank b200: D {nD:,} {0.0:.1f}s | I {nI:,} rec "
