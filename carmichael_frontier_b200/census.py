@@ -107,22 +107,26 @@ class DivisorLattice:
         return [int(q) for q in self.cq[ok & ~divides]]
 
 
+class SieveBoundError(ValueError):
+    """A modulus whose census needs primes beyond the sieve bound."""
+
+
 def census_row(D: int, P: list[int], U: int, U_factors, k: int = 64, sieve_bound: int = SIEVE_BOUND):
     """The census row of divisor D with pool P (ascending), or None when D cannot carry a k-factor
-    Carmichael number below U."""
+    Carmichael number below U.  Raises SieveBoundError when the answer needs primes above the bound."""
     if len(P) < k:
         # every omitted prime exceeds the sieve bound: bound any completion from below
         lb = math.prod(P) * (sieve_bound + 1) ** (k - len(P))
         if lb < U:
-            raise ValueError(f"D={D}: {len(P)} eligible primes below the sieve bound and a completion could "
-                             "stay below U; raise the sieve bound")
+            raise SieveBoundError(f"D={D}: {len(P)} eligible primes below the sieve bound and a completion "
+                                  "could stay below U; raise the sieve bound")
         return None
     Tk = math.prod(P[:k])
     if Tk >= U:
         return None
     cap = (U - 1) // (Tk // P[k - 1])
     if cap >= sieve_bound:
-        raise ValueError(f"D={D}: cap {cap} reaches the sieve bound; raise it")
+        raise SieveBoundError(f"D={D}: cap {cap} reaches the sieve bound; raise it")
     Pc = [q for q in P if q <= cap]
     rmax = 0
     for r in range(1, k + 1):
@@ -252,4 +256,192 @@ def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: in
     if hits:
         out["completions"] = hits
     return out
+
+
+# -- lambda-neighbourhood census ------------------------------------------------------------
+
+# The two moduli of the reference's exclusion theorems: every 64-factor Carmichael number below the
+# record N has a prime q with (q-1) not dividing M0 and a prime q' with (q'-1) not dividing lambda(N)
+# (gpu/lambda_neighbourhood.py:61, 78-79).
+WITNESS_M0 = 1768248177696000
+WITNESS_LN = 155016423578016000
+
+
+def two_witness_min(P, U: int, M0: int = WITNESS_M0, LN: int = WITNESS_LN, k: int = 64):
+    """Smallest k-product from the ascending pool P that contains a prime q with (q-1) not dividing M0
+    and a prime q' with (q'-1) not dividing LN (one prime may be both), or None when none exists
+    (gpu/lambda_neighbourhood.py:78-97)."""
+    def fill(req):
+        rest = [q for q in P if q not in req]
+        if len(rest) < k - len(req):
+            return None
+        return math.prod(req + rest[:k - len(req)])
+
+    best = None
+    both = [q for q in P if M0 % (q - 1) and LN % (q - 1)]
+    if both:
+        v = fill([both[0]])
+        best = v if best is None or (v is not None and v < best) else best
+    only0 = [q for q in P if M0 % (q - 1) and LN % (q - 1) == 0]
+    onlyN = [q for q in P if LN % (q - 1) and M0 % (q - 1) == 0]
+    if only0 and onlyN:
+        v = fill(sorted([only0[0], onlyN[0]]))
+        best = v if best is None or (v is not None and v < best) else best
+    return best
+
+
+class _Candidates:
+    """Primes q <= bound with (q-1) dividing L, with the exponent vectors of q-1 over L's primes, for
+    the pools of the divisors of L: relaxed pool of D = {q : (q-1) | D}, pool Q(D) = relaxed pool
+    minus the primes dividing D."""
+
+    def __init__(self, L_fm: dict, sieve_bound: int):
+        self.primes = sorted(L_fm)
+        isp = _is_prime_table(sieve_bound)
+        qs, vecs = [], []
+
+        def walk(i, d, vec):                      # divisors of L up to the bound only
+            if i == len(self.primes):
+                if 3 <= d + 1 <= sieve_bound and isp[d + 1]:
+                    qs.append(d + 1)
+                    vecs.append(tuple(vec))
+                return
+            p = self.primes[i]
+            for e in range(L_fm[p] + 1):
+                if d * p ** e > sieve_bound:
+                    break
+                vec.append(e)
+                walk(i + 1, d * p ** e, vec)
+                vec.pop()
+        walk(0, 1, [])
+        order = sorted(range(len(qs)), key=lambda j: qs[j])
+        self.q = np.asarray([qs[j] for j in order], dtype=np.int64)
+        self.E = np.asarray([vecs[j] for j in order], dtype=np.int16).reshape(len(order), len(self.primes))
+        self.pidx = np.asarray([self.primes.index(int(q)) if int(q) in L_fm else -1 for q in self.q],
+                               dtype=np.int64)
+
+    def pools(self, e) -> tuple[list[int], list[int]]:
+        """(relaxed pool, pool) of the divisor with exponent vector e (over L's primes)."""
+        e = np.asarray(e, dtype=np.int16)
+        ok = (self.E <= e).all(axis=1)
+        inL = self.pidx >= 0
+        divides = np.zeros(len(self.q), dtype=bool)
+        divides[inL] = e[self.pidx[inL]] >= 1
+        return [int(x) for x in self.q[ok]], [int(x) for x in self.q[ok & ~divides]]
+
+
+def _relaxed_survives(Pr, U, k, sieve_bound, M0, LN) -> bool:
+    """False only when even the relaxed pool cannot give a qualifying k-product below U; both tests are
+    monotone in D over the relaxed pool, so pruning on them is sound (gpu/lambda_neighbourhood.py:62-77)."""
+    if len(Pr) < k:
+        return math.prod(Pr) * (sieve_bound + 1) ** (k - len(Pr)) < U
+    if math.prod(Pr[:k]) >= U:
+        return False
+    w = two_witness_min(Pr, U, M0, LN, k)
+    return w is not None and w < U
+
+
+def _neighbour_job(seed: int, p: int, U: int, U_factors, k: int, sieve_bound: int, M0: int, LN: int):
+    """Rows of the new moduli D | (seed or seed*q) * p with p | D, as gpu/lambda_neighbourhood.py:99-149:
+    a top-down walk over exponent vectors (p's exponent fixed at 1) from each neighbour, pruned where the
+    relaxed pool fails, sharing visits between the neighbours of one (seed, p)."""
+    sfm = factorize(seed)
+    if seed % p == 0:
+        return {}, []
+    L_fm = {q: e + 1 for q, e in sfm.items()}
+    L_fm[p] = 1
+    cand = _Candidates(L_fm, sieve_bound)
+    col = {q: i for i, q in enumerate(cand.primes)}
+    variants = [(None, 0, dict(sfm))] + [(q, -1, {**sfm, q: e + 1}) for q, e in sfm.items()]
+    seen: dict = {}
+    rows: dict = {}
+    problems: list = []
+    for q, j, fm in variants:
+        primes = [x for x in fm if x != p]
+        emax = [fm[x] for x in primes]
+        out = []
+        stack = [list(emax)]
+
+        def visit(vec):
+            D = p * math.prod(x ** e for x, e in zip(primes, vec))
+            if D in seen:
+                return False
+            e_full = [0] * len(cand.primes)
+            for x, ex in zip(primes, vec):
+                e_full[col[x]] = ex
+            e_full[col[p]] = 1
+            relaxed, pool = cand.pools(e_full)
+            if not _relaxed_survives(relaxed, U, k, sieve_bound, M0, LN):
+                seen[D] = False
+                return False
+            seen[D] = True
+            try:
+                row = census_row(D, pool, U, U_factors, k, sieve_bound)
+            except SieveBoundError:
+                problems.append(("SIEVE", D))
+                row = None
+            if row is not None:
+                out.append(row)
+            return True
+
+        # depth-first in the reference's order: a node, then its children by decrementing each exponent
+        def rec(vec):
+            if not visit(vec):
+                return
+            for i in range(len(vec)):
+                if vec[i] > 0:
+                    v2 = list(vec)
+                    v2[i] -= 1
+                    rec(v2)
+        rec(list(emax))
+        for r in out:
+            if r["D"] not in rows:
+                rows[r["D"]] = dict(r, seed=str(seed), q=q, j=j, p=p)
+    return rows, problems
+
+
+def _neighbour_job_star(args):
+    return _neighbour_job(*args)
+
+
+def lambda_neighbourhood(seeds, pmax: int, U: int, U_factors, k: int = 64, sieve_bound: int = SIEVE_BOUND,
+                         M0: int = WITNESS_M0, LN: int = WITNESS_LN, procs: int = 1) -> tuple[list[dict], list]:
+    """New candidate moduli one step from the seed moduli (gpu/lambda_neighbourhood.py:151-188): for every
+    seed M and prime 3 <= p <= pmax not dividing M, the divisors D of M*p and of M*q*p (q a prime of M)
+    with p | D that can carry a k-factor Carmichael number below U, kept when their cheapest k-product
+    with both exclusion witnesses is below U.  Returns (rows sorted richest first, sieve problems)."""
+    isp = _is_prime_table(max(pmax, 3))
+    primes = [q for q in range(3, pmax + 1) if isp[q]]
+    seeds = [int(m) for m in seeds]
+    jobs = [(M, q, int(U), list(U_factors), k, sieve_bound, M0, LN) for M in seeds for q in primes]
+    covered = set()
+    for M in seeds:
+        covered.update(DivisorLattice(M, sieve_bound).values)
+    results = []
+    if procs > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(procs) as pool:
+            results = pool.map(_neighbour_job_star, jobs, chunksize=1)
+    else:
+        results = [_neighbour_job(*a) for a in jobs]
+    rows: dict = {}
+    problems: list = []
+    for r, pr in results:                      # job order (the reference keeps the first to finish)
+        problems += pr
+        for D, row in r.items():
+            if D in covered:
+                continue
+            if D not in rows or row["digits_T64"] < rows[D]["digits_T64"]:
+                rows[D] = row
+    kept = []
+    for row in rows.values():
+        D = row["D"]
+        lat = _Candidates({**factorize(D)}, sieve_bound)
+        _, pool = lat.pools([factorize(D)[x] for x in lat.primes])
+        w = two_witness_min([q for q in pool if q <= row["cap"]], U, M0, LN, k)
+        if w is None or w >= U:
+            continue
+        kept.append(dict(row, w2_digits=len(str(w))))
+    kept.sort(key=lambda r: (r["w2_digits"], r["digits_T64"], -r["rmax"], r["D"]))
+    return kept, problems
 

@@ -8,10 +8,14 @@ primes to tests/golden/census_lambdaJ.json.  It also reads the reference's run r
 (gpu/records/lambdaN_U524394558743/D<D>.log, one per survivor, written by gpu/run_mstar_family.py
 through gpu/mitm_gpu_mstar_driver.py) and keeps, per survivor, the base check and every instance line
 (radius, affordable insertion primes, D and I record counts after the bounds, residue pairs,
-completions below U).
+completions below U).  Finally it runs the reference's lambda-neighbourhood census
+(gpu/lambda_neighbourhood.py) for the seed M0 = 1768248177696000 with new primes up to 19 and writes its
+rows to tests/golden/nbhd_M0_p19.json.
 """
 import glob
 import importlib.util
+import subprocess
+import tempfile
 import json
 import math
 import os
@@ -40,6 +44,15 @@ def main():
                "lambda_factorization": {str(k): v for k, v in fm.items()},
                "survivors": sorted(rows, key=key), "runs": runs}, open(OUT, "w"), indent=0)
     print("wrote", OUT, len(rows), "rows", sum(len(v["instances"]) for v in runs.values()), "instances")
+    with tempfile.TemporaryDirectory() as td:
+        nb = os.path.join(td, "nb.json")
+        subprocess.run([sys.executable, os.path.join(REF, "gpu", "lambda_neighbourhood.py"), "--seeds",
+                        "1768248177696000", "--pmax", "19", "--out", nb, "--procs", "1"], check=True)
+        d = json.load(open(nb))
+    out2 = os.path.join(os.path.dirname(OUT), "nbhd_M0_p19.json")
+    json.dump({"U": d["U"], "seeds": d["seeds"], "pmax": d["pmax"], "sieve_problems": d["sieve_problems"],
+               "survivors": d["survivors"]}, open(out2, "w"), indent=0)
+    print("wrote", out2, len(d["survivors"]), "rows")
 
 
 INST = re.compile(r" r=(\d+) h<=(\d+) \|INS\|=(\d+)(?:/(\d+))? (host-exact|dfilter)[^:]*: D ([\d,]+).*?\| I ([\d,]+) "

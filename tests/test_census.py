@@ -4,9 +4,12 @@ The divisor-family census of the incumbent of results_k64_best_global.json must 
 118 survivor rows exactly (tests/golden/census_lambdaJ.json, made by make_golden_census.py from
 gpu/divisor_family_census.py and gpu/divisor_family_lambdaJ.json), and the driver bounds that the
 family runs use (radii at which some h-stratum can beat U, the h bound, the affordable insertion pool)
-must reproduce every instance line of the reference's records of that family.
+must reproduce every instance line of the reference's records of that family.  The lambda-neighbourhood
+census (new moduli one step from a seed) must give the reference's rows for the seed M0 and new primes up
+to 19 (tests/golden/nbhd_M0_p19.json, from gpu/lambda_neighbourhood.py).
 """
 import json
+import math
 import os
 
 import pytest
@@ -65,3 +68,22 @@ def test_family_instances_cover_the_survivors(fam):
         assert x.B == int(fam["U"]) - 1 and 0 <= r <= min(3, row["rmax"])
     with pytest.raises(ValueError):
         C.census_row(30, [7, 11, 31], 10 ** 400, [], k=64)      # too few primes and a completion below U
+
+
+def test_lambda_neighbourhood_matches_reference_census(fam):
+    # new moduli one step from M0 (new primes up to 19): the reference's rows, order and provenance
+    with open(os.path.join(os.path.dirname(GOLD), "nbhd_M0_p19.json")) as f:
+        ref = json.load(f)
+    U = int(fam["U"])
+    assert int(ref["U"]) == U
+    rows, problems = C.lambda_neighbourhood([int(x) for x in ref["seeds"]], ref["pmax"], U, fam["factors"])
+    assert problems == [] and ref["sieve_problems"] == []
+    assert rows == ref["survivors"]
+
+
+def test_two_witness_min_small_cases():
+    # a pool of 64 primes: the cheapest product holding both witnesses, or None without them
+    P = [q for q in range(3, 2000) if all(q % d for d in range(2, int(q ** 0.5) + 1))][:70]
+    assert C.two_witness_min(P, 10 ** 300, M0=math.prod(q - 1 for q in P), LN=1) is None
+    w = C.two_witness_min(P, 10 ** 300, M0=1, LN=1)
+    assert w == math.prod(P[:64])
