@@ -5,8 +5,9 @@
 //
 // Sort: one histogram kernel reads every key once and counts all 8-bit digits
 // of all passes; each pass is then ONE kernel (onesweep): a CTA takes the next
-// tile ticket, ranks its keys stably in shared memory (warp match_any
-// ranking over a warp-striped tile, so equal digits keep input order),
+// tile ticket, ranks its keys stably in shared memory (per warp, item by item
+// over a warp-striped tile, lanes of one digit matched through a shared mask,
+// so equal digits keep input order),
 // publishes its per-digit counts, resolves its global digit offsets by
 // decoupled look-back over the tiles before it (bounded spin), and scatters
 // keys, then ids.  Passes whose digit is equal for every key are skipped by the
@@ -63,21 +64,6 @@ __global__ void k_sort_hist_scan(const u64* __restrict__ hist, u64* __restrict__
     excl[p * kRadix + c + lane] = run + incl - v;
     run += __shfl_sync(0xffffffffu, incl, 31);
   }
-}
-
-// Lanes of this warp whose BITS-bit value (the 8-bit digit; a ninth bit marks
-// "no item" in a partial tile) equals this lane's, from one ballot per bit (the
-// vote unit issues these at full rate, where a match-any instruction is far slower).
-template <int BITS>
-__device__ __forceinline__ u32 peer_mask(u32 d) {
-  u32 m = 0xffffffffu;
-#pragma unroll
-  for (int b = 0; b < BITS; ++b) {
-    const u32 bit = (d >> b) & 1u;
-    const u32 v = __ballot_sync(0xffffffffu, bit);
-    m &= bit ? v : ~v;
-  }
-  return m;
 }
 
 __device__ __forceinline__ u32 lanemask_lt() {
@@ -141,7 +127,7 @@ __device__ __forceinline__ void write_tile(const u64* s_v, const unsigned char* 
 
 constexpr int kLookWin = 8;           // predecessor tiles read per look-back round trip
 constexpr u32 kMbarLimit = 1u << 22;  // try_wait rounds (each suspends for a while) before giving up
-constexpr size_t kPassSmem = (size_t)kSortTile * 16 + (size_t)kSortTile + (size_t)kWarps * kRadix * 4;
+constexpr size_t kPassSmem = (size_t)kSortTile * 16 + (size_t)kSortTile + (size_t)kWarps * kRadix * 8;
 
 // One onesweep pass over the digit at bit `shift`.  Two CTAs per SM.  BULK: the
 // tile's keys and ids are brought into shared memory by two bulk copies at the
@@ -158,6 +144,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
   u64* s_iin = s_kin + kSortTile;                            // tile ids
   unsigned char* s_dj = (unsigned char*)(s_iin + kSortTile); // digit of staged element j
   u32* s_wc = (u32*)(s_dj + kSortTile);                      // [kWarps][256] warp digit counts
+  u32* s_mm = s_wc + kWarps * kRadix;                        // [kWarps][256] lanes holding each digit
   __shared__ __align__(8) u64 s_bar[2];
   __shared__ u32 s_tile;
   __shared__ u32 s_dcnt[kRadix];
@@ -196,7 +183,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
       s_iin[j] = iin[base + j];
     }
   }
-  for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortBlock) s_wc[i] = 0;
+  for (int i = threadIdx.x; i < 2 * kWarps * kRadix; i += kSortBlock) s_wc[i] = 0;   // s_wc and s_mm
   __syncthreads();
   if (BULK && !mbar_wait(&s_bar[0], 0, kMbarLimit)) {
     atomicOr(err, CF_ERR_SPIN_LIMIT);
@@ -205,34 +192,37 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   u64 key[kSortItems];
   u32 loc[kSortItems];                      // local offset (low 16 bits) | digit << 16
-  u32 peers[kSortItems];
   const u32 lt = lanemask_lt();
   u32* wc = s_wc + wid * kRadix;
-  // the keys and their peer masks first (independent of one another), then the
-  // per-item counter chain of this warp, so the loads overlap
+  u32* mm = s_mm + wid * kRadix;
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
     const int e = wid * 32 * kSortItems + it * 32 + lane;
     key[it] = e < tv ? s_kin[e] : 0ull;
   }
+  // stable rank within the warp, item by item: the lanes of one digit find each other
+  // through a shared mask (one atomic OR each), the group's lowest lane takes the
+  // group's slice of the warp's digit counter and clears the mask, and the slice's
+  // start reaches the group by shuffle
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
     const int e = wid * 32 * kSortItems + it * 32 + lane;
     const u32 d = e < tv ? (u32)((key[it] >> shift) & 0xff) : 0x100u;
-    loc[it] = d << 16;
-    peers[it] = tv == kSortTile ? peer_mask<8>(d) : peer_mask<9>(d);
-  }
-#pragma unroll
-  for (int it = 0; it < kSortItems; ++it) {
-    const u32 d = loc[it] >> 16;
     const bool valid = d < 0x100u;
-    u32 cnt = 0;
-    if (valid) cnt = wc[d];
+    if (valid) atomicOr(&mm[d], 1u << lane);
     __syncwarp();
-    const u32 r = __popc(peers[it] & lt);
-    if (valid && r == 0) wc[d] = cnt + __popc(peers[it]);
+    const u32 peers = valid ? mm[d] : 0u;
+    const int leader = valid ? __ffs(peers) - 1 : lane;
     __syncwarp();
-    loc[it] |= cnt + r;
+    u32 base = 0;
+    if (valid && lane == leader) {
+      base = wc[d];
+      wc[d] = base + __popc(peers);
+      mm[d] = 0u;
+    }
+    base = __shfl_sync(0xffffffffu, base, leader);
+    __syncwarp();
+    loc[it] = (d << 16) | (base + __popc(peers & lt));
   }
   __syncthreads();
   if (threadIdx.x < kRadix) {                 // per digit: exclusive over warps, tile total
