@@ -152,3 +152,18 @@ def test_batched_partitioned_range_overflow_falls_back(cuda):
     ref = BatchSolver(cuda, tuning=BatchTuning(part_build=False)).solve(insts, i_limit=lim)
     for a, b in zip(got, ref):
         assert summary(a) == summary(b)
+
+
+def test_batched_partitioned_build_with_bloom_level(cuda):
+    # the Bloom first level forced on every table (its bits are set by the scatter kernel)
+    from carmichael_frontier_b200.solve import Tuning
+    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config3(4)]
+    lim = 1 << 20
+    bloom = Tuning(l2_table_bytes=0, max_fbits=18)
+    bs = BatchSolver(cuda, tuning=BatchTuning(dtab=bloom, part_min_buckets=16))
+    prep = bs.prepare(insts, i_limit=lim)
+    assert all(s is None or s[1] > 0 for s in prep.shapes) and sum(b.n_part for b in prep.batches) == len(insts)
+    got = bs.run(prep)
+    ref = BatchSolver(cuda, tuning=BatchTuning(part_build=False)).solve(insts, i_limit=lim)
+    for a, b in zip(got, ref):
+        assert summary(a) == summary(b)

@@ -122,3 +122,11 @@ def test_partitioned_table_build_matches_in_place(cuda, golden):
                Tuning(part_min_buckets=16, part_sigma=-6.0), Tuning(part_min_buckets=16, dtab_load=12.0)):
         s = Solver(cuda, tuning=tu)
         assert [_pair_summary(s.solve_instance(x, i_limit=lim)) for x in insts] == ref
+
+
+def test_partitioned_table_build_with_bloom_level(cuda, golden):
+    g = golden["config2"][2]
+    s = Solver(cuda, tuning=Tuning(strategy="fused", l2_table_bytes=0, max_fbits=18, part_min_buckets=16))
+    res = s.solve(g["M"], g["Q"], g["B0"], g["r"], int(g["B"]))
+    assert res.plan["fbits"] > 0
+    assert as_lists(res.pairs) == g["pairs"]
