@@ -572,11 +572,11 @@ def run_census(args):
     def timed(rws, rmax):
         torch.cuda.synchronize(dev)
         a = time.perf_counter()
-        o = C.family_run(rws, U, r_max=rmax, solver=s)
+        o, hits = C.family_run(rws, U, r_max=rmax, solver=s)
         torch.cuda.synchronize(dev)
-        return o, time.perf_counter() - a
+        return o, hits, time.perf_counter() - a
 
-    out, t_fam = timed(rows, 10)
+    out, hits, t_fam = timed(rows, 10)
     n_inst = sum(len(out[r["D"]]["instances"]) for r in rows)
     recs = sum(x["nD"] + x["nI"] for r in rows for x in out[r["D"]]["instances"])
     same = all(out[r["D"]]["instances"] == [x for x in fam["runs"][str(r["D"])]["instances"]
@@ -584,7 +584,7 @@ def run_census(args):
                for r in rows)
     skipped = sum(len(out[r["D"]]["skipped"]) for r in rows)
     sample = random.Random(1).sample(nb["survivors"], min(100, len(nb["survivors"])))
-    out2, t_nb = timed(sample, 6)
+    out2, hits2, t_nb = timed(sample, 6)
     n2 = sum(len(out2[r["D"]]["instances"]) for r in sample if "instances" in out2[r["D"]])
     recs2 = sum(x["nD"] + x["nI"] for r in sample if "instances" in out2[r["D"]] for x in out2[r["D"]]["instances"])
     clk = clocks.stop()
@@ -596,10 +596,10 @@ def run_census(args):
         "config": {"workload": "census_lambdaJ_family_r1-10", "survivors": len(rows), "census_s": t_census},
         "family": {"instances": n_inst, "skipped_over_128_bits": skipped, "records": recs,
                    "records_per_s": recs / t_fam, "s": t_fam, "same_as_reference_records": same,
-                   "completions_below_U": len(out.get("completions", []))},
+                   "completions_below_U": len(hits)},
         "neighbourhood_sample": {"moduli": len(sample), "instances": n2, "records": recs2, "s": t_nb,
                                  "instances_per_s": n2 / t_nb, "records_per_s": recs2 / t_nb,
-                                 "completions_below_U": len(out2.get("completions", []))},
+                                 "completions_below_U": len(hits2)},
         "clocks": clk}))
 
 

@@ -217,14 +217,18 @@ def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: in
     driver's Icap/Dmin/affordable-pool bounds, product-bounded producers and record join on the GPU).
     Radii whose bounds need more than 128-bit products are reported as skipped.
 
-    Returns {D: {"base_carmichael", "base_below_U", "instances": [per-radius counts], "skipped": [r]}};
-    consider(key, factors, label) receives every completion below U (defaults to collecting them)."""
+    Returns (runs, completions): runs = {D: {"base_carmichael", "base_below_U", "instances": [per-radius
+    counts], "skipped": [r]}}; completions = the (key, factors, label) of every completion below U that
+    was given to consider(key, factors, label) (the default consider only collects them)."""
     from . import bsolve, driver
     from .certify import verify_certificate
     from .solve import Instance, Solver, Tuning
     hits = []
-    if consider is None:
-        consider = lambda key, fac, label: hits.append((key, tuple(fac), label)) or True
+    user = consider
+
+    def consider(key, fac, label):
+        hits.append((key, tuple(fac), label))
+        return user(key, fac, label) if user is not None else True
     log = log or (lambda s: None)
     solver = solver or Solver(tuning=Tuning(strategy="bounded"))
     out = {}
@@ -253,9 +257,7 @@ def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: in
             driver.run_instance("ksmall", base, INS, r, h, D, U, split, consider, log, st, solver)
             rec["instances"].append(st["last"])
         out[D] = rec
-    if hits:
-        out["completions"] = hits
-    return out
+    return out, hits
 
 
 # -- lambda-neighbourhood census ------------------------------------------------------------

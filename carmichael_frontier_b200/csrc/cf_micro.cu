@@ -1,4 +1,4 @@
-// cf_micro.cu -- microbenchmarks that measure the ceilings the kernels are judged
+// cf_micro.cu -- microbenchmarks that measure the ceilings the kernels are compared
 // against on the running GPU:
 //   cf_micro_l2_probe : random 32-byte reads from a table (L2-resident when it is
 //                       small): the ceiling of the fused probe, which reads one

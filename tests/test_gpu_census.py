@@ -21,8 +21,9 @@ def test_family_run_matches_reference_records(cuda):
     with open(GOLD) as f:
         fam = json.load(f)
     U = int(fam["U"])
-    out = C.family_run(fam["survivors"], U, r_max=6, solver=Solver(cuda, tuning=Tuning(strategy="bounded")))
-    assert "completions" not in out                         # the reference found none below U either
+    out, completions = C.family_run(fam["survivors"], U, r_max=6,
+                                    solver=Solver(cuda, tuning=Tuning(strategy="bounded")))
+    assert completions == []                                # the reference found none below U either
     n = 0
     for row in fam["survivors"]:
         got, ref = out[row["D"]], fam["runs"][str(row["D"])]
