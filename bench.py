@@ -287,8 +287,9 @@ def run_ours(args):
 
     # ---- end-to-end region: the public API from host inputs (tables built and copied every step)
     _default_solvers.clear()
-    w0 = timed[0]                            # one untimed call: the public solver's device buffers
-    public_solve(w0.M, w0.Q, w0.B0, w0.r, w0.B, device=dev, strategy=args.strategy)
+    if timed:                                # one untimed call: the public solver's device buffers
+        w0 = timed[0]
+        public_solve(w0.M, w0.Q, w0.B0, w0.r, w0.B, device=dev, strategy=args.strategy)
     for s0 in _default_solvers.values():
         s0.tables._cache.clear()
         s0.h2d_desc_bytes = 0
