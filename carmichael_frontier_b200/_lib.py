@@ -94,7 +94,7 @@ SIGNATURES = [
     ("cf_batch_part_tile", u32, []),
     ("cf_batch_part_max_ranges", u32, []),
     ("cf_batch_ovf_bytes", sz, []),
-    ("cf_batch_part", C.c_int, [C.c_int, vp, vp, u32, vp, vp, u32, vp, vp, C.c_int, u32, vp]),
+    ("cf_batch_part", C.c_int, [C.c_int, vp, vp, u32, vp, vp, u32, vp, vp, C.c_int, C.c_int, u32, vp]),
     ("cf_sort_tmp_bytes", sz, [u64]),
     ("cf_sort_pairs", C.c_int, [vp, vp, u64, C.c_int, vp, sz, vp]),
     ("cf_sort_pairs_noalloc_max", u64, []),

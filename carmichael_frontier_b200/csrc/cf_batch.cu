@@ -185,10 +185,11 @@ k_batch(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart /*[n
 constexpr int kPlbMin = 9;                    // 512-bucket ranges: 80 KB, two CTAs per SM
 constexpr int kPlbMax = 10;                   // 1024-bucket ranges: 160 KB, one CTA per SM
 constexpr int kScBlock = 256;
-constexpr int kScMinBlocks = 3;               // CTAs per SM (64 KB of shared memory each)
-constexpr int kScTile = 4096;                 // records per scatter ticket (16 per thread)
+constexpr int kScMinBlocks = 4;               // CTAs per SM (55.6 KB of shared memory each)
+constexpr int kScTile = 4064;                 // records per scatter ticket (508 per warp): 4 CTAs
+                                              // of 56 KB fit the SM's 228 KB with their 1 KB reserves
 constexpr int kScWarpRecs = kScTile / (kScBlock / 32);
-constexpr u32 kScMaxParts = 4096;             // bucket ranges per modulus (bbits <= plb + 12)
+constexpr u32 kScMaxParts = 2048;             // bucket ranges per modulus (bbits <= plb + 11)
 constexpr size_t kScSmem = (size_t)kScTile * 12 + (size_t)kScMaxParts * 4;
 constexpr int kPlItems = 8;                   // records a thread loads before claiming (more loop if needed)
 template <int PLB>
@@ -260,6 +261,10 @@ __device__ __forceinline__ bool scatter_gen(const CfBatchMod& md, u64 first, u32
   return true;
 }
 
+// RF = 0: any radius (a switch into the radius-templated generator); RF = 1..8: only
+// moduli of that radius (the others have no tickets), with the generator's registers
+// sized for it -- fitting four CTAs per SM.
+template <int RF>
 __global__ void __launch_bounds__(kScBlock, kScMinBlocks)
 k_bscatter(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart, u32 nmod,
            unsigned long long* __restrict__ queue, u32* __restrict__ err) {
@@ -292,7 +297,9 @@ k_bscatter(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart, 
     __syncthreads();
     if (good) {
       bool g = true;
-      switch (md.r) {
+      if (RF != 0) {
+        g = md.r == RF && scatter_gen<RF != 0 ? RF : 1>(md, first, count, s_kw, s_pp, s_f32, s_h);
+      } else switch (md.r) {
         case 1: g = scatter_gen<1>(md, first, count, s_kw, s_pp, s_f32, s_h); break;
         case 2: g = scatter_gen<2>(md, first, count, s_kw, s_pp, s_f32, s_h); break;
         case 3: g = scatter_gen<3>(md, first, count, s_kw, s_pp, s_f32, s_h); break;
@@ -571,10 +578,21 @@ extern "C" size_t cf_batch_ovf_bytes(void) { return sizeof(CfOvf); }
 // cf_batch_ovf_bytes(), *novf zeroed before phase 1.  Errors go to *err:
 // CF_ERR_PART_OVERFLOW when a range received more than pcap records (the caller
 // rebuilds in place), CF_ERR_TABLE_FULL when the overflow list ran out.
+template <int RF>
+static cudaError_t launch_scatter(const void* mods, const u64* tstart, u32 nmod, void* queue, u32* err, u32 grid,
+                                  int sms, cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(k_bscatter<RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScSmem);
+  if (e != cudaSuccess) return e;
+  k_bscatter<RF><<<grid ? grid : (u32)sms * kScMinBlocks, kScBlock, kScSmem, st>>>(
+      (const CfBatchMod*)mods, tstart, nmod, (unsigned long long*)queue, err);
+  return cudaGetLastError();
+}
+
 extern "C" int cf_batch_part(int phase, const void* mods, const u64* tstart, u32 nmod, void* queue, void* ovf,
-                             u32 ovf_cap, u32* novf, u32* err, int part_lb, u32 grid, void* stream) {
+                             u32 ovf_cap, u32* novf, u32* err, int part_lb, int radius, u32 grid, void* stream) {
   if (phase < 0 || phase > 2 || !mods || nmod == 0 || !err || (phase < 2 && (!tstart || !queue)) ||
-      (phase > 0 && (!novf || (ovf_cap && !ovf))) || (phase == 1 && (part_lb < kPlbMin || part_lb > kPlbMax))) {
+      (phase > 0 && (!novf || (ovf_cap && !ovf))) || (phase == 1 && (part_lb < kPlbMin || part_lb > kPlbMax)) ||
+      radius < 0 || radius > kBatchMaxR) {
     cf_set_error("cf_batch_part: bad arguments%s", "");
     return CF_EBADARG;
   }
@@ -583,10 +601,19 @@ extern "C" int cf_batch_part(int phase, const void* mods, const u64* tstart, u32
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (phase == 0) {
-    cudaError_t e = cudaFuncSetAttribute(k_bscatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kScSmem);
-    if (e != cudaSuccess) return cf_cuda_status(e, "cf_batch_part: smem attribute");
-    k_bscatter<<<grid ? grid : (u32)sms * kScMinBlocks, kScBlock, kScSmem, st>>>((const CfBatchMod*)mods, tstart, nmod,
-                                                                 (unsigned long long*)queue, err);
+    cudaError_t e;
+    switch (radius) {
+      case 1: e = launch_scatter<1>(mods, tstart, nmod, queue, err, grid, sms, st); break;
+      case 2: e = launch_scatter<2>(mods, tstart, nmod, queue, err, grid, sms, st); break;
+      case 3: e = launch_scatter<3>(mods, tstart, nmod, queue, err, grid, sms, st); break;
+      case 4: e = launch_scatter<4>(mods, tstart, nmod, queue, err, grid, sms, st); break;
+      case 5: e = launch_scatter<5>(mods, tstart, nmod, queue, err, grid, sms, st); break;
+      case 6: e = launch_scatter<6>(mods, tstart, nmod, queue, err, grid, sms, st); break;
+      case 7: e = launch_scatter<7>(mods, tstart, nmod, queue, err, grid, sms, st); break;
+      case 8: e = launch_scatter<8>(mods, tstart, nmod, queue, err, grid, sms, st); break;
+      default: e = launch_scatter<0>(mods, tstart, nmod, queue, err, grid, sms, st); break;
+    }
+    if (e != cudaSuccess) return cf_cuda_status(e, "cf_batch_part(scatter)");
   } else if (phase == 1) {
     cudaError_t e;
     if (part_lb == kPlbMax) {

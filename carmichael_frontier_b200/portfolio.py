@@ -70,7 +70,7 @@ class _Batch:
     tsD: object = None                 # device u64[nmod+1] ticket prefix sums, table sides (build)
     tsI: object = None                 # device u64[nmod+1] ticket prefix sums, probing sides
     tsD_all: object = None             # table-side tickets with every modulus built in place
-    tsS: object = None                 # scatter tickets of the partitioned build (0 for in-place moduli)
+    tsS: object = None                 # scatter tickets of the partitioned build per radius {r: prefix sums}
     tsP: object = None                 # bucket ranges of the partitioned build (0 for in-place moduli)
     n_part: int = 0                    # moduli of this batch with the partitioned build
     use_part: bool = True              # False after a bucket range overflowed: build in place
@@ -270,7 +270,11 @@ class BatchSolver:
             b.tsD_all = _prefix(build)
             b.tsD = _prefix([0 if j in b._part else v for j, v in enumerate(build)])
             b.tsI = _prefix([-(-max(nD[k], nI[k]) // t) for k in b.idx])
-            b.tsS = _prefix([-(-min(nD[k], nI[k]) // tile) if j in b._part else 0 for j, k in enumerate(b.idx)])
+            # one scatter launch per radius present, each with a generator specialised for it
+            b.tsS = {}
+            for rr in sorted({insts[k].r for j, k in enumerate(b.idx) if j in b._part}):
+                b.tsS[rr] = _prefix([-(-min(nD[k], nI[k]) // tile) if j in b._part and insts[k].r == rr else 0
+                                     for j, k in enumerate(b.idx)])
             b.tsP = _prefix([b._part[j][0] if j in b._part else 0 for j in range(len(b.idx))])
         prep = PreparedPortfolio(insts, i_limit, nD, nI, shapes, batches, fallback, trivial, blob, tails,
                                  tu.pair_capacity)
@@ -325,11 +329,14 @@ class BatchSolver:
         if part:
             oc = self.tuning.ovf_capacity
             lb = self.tuning.part_lb
-            ck(lib.cf_batch_part(0, dp(b.mods), dp(b.tsS), nmod, m + 32, None, 0, m + 24, m + 20, lb, 0, sh),
-               "cf_batch_part(scatter)")
-            ck(lib.cf_batch_part(1, dp(b.mods), dp(b.tsP), nmod, m + 40, dp(ovf), oc, m + 24, m + 20, lb, 0, sh),
-               "cf_batch_part(place)")
-            ck(lib.cf_batch_part(2, dp(b.mods), None, nmod, None, dp(ovf), oc, m + 24, m + 20, lb, 0, sh),
+            for i, (rr, ts) in enumerate(sorted(b.tsS.items())):
+                if i:
+                    misc[32:40].zero_()         # the scatter queue head, for the next radius
+                ck(lib.cf_batch_part(0, dp(b.mods), dp(ts), nmod, m + 32, None, 0, m + 24, m + 20, lb, rr, 0, sh),
+                   "cf_batch_part(scatter)")
+            ck(lib.cf_batch_part(1, dp(b.mods), dp(b.tsP), nmod, m + 40, dp(ovf), oc, m + 24, m + 20, lb, 0, 0,
+                                 sh), "cf_batch_part(place)")
+            ck(lib.cf_batch_part(2, dp(b.mods), None, nmod, None, dp(ovf), oc, m + 24, m + 20, lb, 0, 0, sh),
                "cf_batch_part(fix)")
         ck(lib.cf_batch_run(0, dp(b.mods), dp(b.tsD if part else b.tsD_all), nmod, tu.ticket, m, dp(pairs), dp(pmod),
                             maxp, m + 16, m + 20, None, tu.grid, sh), "cf_batch_run(build)")

@@ -393,10 +393,11 @@ class Solver:
         scr[: up(nparts * 4) + 64].zero_()
         err = dp(misc) + 4
         lb = self.tuning.part_lb
-        ck(lib.cf_batch_part(0, mods, tsS, 1, pmisc, None, 0, pmisc + 24, err, lb, 0, sh), "cf_batch_part(scatter)")
-        ck(lib.cf_batch_part(1, mods, tsP, 1, pmisc + 8, ovf, ocap, pmisc + 24, err, lb, 0, sh),
+        ck(lib.cf_batch_part(0, mods, tsS, 1, pmisc, None, 0, pmisc + 24, err, lb, inst.r, 0, sh),
+           "cf_batch_part(scatter)")
+        ck(lib.cf_batch_part(1, mods, tsP, 1, pmisc + 8, ovf, ocap, pmisc + 24, err, lb, 0, 0, sh),
            "cf_batch_part(place)")
-        ck(lib.cf_batch_part(2, mods, None, 1, None, ovf, ocap, pmisc + 24, err, lb, 0, sh), "cf_batch_part(fix)")
+        ck(lib.cf_batch_part(2, mods, None, 1, None, ovf, ocap, pmisc + 24, err, lb, 0, 0, sh), "cf_batch_part(fix)")
 
     def _enqueue_partition(self, inst: Instance, plan: dict, marks: list | None):
         """Partitioned generation of both sides and the shared-memory partition join."""

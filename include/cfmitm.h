@@ -289,6 +289,8 @@ int cf_batch_run(int mode, const void* mods, const uint64_t* tstart, uint32_t nm
  * cf_batch_part_max_ranges()); 0 for moduli
  * built by mode 0.  queue: device u64 zeroed before phases 0 and 1; ovf:
  * ovf_cap entries of cf_batch_ovf_bytes(), *novf zeroed before phase 1.
+ * radius (phase 0): 1..cf_batch_max_r() runs a generator specialised for moduli of that radius (the
+ * others must have no tickets in tstart), 0 one for any radius.
  * CF_ERR_PART_OVERFLOW in *err: a range received more than pcap records and
  * the caller rebuilds the batch with mode 0.  The table is the one mode 0 builds
  * (same slots rule), so mode 1 probes it unchanged.  Replaces, like mode 0, the
@@ -299,7 +301,8 @@ uint32_t cf_batch_part_tile(void);
 uint32_t cf_batch_part_max_ranges(void);
 size_t cf_batch_ovf_bytes(void);
 int cf_batch_part(int phase, const void* mods, const uint64_t* tstart, uint32_t nmod, void* queue, void* ovf,
-                  uint32_t ovf_cap, uint32_t* novf, uint32_t* err, int part_lb, uint32_t grid, void* stream);
+                  uint32_t ovf_cap, uint32_t* novf, uint32_t* err, int part_lb, int radius, uint32_t grid,
+                  void* stream);
 
 /* ---- sorted-side drop-ins ------------------------------------------------ */
 

@@ -66,18 +66,19 @@ def test_batch_descriptor_layout():
 def test_batch_partitioned_build_constants_and_arguments():
     lib = _lib.load()
     assert (lib.cf_batch_part_buckets(9), lib.cf_batch_part_buckets(10), lib.cf_batch_part_buckets(8)) == (512, 1024, 0)
-    assert lib.cf_batch_part_tile() == 4096
-    assert lib.cf_batch_part_max_ranges() == 4096
+    assert lib.cf_batch_part_tile() == 4064
+    assert lib.cf_batch_part_max_ranges() == 2048
     assert lib.cf_batch_ovf_bytes() == 24
     one = np.zeros(8, dtype=np.uint64)
     p = one.ctypes.data
     # bad phase, missing queue or tickets, missing overflow counter: rejected before any device call
-    assert lib.cf_batch_part(3, p, p, 1, p, p, 1, p, p, 10, 0, None) == _lib.CF_EBADARG
-    assert lib.cf_batch_part(0, p, None, 1, p, None, 0, None, p, 10, 0, None) == _lib.CF_EBADARG
-    assert lib.cf_batch_part(1, p, p, 1, None, p, 1, p, p, 10, 0, None) == _lib.CF_EBADARG
-    assert lib.cf_batch_part(1, p, p, 1, p, p, 1, p, p, 11, 0, None) == _lib.CF_EBADARG   # range size
-    assert lib.cf_batch_part(2, p, None, 1, None, p, 1, None, p, 10, 0, None) == _lib.CF_EBADARG
-    assert lib.cf_batch_part(0, p, p, 0, p, None, 0, None, p, 10, 0, None) == _lib.CF_EBADARG
+    assert lib.cf_batch_part(3, p, p, 1, p, p, 1, p, p, 10, 0, 0, None) == _lib.CF_EBADARG
+    assert lib.cf_batch_part(0, p, None, 1, p, None, 0, None, p, 10, 0, 0, None) == _lib.CF_EBADARG
+    assert lib.cf_batch_part(1, p, p, 1, None, p, 1, p, p, 10, 0, 0, None) == _lib.CF_EBADARG
+    assert lib.cf_batch_part(1, p, p, 1, p, p, 1, p, p, 11, 0, 0, None) == _lib.CF_EBADARG   # range size
+    assert lib.cf_batch_part(2, p, None, 1, None, p, 1, None, p, 10, 0, 0, None) == _lib.CF_EBADARG
+    assert lib.cf_batch_part(0, p, p, 0, p, None, 0, None, p, 10, 0, 0, None) == _lib.CF_EBADARG
+    assert lib.cf_batch_part(0, p, p, 1, p, None, 0, None, p, 10, 9, 0, None) == _lib.CF_EBADARG   # radius
 
 
 def _hostkey(M, v):
