@@ -185,9 +185,9 @@ k_batch(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart /*[n
 constexpr int kPlbMin = 9;                    // 512-bucket ranges: 80 KB, two CTAs per SM
 constexpr int kPlbMax = 10;                   // 1024-bucket ranges: 160 KB, one CTA per SM
 constexpr int kScBlock = 256;
-constexpr int kScMinBlocks = 4;               // CTAs per SM (55.6 KB of shared memory each)
-constexpr int kScTile = 4064;                 // records per scatter ticket (508 per warp): 4 CTAs
-                                              // of 56 KB fit the SM's 228 KB with their 1 KB reserves
+constexpr int kScMinBlocks = 3;               // CTAs per SM (registers for the pipelined generator)
+constexpr int kScTile = 4064;                 // records per scatter ticket (508 per warp; 56 KB of
+                                              // shared memory per CTA)
 constexpr int kScWarpRecs = kScTile / (kScBlock / 32);
 constexpr u32 kScMaxParts = 2048;             // bucket ranges per modulus (bbits <= plb + 11)
 constexpr size_t kScSmem = (size_t)kScTile * 12 + (size_t)kScMaxParts * 4;
@@ -232,15 +232,25 @@ __device__ __forceinline__ bool scatter_gen(const CfBatchMod& md, u64 first, u32
   w.init(rank0 + first + wbeg, n, binom, ar, st, hd->tail_n);
   const int plb = (int)md.plb;
   const u32 pmask = md.bbits > plb ? ~0u : 0u;
+  // software-pipelined: the next step's tail entry is loaded before this step's record is hashed and
+  // staged, so the table read overlaps the work instead of stalling the warp
+  int unused[R - B > 0 ? R - B : 1];
+  CfElt32 qn = st;
+  u64 jn;
+  w.template step<false>(n, binom, ar, lane, qn, jn, unused);
+  CfTailEnt en = (u32)lane < wcnt ? tail[jn] : CfTailEnt{};
   for (u32 off = 0; off < wcnt; off += 32) {     // uniform across the warp
-    CfElt32 q = st;
-    u64 j;
-    int unused[R - B > 0 ? R - B : 1];
-    w.template step<false>(n, binom, ar, lane, q, j, unused);
+    const CfElt32 q = qn;
+    const CfTailEnt e = en;
+    if (off + 32 < wcnt) {
+      qn = st;
+      w.template step<false>(n, binom, ar, lane, qn, jn, unused);
+      if (off + 32 + (u32)lane < wcnt) en = tail[jn];
+    }
     if (off + (u32)lane < wcnt) {
       u64 X;
       u32 x2;
-      cf_fuse_res(q, tail[j], ar.md, minv, X, x2);
+      cf_fuse_res(q, e, ar.md, minv, X, x2);
       if (md.bloom) {
         const CfBloomKey bk = cf_bloom_key(X, x2, md.fbits);
         u32* blk = md.bloom + (u64)bk.block * 8;
