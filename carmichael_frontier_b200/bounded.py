@@ -179,7 +179,7 @@ class BoundedGenerator:
     def _setup_I(self, INS, r, M, P0, Icap, split, hmax):
         INS = [int(p) for p in INS]
         n = len(INS)
-        assert 1 <= r <= 16 and n <= 1024 and 2 <= M < (1 << 62)
+        assert 1 <= r <= 16 and n <= 1024 and 2 <= M < (1 << 64)
         assert all(INS[i] < INS[i + 1] for i in range(n - 1)), "INS must be strictly ascending"
         assert Icap - 1 < U128, "Icap needs more than 128 bits"
         if Icap <= 1 or n < r:
@@ -224,7 +224,7 @@ class BoundedGenerator:
         mode = int(bitmask)
         if mode == 0 and r > 10:
             mode = 1
-        assert mode in (0, 1, 2) and 1 <= r <= 16 and 2 <= M < (1 << 62)
+        assert mode in (0, 1, 2) and 1 <= r <= 16 and 2 <= M < (1 << 64)
         assert n <= (1024 if mode == 2 else 64), "packed and mask ids need a base of at most 64 primes"
         assert all(B[i] < B[i + 1] for i in range(n - 1)), "the base must be strictly ascending"
         if mode == 2:

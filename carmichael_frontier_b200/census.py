@@ -164,15 +164,14 @@ def family_instances(rows, U: int, r_min: int = 1, r_max: int | None = None, k: 
                      sieve_bound: int = SIEVE_BOUND, with_base: bool = True):
     """(row, radius, Instance) for every survivor row: radius 0 (the k smallest primes themselves, when
     with_base) and radii r_min..min(rmax, r_max), each over the full capped pool with bound n < U -- the
-    per-family runs of gpu/run_mstar_family.py:66-94, here as one portfolio.  Rows whose modulus is 2^62
-    or more are skipped (keys are u64 residues), as the reference marks moduli of 2^64 and more
-    unsupported."""
+    per-family runs of gpu/run_mstar_family.py:66-94, here as one portfolio.  Rows whose modulus is 2^64
+    or more are skipped (keys are u64 residues), as the reference marks them unsupported."""
     from .solve import Instance
     out = []
-    pools = _Pools([int(r["D"]) for r in rows if int(r["D"]) < 1 << 62], sieve_bound)
+    pools = _Pools([int(r["D"]) for r in rows if int(r["D"]) < 1 << 64], sieve_bound)
     for row in rows:
         D, cap, rmax = int(row["D"]), int(row["cap"]), int(row["rmax"])
-        if D >= 1 << 62:
+        if D >= 1 << 64:
             continue
         P = pools(D)
         Pc = [q for q in P if q <= cap]
@@ -232,11 +231,11 @@ def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: in
     log = log or (lambda s: None)
     solver = solver or Solver(tuning=Tuning(strategy="bounded"))
     out = {}
-    pools = _Pools([int(r["D"]) for r in rows if int(r["D"]) < 1 << 62], sieve_bound)
+    pools = _Pools([int(r["D"]) for r in rows if int(r["D"]) < 1 << 64], sieve_bound)
     for row in rows:
         D, cap, rmax = int(row["D"]), int(row["cap"]), int(row["rmax"])
-        if D >= 1 << 62:
-            out[D] = {"unsupported": "modulus of 2^62 or more (u64 residue keys)"}
+        if D >= 1 << 64:
+            out[D] = {"unsupported": "modulus of 2^64 or more (u64 residue keys)"}
             continue
         P = pools(D)
         Pc = [q for q in P if q <= cap]

@@ -2,7 +2,7 @@
 // exchange meet-in-the-middle residue join, and by the host code that prepares
 // the tables.
 //
-// Residue representation ("key form").  The modulus M (< 2^62) is split as
+// Residue representation ("key form").  The modulus M (< 2^64, odd part < 2^63) is split as
 // M = 2^a * m with m odd.  A residue x mod M is held as
 //     key(x) = (X << a) | (x mod 2^a),   X = x * 2^64 mod m   (Montgomery form)
 // which is a bijection of [0, M) onto [0, M): equal keys <=> equal residues,
@@ -67,7 +67,7 @@ CF_HD u64 cf_mul_key(u64 kx, u64 ky, const CfMod& md) {
 // mod M (Chinese remainder theorem), packed as key = (x mod m) << a | x mod 2^a.
 // ---------------------------------------------------------------------------
 struct CfMod32 {
-  u64 m;      // odd part of M (< 2^62)
+  u64 m;      // odd part of M (< 2^63: values stay below 2m < 2^64)
   u64 mask2;  // 2^a - 1
   u32 ninv;   // -m^-1 mod 2^32
   u32 ml, mh; // low and high 32-bit halves of m

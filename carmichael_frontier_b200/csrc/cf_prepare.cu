@@ -41,8 +41,11 @@ struct HostMod {
   int a;
 };
 
+// Any M >= 2 whose odd part m is below 2^63 (every even M below 2^64): the lazy 32-bit-radix
+// Montgomery step keeps its values below 2m < 2^64, and key = X << a | x mod 2^a stays a
+// bijection of [0, M) (X < m).
 static int host_mod_init(u64 M, HostMod* h) {
-  if (M < 2 || M >= (1ull << 62)) return CF_EBADARG;
+  if (M < 2 || (M >> __builtin_ctzll(M)) >= (1ull << 63)) return CF_EBADARG;
   h->M = M;
   h->a = __builtin_ctzll(M);
   h->m = M >> h->a;
@@ -70,7 +73,10 @@ extern "C" int cf_pool_prepare(const u64* primes, int n, int r, u64 M, u64 mult,
   if (r < 1 || r > CF_MAX_R || r > n) { cf_set_error("cf_pool_prepare: radius out of range (1..16, <= n)%s", ""); return CF_EBADARG; }
   if (out_bytes < cf_pool_bytes(n, r)) { cf_set_error("cf_pool_prepare: table buffer too small%s", ""); return CF_EBADARG; }
   HostMod h;
-  if (host_mod_init(M, &h) != CF_OK) { cf_set_error("cf_pool_prepare: need 2 <= M < 2^62%s", ""); return CF_EBADARG; }
+  if (host_mod_init(M, &h) != CF_OK) {
+    cf_set_error("cf_pool_prepare: need 2 <= M < 2^64 with an odd part below 2^63%s", "");
+    return CF_EBADARG;
+  }
   u64* w = (u64*)out;
   memset(w, 0, cf_pool_bytes(n, r));
   CfPoolHdr* hd = (CfPoolHdr*)w;

@@ -11,7 +11,7 @@
 // publishes its per-digit counts, resolves its global digit offsets by
 // decoupled look-back over the tiles before it (bounded spin), and scatters
 // keys, then ids.  Passes whose digit is equal for every key are skipped by the
-// host, so keys below M < 2^62 cost at most ceil(log2 M / 8) passes.
+// host, so keys below M cost at most ceil(log2 M / 8) passes.
 //
 // Merge join: every thread takes a run of consecutive sorted I keys, finds the
 // first D key >= its first key by binary search and then gallops forward;

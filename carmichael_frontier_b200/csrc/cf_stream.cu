@@ -104,7 +104,7 @@ unsigned grid_of(u64 n, u64 per) {
 // counts[p] += number of keys[0..n) in residue range p = floor(key * 2^pbits / M)
 // (counts zeroed by the caller; 1 <= pbits <= 12, keys canonical, < M).
 extern "C" int cf_part_hist(const u64* keys, u64 n, u64 M, int pbits, u64* counts, void* stream) {
-  if (!counts || (n && !keys) || pbits < 1 || pbits > 12 || M < 2 || M >= (1ull << 63)) {
+  if (!counts || (n && !keys) || pbits < 1 || pbits > 12 || M < 2) {
     cf_set_error("cf_part_hist: bad arguments%s", "");
     return CF_EBADARG;
   }
@@ -120,8 +120,7 @@ extern "C" int cf_part_hist(const u64* keys, u64 n, u64 M, int pbits, u64* count
 // the caller sizes each partition by cf_part_hist).
 extern "C" int cf_part_scatter(const u64* keys, const u64* ids, u64 n, u64 M, int pbits, u64* cursor, u64* okeys,
                                u64* oids, void* stream) {
-  if (!cursor || (n && (!keys || !ids || !okeys || !oids)) || pbits < 1 || pbits > 12 || M < 2 ||
-      M >= (1ull << 63)) {
+  if (!cursor || (n && (!keys || !ids || !okeys || !oids)) || pbits < 1 || pbits > 12 || M < 2) {
     cf_set_error("cf_part_scatter: bad arguments%s", "");
     return CF_EBADARG;
   }

@@ -8,7 +8,7 @@ INS with prod(I) < Icap and at most hmax primes > split; key = P0*prod(I) mod M,
 id = colex rank -- in the same (lexicographic) order.  The kernels are the
 level-by-level expansion of csrc/cf_bgen.cu, not a per-thread depth-first walk,
 so deep radii balance as well as shallow ones.  Differences: r may be 1..16 (the
-reference accepts 3..8) and M must be below 2^62 (the reference: 2^64).
+reference accepts 3..8) and M must be below 2^64 with an odd part below 2^63 (the reference: 2^64).
 """
 from __future__ import annotations
 
@@ -20,7 +20,7 @@ def generate_chunks(INS, r, M, P0, Icap, split=None, hmax=None, max_records=200_
     """Yield (keys, ids) torch uint64 chunks covering exactly the filtered r-subsets of INS;
     the generator's return value is the total record count.  block_bytes is accepted for
     signature compatibility (frontier memory is bounded by the generator's max_nodes)."""
-    assert 1 <= r <= 16 and len(INS) <= 1024 and 1 <= M < (1 << 62), "need 1 <= r <= 16, n <= 1024, M < 2^62"
+    assert 1 <= r <= 16 and len(INS) <= 1024 and 1 <= M < (1 << 64), "need 1 <= r <= 16, n <= 1024, M < 2^64"
     if Icap <= 1:
         return 0
     gen = generator(device).generate_I(INS, r, M, P0, Icap, split, hmax, max_records=max(1, int(max_records)))

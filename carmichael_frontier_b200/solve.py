@@ -150,8 +150,8 @@ class Instance:
     @staticmethod
     def build(M: int, Q, B0, r: int, B: int) -> "Instance":
         M, r, B = int(M), int(r), int(B)
-        if not (2 <= M < (1 << 62)):
-            raise ValueError("M must satisfy 2 <= M < 2^62 (keys are u64 residues)")
+        if not (2 <= M < (1 << 64)) or (M >> ((M & -M).bit_length() - 1)) >= 1 << 63:
+            raise ValueError("M must satisfy 2 <= M < 2^64 with an odd part below 2^63 (keys are u64 residues)")
         base = sorted(int(p) for p in B0)
         if len(set(base)) != len(base):
             raise ValueError("B0 has repeated primes")

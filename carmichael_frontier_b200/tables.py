@@ -16,7 +16,7 @@ from . import _lib
 
 MAX_POOL = 1024
 MAX_R = 10
-M_LIMIT = 1 << 62
+M_LIMIT = 1 << 64
 
 
 def pool_table_host(primes, r: int, M: int, mult: int) -> np.ndarray:

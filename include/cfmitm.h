@@ -63,7 +63,7 @@ const char* cf_last_error_string(void);
 size_t cf_pool_bytes(int n, int r);
 
 /* Fill a pool table (host buffer) for the r-subsets of primes[0..n-1] modulo M
- * (2 <= M < 2^62) with leading multiplier `mult` (the D side of a solve uses
+ * (2 <= M < 2^64, odd part below 2^63) with leading multiplier `mult` (the D side of a solve uses
  * (prod B0)^-1 mod M, the I side 1; gen_records' `mult` argument otherwise).
  * Holds each prime in key form, log2 of each prime and the binomial table.
  * Replaces the host half of generate(): gpu/mitm_gpu2.py:70-93. */

@@ -130,3 +130,37 @@ def test_partitioned_table_build_with_bloom_level(cuda, golden):
     res = s.solve(g["M"], g["Q"], g["B0"], g["r"], int(g["B"]))
     assert res.plan["fbits"] > 0
     assert as_lists(res.pairs) == g["pairs"]
+
+
+@pytest.mark.parametrize("M", [5257444553750188800, 12267370625417107200, 17524815179167296000])
+def test_moduli_between_2_62_and_2_64(cuda, M):
+    # moduli of 63 and 64 bits (the reference's campaign has 4,041 in [2^62, 2^64)): every strategy
+    # and the batched portfolio against the exhaustive oracle
+    from carmichael_frontier_b200.portfolio import BatchSolver
+    assert 1 << 62 <= M < 1 << 64
+    Q = W.eligible_pool(M, 5518)
+    insts = []
+    for k, extra, r in ((20, 25, 2), (18, 22, 3)):
+        B0 = Q[:k]
+        insts.append(Instance.build(M, Q[:k + extra], B0, r, W.product(B0) * 10 ** 12))
+    want = []
+    for x in insts:
+        pairs, hits = O.solve_exhaustive(x.M, x.B0 + x.INS, x.B0, x.r, x.B)
+        want.append((as_lists(pairs), [(tuple(D), tuple(I), n) for D, I, n in hits]))
+    for st in ("fused", "partition", "bounded", "auto"):
+        s = Solver(cuda, tuning=Tuning(strategy=st))
+        for x, (pairs, hits) in zip(insts, want):
+            got = s.solve_instance(x)
+            assert [(h.D, h.I, h.n) for h in got.hits] == hits, st
+            if st in ("fused", "partition"):
+                assert as_lists(got.pairs) == pairs, st
+    for x, got, (pairs, hits) in zip(insts, BatchSolver(cuda).solve(insts), want):
+        assert as_lists(got.pairs) == pairs and [(h.D, h.I, h.n) for h in got.hits] == hits
+
+
+def test_modulus_limits(cuda):
+    Q = W.eligible_pool(21621600)
+    with pytest.raises(ValueError):
+        Instance.build(1 << 64, Q, Q[:10], 2, 10 ** 50)          # 2^64 and beyond: not u64 residues
+    with pytest.raises(ValueError):
+        Instance.build((1 << 63) + 1, [3, 5, 7], [3], 1, 10 ** 50)   # odd part of 2^63 or more
