@@ -51,6 +51,7 @@ SIGNATURES = [
     ("cf_last_error_string", C.c_char_p, []),
     ("cf_pool_bytes", sz, [C.c_int, C.c_int]),
     ("cf_pool_prepare", C.c_int, [vp, C.c_int, C.c_int, u64, u64, vp, sz]),
+    ("cf_pool_prepare_split", C.c_int, [vp, C.c_int, C.c_int, u64, C.c_int, u64, u64, vp, sz]),
     ("cf_key_of", u64, [u64, u64]),
     ("cf_canon_of", u64, [u64, u64]),
     ("cf_key_mul", u64, [u64, u64, u64]),

@@ -43,8 +43,9 @@ def caps(inst) -> tuple[int, int]:
 
 
 def applicable(inst) -> bool:
-    """The bounded producers need 128-bit products (and r >= 1, both sides non-empty)."""
-    if inst.r < 1 or len(inst.B0) < inst.r or len(inst.INS) < inst.r:
+    """The bounded producers need 128-bit products, r >= 1, both sides non-empty and M < 2^64 (they
+    carry packed keys from level to level, exact only while the key is the whole residue)."""
+    if inst.r < 1 or len(inst.B0) < inst.r or len(inst.INS) < inst.r or inst.M >= 1 << 64:
         return False
     Icap, Dmin = caps(inst)
     return Icap - 1 < U128 and math.prod(inst.B0[-inst.r:]) < U128 and math.comb(len(inst.INS), inst.r) < 1 << 64 \

@@ -28,7 +28,7 @@ import numpy as np
 
 from . import _lib
 from .certify import verify_certificate
-from .tables import DeviceTables, ncomb, unrank_lex
+from .tables import DeviceTables, ncomb, unrank_lex, wide_modulus
 
 RESULT_DTYPE = np.dtype([("flags", "<u4"), ("r", "<u4"), ("d_idx", "<u2", (16,)), ("i_idx", "<u2", (16,))])
 
@@ -150,8 +150,8 @@ class Instance:
     @staticmethod
     def build(M: int, Q, B0, r: int, B: int) -> "Instance":
         M, r, B = int(M), int(r), int(B)
-        if not (2 <= M < (1 << 64)) or (M >> ((M & -M).bit_length() - 1)) >= 1 << 63:
-            raise ValueError("M must satisfy 2 <= M < 2^64 with an odd part below 2^63 (keys are u64 residues)")
+        if M < 2 or (M >> ((M & -M).bit_length() - 1)) >= 1 << 63:
+            raise ValueError("M must be at least 2 with an odd part below 2^63")
         base = sorted(int(p) for p in B0)
         if len(set(base)) != len(base):
             raise ValueError("B0 has repeated primes")
@@ -185,6 +185,7 @@ def finish_rows(inst: Instance, res: np.ndarray, nD: int, nI: int, plan: dict, v
     hits, screened, above, rejected, pairs = [], 0, 0, 0, []
     bset = inst.B0
     fused = plan.get("strategy") == "fused"
+    wide = wide_modulus(inst.M)                # keys taken mod 2^64: confirm every match exactly
     nres = 0
     for row in res:
         f = int(row["flags"])
@@ -192,11 +193,15 @@ def finish_rows(inst: Instance, res: np.ndarray, nD: int, nI: int, plan: dict, v
             if not fused:
                 rejected += 1
             continue
-        nres += 1
         di = [int(x) for x in row["d_idx"][:r]]
         ii = [int(x) for x in row["i_idx"][:r]]
         D = tuple(bset[i] for i in di)
         I = tuple(inst.INS[i] for i in ii)
+        if wide and (inst.P0 * math.prod(I) - math.prod(D)) % inst.M:
+            if not fused:                     # keys mod 2^64 matched, residues differ
+                rejected += 1
+            continue
+        nres += 1
         pairs.append((D, I))
         if not f & _lib.HIT_SCREEN:
             above += 1

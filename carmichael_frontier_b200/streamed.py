@@ -277,6 +277,8 @@ def streamed_solve(inst, pbits: int = 8, i_limit: int | None = None, device=None
     join only I ranks [0, i_limit).  Returns (SolveResult, stats)."""
     from .solve import Hit, SolveResult
     import time
+    if inst.M >= 1 << 64:
+        raise ValueError("the streamed join partitions canonical u64 residues: M must be below 2^64")
     sj = StreamedJoin(device, pbits, chunk, piece)
     r, M = inst.r, inst.M
     nD = ncomb(len(inst.B0), r)

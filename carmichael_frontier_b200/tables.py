@@ -16,7 +16,19 @@ from . import _lib
 
 MAX_POOL = 1024
 MAX_R = 10
-M_LIMIT = 1 << 64
+M_LIMIT = 1 << 64          # moduli below this have exact u64 keys; larger ones (odd part < 2^63,
+                           # 2-adic part <= 2^32) have keys taken mod 2^64, confirmed exactly
+
+
+def split_modulus(M: int) -> tuple[int, int]:
+    """(odd part m, 2-adic exponent a) of M."""
+    a = (M & -M).bit_length() - 1
+    return M >> a, a
+
+
+def wide_modulus(M: int) -> bool:
+    """True when keys of M are taken mod 2^64 (M of 2^64 or more), so key matches need an exact check."""
+    return M >= M_LIMIT
 
 
 def pool_table_host(primes, r: int, M: int, mult: int) -> np.ndarray:
@@ -28,8 +40,13 @@ def pool_table_host(primes, r: int, M: int, mult: int) -> np.ndarray:
         raise ValueError(f"pool of {n} primes at radius {r} is outside 1..{MAX_POOL} x 1..16")
     pr = np.ascontiguousarray(np.asarray([int(p) for p in primes], dtype=np.uint64))
     out = np.zeros(nbytes, dtype=np.uint8)
-    _lib.check(lib.cf_pool_prepare(pr.ctypes.data, n, r, M, int(mult) % M, out.ctypes.data, nbytes),
-               "cf_pool_prepare")
+    mult = int(mult) % M
+    if M < M_LIMIT:
+        _lib.check(lib.cf_pool_prepare(pr.ctypes.data, n, r, M, mult, out.ctypes.data, nbytes), "cf_pool_prepare")
+    else:
+        m, a = split_modulus(M)
+        _lib.check(lib.cf_pool_prepare_split(pr.ctypes.data, n, r, m, a, mult % m, mult & ((1 << a) - 1),
+                                             out.ctypes.data, nbytes), "cf_pool_prepare_split")
     return out
 
 

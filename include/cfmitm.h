@@ -9,8 +9,10 @@
  * synchronising wait for the device.  The library never throws.
  *
  * Residues are held in "key form" (see carmichael_frontier_b200/csrc/cf_common.cuh):
- * a bijection of [0, M) onto itself, so equal keys <=> equal residues mod M.
- * cf_gen_subsets(..., canon=1) emits canonical residues instead.
+ * a bijection of [0, M) onto itself for M < 2^64, so equal keys <=> equal residues mod M.
+ * Tables made by cf_pool_prepare_split for M >= 2^64 hold keys taken mod 2^64: equal
+ * residues => equal keys only.  cf_gen_subsets(..., canon=1) emits canonical residues
+ * instead (M < 2^64 only).
  *
  * Reference interfaces replaced (paths inside AlexanderEastwood/carmichael-frontier):
  *   gen_records / generate()   gpu/mitm_gpu2.py:24-98
@@ -69,6 +71,15 @@ size_t cf_pool_bytes(int n, int r);
  * Replaces the host half of generate(): gpu/mitm_gpu2.py:70-93. */
 int cf_pool_prepare(const uint64_t* primes, int n, int r, uint64_t M, uint64_t mult, void* out,
                     size_t out_bytes);
+
+/* The same table for M = 2^a * m given by its parts, so M may be 2^64 or more: m odd below 2^63,
+ * 0 <= a <= 32, the multiplier as mult_odd = mult mod m and mult2 = mult mod 2^a.  Keys of such
+ * moduli are the packed residue taken mod 2^64: equal residues give equal keys, and a caller
+ * confirms each key match exactly (the Python layer recomputes the residues with Python
+ * integers before it reports a pair).  No counterpart in
+ * the reference, whose keys are u64 residues below M < 2^64 (gpu/run_mstar_family.py:70-73). */
+int cf_pool_prepare_split(const uint64_t* primes, int n, int r, uint64_t m, int a, uint64_t mult_odd,
+                          uint64_t mult2, void* out, size_t out_bytes);
 
 /* key(v mod M), its inverse, and the product of two keys computed by the
  * kernels' own Montgomery/CRT code compiled for the host (host helpers). */

@@ -158,9 +158,89 @@ def test_moduli_between_2_62_and_2_64(cuda, M):
         assert as_lists(got.pairs) == pairs and [(h.D, h.I, h.n) for h in got.hits] == hits
 
 
+WIDE_MODULI = [36802111876251321600,           # 2^8 * an odd part of 57 bits: 65 bits
+               863845157977978176000,          # 2^9 * an odd part of 61 bits: 70 bits
+               5019589575 << 32]               # 2^32 * an odd part of 33 bits: 65 bits
+
+
+def _packed_residue(M: int, v: int) -> int:
+    # the solve path's key of v mod M: (v mod m) << a | v mod 2^a for M = 2^a * m, m odd, mod 2^64
+    a = (M & -M).bit_length() - 1
+    return (((v % (M >> a)) << a) | (v & ((1 << a) - 1))) & ((1 << 64) - 1)
+
+
+@pytest.mark.parametrize("M", WIDE_MODULI)
+def test_wide_modulus_keys_are_the_residue_keys(cuda, M):
+    # moduli of 2^64 and more: every key of both generators (linear, and the tail walker of the
+    # fused and partition joins) is the packed exact residue taken mod 2^64, so equal residues meet
+    # in the join
+    import torch
+    from carmichael_frontier_b200 import _lib
+    from carmichael_frontier_b200.tables import DeviceTables, unrank_lex
+    assert M >= 1 << 64
+    lib = _lib.load()
+    Q = W.eligible_pool(M, 5518)[:64]
+    n = len(Q)
+    dt = DeviceTables(cuda)
+    rng = random.Random(M & 0xFFFF)
+    for r in (2, 3, 5):
+        mult = rng.randrange(1, M)
+        pool = dt.pool(Q, r, M, mult)
+        tail = dt.tail(Q, r, M, mult, pool)
+        total = math.comb(n, r)
+        count = min(total, 4000)
+        lo = rng.randrange(0, total - count + 1)
+        keys = torch.empty(count, dtype=torch.uint64, device=cuda)
+        ids = torch.empty(count, dtype=torch.uint64, device=cuda)
+        _lib.check(lib.cf_gen_subsets(pool.data_ptr(), n, r, lo, count, 1, 0, 0, keys.data_ptr(), ids.data_ptr(),
+                                      _lib.stream_handle()), "cf_gen_subsets")
+        recs = torch.empty(2 * count, dtype=torch.uint64, device=cuda)
+        counts = torch.zeros(1, dtype=torch.int32, device=cuda)
+        err = torch.zeros(1, dtype=torch.int32, device=cuda)
+        _lib.check(lib.cf_gen_part(pool.data_ptr(), tail.data_ptr(), n, r, lo, count, 0, count, counts.data_ptr(),
+                                   recs.data_ptr(), err.data_ptr(), 0, _lib.stream_handle()), "cf_gen_part")
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0 and int(counts.item()) == count
+        want = {}
+        for t in range(count):
+            S = unrank_lex(lo + t, n, r)
+            want[lo + t] = _packed_residue(M, mult * math.prod(Q[i] for i in S))
+        lin = dict(zip(ids.cpu().numpy().tolist(), keys.cpu().numpy().tolist()))
+        rv = recs.cpu().numpy().reshape(count, 2)
+        walk = {int(i): int(k) for k, i in rv}
+        assert lin == want and walk == want, r
+
+
+@pytest.mark.parametrize("M", WIDE_MODULI[:2])
+def test_wide_modulus_solves(cuda, M):
+    # every strategy and the batched portfolio run on moduli of 2^64 and more and agree with the
+    # exhaustive oracle (equal residues mod M >= 2^64 do not occur at these sizes; the keys above and
+    # the host's exact check of each key match make the join exact)
+    from carmichael_frontier_b200 import bsolve
+    from carmichael_frontier_b200.portfolio import BatchSolver
+    Q = W.eligible_pool(M, 5518)
+    insts = []
+    for k, extra, r in ((20, 25, 2), (18, 22, 3)):
+        B0 = Q[:k]
+        insts.append(Instance.build(M, Q[:k + extra], B0, r, W.product(B0) * 10 ** 12))
+    assert not any(bsolve.applicable(x) for x in insts)     # bounded producers: M < 2^64 only
+    want = []
+    for x in insts:
+        pairs, hits = O.solve_exhaustive(x.M, x.B0 + x.INS, x.B0, x.r, x.B)
+        want.append((as_lists(pairs), [(tuple(D), tuple(I), n) for D, I, n in hits]))
+    for st in ("fused", "partition", "auto"):
+        s = Solver(cuda, tuning=Tuning(strategy=st))
+        for x, (pairs, hits) in zip(insts, want):
+            got = s.solve_instance(x)
+            assert as_lists(got.pairs) == pairs and [(h.D, h.I, h.n) for h in got.hits] == hits, st
+            assert got.n_D == math.comb(len(x.B0), x.r) and got.n_I == math.comb(len(x.INS), x.r)
+    for x, got, (pairs, hits) in zip(insts, BatchSolver(cuda).solve(insts), want):
+        assert as_lists(got.pairs) == pairs and [(h.D, h.I, h.n) for h in got.hits] == hits
+
+
 def test_modulus_limits(cuda):
     Q = W.eligible_pool(21621600)
     with pytest.raises(ValueError):
-        Instance.build(1 << 64, Q, Q[:10], 2, 10 ** 50)          # 2^64 and beyond: not u64 residues
+        Instance.build(1 << 64, Q, Q[:10], 2, 10 ** 50)          # 2-adic part 2^64: above 2^32
     with pytest.raises(ValueError):
         Instance.build((1 << 63) + 1, [3, 5, 7], [3], 1, 10 ** 50)   # odd part of 2^63 or more
