@@ -163,12 +163,10 @@ class Instance:
             raise ValueError("B0 and Q \\ B0 are limited to 1024 primes each")
         if B < 1:
             raise ValueError("size bound B must be >= 1")
-        P0 = 1
-        for p in base:
-            P0 *= p
-        if math.gcd(P0, M) != 1 or any(math.gcd(q, M) != 1 for q in ins):
+        P0 = math.prod(base)
+        if math.gcd(P0 * math.prod(ins), M) != 1:
             raise ValueError("every pool prime must be coprime to M (q does not divide M)")
-        if any(p >= 1 << 31 for p in base) or any(q >= 1 << 31 for q in ins):
+        if (base and base[-1] >= 1 << 31) or (ins and ins[-1] >= 1 << 31):
             raise ValueError("pool primes must be below 2^31")
         if M % (1 << 33) == 0:
             raise ValueError("2^33 divides M: the solve path needs the 2-adic part of M below 2^33")
@@ -244,7 +242,7 @@ class Solver:
             raise RuntimeError("the join runs on a CUDA device only")
         self.stream = stream
         self.tuning = tuning or Tuning()
-        self.tables = DeviceTables(self.device)
+        self.tables = DeviceTables(self.device, stream=stream, async_upload=True)
         self._bufs: dict[str, object] = {}
         self._bounded = None
         self.result_bytes = self.lib.cf_pair_result_bytes()
@@ -295,13 +293,16 @@ class Solver:
             return self._enqueue_fused(inst, plan, marks)
         return self._enqueue_partition(inst, plan, marks)
 
-    def _tables_for(self, inst: Instance):
+    def _side_tables(self, inst: Instance, side: str):
+        """(pool, tail) device tables of one side: D with multiplier (prod B0)^-1, I with 1."""
         M, r = inst.M, inst.r
-        multD = pow(inst.P0, -1, M)
-        poolD = self.tables.pool(inst.B0, r, M, multD)
-        poolI = self.tables.pool(inst.INS, r, M, 1)
-        tailD = self.tables.tail(inst.B0, r, M, multD, poolD)
-        tailI = self.tables.tail(inst.INS, r, M, 1, poolI)
+        primes, mult = (inst.B0, pow(inst.P0, -1, M)) if side == "D" else (inst.INS, 1)
+        pool = self.tables.pool(primes, r, M, mult)
+        return pool, self.tables.tail(primes, r, M, mult, pool)
+
+    def _tables_for(self, inst: Instance):
+        poolD, tailD = self._side_tables(inst, "D")
+        poolI, tailI = self._side_tables(inst, "I")
         screen = self.tables.screen(inst.P0, inst.B, 1e-6)
         return poolD, poolI, tailD, tailI, screen
 
@@ -310,7 +311,6 @@ class Solver:
         torch, lib = self.torch, self.lib
         r = inst.r
         nD, nIt = ncomb(len(inst.B0), r), _i_window(inst, plan)
-        poolD, poolI, tailD, tailI, screen = self._tables_for(inst)
         bbits, fbits = plan["bbits"], plan.get("fbits", 0)
         tbytes = lib.cf_dtab_bytes2(bbits, fbits)
         tab = self._buf("dtab", tbytes)
@@ -328,20 +328,28 @@ class Solver:
         tab[160 * nb: tbytes].zero_()              # fill counters and Bloom filter
         # build on the smaller side (swap: the table holds the I window and the D side probes)
         swap = bool(plan.get("swap")) and nIt < nD
-        sideD = (dp(poolD), dp(tailD), len(inst.B0), nD)
-        sideI = (dp(poolI), dp(tailI), len(inst.INS), nIt)
-        bpool, btail, bn, bcount = sideI if swap else sideD
-        ppool, ptail, pn, pcount = sideD if swap else sideI
+        bside, pside = ("I", "D") if swap else ("D", "I")
+        bn, bcount = (len(inst.INS), nIt) if swap else (len(inst.B0), nD)
+        pn, pcount = (len(inst.B0), nD) if swap else (len(inst.INS), nIt)
         tu = self.tuning
         pshape = None
         if tu.part_build and not plan.get("no_part") and nb >= tu.part_min_buckets and r <= lib.cf_batch_max_r():
             pshape = part_shape(bcount, bbits, tu.part_lb, tu.part_sigma, lib.cf_batch_part_max_ranges())
         self._mark(marks, "start")
         if pshape is not None:
-            self._part_build(inst, plan, pshape, (poolD, poolI, tailD, tailI, screen), tab, nD, nIt, swap, misc)
+            tables = self._tables_for(inst)
+            self._part_build(inst, plan, pshape, tables, tab, nD, nIt, swap, misc)
+            poolD, poolI, tailD, tailI, screen = tables
+            ppool, ptail = (poolD, tailD) if pside == "D" else (poolI, tailI)
         else:
-            ck(lib.cf_dtab_build2(bpool, btail, bn, r, 0, bcount, dp(tab), bbits, fbits, dp(misc) + 4, sh),
+            # the build side's tables first: the table build runs while the host prepares the other side
+            bpool, btail = self._side_tables(inst, bside)
+            ck(lib.cf_dtab_build2(dp(bpool), dp(btail), bn, r, 0, bcount, dp(tab), bbits, fbits, dp(misc) + 4, sh),
                "cf_dtab_build")
+            ppool, ptail = self._side_tables(inst, pside)
+            screen = self.tables.screen(inst.P0, inst.B, 1e-6)
+            poolD, poolI = (bpool, ppool) if bside == "D" else (ppool, bpool)
+        ppool, ptail = dp(ppool), dp(ptail)
         self._mark(marks, "gen_D")
         ck(lib.cf_fused_probe2(ppool, ptail, pn, r, 0, pcount, dp(tab), bbits, fbits, 0, int(swap), dp(pairs),
                                maxp, dp(misc), dp(misc) + 4, self.tuning.fused_grid, sh), "cf_fused_probe")

@@ -51,19 +51,34 @@ def pool_table_host(primes, r: int, M: int, mult: int) -> np.ndarray:
 
 
 class DeviceTables:
-    """Content-keyed cache of device copies of small host tables."""
+    """Content-keyed cache of device copies of small host tables.
 
-    def __init__(self, device, max_entries: int = 64):
+    stream: the torch stream of the uploads and tail builds (None: the current stream).  With
+    async_upload a table is staged in page-locked memory and copied without waiting for the
+    device, so kernels queued before it keep running; the consumer must then launch on the same
+    stream (the single-modulus solver does).  Otherwise the copy returns when the data is on the
+    device, which any stream may use."""
+
+    def __init__(self, device, max_entries: int = 64, stream=None, async_upload: bool = False):
         self.device = device
         self.max_entries = max_entries
+        self.stream = stream
+        self.async_upload = async_upload
         self._cache: dict = {}
 
     def get(self, key, make):
         import torch
         t = self._cache.get(key)
         if t is None:
-            host = make()
-            t = torch.from_numpy(host).to(self.device, non_blocking=False)
+            host = torch.from_numpy(make())
+            if self.async_upload:
+                s = self.stream if self.stream is not None else torch.cuda.current_stream(self.device)
+                host = host.pin_memory()
+                with torch.cuda.stream(s):
+                    t = torch.empty(host.shape, dtype=host.dtype, device=self.device)
+                    t.copy_(host, non_blocking=True)
+            else:
+                t = host.to(self.device, non_blocking=False)
             if len(self._cache) >= self.max_entries:
                 self._cache.pop(next(iter(self._cache)))
             self._cache[key] = t
@@ -81,9 +96,10 @@ class DeviceTables:
         if t is None:
             lib = _lib.load()
             nbytes = lib.cf_tail_bytes(len(primes), r)
-            t = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=self.device)
-            _lib.check(lib.cf_build_tail(pool_dev.data_ptr(), len(primes), r, t.data_ptr(), _lib.stream_handle()),
-                       "cf_build_tail")
+            with torch.cuda.stream(self.stream if self.stream is not None else torch.cuda.current_stream(self.device)):
+                t = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=self.device)
+            _lib.check(lib.cf_build_tail(pool_dev.data_ptr(), len(primes), r, t.data_ptr(),
+                                         _lib.stream_handle(self.stream)), "cf_build_tail")
             if len(self._cache) >= self.max_entries:
                 self._cache.pop(next(iter(self._cache)))
             self._cache[key] = t
