@@ -3,11 +3,13 @@ and the rate of the LSD radix sort (the materialised join's sort_side).
 
     python -m carmichael_frontier_b200.micro            # ceilings, one JSON line
     python -m carmichael_frontier_b200.micro sort N     # cf_sort_pairs on N random 62-bit keys
+    python -m carmichael_frontier_b200.micro gen N      # linear generator (N records), bounded D producer
 bench.py quotes the L2 figure as the fused probe's ceiling.
 """
 from __future__ import annotations
 
 import json
+import math
 
 from . import _lib
 
@@ -81,10 +83,47 @@ def sort_rate(n: int, key_bits: int = 62, reps: int = 3) -> dict:
             "GB_s": (32 * passes + 8) * n / best / 1e9}     # passes + one histogram read of the keys
 
 
+def generation_rate(n: int, dmin_bits: int = 40, reps: int = 3) -> dict:
+    """Residue generation on the k=64 r=5 instance of seed 0: the linear generator (the generate()
+    drop-in, canonical residues and 10-bit packed ids, I ranks [0, n)) and the bounded D producer
+    (every 5-subset of the 64-prime base with product >= 2^dmin_bits, ddump's order)."""
+    import torch
+    from . import mitm_gpu2, workloads as W
+    from .bounded import BoundedGenerator
+    from .solve import Instance
+    w = W.config2(0)
+    inst = Instance.build(w.M, w.Q, w.B0, w.r, w.B)
+    r, M = inst.r, inst.M
+    n = min(n, math.comb(len(inst.INS), r))
+
+    def timed(fn):
+        best, out = None, None
+        for _ in range(reps + 1):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            out = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) * 1e-3
+            best = t if best is None else min(best, t)
+        return best, out
+
+    t_lin, (keys, _ids) = timed(lambda: mitm_gpu2.generate(inst.INS, r, M, 1, 10, 0, n))
+    gen = BoundedGenerator()
+    t_bd, (_k, _i, nd) = timed(lambda: gen.generate_D(inst.B0, r, M, 1 << dmin_bits, bitmask=2))
+    return {"linear": {"records": n, "s": t_lin, "records_per_s": n / t_lin, "GB_s": 16 * n / t_lin / 1e9},
+            "bounded_D": {"records": nd, "dmin_bits": dmin_bits, "s": t_bd, "records_per_s": nd / t_bd,
+                          "of": math.comb(len(inst.B0), r)}}
+
+
 def main() -> None:
     import sys
     if len(sys.argv) > 2 and sys.argv[1] == "sort":
         print(json.dumps(sort_rate(int(sys.argv[2]))))
+        return
+    if len(sys.argv) > 2 and sys.argv[1] == "gen":
+        print(json.dumps(generation_rate(int(sys.argv[2]))))
         return
     out = {"l2_random_32B_reads_per_s": {mb: l2_random_reads(mb) for mb in (8, 32, 64)},
            "hbm_random_32B_reads_per_s": l2_random_reads(4096, iters=256),
