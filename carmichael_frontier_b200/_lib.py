@@ -144,7 +144,10 @@ def ptr(t) -> int | None:
 
 
 def stream_handle(stream=None) -> int | None:
-    """cudaStream_t of a torch stream (current stream when None)."""
+    """cudaStream_t of a torch stream (the current device's current stream when None, read
+    without building a torch Stream object: this runs once per library call)."""
     import torch
-    s = stream if stream is not None else torch.cuda.current_stream()
-    return s.cuda_stream
+    if stream is not None:
+        return stream.cuda_stream
+    torch.cuda._lazy_init()
+    return torch._C._cuda_getCurrentRawStream(torch._C._cuda_getDevice())

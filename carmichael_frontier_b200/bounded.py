@@ -45,9 +45,11 @@ def dmin_table(B, r: int, Dmin: int) -> list[int]:
     """G[t*n + x] = ceil(Dmin / (b_x b_{x-1} ... b_{x-t})) for x >= t (unused otherwise), 0 <= t < r."""
     n = len(B)
     G = [U128 - 1] * (r * n)
-    for t in range(r):
+    for t in range(min(r, n)):
+        w = math.prod(B[:t + 1])                 # window b_{x-t} ... b_x, slid one prime at a time
         for x in range(t, n):
-            w = math.prod(B[x - t:x + 1])
+            if x > t:
+                w = w // B[x - t - 1] * B[x]
             G[t * n + x] = -(-Dmin // w) if Dmin > 0 else 0
     return G
 
@@ -61,12 +63,13 @@ def _cat_u64(parts):
 
 
 def _u128_pairs(vals) -> np.ndarray:
-    a = np.zeros(2 * len(vals), dtype=np.uint64)
+    """(low, high) u64 words of each value, saturated at 2^128 - 1."""
     m = (1 << 64) - 1
-    for i, v in enumerate(vals):
-        v = min(int(v), U128 - 1)
-        a[2 * i] = v & m
-        a[2 * i + 1] = v >> 64
+    top = U128 - 1
+    vs = [v if v < top else top for v in map(int, vals)]
+    a = np.empty(2 * len(vs), dtype=np.uint64)
+    a[0::2] = [v & m for v in vs]
+    a[1::2] = [v >> 64 for v in vs]
     return a
 
 
@@ -82,7 +85,7 @@ class BoundedGenerator:
             raise RuntimeError("bounded generation runs on a CUDA device only")
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
-        self.tables = DeviceTables(self.device)
+        self.tables = DeviceTables(self.device, async_upload=True)   # kernels run on the current stream
         self.max_nodes = max_nodes
         self.launches = 0
 
@@ -106,8 +109,8 @@ class BoundedGenerator:
             limit = self.max_nodes
         torch, lib, dp = self.torch, self.lib, _lib.ptr
         dev = self.device
-        root = np.array([key_of(M, mult % M)], dtype=np.uint64).view(np.int64)    # key form of the multiplier
-        key = torch.from_numpy(root).to(dev)
+        root = key_of(M, mult % M)                                                # key form of the multiplier
+        key = torch.full((1,), root - (1 << 64) if root >> 63 else root, dtype=torch.int64, device=dev)
         alo = torch.ones(1, dtype=torch.int64, device=dev)
         ahi = torch.zeros(1, dtype=torch.int64, device=dev)
         ids = torch.zeros(1, dtype=torch.int64, device=dev)

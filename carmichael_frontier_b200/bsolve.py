@@ -126,6 +126,11 @@ class BoundedSolve:
         return self._finish(inst, pairs, nD, nI, plan, verify)
 
     def _join(self, inst, Icap, Dmin, split, hmax):
+        # the producers launch, fill and upload on the current stream: make it the solver's
+        with self.torch.cuda.stream(self.s._torch_stream()):
+            return self._join_on_stream(inst, Icap, Dmin, split, hmax)
+
+    def _join_on_stream(self, inst, Icap, Dmin, split, hmax):
         torch, lib, dp = self.torch, self.lib, _lib.ptr
         r, M = inst.r, inst.M
         plan = dict(strategy="bounded", Icap=Icap, Dmin=Dmin)

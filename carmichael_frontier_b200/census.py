@@ -228,7 +228,6 @@ def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: in
     def consider(key, fac, label):
         hits.append((key, tuple(fac), label))
         return user(key, fac, label) if user is not None else True
-    log = log or (lambda s: None)
     solver = solver or Solver(tuning=Tuning(strategy="bounded"))
     out = {}
     pools = _Pools([int(r["D"]) for r in rows if int(r["D"]) < 1 << 64], sieve_bound)

@@ -82,7 +82,8 @@ def run_instance(tag, B0, INS, r: int, hmax: int, M: int, U: int, split: int, co
                  state: dict | None = None, solver=None) -> bool:
     """One exchange instance below the bound U, as the driver's run_instance: returns True
     when the instance is complete.  consider(key, factors, label) receives every completion
-    below U (the driver's incumbent update and oracle); log(str) writes the instance line."""
+    below U (the driver's incumbent update and oracle); log(str) writes the instance line
+    (None: no line)."""
     from .solve import Solver, Tuning
     B0s = sorted(B0)
     B0set = set(B0)
@@ -90,7 +91,8 @@ def run_instance(tag, B0, INS, r: int, hmax: int, M: int, U: int, split: int, co
     Icap, Dmin, cap_r, INS_aff = instance_bounds(B0, INS, r, U)
     st = state if state is not None else {}
     if len(INS_aff) < r:
-        log(f"  {tag} r={r}: affordable pool has {len(INS_aff)} < r primes (cap_r={cap_r}); nothing to search")
+        if log is not None:
+            log(f"  {tag} r={r}: affordable pool has {len(INS_aff)} < r primes (cap_r={cap_r}); nothing to search")
         st["instances"] = st.get("instances", 0) + 1
         st["last"] = dict(r=r, hmax=hmax, ins=len(INS_aff), nD=0, nI=0, pairs=0, below_U=0)
         return True
@@ -122,6 +124,8 @@ def run_instance(tag, B0, INS, r: int, hmax: int, M: int, U: int, split: int, co
     st["last"] = dict(r=r, hmax=hmax, ins=len(INS_aff), nD=nD, nI=nI, pairs=len(pairs_idx), below_U=below)
     st["pairs_total"] = st.get("pairs_total", 0) + len(pairs_idx)
     st["completions_below_U"] = st.get("completions_below_U", 0) + below
+    if log is None:                        # no instance line wanted (family runs): skip the allocator query
+        return True
     gb = 0.0
     try:                                   # device memory held by this process's allocator (no driver query)
         import torch

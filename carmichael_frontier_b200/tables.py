@@ -50,6 +50,48 @@ def pool_table_host(primes, r: int, M: int, mult: int) -> np.ndarray:
     return out
 
 
+def _on_stream(stream):
+    """Context making `stream` current, or nothing when it already is (the common case)."""
+    import contextlib
+    import torch
+    if stream.cuda_stream == torch._C._cuda_getCurrentRawStream(stream.device_index):
+        return contextlib.nullcontext()
+    return torch.cuda.stream(stream)
+
+
+class _PinnedRing:
+    """Page-locked staging area for small uploads, allocated once.  A copy takes the next free
+    bytes; before the ring wraps, the streams of every copy issued from it since the last wrap
+    are synchronised, so no copy reads bytes that are being overwritten."""
+
+    def __init__(self, nbytes: int):
+        import torch
+        self.buf = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        self.view = self.buf.numpy()
+        self.off = 0
+        self.streams: dict = {}
+
+    def upload(self, host, dst, stream) -> bool:
+        """Copy host (numpy) into dst (device tensor of the same bytes) on stream without
+        waiting; False when host is larger than the ring."""
+        import torch
+        n = host.nbytes
+        if n > len(self.view):
+            return False
+        if self.off + n > len(self.view):
+            for st in self.streams.values():
+                st.synchronize()
+            self.streams.clear()
+            self.off = 0
+        a = self.off
+        self.view[a:a + n] = host.view(np.uint8).reshape(-1)
+        self.off = (a + n + 63) // 64 * 64
+        with _on_stream(stream):
+            dst.view(torch.uint8).reshape(-1).copy_(self.buf[a:a + n], non_blocking=True)
+        self.streams[stream.cuda_stream] = stream
+        return True
+
+
 class DeviceTables:
     """Content-keyed cache of device copies of small host tables.
 
@@ -59,26 +101,32 @@ class DeviceTables:
     stream (the single-modulus solver does).  Otherwise the copy returns when the data is on the
     device, which any stream may use."""
 
+    RING_BYTES = 4 << 20
+
     def __init__(self, device, max_entries: int = 64, stream=None, async_upload: bool = False):
         self.device = device
         self.max_entries = max_entries
         self.stream = stream
         self.async_upload = async_upload
+        self._ring = None
         self._cache: dict = {}
 
     def get(self, key, make):
         import torch
         t = self._cache.get(key)
         if t is None:
-            host = torch.from_numpy(make())
+            host = make()
             if self.async_upload:
                 s = self.stream if self.stream is not None else torch.cuda.current_stream(self.device)
-                host = host.pin_memory()
-                with torch.cuda.stream(s):
-                    t = torch.empty(host.shape, dtype=host.dtype, device=self.device)
-                    t.copy_(host, non_blocking=True)
+                with _on_stream(s):
+                    t = torch.empty(host.shape, dtype=torch.from_numpy(host[:0]).dtype, device=self.device)
+                if self._ring is None:
+                    self._ring = _PinnedRing(self.RING_BYTES)
+                if not self._ring.upload(host, t, s):
+                    with _on_stream(s):
+                        t.copy_(torch.from_numpy(host), non_blocking=False)
             else:
-                t = host.to(self.device, non_blocking=False)
+                t = torch.from_numpy(host).to(self.device, non_blocking=False)
             if len(self._cache) >= self.max_entries:
                 self._cache.pop(next(iter(self._cache)))
             self._cache[key] = t
@@ -96,7 +144,7 @@ class DeviceTables:
         if t is None:
             lib = _lib.load()
             nbytes = lib.cf_tail_bytes(len(primes), r)
-            with torch.cuda.stream(self.stream if self.stream is not None else torch.cuda.current_stream(self.device)):
+            with _on_stream(self.stream if self.stream is not None else torch.cuda.current_stream(self.device)):
                 t = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=self.device)
             _lib.check(lib.cf_build_tail(pool_dev.data_ptr(), len(primes), r, t.data_ptr(),
                                          _lib.stream_handle(self.stream)), "cf_build_tail")

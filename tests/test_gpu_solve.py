@@ -244,3 +244,25 @@ def test_modulus_limits(cuda):
         Instance.build(1 << 64, Q, Q[:10], 2, 10 ** 50)          # 2-adic part 2^64: above 2^32
     with pytest.raises(ValueError):
         Instance.build((1 << 63) + 1, [3, 5, 7], [3], 1, 10 ** 50)   # odd part of 2^63 or more
+
+
+def test_table_uploads_through_the_staging_ring(cuda):
+    # asynchronous uploads staged in a small page-locked ring that wraps many times arrive intact,
+    # and a table larger than the ring takes the synchronous path
+    import numpy as np
+    import torch
+    from carmichael_frontier_b200.tables import DeviceTables
+    dt = DeviceTables(cuda, max_entries=1000, async_upload=True)
+    dt.RING_BYTES = 4096
+    rng = np.random.default_rng(5)
+    want = {}
+    for i in range(200):
+        a = rng.integers(0, 256, size=int(rng.integers(1, 3000)), dtype=np.uint8)
+        want[i] = a
+        dt.get(("t", i), lambda a=a: a.copy())
+    big = rng.integers(0, 256, size=10000, dtype=np.uint8)
+    dt.get(("big",), lambda: big.copy())
+    torch.cuda.synchronize()
+    for i, a in want.items():
+        assert np.array_equal(dt.get(("t", i), None).cpu().numpy(), a)
+    assert np.array_equal(dt.get(("big",), None).cpu().numpy(), big)
