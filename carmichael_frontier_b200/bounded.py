@@ -92,11 +92,12 @@ class BoundedGenerator:
     # -- primitives -----------------------------------------------------------
     def _scan(self, cnt, F: int):
         torch = self.torch
-        offs = torch.empty(F + 1, dtype=torch.int64, device=self.device)
         nb = self.lib.cf_scan_tmp_bytes(F)
-        tmp = torch.empty(max(nb, 16), dtype=torch.uint8, device=self.device)
-        _lib.check(self.lib.cf_scan_u64(_lib.ptr(cnt), F, _lib.ptr(offs), _lib.ptr(tmp), nb, _lib.stream_handle()),
-                   "cf_scan_u64")
+        ob = (8 * (F + 1) + 255) // 256 * 256            # offsets, then the scan's scratch (one allocation)
+        buf = torch.empty(ob + max(nb, 16), dtype=torch.uint8, device=self.device)
+        offs = buf[:8 * (F + 1)].view(torch.int64)
+        _lib.check(self.lib.cf_scan_u64(_lib.ptr(cnt), F, _lib.ptr(offs), buf.data_ptr() + ob, nb,
+                                        _lib.stream_handle()), "cf_scan_u64")
         self.launches += 2
         return offs
 
@@ -109,17 +110,17 @@ class BoundedGenerator:
             limit = self.max_nodes
         torch, lib, dp = self.torch, self.lib, _lib.ptr
         dev = self.device
-        root = key_of(M, mult % M)                                                # key form of the multiplier
-        key = torch.full((1,), root - (1 << 64) if root >> 63 else root, dtype=torch.int64, device=dev)
-        alo = torch.ones(1, dtype=torch.int64, device=dev)
-        ahi = torch.zeros(1, dtype=torch.int64, device=dev)
-        ids = torch.zeros(1, dtype=torch.int64, device=dev)
-        meta = torch.full((1,), 0xFFFF, dtype=torch.int32, device=dev)
+        # the root node, read-only: key form of the multiplier, product 1, id 0, meta 0xFFFF
+        rt = self.tables.get(("root", M, mult % M), lambda: np.array(
+            [key_of(M, mult % M), 1, 0, 0, 0xFFFF], dtype=np.uint64).view(np.uint8)).view(torch.int64)
+        key, alo, ahi, ids = rt[0:1], rt[1:2], rt[2:3], rt[3:4]
+        meta = rt[4:5].view(torch.int32)[:1]
         F = 1
         sh = _lib.stream_handle()
         for d in range(r):
-            cnt = torch.empty(F, dtype=torch.int64, device=dev)
-            xs = torch.empty(F, dtype=torch.int32, device=dev)
+            cx = torch.empty(F + (F + 1) // 2, dtype=torch.int64, device=dev)   # counts, then first indices
+            cnt = cx[:F]
+            xs = cx[F:].view(torch.int32)[:F]
             _lib.check(lib.cf_bgen_count(side, d, r, n, F, dp(alo), dp(ahi), dp(meta), dp(bounds), split_idx, hmax,
                                          xa, xb, dp(cnt), dp(xs), sh), "cf_bgen_count")
             self.launches += 1
@@ -131,11 +132,9 @@ class BoundedGenerator:
                 return dict(F=0, total=0)
             if limit is not None and total > limit:
                 return None
-            nkey = torch.empty(total, dtype=torch.int64, device=dev)
-            nalo = torch.empty(total, dtype=torch.int64, device=dev)
-            nahi = torch.empty(total, dtype=torch.int64, device=dev)
-            nids = torch.empty(total, dtype=torch.int64, device=dev)
-            nmeta = torch.empty(total, dtype=torch.int32, device=dev)
+            lv = torch.empty(4 * total + (total + 1) // 2, dtype=torch.int64, device=dev)  # one level's nodes
+            nkey, nalo, nahi, nids = (lv[j * total:(j + 1) * total] for j in range(4))
+            nmeta = lv[4 * total:].view(torch.int32)[:total]
             _lib.check(lib.cf_bgen_expand(side, d, r, n, F, dp(pool), dp(key), dp(alo), dp(ahi), dp(ids), dp(meta),
                                           dp(offs), dp(xs), split_idx, bitmask, 0, total, dp(nkey), dp(nalo),
                                           dp(nahi), dp(nids), dp(nmeta), sh), "cf_bgen_expand")
@@ -168,8 +167,8 @@ class BoundedGenerator:
             c0 = 0
             while c0 < total:
                 cc = min(max_records, total - c0)
-                keys = torch.empty(cc, dtype=torch.uint64, device=self.device)
-                ids = torch.empty(cc, dtype=torch.uint64, device=self.device)
+                rec = torch.empty(2 * cc, dtype=torch.uint64, device=self.device)
+                keys, ids = rec[:cc], rec[cc:]
                 _lib.check(lib.cf_bgen_expand(side, r - 1, r, n, fr["F"], dp(pool), dp(fr["key"]), dp(fr["alo"]),
                                               dp(fr["ahi"]), dp(fr["ids"]), dp(fr["meta"]), dp(fr["offs"]),
                                               dp(fr["xs"]), split_idx, bitmask, c0, cc, dp(keys), None, None,
