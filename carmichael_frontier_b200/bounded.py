@@ -12,6 +12,10 @@ The kernels (csrc/cf_bgen.cu) expand the enumeration tree one level at a time; t
 exact bound tables that make every level one contiguous child range per node are
 built here with Python integers, like the reference's quotient table
 (gpu/igen_gpu.py:92-101).
+
+Keys are canonical residues below M for M < 2^64.  For M >= 2^64 (odd part below 2^63,
+2-adic part at most 2^32) a key is the packed residue (x * 2^64 mod m) << a | x mod 2^a
+taken mod 2^64: equal residues give equal keys, and callers confirm key matches exactly.
 """
 from __future__ import annotations
 
@@ -52,6 +56,21 @@ def dmin_table(B, r: int, Dmin: int) -> list[int]:
                 w = w // B[x - t - 1] * B[x]
             G[t * n + x] = -(-Dmin // w) if Dmin > 0 else 0
     return G
+
+
+def _modulus_ok(M: int) -> bool:
+    """M >= 2 with an odd part below 2^63, and a 2-adic part of at most 2^32 when M >= 2^64."""
+    a = (M & -M).bit_length() - 1
+    return M >= 2 and (M >> a) < 1 << 63 and (M < 1 << 64 or a <= 32)
+
+
+def _root_key(M: int, mult: int) -> int:
+    """Key of the root node: key form of mult mod M, or for M >= 2^64 (whose node keys hold the odd
+    part alone) mult * 2^64 mod m, m the odd part of M."""
+    if M < 1 << 64:
+        return key_of(M, mult % M)
+    m = M >> ((M & -M).bit_length() - 1)
+    return (mult % m) * (1 << 64) % m
 
 
 def _cat_u64(parts):
@@ -112,7 +131,7 @@ class BoundedGenerator:
         dev = self.device
         # the root node, read-only: key form of the multiplier, product 1, id 0, meta 0xFFFF
         rt = self.tables.get(("root", M, mult % M), lambda: np.array(
-            [key_of(M, mult % M), 1, 0, 0, 0xFFFF], dtype=np.uint64).view(np.uint8)).view(torch.int64)
+            [_root_key(M, mult), 1, 0, 0, 0xFFFF], dtype=np.uint64).view(np.uint8)).view(torch.int64)
         key, alo, ahi, ids = rt[0:1], rt[1:2], rt[2:3], rt[3:4]
         meta = rt[4:5].view(torch.int32)[:1]
         F = 1
@@ -181,7 +200,7 @@ class BoundedGenerator:
     def _setup_I(self, INS, r, M, P0, Icap, split, hmax):
         INS = [int(p) for p in INS]
         n = len(INS)
-        assert 1 <= r <= 16 and n <= 1024 and 2 <= M < (1 << 64)
+        assert 1 <= r <= 16 and n <= 1024 and _modulus_ok(M)
         assert all(INS[i] < INS[i + 1] for i in range(n - 1)), "INS must be strictly ascending"
         assert Icap - 1 < U128, "Icap needs more than 128 bits"
         if Icap <= 1 or n < r:
@@ -226,7 +245,7 @@ class BoundedGenerator:
         mode = int(bitmask)
         if mode == 0 and r > 10:
             mode = 1
-        assert mode in (0, 1, 2) and 1 <= r <= 16 and 2 <= M < (1 << 64)
+        assert mode in (0, 1, 2) and 1 <= r <= 16 and _modulus_ok(M)
         assert n <= (1024 if mode == 2 else 64), "packed and mask ids need a base of at most 64 primes"
         assert all(B[i] < B[i + 1] for i in range(n - 1)), "the base must be strictly ascending"
         if mode == 2:

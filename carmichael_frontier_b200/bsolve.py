@@ -26,7 +26,7 @@ import numpy as np
 from . import _lib
 from .bounded import U128
 from .certify import verify_certificate
-from .tables import unrank_colex
+from .tables import unrank_colex, wide_modulus
 
 RANK_LIMIT = 1 << 32          # positions in the join table are 32-bit
 
@@ -43,9 +43,8 @@ def caps(inst) -> tuple[int, int]:
 
 
 def applicable(inst) -> bool:
-    """The bounded producers need 128-bit products, r >= 1, both sides non-empty and M < 2^64 (they
-    carry packed keys from level to level, exact only while the key is the whole residue)."""
-    if inst.r < 1 or len(inst.B0) < inst.r or len(inst.INS) < inst.r or inst.M >= 1 << 64:
+    """The bounded producers need 128-bit products (and r >= 1, both sides non-empty)."""
+    if inst.r < 1 or len(inst.B0) < inst.r or len(inst.INS) < inst.r:
         return False
     Icap, Dmin = caps(inst)
     return Icap - 1 < U128 and math.prod(inst.B0[-inst.r:]) < U128 and math.comb(len(inst.INS), inst.r) < 1 << 64 \
@@ -68,6 +67,7 @@ class BoundedSolve:
     Otherwise the I leaves are written and the table is built on them."""
 
     LEAF_CHUNK = 1 << 30          # I leaves per probe launch
+    WIDE_LEAF_CHUNK = 1 << 26     # I leaves written per chunk for M >= 2^64 (16 bytes each)
 
     def __init__(self, solver):
         from .bounded import BoundedGenerator
@@ -172,15 +172,32 @@ class BoundedSolve:
             plan["table"] = "D"
             tab, bb, fb = self._table(Dk, nD, plan)
             chain = [first] + ([second] if second is not None else [])
+            wide = wide_modulus(M)
+            chunk = self.WIDE_LEAF_CHUNK if wide else self.LEAF_CHUNK
             for fr in _chain(chain, blocks):
                 total = fr["total"]
                 nI += total
-                for c0 in range(0, total, self.LEAF_CHUNK):
-                    cc = min(self.LEAF_CHUNK, total - c0)
-                    pv, maxp = self._probe(lambda pairs, mp, fr=fr, c0=c0, cc=cc: _lib.check(
-                        lib.cf_bgen_probe(r, len(inst.INS), fr["F"], dp(poolI), dp(fr["key"]), dp(fr["ids"]),
-                                          dp(fr["offs"]), dp(fr["xs"]), c0, cc, dp(tab), bb, fb, dp(pairs), mp,
-                                          dp(self.misc), dp(self.misc) + 4, sh), "cf_bgen_probe"), maxp)
+                for c0 in range(0, total, chunk):
+                    cc = min(chunk, total - c0)
+                    if wide:
+                        # the fused leaf probe hashes canonical residues: write the leaves, then probe
+                        lb = self.s._buf("bleaf", 16 * cc)
+                        Ik, Iid = lb[:8 * cc].view(torch.int64), lb[8 * cc:16 * cc].view(torch.int64)
+                        _lib.check(lib.cf_bgen_expand(0, r - 1, r, len(inst.INS), fr["F"], dp(poolI), dp(fr["key"]),
+                                                      dp(fr["alo"]), dp(fr["ahi"]), dp(fr["ids"]), dp(fr["meta"]),
+                                                      dp(fr["offs"]), dp(fr["xs"]), len(inst.INS), 0, c0, cc,
+                                                      dp(Ik), None, None, dp(Iid), None, sh), "cf_bgen_expand(records)")
+                        pv, maxp = self._probe(lambda pairs, mp, Ik=Ik, cc=cc: _lib.check(
+                            lib.cf_rec_probe(dp(Ik), cc, dp(tab), bb, fb, 0, dp(pairs), mp, dp(self.misc),
+                                             dp(self.misc) + 4, sh), "cf_rec_probe"), maxp)
+                        if pv is not None:
+                            iid = Iid[torch.from_numpy(pv[:, 1].astype(np.int64)).to(self.s.device)]
+                            pv[:, 1] = iid.cpu().numpy().view(np.uint64)
+                    else:
+                        pv, maxp = self._probe(lambda pairs, mp, fr=fr, c0=c0, cc=cc: _lib.check(
+                            lib.cf_bgen_probe(r, len(inst.INS), fr["F"], dp(poolI), dp(fr["key"]), dp(fr["ids"]),
+                                              dp(fr["offs"]), dp(fr["xs"]), c0, cc, dp(tab), bb, fb, dp(pairs), mp,
+                                              dp(self.misc), dp(self.misc) + 4, sh), "cf_bgen_probe"), maxp)
                     if pv is not None:
                         cands.append(pv)
         pairs = []
@@ -190,11 +207,16 @@ class BoundedSolve:
             dk = Dk.view(torch.int64)[dpos].cpu().numpy().view(np.uint64)
             di = Did.view(torch.int64)[dpos].cpu().numpy().view(np.uint64)
             P0m = inst.P0 % M
+            wide = wide_modulus(M)             # keys taken mod 2^64: compare the residues themselves
             for j in range(len(pv)):
                 ii = unrank_colex(int(pv[j, 1]), r, len(inst.INS))
-                if (P0m * math.prod(inst.INS[x] for x in ii)) % M != int(dk[j]):
+                dd = unrank_colex(int(di[j]), r, len(inst.B0))
+                if wide:
+                    if (inst.P0 * math.prod(inst.INS[x] for x in ii) - math.prod(inst.B0[x] for x in dd)) % M:
+                        continue
+                elif (P0m * math.prod(inst.INS[x] for x in ii)) % M != int(dk[j]):
                     continue                   # fingerprint collision, not an equal-residue pair
-                pairs.append((unrank_colex(int(di[j]), r, len(inst.B0)), ii))
+                pairs.append((dd, ii))
         return pairs, nD, nI, plan
 
     def _finish(self, inst, pairs, nD, nI, plan, verify):

@@ -164,14 +164,15 @@ def family_instances(rows, U: int, r_min: int = 1, r_max: int | None = None, k: 
                      sieve_bound: int = SIEVE_BOUND, with_base: bool = True):
     """(row, radius, Instance) for every survivor row: radius 0 (the k smallest primes themselves, when
     with_base) and radii r_min..min(rmax, r_max), each over the full capped pool with bound n < U -- the
-    per-family runs of gpu/run_mstar_family.py:66-94, here as one portfolio.  Rows whose modulus is 2^64
-    or more are skipped (keys are u64 residues), as the reference marks them unsupported."""
+    per-family runs of gpu/run_mstar_family.py:66-94, here as one portfolio.  Rows whose modulus has an
+    odd part of 2^63 or more, or a 2-adic part above 2^32, are skipped (the reference skips every
+    modulus of 2^64 or more)."""
     from .solve import Instance
     out = []
-    pools = _Pools([int(r["D"]) for r in rows if int(r["D"]) < 1 << 64], sieve_bound)
+    pools = _Pools([int(r["D"]) for r in rows if _searchable(int(r["D"]))], sieve_bound)
     for row in rows:
         D, cap, rmax = int(row["D"]), int(row["cap"]), int(row["rmax"])
-        if D >= 1 << 64:
+        if not _searchable(D):
             continue
         P = pools(D)
         Pc = [q for q in P if q <= cap]
@@ -183,6 +184,13 @@ def family_instances(rows, U: int, r_min: int = 1, r_max: int | None = None, k: 
         for r in radii:
             out.append((row, r, Instance.build(D, Pc, base, r, U - 1)))
     return out
+
+
+def _searchable(D: int) -> bool:
+    """Moduli the joins take: odd part below 2^63 and 2-adic part at most 2^32 (D may be 2^64 or
+    more: keys are then taken mod 2^64 and matches confirmed exactly)."""
+    a = (D & -D).bit_length() - 1
+    return D >= 2 and (D >> a) < 1 << 63 and a <= 32
 
 
 def _top_index(D: int) -> int:
@@ -230,11 +238,11 @@ def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: in
         return user(key, fac, label) if user is not None else True
     solver = solver or Solver(tuning=Tuning(strategy="bounded"))
     out = {}
-    pools = _Pools([int(r["D"]) for r in rows if int(r["D"]) < 1 << 64], sieve_bound)
+    pools = _Pools([int(r["D"]) for r in rows if _searchable(int(r["D"]))], sieve_bound)
     for row in rows:
         D, cap, rmax = int(row["D"]), int(row["cap"]), int(row["rmax"])
-        if D >= 1 << 64:
-            out[D] = {"unsupported": "modulus of 2^64 or more (u64 residue keys)"}
+        if not _searchable(D):
+            out[D] = {"unsupported": "odd part of 2^63 or more, or 2-adic part above 2^32"}
             continue
         P = pools(D)
         Pc = [q for q in P if q <= cap]

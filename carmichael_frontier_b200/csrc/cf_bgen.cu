@@ -131,7 +131,12 @@ k_bgen_expand(int d, int r, int n, u64 F, const u64* __restrict__ pool, const u6
   const int x = SIDE == 0 ? (int)(xs[p] + j) : (int)(xs[p] - j);
   const CfPoolHdr* hd = (const CfPoolHdr*)pool;
   const CfMod md = cf_mod_from_hdr(hd);
-  const u64 kk = cf_mul_key(key[p], pool[cf_pool_off_pkey(n) + x], md);
+  const u64 prime = pool[cf_pool_off_prime(n) + x];
+  // M of 2^64 or more (header M = 0, cf_pool_prepare_split): a node key is the odd part alone in
+  // Montgomery form (x * 2^64 mod m); x mod 2^a follows from the node's exact product A.
+  const bool wide = hd->M == 0;
+  const u64 kk = wide ? cf_redc_mul(key[p], cf_redc_mul(prime, hd->r2, md.m, md.minv), md.m, md.minv)
+                      : cf_mul_key(key[p], pool[cf_pool_off_pkey(n) + x], md);
   u64 nid;
   if (SIDE == 0) {
     nid = id[p] + pool[cf_pool_off_binom(n) + (size_t)x * (r + 1) + (d + 1)];   // colex: + C(x, d+1)
@@ -141,13 +146,15 @@ k_bgen_expand(int d, int r, int n, u64 F, const u64* __restrict__ pool, const u6
     nid = bitmask ? (id[p] | (1ull << x)) : (id[p] | ((u64)x << (6 * (r - 1 - d))));
   }
   if (LEAF) {
-    okey[k] = cf_key_to_canon(kk, md, hd->inv2a, hd->inv2aR);
+    // wide: the packed residue (x mod m in Montgomery form) << a | x mod 2^a, taken mod 2^64
+    okey[k] = wide ? (kk << md.a) | ((hd->x20 * (alo[p] * prime)) & md.mask2)
+                   : cf_key_to_canon(kk, md, hd->inv2a, hd->inv2aR);
     oid[k] = nid;
   } else {
     U128 A;
     A.lo = alo[p];
     A.hi = ahi[p];
-    const U128 A2 = u128_mul64(A, pool[cf_pool_off_prime(n) + x]);
+    const U128 A2 = u128_mul64(A, prime);
     const u32 mt = meta[p];
     const u32 nl = (mt >> 16) + (SIDE == 0 && x >= split_idx ? 1u : 0u);
     okey[k] = kk;
@@ -269,7 +276,9 @@ extern "C" int cf_bgen_count(int side, int d, int r, int n, u64 F, const u64* al
 // Write the children [c0, c0+cc) of the depth-d frontier (offs = cf_scan_u64 of
 // the counts).  d < r-1: child nodes (okey, oalo, oahi, oid, ometa); d = r-1:
 // records (okey = canonical residue, oid = id).  pool: the side's pool table
-// (cf_pool_prepare with mult = P0 for the I side, 1 for the D side).
+// (cf_pool_prepare with mult = P0 for the I side, 1 for the D side).  A pool of
+// cf_pool_prepare_split for M >= 2^64: node keys hold the odd part in Montgomery
+// form and records the packed residue taken mod 2^64.
 extern "C" int cf_bgen_expand(int side, int d, int r, int n, u64 F, const void* pool, const u64* key, const u64* alo,
                               const u64* ahi, const u64* id, const u32* meta, const u64* offs, const u32* xs,
                               int split_idx, int bitmask, u64 c0, u64 cc, u64* okey, u64* oalo, u64* oahi, u64* oid,

@@ -211,6 +211,42 @@ def test_wide_modulus_keys_are_the_residue_keys(cuda, M):
         assert lin == want and walk == want, r
 
 
+@pytest.mark.parametrize("M", WIDE_MODULI)
+def test_wide_modulus_bounded_records(cuda, M):
+    # the bounded producers on moduli of 2^64 and more: the D and I records are the subsets within
+    # the product bounds, each keyed by the packed residue (x 2^64 mod m) << a | x mod 2^a, mod 2^64
+    import itertools
+    from carmichael_frontier_b200.bounded import BoundedGenerator
+    from carmichael_frontier_b200.tables import unrank_colex
+    a = (M & -M).bit_length() - 1
+    m = M >> a
+
+    def packed(v):
+        return ((((v % m) << 64) % m) << a | (v & ((1 << a) - 1))) & ((1 << 64) - 1)
+
+    Q = W.eligible_pool(M, 5518)
+    B0, INS, r = Q[:24], Q[24:60], 3
+    P0 = math.prod(B0)
+    gen = BoundedGenerator(cuda)
+    dprods = sorted(math.prod(c) for c in itertools.combinations(B0, r))
+    Dmin = dprods[len(dprods) // 2]
+    k, i, nd = gen.generate_D(B0, r, M, Dmin, bitmask=2)
+    got = dict(zip(i.cpu().numpy().tolist(), k.cpu().numpy().tolist()))
+    assert nd == len(got) == sum(1 for v in dprods if v >= Dmin)
+    for cid, key in got.items():
+        v = math.prod(B0[x] for x in unrank_colex(cid, r, len(B0)))
+        assert v >= Dmin and key == packed(v)
+    iprods = sorted(math.prod(c) for c in itertools.combinations(INS, r))
+    Icap = iprods[len(iprods) // 2]
+    recs = {}
+    for kk, ii in gen.generate_I(INS, r, M, P0, Icap):
+        recs.update(zip(ii.cpu().numpy().tolist(), kk.cpu().numpy().tolist()))
+    assert len(recs) == sum(1 for v in iprods if v < Icap)
+    for cid, key in recs.items():
+        v = math.prod(INS[x] for x in unrank_colex(cid, r, len(INS)))
+        assert v < Icap and key == packed(P0 * v)
+
+
 @pytest.mark.parametrize("M", WIDE_MODULI[:2])
 def test_wide_modulus_solves(cuda, M):
     # every strategy and the batched portfolio run on moduli of 2^64 and more and agree with the
@@ -223,17 +259,19 @@ def test_wide_modulus_solves(cuda, M):
     for k, extra, r in ((20, 25, 2), (18, 22, 3)):
         B0 = Q[:k]
         insts.append(Instance.build(M, Q[:k + extra], B0, r, W.product(B0) * 10 ** 12))
-    assert not any(bsolve.applicable(x) for x in insts)     # bounded producers: M < 2^64 only
+    assert all(bsolve.applicable(x) for x in insts)
     want = []
     for x in insts:
         pairs, hits = O.solve_exhaustive(x.M, x.B0 + x.INS, x.B0, x.r, x.B)
         want.append((as_lists(pairs), [(tuple(D), tuple(I), n) for D, I, n in hits]))
-    for st in ("fused", "partition", "auto"):
+    for st in ("fused", "partition", "bounded", "auto"):
         s = Solver(cuda, tuning=Tuning(strategy=st))
         for x, (pairs, hits) in zip(insts, want):
             got = s.solve_instance(x)
-            assert as_lists(got.pairs) == pairs and [(h.D, h.I, h.n) for h in got.hits] == hits, st
-            assert got.n_D == math.comb(len(x.B0), x.r) and got.n_I == math.comb(len(x.INS), x.r)
+            assert [(h.D, h.I, h.n) for h in got.hits] == hits, st
+            if st in ("fused", "partition"):
+                assert as_lists(got.pairs) == pairs, st
+                assert got.n_D == math.comb(len(x.B0), x.r) and got.n_I == math.comb(len(x.INS), x.r)
     for x, got, (pairs, hits) in zip(insts, BatchSolver(cuda).solve(insts), want):
         assert as_lists(got.pairs) == pairs and [(h.D, h.I, h.n) for h in got.hits] == hits
 

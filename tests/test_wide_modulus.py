@@ -65,7 +65,7 @@ def test_instance_limits():
     M = WIDE[0]
     Q = W.eligible_pool(M, 5518)
     x = Instance.build(M, Q[:40], Q[:20], 2, 10 ** 90)
-    assert x.M == M and tables.wide_modulus(M) and not bsolve.applicable(x)
+    assert x.M == M and tables.wide_modulus(M) and bsolve.applicable(x)
     with pytest.raises(ValueError):
         Instance.build(((1 << 63) + 1) << 4, [3, 5, 7], [3], 1, 10 ** 50)   # odd part of 2^63 or more
     with pytest.raises(ValueError):
