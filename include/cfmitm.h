@@ -213,7 +213,10 @@ int cf_check_pairs(const void* poolD, const void* poolI, const void* screen, int
  * cf_bgen_count writes each node's child count and first child index;
  * cf_scan_u64 turns counts into offsets (offs[F] = total); cf_bgen_expand writes
  * children [c0, c0+cc): nodes for d < r-1, records {canonical key, id} for
- * d = r-1.  First indices can be restricted to [xa, xb) at depth 0. */
+ * d = r-1.  First indices can be restricted to [xa, xb) at depth 0.  With a
+ * cf_pool_prepare_split pool of M >= 2^64, node keys hold x * 2^64 mod m (the root
+ * key: mult * 2^64 mod m) and record keys the packed residue
+ * (x * 2^64 mod m) << a | x mod 2^a taken mod 2^64; callers confirm matches exactly. */
 size_t cf_scan_tmp_bytes(uint64_t n);
 int cf_scan_u64(const uint64_t* in, uint64_t n, uint64_t* out, void* tmp, size_t tmp_bytes, void* stream);
 int cf_bgen_count(int side, int d, int r, int n, uint64_t F, const uint64_t* alo, const uint64_t* ahi,
@@ -240,7 +243,9 @@ int cf_rec_probe(const uint64_t* keys, uint64_t n, const void* tab, int bbits, i
  * node arrays, offsets and first child indices of cf_bgen_count / cf_scan_u64)
  * are computed in registers and probed, never written; candidates are
  * {D position, I colex id}.  Replaces the igen chunks x sorted D chunks join of
- * gpu/mitm_gpu_mstar_driver.py:241-262 when the I side is the large one. */
+ * gpu/mitm_gpu_mstar_driver.py:241-262 when the I side is the large one.  It hashes
+ * canonical residues: pools of M < 2^64 only (write the leaves with cf_bgen_expand and
+ * probe them with cf_rec_probe otherwise). */
 int cf_bgen_probe(int r, int n, uint64_t F, const void* pool, const uint64_t* key, const uint64_t* id,
                   const uint64_t* offs, const uint32_t* xs, uint64_t c0, uint64_t cc, const void* tab, int bbits,
                   int fbits, void* pairs, uint32_t max_pairs, uint32_t* npairs, uint32_t* err, void* stream);
