@@ -33,3 +33,29 @@ def test_family_run_matches_reference_records(cuda):
         assert got["instances"] == want, row["D"]
         n += len(want)
     assert n > 500
+
+
+def test_family_run_on_a_modulus_above_2_64(cuda):
+    # a census row of 2^64 or more (the reference marks these unsupported) runs through the driver's
+    # bounds and the bounded join; each instance's D and I record counts equal the subsets within the
+    # bounds, counted here with Python integers
+    import itertools
+    import math
+    from carmichael_frontier_b200 import driver, workloads as W
+    M = 36802111876251321600                       # 2^8 * an odd part of 57 bits: 65 bits
+    assert M >= 1 << 64
+    Q = W.eligible_pool(M, 5518)
+    base, INS = Q[:64], Q[64:]
+    U = math.prod(base) * 10
+    out, completions = C.family_run([{"D": M, "cap": 5518, "rmax": 2}], U, r_max=2,
+                                    solver=Solver(cuda, tuning=Tuning(strategy="bounded")))
+    rec = out[M]
+    assert completions == [] and rec["skipped"] == [] and len(rec["instances"]) >= 1
+    for x in rec["instances"]:
+        r, h = x["r"], x["hmax"]
+        Icap, Dmin, _cap_r, aff = driver.instance_bounds(base, INS, r, U)
+        nD = sum(1 for c in itertools.combinations(base, r) if math.prod(c) >= Dmin)
+        nI = sum(1 for c in itertools.combinations(aff, r)
+                 if math.prod(c) < Icap and sum(p > 4000 for p in c) <= h)
+        assert (x["nD"], x["nI"]) == (nD, nI), r
+        assert 0 < nD < math.comb(len(base), r) or 0 < nI < math.comb(len(aff), r)
