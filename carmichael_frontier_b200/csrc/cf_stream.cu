@@ -24,8 +24,10 @@ constexpr int kPartTile = 8192;          // records per CTA tile (16 per thread)
 
 __device__ __forceinline__ u32 range_part(u64 key, u64 M, int pbits) {
   // floor(key * 2^pbits / M) for key < M: the quotient is below 2^pbits, found by a
-  // binary search on q * M <= key * 2^pbits with both sides as 128-bit (hi, lo)
+  // binary search on q * M <= key * 2^pbits with both sides as 128-bit (hi, lo).
+  // M = 0 stands for 2^64 (keys of a modulus of 2^64 or more, taken mod 2^64).
   const u64 rh = key >> (64 - pbits), rl = key << pbits;
+  if (M == 0) return (u32)rh;
   u32 a = 0, z = (1u << pbits) - 1;
   while (a < z) {
     const u32 mid = (a + z + 1) >> 1;
@@ -104,7 +106,7 @@ unsigned grid_of(u64 n, u64 per) {
 // counts[p] += number of keys[0..n) in residue range p = floor(key * 2^pbits / M)
 // (counts zeroed by the caller; 1 <= pbits <= 12, keys canonical, < M).
 extern "C" int cf_part_hist(const u64* keys, u64 n, u64 M, int pbits, u64* counts, void* stream) {
-  if (!counts || (n && !keys) || pbits < 1 || pbits > 12 || M < 2) {
+  if (!counts || (n && !keys) || pbits < 1 || pbits > 12 || M == 1) {
     cf_set_error("cf_part_hist: bad arguments%s", "");
     return CF_EBADARG;
   }
@@ -120,7 +122,7 @@ extern "C" int cf_part_hist(const u64* keys, u64 n, u64 M, int pbits, u64* count
 // the caller sizes each partition by cf_part_hist).
 extern "C" int cf_part_scatter(const u64* keys, const u64* ids, u64 n, u64 M, int pbits, u64* cursor, u64* okeys,
                                u64* oids, void* stream) {
-  if (!cursor || (n && (!keys || !ids || !okeys || !oids)) || pbits < 1 || pbits > 12 || M < 2) {
+  if (!cursor || (n && (!keys || !ids || !okeys || !oids)) || pbits < 1 || pbits > 12 || M == 1) {
     cf_set_error("cf_part_scatter: bad arguments%s", "");
     return CF_EBADARG;
   }

@@ -88,9 +88,9 @@ class StreamedJoin:
         self.d2h_bytes = 0
 
     # -- spill ---------------------------------------------------------------------
-    def _gen(self, pool, n, r, lo, cnt, keys, ids, sh):
-        _lib.check(self.lib.cf_gen_subsets(_lib.ptr(pool), n, r, lo, cnt, 1, 0, 1, _lib.ptr(keys), _lib.ptr(ids), sh),
-                   "cf_gen_subsets")
+    def _gen(self, pool, n, r, lo, cnt, keys, ids, sh, canon: int = 1):
+        _lib.check(self.lib.cf_gen_subsets(_lib.ptr(pool), n, r, lo, cnt, 1, 0, canon, _lib.ptr(keys), _lib.ptr(ids),
+                                           sh), "cf_gen_subsets")
         self.launches += 1
 
     def host_buffers(self, n: int):
@@ -111,6 +111,8 @@ class StreamedJoin:
         N = total - lo
         P = 1 << self.pbits
         pool = self.tables.pool(primes, r, M, mult)
+        # M >= 2^64: packed residue keys taken mod 2^64, partitioned as if M were 2^64 (argument 0)
+        canon, Mp = (0, 0) if M >= 1 << 64 else (1, M)
         dev = self.device
         sh = _lib.stream_handle()
         cap = min(self.chunk, max(N, 1))
@@ -120,8 +122,8 @@ class StreamedJoin:
         counts = torch.zeros(P, dtype=torch.int64, device=dev)
         for c0 in range(lo, total, cap):
             cnt = min(cap, total - c0)
-            self._gen(pool, n, r, c0, cnt, gk, gi, sh)
-            _lib.check(lib.cf_part_hist(dp(gk), cnt, M, self.pbits, dp(counts), sh), "cf_part_hist")
+            self._gen(pool, n, r, c0, cnt, gk, gi, sh, canon)
+            _lib.check(lib.cf_part_hist(dp(gk), cnt, Mp, self.pbits, dp(counts), sh), "cf_part_hist")
             self.launches += 1
         cnts = counts.cpu().numpy()
         off = np.zeros(P + 1, dtype=np.int64)
@@ -144,14 +146,14 @@ class StreamedJoin:
         for k, c0 in enumerate(range(lo, total, cap)):
             cnt = min(cap, total - c0)
             sk, si = stage[k & 1]
-            self._gen(pool, n, r, c0, cnt, gk, gi, sh)
+            self._gen(pool, n, r, c0, cnt, gk, gi, sh, canon)
             pc = torch.zeros(P, dtype=torch.int64, device=dev)
-            _lib.check(lib.cf_part_hist(dp(gk), cnt, M, self.pbits, dp(pc), sh), "cf_part_hist")
+            _lib.check(lib.cf_part_hist(dp(gk), cnt, Mp, self.pbits, dp(pc), sh), "cf_part_hist")
             loc = torch.zeros(P + 1, dtype=torch.int64, device=dev)
             loc[1:] = torch.cumsum(pc, 0)
             cursor = loc[:-1].clone()
             comp.wait_event(free[k & 1])                            # this staging set was copied out
-            _lib.check(lib.cf_part_scatter(dp(gk), dp(gi), cnt, M, self.pbits, dp(cursor), dp(sk), dp(si), sh),
+            _lib.check(lib.cf_part_scatter(dp(gk), dp(gi), cnt, Mp, self.pbits, dp(cursor), dp(sk), dp(si), sh),
                        "cf_part_scatter")
             self.launches += 2
             ready = torch.cuda.Event()
@@ -277,8 +279,6 @@ def streamed_solve(inst, pbits: int = 8, i_limit: int | None = None, device=None
     join only I ranks [0, i_limit).  Returns (SolveResult, stats)."""
     from .solve import Hit, SolveResult
     import time
-    if inst.M >= 1 << 64:
-        raise ValueError("the streamed join partitions canonical u64 residues: M must be below 2^64")
     sj = StreamedJoin(device, pbits, chunk, piece)
     r, M = inst.r, inst.M
     nD = ncomb(len(inst.B0), r)
@@ -298,6 +298,8 @@ def streamed_solve(inst, pbits: int = 8, i_limit: int | None = None, device=None
     for dpos, ipos in cand:
         D_ = tuple(inst.B0[x] for x in unrank_lex(int(dids[int(dpos)]), len(inst.B0), r))
         I_ = tuple(inst.INS[x] for x in unrank_lex(int(iids[int(ipos)]), len(inst.INS), r))
+        if M >= 1 << 64 and (inst.P0 * math.prod(I_) - math.prod(D_)) % M:
+            continue                      # keys equal mod 2^64, residues differ
         pairs.append((D_, I_))
         dset = set(D_)
         fac = tuple(sorted([p for p in inst.B0 if p not in dset] + list(I_)))

@@ -254,7 +254,9 @@ int cf_bgen_probe(int r, int n, uint64_t F, const void* pool, const uint64_t* ke
 
 /* Range partitioning of canonical {key, id} records (key < M) for sides larger than
  * HBM: partition p = floor(key * 2^pbits / M) (1 <= pbits <= 12), so equal residues
- * meet in the same partition and partitions can be joined one at a time.
+ * meet in the same partition and partitions can be joined one at a time.  M = 0
+ * stands for 2^64: any u64 keys (the packed residues mod 2^64 of a modulus of 2^64 or
+ * more), p = key >> (64 - pbits).
  * cf_part_hist adds the partition sizes of keys[0..n) to counts[2^pbits];
  * cf_part_scatter writes each record to out[cursor[p]++] (cursor = the partitions'
  * start offsets from a cf_part_hist of the same keys; order inside a partition is

@@ -1,5 +1,6 @@
 """Streamed (out-of-core) join: residue-range partitioning and the partition-by-partition
 join through pinned host memory, against numpy and the reference's mitm64 pair sets."""
+import math
 import random
 
 import numpy as np
@@ -43,6 +44,60 @@ def test_range_partition_matches_numpy(cuda, pbits):
         a, b = off[p], off[p + 1]
         assert np.array_equal(np.sort(gi[a:b]), np.nonzero(part == p)[0].astype(np.uint64))
     assert np.array_equal(keys[gi.astype(np.int64)], gk)
+
+
+@pytest.mark.parametrize("pbits", [1, 8, 12])
+def test_range_partition_of_keys_mod_2_64(cuda, pbits):
+    # M = 0 stands for 2^64 (keys of a modulus of 2^64 or more): any u64 key, partition = top bits
+    import torch
+    rng = np.random.default_rng(100 + pbits)
+    n = 200_003
+    keys = rng.integers(0, 2 ** 64, n, dtype=np.uint64, endpoint=False)
+    keys[:4] = [0, 2 ** 64 - 1, 2 ** 63, 2 ** 63 - 1]
+    ids = np.arange(n, dtype=np.uint64)
+    lib = _lib.load()
+    dk = torch.from_numpy(keys.view(np.int64)).to(cuda)
+    di = torch.from_numpy(ids.view(np.int64)).to(cuda)
+    P = 1 << pbits
+    cnt = torch.zeros(P, dtype=torch.int64, device=cuda)
+    _lib.check(lib.cf_part_hist(_lib.ptr(dk), n, 0, pbits, _lib.ptr(cnt), None), "hist")
+    part = (keys >> np.uint64(64 - pbits)).astype(np.int64)
+    want = np.bincount(part, minlength=P)
+    assert np.array_equal(cnt.cpu().numpy(), want)
+    off = np.concatenate([[0], np.cumsum(want)])
+    cur = torch.from_numpy(off[:-1].copy()).to(cuda)
+    ok_, oi = torch.empty_like(dk), torch.empty_like(di)
+    _lib.check(lib.cf_part_scatter(_lib.ptr(dk), _lib.ptr(di), n, 0, pbits, _lib.ptr(cur), _lib.ptr(ok_),
+                                   _lib.ptr(oi), None), "scatter")
+    gi = oi.cpu().numpy().view(np.uint64)
+    for p in range(P):
+        a, b = off[p], off[p + 1]
+        assert np.array_equal(np.sort(gi[a:b]), np.nonzero(part == p)[0].astype(np.uint64))
+    assert np.array_equal(keys[gi.astype(np.int64)], ok_.cpu().numpy().view(np.uint64))
+
+
+def test_streamed_solve_on_a_modulus_above_2_64(cuda):
+    # M >= 2^64: the spilled keys are the packed residues mod 2^64, grouped by their top bits, and
+    # the streamed solve agrees with the exhaustive oracle
+    from carmichael_frontier_b200.tables import unrank_lex
+    M = 36802111876251321600
+    a = (M & -M).bit_length() - 1
+    m = M >> a
+    Q = W.eligible_pool(M, 5518)
+    for k, extra, r in ((20, 25, 2), (18, 22, 3)):
+        inst = Instance.build(M, Q[:k + extra], Q[:k], r, W.product(Q[:k]) * 10 ** 12)
+        res, _ = streamed_solve(inst, pbits=4, device=cuda, chunk=1 << 9, piece=1 << 7)
+        pairs, hits = O.solve_exhaustive(inst.M, inst.B0 + inst.INS, inst.B0, inst.r, inst.B)
+        assert sorted(res.pairs) == sorted(pairs) and [(h.D, h.I, h.n) for h in res.hits] == \
+            [(tuple(D), tuple(I), n) for D, I, n in hits]
+    side = StreamedJoin(cuda, 4, 1 << 9, 1 << 7).spill(inst.INS, r, M, inst.P0 % M)
+    keys, ids = side.keys_np(), side.ids_np()
+    assert side.n == len(keys) == len(ids) == math.comb(len(inst.INS), r)
+    for p in range(16):
+        for j in range(int(side.off[p]), int(side.off[p + 1])):
+            v = inst.P0 * math.prod(inst.INS[x] for x in unrank_lex(int(ids[j]), len(inst.INS), r))
+            assert int(keys[j]) == ((v % m) << a | (v & ((1 << a) - 1))) & ((1 << 64) - 1)
+            assert int(keys[j]) >> 60 == p
 
 
 @pytest.mark.parametrize("idx", [2, 4])

@@ -95,11 +95,3 @@ def test_key_match_with_different_residues_is_dropped(strategy):
     res = finish_rows(xn, row, 66, 153, plan, verify=True)
     assert res.residue_pairs == 1 and res.pairs == [((xn.B0[0], xn.B0[1]), (xn.INS[0], xn.INS[1]))]
 
-
-def test_streamed_join_refuses_wide_moduli():
-    from carmichael_frontier_b200.streamed import streamed_solve
-    Q = W.eligible_pool(WIDE[0], 5518)
-    x = Instance.build(WIDE[0], Q[:40], Q[:20], 2, 10 ** 90)
-    with pytest.raises(ValueError):
-        streamed_solve(x)
-
