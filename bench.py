@@ -14,6 +14,13 @@ shards by modulus; no data-path collective): weak scaling.
 --impl reference times the reference's own CPU engine (src/mitm64.cpp built
 from source into oracle/_ref/, all host threads) on a bounded sample of the
 same workload and prints the same JSON line with "impl": "reference".
+
+The default line also carries the rest of the headline metric, measured in the
+same run after the timed regions: "portfolio" (moduli solved/s of the batched
+persistent form against the per-modulus fused form, the plain one-launch-per-
+stage mitm_gpu2 form and the reference's mitm64 on all host cores, on the same
+seeded moduli) and "serving" (p50/p99 solve latency, continuous batching
+against serial, at one offered load).  --no-extras leaves them out.
 """
 from __future__ import annotations
 
@@ -35,7 +42,7 @@ UNIT = "records/s"
 WORKLOAD = "k64_r5_single_modulus"
 SEED_POOL = 64          # candidate seeds for the step sequence
 BYTES_PER_RECORD = 32   # algorithmic: one 16-B {key,id} write + one 16-B read per record entering the join
-L2_RANDOM_SECTOR_READS = 2.0e11   # random 32-byte loads/s from an L2-resident table (cf_micro_l2_probe on B200)
+D_BUILD_SHARE = 0.05    # reference-engine samples: the serial D-side build at most ~5% of a step
 
 
 def parse_args():
@@ -58,6 +65,9 @@ def parse_args():
     ap.add_argument("--requests", type=int, default=120)
     ap.add_argument("--loads", default="3,5,8", help="offered requests/s of the serving runs")
     ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--no-extras", action="store_true", help="default line without the portfolio/serving keys")
+    ap.add_argument("--extra-requests", type=int, default=60, help="serving requests in the default line")
+    ap.add_argument("--extra-load", type=float, default=3.0, help="offered requests/s in the default line")
     return ap.parse_args()
 
 
@@ -143,36 +153,64 @@ def gpu_uuid(torch, dev) -> str | None:
 
 
 # ------------------------------------------------------------------ CPU baseline (reference engine)
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def cpu_sample(w, cores: int, seconds: float):
-    """Bounded sample of one modulus for the CPU engine: the full D side and the I side over the
-    n' smallest insertion primes, n' the largest with C(n',5) <= ~seconds of work on `cores`."""
-    ins = list(w.INS)
-    budget = max(1_000_000, int(seconds * 4.0e6 * cores))   # ~4M I leaves/s per core (measured mitm64 rate)
-    n2 = w.r
-    while n2 < len(ins) and math.comb(n2 + 1, w.r) <= budget:
+    """Bounded sample of one modulus for the CPU engine: the r-subsets of the nb largest base
+    primes against those of the n' smallest insertion primes.  mitm64 builds its D side on one
+    thread before its I threads start (src/mitm64.cpp:50-71, 137-140), so nb is chosen to keep that
+    build near D_BUILD_SHARE of the step (~4M D leaves/s on one core) and n' to fill the rest of
+    `seconds` at ~4M I leaves/s per core."""
+    r = w.r
+    base, ins = sorted(w.B0), list(w.INS)
+    d_budget = max(10_000, int(D_BUILD_SHARE * seconds * 4.0e6))
+    nb = r
+    while nb < len(base) and math.comb(nb + 1, r) <= d_budget:
+        nb += 1
+    i_budget = max(1_000_000, int((1 - D_BUILD_SHARE) * seconds * 4.0e6 * cores))
+    n2 = r
+    while n2 < len(ins) and math.comb(n2 + 1, r) <= i_budget:
         n2 += 1
-    return ins[:n2]
+    return base[-nb:], ins[:n2]
 
 
 def run_cpu_engine(w, cores: int, seconds: float):
+    """Time the reference's mitm64 (all host threads) on a bounded sample of modulus w.
+    Returns (records, seconds, kind, cores, sample text, stage dict)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import re
     import oracle as O
     from carmichael_frontier_b200.workloads import product
-    ins = cpu_sample(w, cores, seconds)
-    P0 = product(w.B0)
+    base, ins = cpu_sample(w, cores, seconds)
+    P0 = product(base)
     Icap = product(ins[-w.r:]) + 1         # unpruned I side (every r-subset), as the GPU join
-    n_rec = math.comb(len(w.B0), w.r) + math.comb(len(ins), w.r)
-    sample = (f"{w.name}: full D side C({len(w.B0)},{w.r}) + I side over the {len(ins)} smallest of "
-              f"{len(w.INS)} insertion primes (C({len(ins)},{w.r}) = {math.comb(len(ins), w.r):,})")
+    n_d, n_i = math.comb(len(base), w.r), math.comb(len(ins), w.r)
+    sample = (f"{w.name}: D side over the {len(base)} largest base primes (C({len(base)},{w.r}) = {n_d:,}) x I side "
+              f"over the {len(ins)} smallest of {len(w.INS)} insertion primes (C({len(ins)},{w.r}) = {n_i:,})")
     if O.ref_binary("mitm64"):
         t0 = time.perf_counter()
-        O.run_ref_mitm64(w.M, list(w.B0), ins, w.r, P0, Icap, 1, cores)
+        _m, err = O.run_ref_mitm64(w.M, base, ins, w.r, P0, Icap, 1, cores)
         dt = time.perf_counter() - t0
-        return n_rec, dt, "reference", cores, sample
+        m = re.search(r"D_leaves=(\d+) .*\(([\d.]+)s\)\s+I_leaves=(\d+) .*\(([\d.]+)s\)", err)
+        stages = None
+        if m:
+            td, il, ti = float(m.group(2)), int(m.group(3)), float(m.group(4))
+            stages = {"d_build_s": td, "i_leaves": il, "i_s": ti, "i_leaves_per_s": il / ti if ti > 0 else None,
+                      "d_build_share": td / dt if dt > 0 else None}
+        return n_d + n_i, dt, "reference", cores, sample, stages
     t0 = time.perf_counter()                # the C restatement (single thread) when the binary is absent
-    O.mitm64_matches(w.B0, ins, w.r, w.M, P0, Icap)
+    O.mitm64_matches(base, ins, w.r, w.M, P0, Icap)
     dt = time.perf_counter() - t0
-    return n_rec, dt, "port", 1, sample + " [oracle port, 1 thread]"
+    return n_d + n_i, dt, "port", 1, sample + " [oracle port, 1 thread]", None
 
 
 def run_reference(args):
@@ -182,13 +220,17 @@ def run_reference(args):
     cores = os.cpu_count() or 1
     seeds = step_seeds(args.steps + args.warmup, 1, 0)
     per_step = max(2.0, min(8.0, 150.0 / max(1, args.steps + args.warmup)))
-    recs = tsum = 0.0
+    recs = tsum = dsum = ileaves = isum = 0.0
     kind = ncores = sample = None
     for i, w in enumerate(seeds):
-        n, dt, kind, ncores, sample = run_cpu_engine(w, cores, per_step)
+        n, dt, kind, ncores, sample, st = run_cpu_engine(w, cores, per_step)
         if i >= args.warmup:
             recs += n
             tsum += dt
+            if st:
+                dsum += st["d_build_s"]
+                ileaves += st["i_leaves"]
+                isum += st["i_s"]
     value = recs / tsum
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tsum / args.steps, "higher_is_better": True,
@@ -196,7 +238,10 @@ def run_reference(args):
             "impl": "reference",
             "config": {"workload": WORKLOAD, "engine": "src/mitm64.cpp (built from source, -O3, all host threads)",
                        "sample_per_step": "bounded: " + (sample or "")},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": kind, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": kind, "sample": sample,
+                             "cpu_model": cpu_model(),
+                             "d_build_share": dsum / tsum if tsum else None,
+                             "i_leaves_per_s": ileaves / isum if isum else None},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -344,10 +389,27 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            n, dt, kind, cores, sample = run_cpu_engine(timed[0], os.cpu_count() or 1, args.cpu_seconds)
-            cpu = {"value": n / dt, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+            n, dt, kind, cores, sample, st = run_cpu_engine(timed[0], os.cpu_count() or 1, args.cpu_seconds)
+            cpu = {"value": n / dt, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+                   "cpu_model": cpu_model(), "stages": st}
         except Exception as e:            # report, never fail the GPU line
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None, "sample": f"failed: {e}"}
+
+    # ceiling of the fused probe, measured in this run on this GPU: random 32-byte reads from an
+    # L2-resident table the size of the k=64 r=5 fingerprint array (2^20 buckets x 32 B)
+    l2_ceiling = None
+    if rank == 0:
+        try:
+            from carmichael_frontier_b200.measure.micro import l2_random_reads
+            l2_ceiling = l2_random_reads(32)
+        except Exception as e:            # report, never fail the GPU line
+            l2_ceiling = None
+            print(f"l2 ceiling not measured: {e}", file=sys.stderr)
+
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras and args.case is None:
+        extras["portfolio"] = measure_portfolio(dev, args, compact=True)
+        extras["serving"] = measure_serving(dev, args, [args.extra_load], args.extra_requests, compact=True)
 
     if rank == 0:
         kern = {k: {"ms_total": 1e3 * v} for k, v in kt.items()}
@@ -373,17 +435,20 @@ def run_ours(args):
                        "parallelism": f"modulus-sharded x{world}", "records_per_gpu": recs},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per D and per I record "
+                                            "of one capture (profiles/k_fused_k64_r5_seed0.md), scaled by this "
+                                            "run's record counts" if traffic is not None else None),
                          "kernel": ("k_fused build + probe" if solver.tuning.strategy == "fused"
                                     else "k_gen_part + k_join_part") + " (join path, 32 B/record)",
                          "peak_source": peak_src},
             "strategy": solver.tuning.strategy,
             "kernels": kern,
             "l2_probe": ({"achieved_probes_per_s": n_probe / kt["probe"],
-                          "ceiling_probes_per_s": L2_RANDOM_SECTOR_READS,
-                          "frac": n_probe / kt["probe"] / L2_RANDOM_SECTOR_READS,
+                          "ceiling_probes_per_s": l2_ceiling,
+                          "frac": n_probe / kt["probe"] / l2_ceiling,
                           "note": "one 32-byte L2 sector read per probing record; ceiling = random 32-B loads/s "
-                                  "measured on this B200"}
-                         if kt["probe"] > 0 else None),
+                                  "from a 32 MiB table, measured in this run (measure/cf_micro.cu)"}
+                         if kt["probe"] > 0 and l2_ceiling else None),
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // max(1, len(timed)),
                     "d2h_bytes_per_step": d2h // max(1, len(timed)), "api": "carmichael_frontier_b200.solve"},
@@ -392,30 +457,28 @@ def run_ours(args):
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
                        "samples": clk["samples"]},
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
 
 
 # ------------------------------------------------------------------ portfolio (batched vs per-modulus)
-def run_portfolio(args):
+def measure_portfolio(dev, args, compact: bool = False) -> dict:
     """Seeded 1024-modulus portfolio (k=64, pools 120..400, r in {4,5,6}, B=10^148); every
     modulus joined over its full D side and the first --i-limit I ranks (a bounded sample:
-    the unpruned I sides total ~1e14 records).  Forms: batched persistent kernels (CUDA
-    graphs replayed), this library's per-modulus fused solve, and the reference's
-    per-modulus mitm_gpu2 form (generate / sort_side / join_sorted) on the first
-    --plain-moduli moduli."""
+    the unpruned I sides total ~1e14 records).  Forms, all on the same moduli: batched
+    persistent kernels (CUDA graphs replayed), this library's per-modulus fused solve, the
+    reference's per-modulus mitm_gpu2 form (generate / sort_side / join_sorted per stage), and
+    the reference's mitm64 on all host cores (a bounded sample of one modulus, as records/s and
+    the moduli/s it amounts to at the GPU sample's records per modulus)."""
     import torch
     from carmichael_frontier_b200 import Solver, workloads as W
     from carmichael_frontier_b200.portfolio import BatchSolver, run_per_modulus, run_plain
     from carmichael_frontier_b200.solve import Instance
-    rank, world, local = dist_env()
-    if rank != 0:
-        return
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
     lim = args.i_limit
-    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config3(args.moduli)]
+    ws = W.config3(args.moduli)
+    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in ws]
     bs = BatchSolver(dev)
     t0 = time.perf_counter()
     prep = bs.prepare(insts, lim)
@@ -424,11 +487,12 @@ def run_portfolio(args):
     recs = prep.records
     clocks = ClockSampler(gpu_uuid(torch, dev))
     clocks.start()
-    for _ in range(args.warmup):
-        ref = bs.run(prep, graphs=True)
+    steps = 3 if compact else args.steps
+    for _ in range(1 if compact else args.warmup):
+        bs.run(prep, graphs=True)
     torch.cuda.synchronize(dev)
     times = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         t0 = time.perf_counter()
         res = bs.run(prep, graphs=True)
         torch.cuda.synchronize(dev)
@@ -441,7 +505,7 @@ def run_portfolio(args):
     per = run_per_modulus(insts, i_limit=lim, solver=one)
     torch.cuda.synchronize(dev)
     t_p = time.perf_counter() - t0
-    npl = min(args.plain_moduli, len(insts))
+    npl = len(insts) if compact else min(args.plain_moduli, len(insts))
     run_plain(insts[:1], i_limit=1 << 16, device=dev)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -449,57 +513,68 @@ def run_portfolio(args):
     torch.cuda.synchronize(dev)
     t_pl = time.perf_counter() - t0
     clk = clocks.stop()
+    bs.release(prep)
     rec_pl = sum(prep.nD[k] + prep.nI[k] for k in range(npl))
-    same = [(a.residue_pairs, a.pairs, [h.n for h in a.hits]) for a in res] == \
-           [(a.residue_pairs, a.pairs, [h.n for h in a.hits]) for a in per]
-    same_plain = [(a.residue_pairs, sorted(a.pairs), [h.n for h in a.hits]) for a in res[:npl]] == \
-                 [(a.residue_pairs, sorted(a.pairs), [h.n for h in a.hits]) for a in plain]
+    key = lambda a: (a.residue_pairs, sorted(a.pairs), [h.n for h in a.hits])
+    same = [key(a) for a in res] == [key(a) for a in per]
+    same_plain = [key(a) for a in res[:npl]] == [key(a) for a in plain]
     cpu = None
     if not args.no_cpu_baseline:
         try:
-            w0 = W.config3(1)[0]
-            n, dt, kind, cores, sample = run_cpu_engine(w0, os.cpu_count() or 1, args.cpu_seconds)
-            cpu = {"value": n / dt, "unit": "records/s", "cores": cores, "kind": kind, "sample": sample,
-                   "moduli_per_s_equiv": (n / dt) / (recs / len(insts))}
+            n, dt, kind, cores, sample, st = run_cpu_engine(ws[0], os.cpu_count() or 1, args.cpu_seconds / 2)
+            rate = n / dt
+            cpu = {"records_per_s": rate, "moduli_per_s_equiv": rate / (recs / len(insts)), "cores": cores,
+                   "cpu_model": cpu_model(), "kind": kind, "sample": sample, "stages": st}
         except Exception as e:
-            cpu = {"value": None, "unit": "records/s", "sample": f"failed: {e}"}
-    line = {"metric": "portfolio moduli solved/s (batched persistent kernels)", "value": len(insts) / t_b,
-            "unit": "moduli/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * t_b, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u64", "data": "synthetic (seeded moduli)",
-            "config": {"workload": "portfolio_1024_k64_r456", "moduli": len(insts), "i_limit": lim,
-                       "records": recs, "batches": len(prep.batches), "prepare_s": t_prep,
-                       "sample": f"full D sides, I ranks [0, {lim}) per modulus"},
-            "forms": {
-                "batched": {"moduli_per_s": len(insts) / t_b, "records_per_s": recs / t_b, "s": t_b,
-                            "graphs": True, "launches_per_batch": 4},
-                "per_modulus_fused": {"moduli_per_s": len(insts) / t_p, "records_per_s": recs / t_p, "s": t_p,
-                                      "same_results": same},
-                "plain_mitm_gpu2": {"moduli": npl, "moduli_per_s": npl / t_pl, "records_per_s": rec_pl / t_pl,
-                                    "s": t_pl, "same_results": same_plain},
-            },
-            "speedup_vs_plain_records": (recs / t_b) / (rec_pl / t_pl),
-            "hits": sum(len(x.hits) for x in res), "residue_pairs": sum(x.residue_pairs for x in res),
-            "cpu_baseline": cpu,
-            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
-                       "samples": clk["samples"]}}
-    print(json.dumps(line), flush=True)
+            cpu = {"records_per_s": None, "sample": f"failed: {e}"}
+    out = {
+        "workload": "portfolio_1024_k64_r456", "moduli": len(insts), "i_limit": lim, "records": recs,
+        "sample": f"full D sides, I ranks [0, {lim}) per modulus; every form on the same {len(insts)} moduli"
+                  if npl == len(insts) else f"full D sides, I ranks [0, {lim}); plain form on the first {npl}",
+        "batched": {"moduli_per_s": len(insts) / t_b, "records_per_s": recs / t_b, "s": t_b, "graphs": True},
+        "per_modulus_fused": {"moduli_per_s": len(insts) / t_p, "records_per_s": recs / t_p, "s": t_p,
+                              "same_results": same},
+        "plain_mitm_gpu2": {"moduli": npl, "moduli_per_s": npl / t_pl, "records_per_s": rec_pl / t_pl, "s": t_pl,
+                            "same_results": same_plain},
+        "batched_over_plain": (len(insts) / t_b) / (npl / t_pl),
+        "mitm64_all_cores": cpu,
+        "batched_over_mitm64": ((recs / t_b) / cpu["records_per_s"]) if cpu and cpu.get("records_per_s") else None,
+        "targets": {"batched_over_plain": 10.0, "batched_over_mitm64": 50.0},
+        "hits": sum(len(x.hits) for x in res), "residue_pairs": sum(x.residue_pairs for x in res),
+        "prepare_s": t_prep, "batches": len(prep.batches),
+        "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                   "samples": clk["samples"]},
+    }
+    return out
 
 
-# ------------------------------------------------------------------ serving (continuous batching)
-def run_serving(args):
-    """The first --requests requests of the seeded serving stream (k = 64..100, pools 80..320,
-    r = 3..6, B = prod(B0) * 10^4), Poisson arrivals at three offered loads, served by the
-    continuous-batching loop; the serial form (one request at a time) at the same loads."""
+def run_portfolio(args):
     import torch
-    from carmichael_frontier_b200 import Solver, Tuning, serve, workloads as W
-    from carmichael_frontier_b200.solve import Instance
     rank, world, local = dist_env()
     if rank != 0:
         return
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config5_requests(args.requests)]
+    p = measure_portfolio(dev, args)
+    line = {"metric": "portfolio moduli solved/s (batched persistent kernels)", "value": p["batched"]["moduli_per_s"],
+            "unit": "moduli/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * p["batched"]["s"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded moduli)",
+            "config": {"workload": p["workload"], "moduli": p["moduli"], "i_limit": p["i_limit"],
+                       "records": p["records"], "sample": p["sample"]},
+            "portfolio": p, "clocks": p["clocks"]}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ serving (continuous batching)
+def measure_serving(dev, args, loads, requests: int, compact: bool = False) -> dict:
+    """The first `requests` requests of the seeded serving stream (k = 64..100, pools 80..320,
+    r = 3..6, B = prod(B0) * 10^4), Poisson arrivals at each offered load, served by the
+    continuous-batching loop; the serial form (one request at a time) at the same loads."""
+    import torch
+    from carmichael_frontier_b200 import Solver, Tuning, serve, workloads as W
+    from carmichael_frontier_b200.solve import Instance
+    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config5_requests(requests)]
     warm = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config5_requests(8, seed=1)]
     alone = Solver(dev, tuning=Tuning(strategy="auto", max_nodes=1 << 22))
     for x in warm:
@@ -507,11 +582,11 @@ def run_serving(args):
     torch.cuda.synchronize(dev)
     clocks = ClockSampler(gpu_uuid(torch, dev))
     clocks.start()
-    loads = [float(x) for x in args.loads.split(",")]
     out = {"continuous": [], "serial": []}
+    same = True
     for rate in loads:
         srv = serve.Server(dev, slots=args.slots, strategy="auto").start()
-        st, _ = serve.run_poisson(srv, insts, rate=rate, seed=7)
+        st, tickets = serve.run_poisson(srv, insts, rate=rate, seed=7)
         srv.stop()
         out["continuous"].append(st)
         torch.cuda.empty_cache()
@@ -521,20 +596,39 @@ def run_serving(args):
             torch.cuda.synchronize(dev)
             alone._bufs.clear()
             return r
-        st2, _ = serve.run_serial(one, insts, rate=rate, seed=7)
+        st2, res2 = serve.run_serial(one, insts, rate=rate, seed=7)
         out["serial"].append(st2)
+        pairs = lambda ts: [sorted(t.result.pairs) if t.result is not None else None for t in ts]  # noqa: E731
+        same = same and pairs(tickets) == pairs(res2)
     clk = clocks.stop()
-    mid = out["continuous"][len(loads) // 2]
-    line = {"metric": "serving p50/p99 solve latency (ms) and requests/s", "value": mid["p99_ms"], "unit": "ms (p99)",
-            "n_gpus": 1, "steps": len(insts), "warmup": len(warm), "ms_per_step": mid["mean_ms"],
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
-            "data": "synthetic (seeded request stream)",
-            "config": {"workload": "serving_k64-100_r3-6", "requests": len(insts), "slots": args.slots,
-                       "offered_rps": loads, "arrivals": "Poisson, seed 7",
-                       "sample": f"first {len(insts)} of the 10,000-request stream"},
-            "continuous": out["continuous"], "serial": out["serial"],
+    keep = ("offered_rps", "throughput_rps", "p50_ms", "p99_ms", "mean_ms", "errors") if compact else None
+    trim = (lambda d: {k: d[k] for k in keep if k in d}) if keep else (lambda d: d)
+    return {"workload": "serving_k64-100_r3-6", "requests": len(insts), "slots": args.slots, "offered_rps": loads,
+            "arrivals": "Poisson, seed 7", "sample": f"first {len(insts)} of the seeded 10,000-request stream",
+            "continuous": [trim(x) for x in out["continuous"]], "serial": [trim(x) for x in out["serial"]],
+            "same_results_alone_and_in_the_mix": same,
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
                        "samples": clk["samples"]}}
+
+
+def run_serving(args):
+    import torch
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    loads = [float(x) for x in args.loads.split(",")]
+    sv = measure_serving(dev, args, loads, args.requests)
+    mid = sv["continuous"][len(loads) // 2]
+    line = {"metric": "serving p50/p99 solve latency (ms) and requests/s", "value": mid["p99_ms"], "unit": "ms (p99)",
+            "n_gpus": 1, "steps": sv["requests"], "warmup": 8, "ms_per_step": mid["mean_ms"],
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic (seeded request stream)",
+            "config": {"workload": sv["workload"], "requests": sv["requests"], "slots": sv["slots"],
+                       "offered_rps": loads, "arrivals": sv["arrivals"], "sample": sv["sample"]},
+            "continuous": sv["continuous"], "serial": sv["serial"],
+            "same_results_alone_and_in_the_mix": sv["same_results_alone_and_in_the_mix"], "clocks": sv["clocks"]}
     print(json.dumps(line), flush=True)
 
 

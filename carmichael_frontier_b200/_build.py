@@ -17,6 +17,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libcfmitm.so")
+MICRO_SRC = os.path.join(PKG, "measure", "cf_micro.cu")
+MICRO_LIB = os.path.join(PKG, "libcfmicro.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
@@ -52,12 +54,28 @@ def headers_mtime() -> float:
     return max((os.path.getmtime(h) for h in hs), default=0.0)
 
 
+def build_micro(force: bool = False) -> str:
+    """Compile the measurement kernels (measure/cf_micro.cu) into libcfmicro.so."""
+    if not force and os.path.exists(MICRO_LIB) and os.path.getmtime(MICRO_LIB) >= max(
+            os.path.getmtime(MICRO_SRC), headers_mtime(), os.path.getmtime(__file__)):
+        return MICRO_LIB
+    cmd = [nvcc(), *ARCH, *FLAGS, "-shared", MICRO_SRC, "-o", MICRO_LIB + ".tmp", "-lcudart_static", "-lrt",
+           "-lpthread", "-ldl"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {MICRO_SRC}:\n{r.stderr}")
+    os.replace(MICRO_LIB + ".tmp", MICRO_LIB)
+    return MICRO_LIB
+
+
 def build(force: bool = False, verbose_ptxas: bool = False) -> str:
-    """Compile every csrc/*.cu and link libcfmitm.so; returns the library path."""
+    """Compile every csrc/*.cu and link libcfmitm.so, then the measurement library; returns
+    the path of libcfmitm.so."""
     os.makedirs(OBJ, exist_ok=True)
     srcs = sources()
     newest = max([os.path.getmtime(s) for s in srcs] + [headers_mtime(), os.path.getmtime(__file__)])
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
+        build_micro(force)
         return LIB
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose_ptxas), srcs))
@@ -67,6 +85,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")
     os.replace(tmp, LIB)
+    build_micro(force)
     return LIB
 
 

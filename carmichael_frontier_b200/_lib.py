@@ -102,8 +102,6 @@ SIGNATURES = [
     ("cf_sort_pairs_noalloc", C.c_int, [vp, vp, u64, C.c_int, vp]),
     ("cf_merge_run_bytes", sz, []),
     ("cf_merge_join_runs", C.c_int, [vp, u64, vp, u64, vp, u64, vp, vp, vp, vp]),
-    ("cf_micro_l2_probe", C.c_int, [vp, u64, C.c_int, u32, vp, vp]),
-    ("cf_micro_mulhi", C.c_int, [C.c_int, u32, vp, vp]),
 ]
 
 _lib = None

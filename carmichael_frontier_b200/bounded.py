@@ -202,7 +202,10 @@ class BoundedGenerator:
         n = len(INS)
         assert 1 <= r <= 16 and n <= 1024 and _modulus_ok(M)
         assert all(INS[i] < INS[i + 1] for i in range(n - 1)), "INS must be strictly ascending"
-        assert Icap - 1 < U128, "Icap needs more than 128 bits"
+        # the bound table saturates at 2^128 - 1, which is exact while every inner node's product (at
+        # most r - 1 primes) stays below 2^128: A <= 2^128 - 1 <= H whenever the true H exceeds it
+        assert Icap - 1 < U128 or math.prod(INS[-(r - 1):] if r > 1 else []) < U128, \
+            "Icap and the inner products need more than 128 bits"
         if Icap <= 1 or n < r:
             return None
         assert math.comb(n, r) < 1 << 64, "rank ids would overflow u64"

@@ -51,6 +51,21 @@ def applicable(inst) -> bool:
         and math.comb(len(inst.B0), inst.r) < 1 << 64
 
 
+def bounds_fit(B0, INS, r: int, Icap: int) -> bool:
+    """True when the bounded producers can run an instance given by its sides and exclusive I cap:
+    1 <= r <= 16, both sides hold r primes, at most 1024 primes each, the products of r base primes
+    below 2^128, the I cap below 2^128 or else the products of r - 1 insertion primes below 2^128
+    (the I bound table then saturates exactly), and colex ids of either side below 2^64.  The
+    reference's GPU producer stops at an I cap of 2^128 (gpu/igen_gpu.py:83,103-105) and its driver
+    sends such instances to a host join (gpu/mitm_gpu_mstar_driver.py:150-183,207)."""
+    B0, INS = sorted(B0), list(INS)
+    if not (1 <= r <= 16) or len(B0) < r or len(INS) < r or len(B0) > 1024 or len(INS) > 1024:
+        return False
+    inner_fits = Icap - 1 < U128 or math.prod(INS[-(r - 1):] if r > 1 else []) < U128
+    return inner_fits and math.prod(B0[-r:]) < U128 and math.comb(len(INS), r) < 1 << 64 \
+        and math.comb(len(B0), r) < 1 << 64
+
+
 def prunes(inst) -> bool:
     """True when the bound removes part of either side (else the fused join is cheaper)."""
     r = inst.r

@@ -222,14 +222,15 @@ def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: in
     k smallest primes of the capped pool checked as a Carmichael number below U (radius 0), then each
     radius r_min..min(rmax, r_max) at the driver's h-stratum bound, through ``driver.run_instance`` (the
     driver's Icap/Dmin/affordable-pool bounds, product-bounded producers and record join on the GPU).
-    Radii whose bounds need more than 128-bit products are reported as skipped.
+    Radii 1..16 are run; radii whose bounds need more than 128-bit products (or colex ids of 2^64 and
+    more) are reported as skipped.
 
     Returns (runs, completions): runs = {D: {"base_carmichael", "base_below_U", "instances": [per-radius
     counts], "skipped": [r]}}; completions = the (key, factors, label) of every completion below U that
     was given to consider(key, factors, label) (the default consider only collects them)."""
     from . import bsolve, driver
     from .certify import verify_certificate
-    from .solve import Instance, Solver, Tuning
+    from .solve import Solver, Tuning
     hits = []
     user = consider
 
@@ -256,7 +257,8 @@ def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: in
             h = driver.hmax_for(base, INS, r, U, split)
             if h < 0:
                 continue
-            if r > 10 or not bsolve.applicable(Instance.build(D, Pc, base, r, U - 1)):
+            Icap, _Dmin, _cap_r, aff = driver.instance_bounds(base, INS, r, U)
+            if len(aff) >= r and not bsolve.bounds_fit(base, aff, r, Icap):
                 rec["skipped"].append(r)
                 continue
             st: dict = {}

@@ -27,7 +27,8 @@
 // its parent by binary search over the scanned offsets -- every thread does the
 // same work whatever the shape of the tree.  The last level writes the records
 // (canonical keys) directly, in the reference's order.  The product never
-// overflows: on the I side A * a_x <= Icap - 1 < 2^128 for every kept child;
+// overflows: on the I side the host checks that Icap - 1 < 2^128 (A * a_x <= Icap - 1 for every kept
+// child) or, for larger caps (the table then saturates at 2^128 - 1), that r - 1 primes multiply below 2^128;
 // on the D side the host checks that the r largest primes multiply below 2^128.
 #include "cf_abi_internal.h"
 

@@ -185,10 +185,20 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
   }
   for (int i = threadIdx.x; i < 2 * kWarps * kRadix; i += kSortBlock) s_wc[i] = 0;   // s_wc and s_mm
   __syncthreads();
-  if (BULK && !mbar_wait(&s_bar[0], 0, kMbarLimit)) {
-    atomicOr(err, CF_ERR_SPIN_LIMIT);
-    mbar_wait(&s_bar[0], 0, kMbarLimit);
+  // A tile whose keys never arrived (both bounded waits ran out, practically unreachable) is
+  // ranked as empty: it publishes zero counts, so its successors' look-back still ends and
+  // every position they compute stays below n, and it writes nothing.  The error word makes
+  // the call return CF_ETIMEOUT.
+  bool keys_lost = false;
+  if (BULK) {
+    bool ok = mbar_wait(&s_bar[0], 0, kMbarLimit);
+    if (!ok) {
+      atomicOr(err, CF_ERR_SPIN_LIMIT);
+      ok = mbar_wait(&s_bar[0], 0, kMbarLimit);
+    }
+    keys_lost = __syncthreads_or(!ok) != 0;
   }
+  const int tr = keys_lost ? 0 : tv;          // items ranked and written
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   u64 key[kSortItems];
   u32 loc[kSortItems];                      // local offset (low 16 bits) | digit << 16
@@ -198,7 +208,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
     const int e = wid * 32 * kSortItems + it * 32 + lane;
-    key[it] = e < tv ? s_kin[e] : 0ull;
+    key[it] = e < tr ? s_kin[e] : 0ull;
   }
   // stable rank within the warp, item by item: the lanes of one digit find each other
   // through a shared mask (one atomic OR each), the group's lowest lane takes the
@@ -207,7 +217,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
     const int e = wid * 32 * kSortItems + it * 32 + lane;
-    const u32 d = e < tv ? (u32)((key[it] >> shift) & 0xff) : 0x100u;
+    const u32 d = e < tr ? (u32)((key[it] >> shift) & 0xff) : 0x100u;
     const bool valid = d < 0x100u;
     if (valid) atomicOr(&mm[d], 1u << lane);
     __syncwarp();
@@ -309,12 +319,25 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
     }
   }
   __syncthreads();
-  write_tile(s_kin, s_dj, s_gbase, kout, tv);
-  if (BULK && !mbar_wait(&s_bar[1], 0, kMbarLimit)) {
-    atomicOr(err, CF_ERR_SPIN_LIMIT);
-    mbar_wait(&s_bar[1], 0, kMbarLimit);
+  write_tile(s_kin, s_dj, s_gbase, kout, tr);
+  bool ids_lost = false;
+  if (BULK) {
+    bool ok = mbar_wait(&s_bar[1], 0, kMbarLimit);
+    if (!ok) {
+      atomicOr(err, CF_ERR_SPIN_LIMIT);
+      ok = mbar_wait(&s_bar[1], 0, kMbarLimit);
+    }
+    ids_lost = __syncthreads_or(!ok) != 0;
+  } else {
+    __syncthreads();
   }
-  __syncthreads();
+  if (keys_lost || ids_lost) {
+    // nothing more is written; before the CTA gives up its shared memory, wait (bounded) once
+    // more for copies still in flight, so a late copy is unlikely to land in a later CTA's tile
+    if (keys_lost) mbar_wait(&s_bar[0], 0, kMbarLimit);
+    if (ids_lost || keys_lost) mbar_wait(&s_bar[1], 0, kMbarLimit);
+    return;
+  }
   {
     u64 idv[kSortItems];
 #pragma unroll
@@ -327,7 +350,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
       if ((loc[it] >> 16) < 0x100u) s_kin[loc[it] & 0xffffu] = idv[it];
   }
   __syncthreads();
-  write_tile(s_kin, s_dj, s_gbase, iout, tv);
+  write_tile(s_kin, s_dj, s_gbase, iout, tr);
 }
 
 // ---------------------------------------------------------------------------

@@ -1,12 +1,14 @@
-// cf_micro.cu -- microbenchmarks that measure the ceilings the kernels are compared
-// against on the running GPU:
+// cf_micro.cu -- measurement tooling, built into its own libcfmicro.so (not part of
+// libcfmitm.so or include/cfmitm.h): microbenchmarks that measure the ceilings the
+// kernels are compared against on the running GPU:
 //   cf_micro_l2_probe : random 32-byte reads from a table (L2-resident when it is
 //                       small): the ceiling of the fused probe, which reads one
 //                       32-byte fingerprint sector per record.
 //   cf_micro_mulhi    : 64-bit Montgomery products (two mul.hi.u64 and two
 //                       mul.lo.u64 each) per second, eight independent chains per
 //                       thread: the integer ceiling of residue generation.
-#include "cf_abi_internal.h"
+#include <cuda_runtime.h>
+#include "cf_common.cuh"
 
 namespace {
 
@@ -41,20 +43,19 @@ k_micro_mul(int iters, u64 m, u64 minv, u64* __restrict__ sink) {
 
 }  // namespace
 
+// Both return 0, -1 for bad arguments, or the cudaError_t of the launch (positive).
 extern "C" int cf_micro_l2_probe(const void* table, u64 bucket_mask, int iters, u32 blocks, u64* sink,
                                  void* stream) {
-  if (!table || !sink || iters < 1 || blocks < 1) { cf_set_error("cf_micro_l2_probe: bad arguments%s", ""); return CF_EBADARG; }
+  if (!table || !sink || iters < 1 || blocks < 1) return -1;
   k_micro_l2<<<blocks, 512, 0, (cudaStream_t)stream>>>((const uint4*)table, bucket_mask, iters, sink);
-  CF_LAUNCH_CHECK("cf_micro_l2_probe");
-  return CF_OK;
+  return (int)cudaGetLastError();
 }
 
 extern "C" int cf_micro_mulhi(int iters, u32 blocks, u64* sink, void* stream) {
-  if (!sink || iters < 1 || blocks < 1) { cf_set_error("cf_micro_mulhi: bad arguments%s", ""); return CF_EBADARG; }
+  if (!sink || iters < 1 || blocks < 1) return -1;
   const u64 m = (1ull << 61) - 1;               // odd modulus below 2^62
   u64 minv = m;
   for (int i = 0; i < 6; ++i) minv *= 2 - m * minv;
   k_micro_mul<<<blocks, 256, 0, (cudaStream_t)stream>>>(iters, m, minv, sink);
-  CF_LAUNCH_CHECK("cf_micro_mulhi");
-  return CF_OK;
+  return (int)cudaGetLastError();
 }

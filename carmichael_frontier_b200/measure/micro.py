@@ -1,35 +1,49 @@
 """Measured ceilings on the running GPU (random L2 sector reads, 64-bit Montgomery products)
-and the rate of the LSD radix sort (the materialised join's sort_side).
+and the rates of the LSD radix sort (the materialised join's sort_side) and of generation.
 
-    python -m carmichael_frontier_b200.micro            # ceilings, one JSON line
-    python -m carmichael_frontier_b200.micro sort N     # cf_sort_pairs on N random 62-bit keys
-    python -m carmichael_frontier_b200.micro gen N      # linear generator (N records), bounded D producer
-bench.py quotes the L2 figure as the fused probe's ceiling.
+    python -m carmichael_frontier_b200.measure.micro            # ceilings, one JSON line
+    python -m carmichael_frontier_b200.measure.micro sort N     # cf_sort_pairs on N random 62-bit keys
+    python -m carmichael_frontier_b200.measure.micro gen N      # linear generator, bounded D producer
+bench.py measures the L2 figure in its own run as the fused probe's ceiling.  The ceiling kernels
+live in libcfmicro.so (measure/cf_micro.cu), apart from the library's C ABI.
 """
 from __future__ import annotations
 
 import json
 import math
 
-from . import _lib
+from .. import _lib
+from . import load as _load_micro
+
+
+class _Micro:
+    """libcfmicro.so with the library's status check."""
+
+    def __getattr__(self, name):
+        return getattr(_load_micro(), name)
+
+
+def _mcheck(status: int, where: str) -> None:
+    if status != 0:
+        raise RuntimeError(f"{where}: status {status}")
 
 
 def l2_random_reads(table_mb: int = 32, iters: int = 2048, reps: int = 3) -> float:
     """Random 32-byte reads per second from a table of `table_mb` MiB."""
     import torch
-    lib = _lib.load()
+    lib = _Micro()
     nb = (table_mb << 20) // 32
     nb = 1 << (nb.bit_length() - 1)
     tab = torch.randint(0, 1 << 30, (nb * 8,), dtype=torch.int32, device="cuda")
     sink = torch.zeros(2, dtype=torch.int64, device="cuda")
     blocks = torch.cuda.get_device_properties(0).multi_processor_count * 4
     sh = torch.cuda.current_stream().cuda_stream
-    _lib.check(lib.cf_micro_l2_probe(tab.data_ptr(), nb - 1, 64, blocks, sink.data_ptr(), sh), "l2 probe")
+    _mcheck(lib.cf_micro_l2_probe(tab.data_ptr(), nb - 1, 64, blocks, sink.data_ptr(), sh), "l2 probe")
     best = 0.0
     for _ in range(reps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        _lib.check(lib.cf_micro_l2_probe(tab.data_ptr(), nb - 1, iters, blocks, sink.data_ptr(), sh), "l2 probe")
+        _mcheck(lib.cf_micro_l2_probe(tab.data_ptr(), nb - 1, iters, blocks, sink.data_ptr(), sh), "l2 probe")
         e1.record()
         torch.cuda.synchronize()
         best = max(best, blocks * 512 * iters / (e0.elapsed_time(e1) * 1e-3))
@@ -39,16 +53,16 @@ def l2_random_reads(table_mb: int = 32, iters: int = 2048, reps: int = 3) -> flo
 def montgomery_products(iters: int = 4096, reps: int = 3) -> float:
     """64-bit Montgomery products per second."""
     import torch
-    lib = _lib.load()
+    lib = _Micro()
     sink = torch.zeros(2, dtype=torch.int64, device="cuda")
     blocks = torch.cuda.get_device_properties(0).multi_processor_count * 8
     sh = torch.cuda.current_stream().cuda_stream
-    _lib.check(lib.cf_micro_mulhi(16, blocks, sink.data_ptr(), sh), "mulhi")
+    _mcheck(lib.cf_micro_mulhi(16, blocks, sink.data_ptr(), sh), "mulhi")
     best = 0.0
     for _ in range(reps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        _lib.check(lib.cf_micro_mulhi(iters, blocks, sink.data_ptr(), sh), "mulhi")
+        _mcheck(lib.cf_micro_mulhi(iters, blocks, sink.data_ptr(), sh), "mulhi")
         e1.record()
         torch.cuda.synchronize()
         best = max(best, blocks * 256 * iters * 8 / (e0.elapsed_time(e1) * 1e-3))
@@ -88,9 +102,9 @@ def generation_rate(n: int, dmin_bits: int = 40, reps: int = 3) -> dict:
     drop-in, canonical residues and 10-bit packed ids, I ranks [0, n)) and the bounded D producer
     (every 5-subset of the 64-prime base with product >= 2^dmin_bits, ddump's order)."""
     import torch
-    from . import mitm_gpu2, workloads as W
-    from .bounded import BoundedGenerator
-    from .solve import Instance
+    from .. import mitm_gpu2, workloads as W
+    from ..bounded import BoundedGenerator
+    from ..solve import Instance
     w = W.config2(0)
     inst = Instance.build(w.M, w.Q, w.B0, w.r, w.B)
     r, M = inst.r, inst.M

@@ -35,6 +35,15 @@ from .certify import verify_certificate
 from .tables import DeviceTables, ncomb, unrank_lex
 
 
+def range_partition(keys: np.ndarray, M: int, pbits: int) -> np.ndarray:
+    """Residue-range partition floor(key * 2^pbits / M) of uint64 keys below M (M >= 2^64: the top
+    pbits bits), exactly, through the partition boundaries ceil(j * M / 2^pbits)."""
+    P = 1 << pbits
+    Mx = min(int(M), 1 << 64)
+    bounds = np.array([-(-(j * Mx) // P) for j in range(1, P)], dtype=np.uint64)
+    return np.searchsorted(bounds, np.asarray(keys, dtype=np.uint64), side="right").astype(np.int64)
+
+
 @dataclass
 class HostSide:
     """One side in pinned host memory, grouped by residue-range partition."""
@@ -60,7 +69,7 @@ class HostSide:
         """From an (N, 2) uint64 array of {key, id} records (the dumpers' format), on the host."""
         import torch
         keys = rec[:, 0].astype(np.uint64)
-        part = ((keys.astype(object) << pbits) // M).astype(np.int64) if len(keys) else np.zeros(0, np.int64)
+        part = range_partition(keys, M, pbits)
         order = np.argsort(part, kind="stable")
         off = np.zeros((1 << pbits) + 1, dtype=np.int64)
         np.add.at(off, part + 1, 1)
@@ -105,55 +114,98 @@ class StreamedJoin:
         """Generate the records of ranks [lo, hi) on the device and leave them, grouped by
         residue range, in pinned host memory (`out`: arrays from host_buffers, else
         allocated here)."""
-        torch, lib, dp = self.torch, self.lib, _lib.ptr
+        torch = self.torch
         n = len(primes)
         total = ncomb(n, r) if hi is None else hi
-        N = total - lo
-        P = 1 << self.pbits
         pool = self.tables.pool(primes, r, M, mult)
-        # M >= 2^64: packed residue keys taken mod 2^64, partitioned as if M were 2^64 (argument 0)
-        canon, Mp = (0, 0) if M >= 1 << 64 else (1, M)
+        # M >= 2^64: packed residue keys taken mod 2^64, partitioned as if M were 2^64
+        canon = 0 if M >= 1 << 64 else 1
+        sh = _lib.stream_handle()
+        cap = min(self.chunk, max(total - lo, 1))
+        gk = torch.empty(cap, dtype=torch.uint64, device=self.device)
+        gi = torch.empty(cap, dtype=torch.uint64, device=self.device)
+
+        def chunks():
+            for c0 in range(lo, total, cap):
+                cnt = min(cap, total - c0)
+                self._gen(pool, n, r, c0, cnt, gk, gi, sh, canon)
+                yield gk[:cnt], gi[:cnt]
+        return self.spill_records(chunks, M, out=out, cap=cap)
+
+    def spill_records(self, chunks, M: int, out=None, cap: int | None = None) -> HostSide:
+        """Partition a side given as record chunks by residue range into pinned host memory.
+
+        chunks: a callable returning an iterable of (keys, ids) chunks -- uint64 device tensors
+        (a producer's output) or host arrays (numpy uint64 or torch tensors: a dumper's
+        records), each at most `cap` records; it is called twice, once for the partition sizes
+        and once for the scatter, and must yield the same records both times.  Keys below M,
+        or any u64 key for M >= 2^64 (partitioned as if M were 2^64)."""
+        torch, lib, dp = self.torch, self.lib, _lib.ptr
+        P = 1 << self.pbits
+        Mp = 0 if M >= 1 << 64 else M
         dev = self.device
         sh = _lib.stream_handle()
-        cap = min(self.chunk, max(N, 1))
-        gk = torch.empty(cap, dtype=torch.uint64, device=dev)
-        gi = torch.empty(cap, dtype=torch.uint64, device=dev)
-        # pass 1: partition sizes of the whole side (generation is cheap next to the copies)
+        cap = cap or self.chunk
+        up = [None, None]
+
+        def on_device(k, i, slot):
+            """A chunk as device tensors (host chunks go through one staging buffer pair per slot)."""
+            if isinstance(k, torch.Tensor) and k.is_cuda:
+                return k.view(torch.uint64), i.view(torch.uint64)
+            k = torch.from_numpy(np.ascontiguousarray(k).view(np.int64)) if isinstance(k, np.ndarray) else k
+            i = torch.from_numpy(np.ascontiguousarray(i).view(np.int64)) if isinstance(i, np.ndarray) else i
+            if up[slot] is None or up[slot][0].numel() < k.numel():
+                up[slot] = (torch.empty(max(cap, k.numel()), dtype=torch.int64, device=dev),
+                            torch.empty(max(cap, k.numel()), dtype=torch.int64, device=dev))
+            uk, ui = up[slot]
+            uk[: k.numel()].copy_(k.view(torch.int64))
+            ui[: i.numel()].copy_(i.view(torch.int64))
+            self.h2d_bytes += 16 * k.numel()
+            return uk[: k.numel()].view(torch.uint64), ui[: i.numel()].view(torch.uint64)
+
+        # pass 1: partition sizes of the whole side
         counts = torch.zeros(P, dtype=torch.int64, device=dev)
-        for c0 in range(lo, total, cap):
-            cnt = min(cap, total - c0)
-            self._gen(pool, n, r, c0, cnt, gk, gi, sh, canon)
-            _lib.check(lib.cf_part_hist(dp(gk), cnt, Mp, self.pbits, dp(counts), sh), "cf_part_hist")
-            self.launches += 1
+        N = 0
+        for k, i in chunks():
+            k, i = on_device(k, i, 0)
+            if k.numel():
+                _lib.check(lib.cf_part_hist(dp(k), k.numel(), Mp, self.pbits, dp(counts), sh), "cf_part_hist")
+                self.launches += 1
+            N += k.numel()
         cnts = counts.cpu().numpy()
         off = np.zeros(P + 1, dtype=np.int64)
         off[1:] = np.cumsum(cnts)
+        assert off[-1] == N
         if out is not None and out[0].numel() >= N and out[1].numel() >= N:
             hk, hi_ = out
         else:
             hk, hi_ = self.host_buffers(N)
-        # pass 2: generate, partition on the device, copy each partition slice to its host
-        # offset on the copy stream; two staging sets, so chunk k+1 is generated and
-        # partitioned while chunk k is copied out
-        stage = [(torch.empty(cap, dtype=torch.uint64, device=dev), torch.empty(cap, dtype=torch.uint64, device=dev))
-                 for _ in range(2)]
+        # pass 2: partition each chunk on the device and copy each partition slice to its host
+        # offset on the copy stream; two staging sets, so chunk k+1 is produced and partitioned
+        # while chunk k is copied out
+        stage = [None, None]
         free = [torch.cuda.Event(), torch.cuda.Event()]
         for e in free:
             e.record()
         cur_host = off[:-1].copy()
         cstream = self.copy_stream
         comp = torch.cuda.current_stream(dev)
-        for k, c0 in enumerate(range(lo, total, cap)):
-            cnt = min(cap, total - c0)
-            sk, si = stage[k & 1]
-            self._gen(pool, n, r, c0, cnt, gk, gi, sh, canon)
+        for kk, (k, i) in enumerate(chunks()):
+            cnt = k.numel()
+            if cnt == 0:
+                continue
+            comp.wait_event(free[kk & 1])                           # this staging set was copied out
+            k, i = on_device(k, i, kk & 1)
+            if stage[kk & 1] is None or stage[kk & 1][0].numel() < cnt:
+                stage[kk & 1] = (torch.empty(max(cap, cnt), dtype=torch.uint64, device=dev),
+                                 torch.empty(max(cap, cnt), dtype=torch.uint64, device=dev))
+            sk, si = stage[kk & 1]
             pc = torch.zeros(P, dtype=torch.int64, device=dev)
-            _lib.check(lib.cf_part_hist(dp(gk), cnt, Mp, self.pbits, dp(pc), sh), "cf_part_hist")
+            _lib.check(lib.cf_part_hist(dp(k), cnt, Mp, self.pbits, dp(pc), sh), "cf_part_hist")
             loc = torch.zeros(P + 1, dtype=torch.int64, device=dev)
             loc[1:] = torch.cumsum(pc, 0)
             cursor = loc[:-1].clone()
-            comp.wait_event(free[k & 1])                            # this staging set was copied out
-            _lib.check(lib.cf_part_scatter(dp(gk), dp(gi), cnt, Mp, self.pbits, dp(cursor), dp(sk), dp(si), sh),
+            _lib.check(lib.cf_part_scatter(dp(k), dp(i), cnt, Mp, self.pbits, dp(cursor), dp(sk), dp(si), sh),
                        "cf_part_scatter")
             self.launches += 2
             ready = torch.cuda.Event()
@@ -168,8 +220,8 @@ class StreamedJoin:
                         hk[h:h + b - a].copy_(sk[a:b].view(torch.int64), non_blocking=True)
                         hi_[h:h + b - a].copy_(si[a:b].view(torch.int64), non_blocking=True)
                         cur_host[p] += b - a
-                free[k & 1] = torch.cuda.Event()
-                free[k & 1].record(cstream)
+                free[kk & 1] = torch.cuda.Event()
+                free[kk & 1].record(cstream)
             self.d2h_bytes += 16 * cnt
         cstream.synchronize()
         assert np.array_equal(cur_host, off[1:]), "partition sizes changed between the passes"

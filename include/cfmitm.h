@@ -351,17 +351,6 @@ size_t cf_merge_run_bytes(void);
 int cf_merge_join_runs(const uint64_t* Dk, uint64_t nD, const uint64_t* Ik, uint64_t nI, void* runs,
                        uint64_t max_runs, uint64_t* nruns, uint64_t* npairs, uint32_t* err, void* stream);
 
-/* ---- measurement helpers ------------------------------------------------ */
-
-/* Random 32-byte reads (two 16-byte loads) from `table` (2*(bucket_mask+1)
- * uint4 entries): blocks x 512 threads x iters reads; the ceiling of the fused
- * probe.  cf_micro_mulhi: blocks x 256 threads x iters x 8 64-bit Montgomery
- * products; the integer ceiling of generation.  Neither has a counterpart in
- * the reference (it has no measurement code). */
-int cf_micro_l2_probe(const void* table, uint64_t bucket_mask, int iters, uint32_t blocks, uint64_t* sink,
-                      void* stream);
-int cf_micro_mulhi(int iters, uint32_t blocks, uint64_t* sink, void* stream);
-
 #ifdef __cplusplus
 }
 #endif

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the REFERENCE itself.
 
-Runs only where the reference tree is present (default /root/reference, or
-$CF_REFERENCE_ROOT); the fixtures it writes are committed so that tests run
+Runs only where the reference tree is present ($CF_REFERENCE_ROOT, else
+oracle/build.py's default); the fixtures it writes are committed so that tests run
 without it.  Sources of truth, all the reference's own code:
 
   * gen_records: the CUDA kernel source string in gpu/mitm_gpu2.py:24-66,
@@ -16,8 +16,17 @@ without it.  Sources of truth, all the reference's own code:
     reference dumpers and a numpy join.
   * Known-answer record counts at M0 documented in INTERVAL_THEOREM.md:66-70
     (r = 4, 5, 6 re-counted here with the reference dumpers).
+  * The same M0 instances at every radius the reference's GPU driver path takes
+    (r = 4..13, the counts its record log gpu/records/M0_U539839443357/
+    D1768248177696000.log shows), re-run with the reference dumpers; the
+    records are streamed through an order-independent digest
+    (oracle.record_digest_add) because they reach 7.8e8 per side.
+  * The large-radius instance (pool 160, r = 7) cut to a product-bounded
+    sub-instance of 6.2e8 D and about 2e8 I records, joined from the reference
+    dumpers' records in numpy (config4_bounded).
 
-Usage: python tests/golden/make_golden.py [--quick]
+Usage: CF_REFERENCE_ROOT=<reference tree> python tests/golden/make_golden.py [--quick | --m0-large | --config4]
+(the reference tree defaults to oracle/build.py's REF_SRC).
 """
 from __future__ import annotations
 
@@ -35,11 +44,12 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("CF_REFERENCE_ROOT", "/root/reference")
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, ROOT)
 
 import build as obuild  # noqa: E402  oracle/build.py
+
+REF = obuild.REF_SRC
 from carmichael_frontier_b200 import workloads as W  # noqa: E402
 
 OUT = os.path.join(HERE, "golden.json")
@@ -248,7 +258,173 @@ def m0_kat(radii=(4, 5, 6)):
                             "9": [36755836, 652881611], "11": [6955830, 64758042]})
 
 
+def m0_bounds(r, M, U, B0, INSf, SPLIT):
+    """The driver's per-instance bounds (gpu/mitm_gpu_mstar_driver.py:84-98,188-205) at radius r:
+    (hmax, Icap exclusive, Dmin, affordable INS)."""
+    P0 = W.product(B0)
+    small = [p for p in INSf if p <= SPLIT]
+    large = [p for p in INSf if p > SPLIT]
+    Dmax = W.product(B0[-r:])
+    hmax = -1
+    for h in range(r + 1):
+        if h > len(large) or r - h > len(small):
+            continue
+        if P0 * W.product(small[:r - h]) * W.product(large[:h]) < U * Dmax:
+            hmax = h
+    topI = W.product(INSf[-r:])
+    Icap = max(1, min(topI + 1, (U * Dmax) // P0 + 1))
+    Dmin = (P0 * W.product(INSf[:r])) // U + 1
+    cap_r = (Icap - 1) // W.product(INSf[:r - 1])
+    return hmax, Icap, Dmin, [q for q in INSf if q <= cap_r]
+
+
+def stream_records(cmd, stdin: bytes, env=None, block=1 << 26):
+    """Run a reference dumper; fold its 16-byte stdout records into the order-independent digest.
+    Returns (records read, digest hex, TOTAL from stderr, exit code)."""
+    import oracle as O
+    with tempfile.TemporaryFile() as err:
+        p = subprocess.Popen([cmd], stdin=subprocess.PIPE, stdout=subprocess.PIPE, stderr=err, env=env)
+        p.stdin.write(stdin)
+        p.stdin.close()
+        acc, n, tail = (0, 0, 0), 0, b""
+        while True:
+            buf = p.stdout.read(block)
+            if not buf:
+                break
+            buf = tail + buf
+            cut = len(buf) - len(buf) % 16
+            tail = buf[cut:]
+            a = np.frombuffer(buf[:cut], dtype="<u8").reshape(-1, 2)
+            acc = O.record_digest_add(acc, a[:, 0], a[:, 1])
+            n += a.shape[0]
+        rc = p.wait()
+        err.seek(0)
+        lines = err.read().decode().splitlines()
+    assert not tail
+    tot = int([l for l in lines if l.startswith("TOTAL")][0].split()[1])
+    return n, O.record_digest_hex(acc), tot, rc
+
+
+def m0_kat_large(radii=range(4, 14), threads=8):
+    """M0 known-answer rows at radii 4..13 through the reference dumpers: counts and digests."""
+    M = 1768248177696000
+    U = int(json.load(open(os.path.join(REF, "results_k64_best_global_prev_148_539839443357.json")))["n"])
+    SPLIT = 4000
+    P = W.eligible_pool(M, 82177)
+    B0 = sorted(P)[:64]
+    INSf = sorted(p for p in P if p not in set(B0))
+    P0 = W.product(B0)
+    idump = os.path.join(ROOT, "oracle", "_ref", "mitm64_idump_stream2")
+    ddump = os.path.join(ROOT, "oracle", "_ref", "mitm64_ddump")
+    rows = []
+    for r in radii:
+        hmax, Icap, Dmin, INS = m0_bounds(r, M, U, B0, INSf, SPLIT)
+        assert Icap - 1 < 1 << 128 and hmax >= 0
+        ni, di, ti, rci = stream_records(idump, f"{M} {r} {P0 % M} {Icap} 1 {threads} 0\n64 {' '.join(map(str, B0))}\n"
+                                         f"{len(INS)} {' '.join(map(str, INS))}\n".encode(),
+                                         env=dict(os.environ, IDUMP_RANK="1", IDUMP_SPLIT=str(SPLIT),
+                                                  IDUMP_HMAX=str(hmax)))
+        nd, dd, td, rcd = stream_records(ddump, f"{M} {r} {Dmin}\n64 {' '.join(map(str, B0))}\n".encode())
+        assert rci == 0 and rcd == 0 and ni == ti and nd == td
+        rows.append(dict(r=r, hmax=hmax, n_ins=len(INS), Icap=str(Icap), Dmin=str(Dmin), i_records=ni,
+                         d_records=nd, i_digest=di, d_digest=dd,
+                         d_ids="mask" if r > 10 else "6-bit"))
+        print("m0 large", r, nd, ni, flush=True)
+    return dict(M=M, U=str(U), SPLIT=SPLIT, pool_cap=82177, B0=B0, INS_full=INSf, rows=rows,
+                digest="oracle.record_digest_add (sums mod 2^64 of key, id, ((key*C1)^id)*C2)")
+
+
+def unrank_colex_py(v, r, n):
+    """Colex rank -> ascending index tuple (gpu/mitm_gpu_mstar_driver.py:120-126)."""
+    v, idx, x = int(v), [], n - 1
+    for j in range(r - 1, -1, -1):
+        while math.comb(x, j + 1) > v:
+            x -= 1
+        idx.append(x)
+        v -= math.comb(x, j + 1)
+        x -= 1
+    return tuple(reversed(idx))
+
+
+def config4_bounded(target_i=200_000_000, threads=8):
+    """The large-radius instance (seed-0 modulus, pool of 160 primes, r = 7) cut to a product-bounded
+    sub-instance the reference's dumpers and a sorted join finish in minutes: every D (Dmin = 0, all
+    C(64, 7) = 6.2e8 records) against the I subsets with prod(I) < Icap, Icap chosen for about 2e8 I
+    records.  Reference: src/mitm64_ddump.cpp + src/mitm64_idump_stream2.cpp (IDUMP_RANK=1) and an
+    equal-key join in numpy, the method of gpu/validate_mitm_gpu2_pos.py:23-33."""
+    import oracle as O
+    w = W.config4(0)
+    M, r, B0, INS = w.M, w.r, list(w.B0), list(w.INS)
+    P0 = W.product(B0)
+    # a first guess from the product quantile of random r-subsets, then bisection on exact counts
+    # (each count enumerates about target_i subsets) to the smallest cap, within 0.1%, that
+    # admits at least target_i records
+    import random
+    rng = random.Random(4)
+    frac = target_i / math.comb(len(INS), r)
+    logs = sorted(sum(math.log(p) for p in rng.sample(INS, r)) for _ in range(200_000))
+    guess = int(math.exp(logs[int(frac * len(logs))]))
+    lo, hi = guess * 2 // 3, guess * 3 // 2
+    while O.idump_count(INS, r, M, P0, lo) >= target_i:
+        lo = lo * 2 // 3
+    while O.idump_count(INS, r, M, P0, hi) < target_i:
+        hi = hi * 3 // 2
+    while hi - lo > max(1, lo // 1000):
+        mid = (lo + hi) // 2
+        if O.idump_count(INS, r, M, P0, mid) >= target_i:
+            hi = mid
+        else:
+            lo = mid
+    Icap = hi
+    idump = os.path.join(ROOT, "oracle", "_ref", "mitm64_idump_stream2")
+    ddump = os.path.join(ROOT, "oracle", "_ref", "mitm64_ddump")
+    pi = subprocess.run([idump], input=f"{M} {r} {P0 % M} {Icap} 1 {threads} 0\n64 {' '.join(map(str, B0))}\n"
+                        f"{len(INS)} {' '.join(map(str, INS))}\n".encode(), capture_output=True,
+                        env=dict(os.environ, IDUMP_RANK="1"), check=True)
+    I = np.frombuffer(pi.stdout, dtype=np.uint64).reshape(-1, 2)
+    i_dig = O.record_digest_hex(O.record_digest_add((0, 0, 0), I[:, 0], I[:, 1]))
+    order = np.argsort(I[:, 0], kind="stable")
+    Ik, Iid = I[order, 0].copy(), I[order, 1].copy()
+    del I, order, pi
+    pd = subprocess.Popen([ddump], stdin=subprocess.PIPE, stdout=subprocess.PIPE)
+    pd.stdin.write(f"{M} {r} 0\n64 {' '.join(map(str, B0))}\n".encode())
+    pd.stdin.close()
+    acc, nd, pairs = (0, 0, 0), 0, []
+    while True:
+        buf = pd.stdout.read(1 << 28)
+        if not buf:
+            break
+        D = np.frombuffer(buf, dtype=np.uint64).reshape(-1, 2)
+        acc = O.record_digest_add(acc, D[:, 0], D[:, 1])
+        nd += D.shape[0]
+        a = np.searchsorted(Ik, D[:, 0], side="left")
+        b = np.searchsorted(Ik, D[:, 0], side="right")
+        for j in np.nonzero(b > a)[0]:
+            dd = sorted(B0[(int(D[j, 1]) >> (6 * q)) & 63] for q in range(r))
+            for t in range(a[j], b[j]):
+                ii = [INS[x] for x in unrank_colex_py(Iid[t], r, len(INS))]
+                pairs.append([dd, ii])
+    assert pd.wait() == 0
+    return dict(name=w.name, M=M, r=r, B0=B0, INS=INS, Icap=str(Icap), Dmin="0", i_records=int(len(Ik)),
+                d_records=nd, i_digest=i_dig, d_digest=O.record_digest_hex(acc), pairs=sorted(pairs))
+
+
 def main():
+    if "--config4" in sys.argv:
+        obuild.build_oracle()
+        obuild.build_reference()
+        gold = json.load(open(OUT))
+        gold["config4_bounded"] = config4_bounded()
+        json.dump(gold, open(OUT, "w"), indent=0)
+        print("wrote", OUT, gold["config4_bounded"]["i_records"], len(gold["config4_bounded"]["pairs"]))
+        return
+    if "--m0-large" in sys.argv:
+        obuild.build_reference()
+        gold = json.load(open(OUT))
+        gold["m0_kat_large"] = m0_kat_large()
+        json.dump(gold, open(OUT, "w"), indent=0)
+        print("wrote", OUT)
+        return
     quick = "--quick" in sys.argv
     obuild.build_oracle()
     obuild.build_reference()
@@ -281,6 +457,9 @@ def main():
     gold["positive_control"] = positive_control()
     print("positive control pairs", gold["positive_control"]["pairs"])
     gold["m0_kat"] = m0_kat((4, 5) if quick else (4, 5, 6))
+    if not quick:
+        gold["m0_kat_large"] = m0_kat_large()
+        gold["config4_bounded"] = config4_bounded()
     print("m0", [(x["r"], x["d_records"], x["i_records"]) for x in gold["m0_kat"]["rows"]])
     json.dump(gold, open(OUT, "w"), indent=0)
     print("wrote", OUT)

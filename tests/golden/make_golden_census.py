@@ -1,6 +1,8 @@
 """Golden rows of the divisor-family census and of its family runs (run here, where the reference
 tree exists).
 
+Run as: CF_REFERENCE_ROOT=<reference tree> python tests/golden/make_golden_census.py
+
 Runs the reference's own census (gpu/divisor_family_census.py, imported from the reference tree) for
 the incumbent of results_k64_best_global.json, checks that it reproduces the survivor rows the
 reference committed in gpu/divisor_family_lambdaJ.json, and writes them with the incumbent's size and
@@ -11,6 +13,12 @@ through gpu/mitm_gpu_mstar_driver.py) and keeps, per survivor, the base check an
 completions below U).  Finally it runs the reference's lambda-neighbourhood census
 (gpu/lambda_neighbourhood.py) for the seed M0 = 1768248177696000 with new primes up to 19 and writes its
 rows to tests/golden/nbhd_M0_p19.json.
+
+The second family is the one behind the reference's restricted-minimum theorem: the 111 survivor
+divisors of M0 = 1768248177696000 (gpu/mstar_divisor_family.json) searched below the previous
+148-digit incumbent, with run records in gpu/records/M0_U539839443357/ -- radii up to 14, among them
+M0 itself at r = 7..13 with 2.2e7-3.7e7 D and 6.5e7-7.8e8 I records per radius and 2-78 residue pairs.
+Those records are written, with the rows, to tests/golden/census_M0.json.
 """
 import glob
 import importlib.util
@@ -22,8 +30,27 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "census_lambdaJ.json")
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle"))
+import build as obuild  # noqa: E402  oracle/build.py: where the reference tree is
+
+REF = sys.argv[1] if len(sys.argv) > 1 else obuild.REF_SRC
+OUT = os.path.join(HERE, "census_lambdaJ.json")
+OUT_M0 = os.path.join(HERE, "census_M0.json")
+
+
+def m0_family():
+    """The M0 divisor family's survivor rows and the reference's run records of it."""
+    rows = json.load(open(os.path.join(REF, "gpu", "mstar_divisor_family.json")))
+    prev = json.load(open(os.path.join(REF, "results_k64_best_global_prev_148_539839443357.json")))
+    U = int(prev["n"])
+    runs = read_records(os.path.join(REF, "gpu", "records", "M0_U539839443357"), U)
+    key = lambda r: r["D"]
+    assert sorted(runs) == sorted(str(r["D"]) for r in rows), "records do not cover the survivors"
+    json.dump({"U": str(U), "M0": 1768248177696000, "survivors": sorted(rows, key=key), "runs": runs},
+              open(OUT_M0, "w"), indent=0)
+    n = sum(len(v["instances"]) for v in runs.values())
+    print("wrote", OUT_M0, len(rows), "rows", n, "instances")
 
 
 def main():
@@ -82,4 +109,10 @@ def read_records(folder, U):
 
 
 if __name__ == "__main__":
-    main()
+    if "--m0-only" in sys.argv:
+        sys.argv.remove("--m0-only")
+        REF = sys.argv[1] if len(sys.argv) > 1 else obuild.REF_SRC
+        m0_family()
+    else:
+        main()
+        m0_family()

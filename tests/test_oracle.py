@@ -102,3 +102,15 @@ def test_config2_fixture_consistency(golden):
         assert g["i_leaves"] == math.comb(len(w.INS), 5)
         assert g["d_res"] == g["d_leaves"]        # no D-residue collision: matches == all pairs
         assert g["matches"] == len(g["pairs"])
+
+
+def test_record_digest_device_form_equals_numpy_form():
+    # the GPU tests fold records with int64 tensor arithmetic; it must equal the uint64 numpy form
+    import torch
+    from test_gpu_kat_large import dev_digest_add
+    rng = np.random.default_rng(7)
+    k = rng.integers(0, 1 << 64, size=100_003, dtype=np.uint64)
+    i = rng.integers(0, 1 << 64, size=100_003, dtype=np.uint64)
+    want = O.record_digest_add(O.record_digest_add((0, 0, 0), k[:500], i[:500]), k[500:], i[500:])
+    got = dev_digest_add((0, 0, 0), torch.from_numpy(k.view(np.int64)), torch.from_numpy(i.view(np.int64)))
+    assert got == want
