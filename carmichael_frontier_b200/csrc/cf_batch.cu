@@ -71,6 +71,7 @@ __device__ __forceinline__ bool batch_ticket(const CfBatchMod& md, u32 mod, u64 
   st.X = hd->X0s;
   st.x2 = hd->x20;
   DTab tab;
+  tab.xb = 0;                  // wide side entries
   tab.nb = 1ull << md.bbits;
   tab.fpw = md.fpw;
   tab.side = md.side;
@@ -479,6 +480,7 @@ k_bfix(const CfBatchMod* __restrict__ mods, const CfOvf* __restrict__ ovf, const
     const CfOvf v = ovf[i];
     const CfBatchMod& md = mods[v.mod];
     DTab tab;
+    tab.xb = 0;                  // wide side entries
     tab.nb = 1ull << md.bbits;
     tab.fpw = md.fpw;
     tab.side = md.side;

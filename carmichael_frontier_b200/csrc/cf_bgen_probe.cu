@@ -68,6 +68,7 @@ extern "C" int cf_bgen_probe(int r, int n, u64 F, const void* pool, const u64* k
   }
   if (cc == 0) return CF_OK;
   DTab t;
+  t.xb = 0;                  // wide side entries
   t.nb = 1ull << bbits;
   t.fpw = (u32*)tab;
   t.side = (uint2*)((unsigned char*)tab + t.nb * 32);

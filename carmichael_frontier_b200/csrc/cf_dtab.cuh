@@ -3,12 +3,13 @@
 //
 // 2^bbits buckets of 16 slots.  A bucket's sixteen 16-bit fingerprints (0 =
 // empty) fill one 32-byte sector -- the only data a probe reads; a side array
-// holds, per slot, a second 32-bit fingerprint and the D rank (read only when
-// the 16-bit fingerprint matches); slots are claimed in order by compare-and-swap
-// on the fingerprint words, so "bucket full" is a test of the last slot, and a
-// full bucket continues into the next one.  (The per-bucket fill counters of the
-// layout are no longer used by the build.)  An optional blocked Bloom filter is a first
-// level for tables too large for L2.
+// holds, per slot, more fingerprint bits and the D rank (read only when the
+// 16-bit fingerprint matches).  Slots are claimed in order -- by a per-bucket
+// fill counter (the in-place single-modulus build) or by compare-and-swap on
+// the fingerprint words (record tables, batched in-place builds) -- so "bucket
+// full" is a test of the last slot, and a full bucket continues into the next
+// one.  An optional blocked Bloom filter is a first level for tables too large
+// for L2.
 #pragma once
 #include "cf_abi_internal.h"
 #include "cf_enum.cuh"
@@ -41,19 +42,32 @@ __device__ __forceinline__ void cf_fuse_res(CfElt32 q, const CfTailEnt& e, const
   x2 = ((u32)q.x2 * e.x2) & (u32)md.mask2;          // a <= 32 on this path
 }
 
-// D table: fp16[nb*16] (32 bytes per bucket), then side[nb*16] = {fp32, rank},
-// then the per-bucket fill counters used while building.  "D table" names the
-// structure; it holds whichever side of the join is smaller.
+// D table: fp16[nb*16] (32 bytes per bucket), then the side area (128 bytes per
+// bucket), then the per-bucket fill counters used while building.  "D table"
+// names the structure; it holds whichever side of the join is smaller.
+//
+// Two side formats.  Wide (xb = 0): side[nb*16] = {fp32, rank - rank0}, 8 bytes
+// per slot.  Compact (xb = 8, tables of at most 2^20 buckets, so at most 2^24
+// records): one 32-bit word per slot, (rank - rank0) << 8 | the low 8 bits of
+// the 32-bit fingerprint, at ((u32*)side)[b*16 + s] -- 64 bytes per bucket, half
+// the footprint, so that an in-place build of an L2-sized table keeps its side
+// words in L2 instead of evicting partly written sectors.  The 24 fingerprint
+// bits (16 + 8) leave about 2e-7 false candidates per probe at 7 records per
+// bucket; the exact pair check removes them.
 struct DTab {
   u32* fpw;       // fingerprint words: [nb * 8], two 16-bit fingerprints each
-  uint2* side;    // [nb * 16]: .x = 32-bit fingerprint, .y = rank - rank0
-  u32* fill;      // [nb]: slots claimed so far (build only)
+  uint2* side;    // wide: [nb * 16] {32-bit fingerprint, rank - rank0}; compact: [nb * 16] u32 words
+  u32* fill;      // [nb]: slots claimed so far (builds by fill counter)
   u32* bloom;     // optional first level: [2^fbits * 8] words (256-bit blocks), nullptr if off
   u64 nb;         // buckets (power of two)
   u64 rank0;      // first rank of the build
   int bbits;
   int fbits;
+  u32 xb;         // 0: wide side entries; 8: compact side words
 };
+
+constexpr u32 kCompactXb = 8;
+constexpr int kCompactMaxBbits = 20;
 
 // Blocked Bloom filter over the residues, for D tables too large for L2: a
 // 256-bit block (one 32-byte sector) per key, three bits set in it; a probe
@@ -126,6 +140,35 @@ __device__ __forceinline__ bool dtab_claim(const DTab& t, u64 b, u32 f16, uint2 
   return false;
 }
 
+// Fill a claimed slot s of bucket b: its 16-bit fingerprint (a 16-bit store into
+// the bucket's row) and its side entry in the table's format.
+__device__ __forceinline__ void dtab_place(const DTab& t, u64 b, u32 s, u32 f16, u32 f32, u32 rel) {
+  reinterpret_cast<unsigned short*>(t.fpw)[b * 16 + s] = (unsigned short)f16;
+  if (t.xb)
+    reinterpret_cast<u32*>(t.side)[b * 16 + s] = (rel << kCompactXb) | (f32 & ((1u << kCompactXb) - 1u));
+  else
+    t.side[b * 16 + s] = make_uint2(f32, rel);
+}
+
+// Claim by fill counter: slot s = atomicAdd(fill[b], 1) of bucket b (first_slot,
+// claimed by the caller) or, while s >= 16 (bucket full), of the next buckets.
+// Every claimed slot is written before the build ends, so when probes run the
+// occupied slots of a bucket are a prefix and "bucket full" is "last slot
+// occupied" -- the layout the probe expects.  Returns false if every bucket was
+// full.
+__device__ __forceinline__ bool dtab_claim_fill(const DTab& t, u64 b, u32 first_slot, u32 f16, u32 f32, u32 rel) {
+  u32 s = first_slot;
+  for (u64 tries = 0; tries < t.nb; ++tries) {
+    if (s < 16u) {
+      dtab_place(t, b, s, f16, f32, rel);
+      return true;
+    }
+    b = (b + 1) & (t.nb - 1);
+    s = atomicAdd(t.fill + b, 1u);
+  }
+  return false;
+}
+
 // Insert a residue (X, x2) with its rank; returns false if every bucket was full.
 __device__ __forceinline__ bool dtab_insert(const DTab& t, u64 X, u32 x2, u64 rank) {
   if (t.bloom) {
@@ -176,8 +219,14 @@ static __device__ __noinline__ void probe_slow(const DTab& t, u64 b, u32 f16, u3
       const u32 v = (row[s >> 1] >> (16 * (s & 1))) & 0xffffu;
       full &= (v != 0u);
       if (v == f16) {
-        const uint2 sd = t.side[b * 16 + s];
-        if (sd.x == f32) emit_pair(t.rank0 + sd.y, irank, o);
+        if (t.xb) {
+          const u32 w = reinterpret_cast<const u32*>(t.side)[b * 16 + s];
+          if ((w & ((1u << kCompactXb) - 1u)) == (f32 & ((1u << kCompactXb) - 1u)))
+            emit_pair(t.rank0 + (w >> kCompactXb), irank, o);
+        } else {
+          const uint2 sd = t.side[b * 16 + s];
+          if (sd.x == f32) emit_pair(t.rank0 + sd.y, irank, o);
+        }
       }
     }
     if (!full) return;

@@ -24,6 +24,7 @@ namespace {
 
 constexpr int kFuseBlock = 256;
 constexpr int kFuseSteps = 64;            // 32 x 64 = 2048 consecutive records per warp range
+constexpr int kBuildU = 4;                // build: records per lane whose slot claims are in flight together
 
 struct FuseSmem {
   size_t p32, binom, total;
@@ -56,7 +57,9 @@ __device__ __forceinline__ const u64* fuse_setup(const u64* __restrict__ pool, u
   return sb;
 }
 
-// MODE 0: insert every record of [lo, lo+count) into the D table.
+// MODE 0: insert every record of [lo, lo+count) into the D table, claiming slots
+//         by fill counter with kBuildU records per lane in flight (the build is
+//         bound by the latency of the claims, not by their number).
 // MODE 1: probe every record of [lo, lo+count) against the D table.
 template <int R, int MODE, bool BLOOM>
 __global__ void __launch_bounds__(kFuseBlock)
@@ -99,18 +102,56 @@ k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo
     CfTailWalker<R, B> w;
     w.init(lo + wbase, n, binom, ar, st, hd->tail_n);
     const u64 rank_base = lo + wbase + (u64)lane;
-    for (u32 off = 0; off < left; off += 32) {    // uniform across the warp
-      CfElt32 q = st;
-      u64 j;
-      int unused[R - B > 0 ? R - B : 1];
-      w.template step<false>(n, binom, ar, lane, q, j, unused);
-      if (off + (u32)lane < left) {
-        u64 X;
-        u32 x2;
-        cf_fuse_res(q, tail[j], ar.md, minv, X, x2);
-        if (MODE == 0) {
-          bad |= !dtab_insert(tab, X, x2, rank_base + off);
-        } else {
+    if constexpr (MODE == 0) {
+      for (u32 off = 0; off < left; off += 32u * kBuildU) {   // uniform across the warp
+        u32 bk[kBuildU], f16[kBuildU], f32[kBuildU], rel[kBuildU];
+        bool v[kBuildU];
+#pragma unroll
+        for (int u = 0; u < kBuildU; ++u) {
+          const u32 o = off + 32u * (u32)u;
+          v[u] = false;
+          if (o < left) {                        // uniform: the walker never steps past the range
+            CfElt32 q = st;
+            u64 j;
+            int unused[R - B > 0 ? R - B : 1];
+            w.template step<false>(n, binom, ar, lane, q, j, unused);
+            if (o + (u32)lane < left) {
+              u64 X;
+              u32 x2;
+              cf_fuse_res(q, tail[j], ar.md, minv, X, x2);
+              if (tab.bloom) {
+                const CfBloomKey bl = cf_bloom_key(X, x2, tab.fbits);
+                u32* blk = tab.bloom + (u64)bl.block * 8;
+                atomicOr(blk + bl.w0, bl.m0);
+                atomicOr(blk + bl.w1, bl.m1);
+                atomicOr(blk + bl.w2, bl.m2);
+              }
+              const CfFuseKey fk = cf_fuse_key(X, x2, tab.bbits);
+              bk[u] = fk.bucket;
+              f16[u] = fk.f16;
+              f32[u] = fk.f32;
+              rel[u] = (u32)(rank_base + o - tab.rank0);
+              v[u] = true;
+            }
+          }
+        }
+        u32 slot[kBuildU];
+#pragma unroll
+        for (int u = 0; u < kBuildU; ++u) slot[u] = v[u] ? atomicAdd(tab.fill + bk[u], 1u) : 16u;
+#pragma unroll
+        for (int u = 0; u < kBuildU; ++u)
+          if (v[u]) bad |= !dtab_claim_fill(tab, bk[u], slot[u], f16[u], f32[u], rel[u]);
+      }
+    } else {
+      for (u32 off = 0; off < left; off += 32) {    // uniform across the warp
+        CfElt32 q = st;
+        u64 j;
+        int unused[R - B > 0 ? R - B : 1];
+        w.template step<false>(n, binom, ar, lane, q, j, unused);
+        if (off + (u32)lane < left) {
+          u64 X;
+          u32 x2;
+          cf_fuse_res(q, tail[j], ar.md, minv, X, x2);
           if (BLOOM) {
             const CfBloomKey bk = cf_bloom_key(X, x2, tab.fbits);
             const uint4* blk = (const uint4*)(tab.bloom + (u64)bk.block * 8);
@@ -153,8 +194,9 @@ void dispatch_fused(int mode, const u64* pool, const CfTailEnt* tail, int n, u64
                   : launch_fused<R, 1>(pool, tail, n, lo, count, tab, pairs, max_pairs, npairs, err, grid, swap, st);
 }
 
-DTab make_tab(void* tab, int bbits, int fbits, u64 rank0) {
+DTab make_tab(void* tab, int bbits, int fbits, u64 rank0, int compact) {
   DTab t;
+  t.xb = compact ? kCompactXb : 0u;
   t.nb = 1ull << bbits;
   t.fpw = (u32*)tab;
   t.side = (uint2*)((unsigned char*)tab + t.nb * 32);
@@ -183,21 +225,27 @@ extern "C" size_t cf_dtab_fp_bytes(int bbits) {
   return ((size_t)1 << bbits) * 32;
 }
 
-// Build: insert the D-side records of ranks [lo, lo+count), count < 2^32.  The
-// caller zeroes the fingerprint array (the first cf_dtab_fp_bytes(bbits) bytes),
-// the fill counters (4 * 2^bbits bytes from offset 160 * 2^bbits) and the Bloom
-// filter (when fbits > 0) first.
-extern "C" int cf_dtab_build2(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count, void* tab,
-                              int bbits, int fbits, u32* err, void* stream) {
+// Build: insert the D-side records of ranks [lo, lo+count), count < 2^32, slots
+// claimed by fill counter.  side_format 0: wide side entries; 1: compact side
+// words (tables of at most 2^20 buckets; the probe must be told the same
+// format).  The caller zeroes the fingerprint array (the first
+// cf_dtab_fp_bytes(bbits) bytes), the fill counters (4 * 2^bbits bytes from
+// offset 160 * 2^bbits) and the Bloom filter (when fbits > 0) first.
+extern "C" int cf_dtab_build3(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count, void* tab,
+                              int bbits, int fbits, int side_format, u32* err, void* stream) {
   if (!pool_dev || !tail || !tab || !err || n < 1 || n > CF_MAX_POOL || r < 1 || r > CF_MAX_DISPATCH_R ||
-      bbits < 1 || bbits > 28) {
+      bbits < 1 || bbits > 28 || (side_format != 0 && side_format != 1)) {
     cf_set_error("cf_dtab_build: bad arguments%s", "");
     return CF_EBADARG;
   }
   if (count == 0) return CF_OK;
   if (count >= (1ull << 32)) { cf_set_error("cf_dtab_build: at most 2^32-1 D records per table%s", ""); return CF_EBADARG; }
   if (fbits < 0 || fbits > 26) { cf_set_error("cf_dtab_build: fbits must be 0..26%s", ""); return CF_EBADARG; }
-  const DTab t = make_tab(tab, bbits, fbits, lo);
+  if (side_format == 1 && (bbits > kCompactMaxBbits || count > (1ull << (32 - kCompactXb)))) {
+    cf_set_error("cf_dtab_build: compact side words need at most 2^20 buckets and 2^24 records%s", "");
+    return CF_EBADARG;
+  }
+  const DTab t = make_tab(tab, bbits, fbits, lo, side_format);
   int rc = CF_OK;
   CF_DISPATCH_R(r, dispatch_fused, 0, (const u64*)pool_dev, (const CfTailEnt*)tail, n, lo, count, t, nullptr, 0u,
                 nullptr, err, 0u, 0u, (cudaStream_t)stream, &rc);
@@ -206,29 +254,36 @@ extern "C" int cf_dtab_build2(const void* pool_dev, const void* tail, int n, int
   return CF_OK;
 }
 
+extern "C" int cf_dtab_build2(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count, void* tab,
+                              int bbits, int fbits, u32* err, void* stream) {
+  return cf_dtab_build3(pool_dev, tail, n, r, lo, count, tab, bbits, fbits, 0, err, stream);
+}
+
 extern "C" int cf_dtab_build(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count, void* tab,
                              int bbits, u32* err, void* stream) {
-  return cf_dtab_build2(pool_dev, tail, n, r, lo, count, tab, bbits, 0, err, stream);
+  return cf_dtab_build3(pool_dev, tail, n, r, lo, count, tab, bbits, 0, 0, err, stream);
 }
 
 // Probe: generate the records of ranks [lo, lo+count) of the probing side in
-// registers and append every candidate whose 32-bit fingerprints agree through
+// registers and append every candidate whose fingerprints agree through
 // *npairs (zeroed by the caller); cf_check_pairs then keeps the pairs whose
 // residues are equal.  tab_rank0: first rank of the table's build.  swap = 0:
 // the table holds D records and the I side probes; swap = 1: the table holds I
 // records and the D side probes (build on the smaller side).  Pairs are stored
-// as {D rank, I rank} either way.  grid: CTAs (0 = one per 16384 records).
-extern "C" int cf_fused_probe2(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count,
-                               const void* tab, int bbits, int fbits, u64 tab_rank0, int swap, void* pairs,
-                               u32 max_pairs, u32* npairs, u32* err, u32 grid, void* stream) {
+// as {D rank, I rank} either way.  side_format: the table's (as built).  grid:
+// CTAs (0 = one per 16384 records).
+extern "C" int cf_fused_probe3(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count,
+                               const void* tab, int bbits, int fbits, int side_format, u64 tab_rank0, int swap,
+                               void* pairs, u32 max_pairs, u32* npairs, u32* err, u32 grid, void* stream) {
   if (!pool_dev || !tail || !tab || !npairs || !err || (max_pairs && !pairs) || n < 1 || n > CF_MAX_POOL ||
-      r < 1 || r > CF_MAX_DISPATCH_R || bbits < 1 || bbits > 28 || (swap != 0 && swap != 1)) {
+      r < 1 || r > CF_MAX_DISPATCH_R || bbits < 1 || bbits > 28 || (swap != 0 && swap != 1) ||
+      (side_format != 0 && side_format != 1) || (side_format == 1 && bbits > kCompactMaxBbits)) {
     cf_set_error("cf_fused_probe: bad arguments%s", "");
     return CF_EBADARG;
   }
   if (count == 0) return CF_OK;
   if (fbits < 0 || fbits > 26) { cf_set_error("cf_fused_probe: fbits must be 0..26%s", ""); return CF_EBADARG; }
-  const DTab t = make_tab((void*)tab, bbits, fbits, tab_rank0);
+  const DTab t = make_tab((void*)tab, bbits, fbits, tab_rank0, side_format);
   int rc = CF_OK;
   CF_DISPATCH_R(r, dispatch_fused, 1, (const u64*)pool_dev, (const CfTailEnt*)tail, n, lo, count, t,
                 (CfPair*)pairs, max_pairs, npairs, err, grid, (u32)swap, (cudaStream_t)stream, &rc);
@@ -237,9 +292,16 @@ extern "C" int cf_fused_probe2(const void* pool_dev, const void* tail, int n, in
   return CF_OK;
 }
 
+extern "C" int cf_fused_probe2(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count,
+                               const void* tab, int bbits, int fbits, u64 tab_rank0, int swap, void* pairs,
+                               u32 max_pairs, u32* npairs, u32* err, u32 grid, void* stream) {
+  return cf_fused_probe3(pool_dev, tail, n, r, lo, count, tab, bbits, fbits, 0, tab_rank0, swap, pairs, max_pairs,
+                         npairs, err, grid, stream);
+}
+
 extern "C" int cf_fused_probe(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count,
                               const void* tab, int bbits, u64 d_rank0, void* pairs, u32 max_pairs, u32* npairs,
                               u32* err, u32 grid, void* stream) {
-  return cf_fused_probe2(pool_dev, tail, n, r, lo, count, tab, bbits, 0, d_rank0, 0, pairs, max_pairs, npairs, err,
-                         grid, stream);
+  return cf_fused_probe3(pool_dev, tail, n, r, lo, count, tab, bbits, 0, 0, d_rank0, 0, pairs, max_pairs, npairs,
+                         err, grid, stream);
 }

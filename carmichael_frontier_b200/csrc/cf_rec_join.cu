@@ -15,6 +15,7 @@ namespace {
 
 DTab rec_tab(void* tab, int bbits, int fbits) {
   DTab t;
+  t.xb = 0;                  // wide side entries
   t.nb = 1ull << bbits;
   t.fpw = (u32*)tab;
   t.side = (uint2*)((unsigned char*)tab + t.nb * 32);

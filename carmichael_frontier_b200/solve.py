@@ -335,6 +335,9 @@ class Solver:
         pshape = None
         if tu.part_build and not plan.get("no_part") and nb >= tu.part_min_buckets and r <= lib.cf_batch_max_r():
             pshape = part_shape(bcount, bbits, tu.part_lb, tu.part_sigma, lib.cf_batch_part_max_ranges())
+        # in-place builds of tables of at most 2^20 buckets use compact side words (half the side area,
+        # L2-resident while built); partitioned builds and larger tables the wide entries
+        side_format = 1 if pshape is None and bbits <= 20 else 0
         self._mark(marks, "start")
         if pshape is not None:
             tables = self._tables_for(inst)
@@ -344,15 +347,15 @@ class Solver:
         else:
             # the build side's tables first: the table build runs while the host prepares the other side
             bpool, btail = self._side_tables(inst, bside)
-            ck(lib.cf_dtab_build2(dp(bpool), dp(btail), bn, r, 0, bcount, dp(tab), bbits, fbits, dp(misc) + 4, sh),
-               "cf_dtab_build")
+            ck(lib.cf_dtab_build3(dp(bpool), dp(btail), bn, r, 0, bcount, dp(tab), bbits, fbits, side_format,
+                                  dp(misc) + 4, sh), "cf_dtab_build")
             ppool, ptail = self._side_tables(inst, pside)
             screen = self.tables.screen(inst.P0, inst.B, 1e-6)
             poolD, poolI = (bpool, ppool) if bside == "D" else (ppool, bpool)
         ppool, ptail = dp(ppool), dp(ptail)
         self._mark(marks, "gen_D")
-        ck(lib.cf_fused_probe2(ppool, ptail, pn, r, 0, pcount, dp(tab), bbits, fbits, 0, int(swap), dp(pairs),
-                               maxp, dp(misc), dp(misc) + 4, self.tuning.fused_grid, sh), "cf_fused_probe")
+        ck(lib.cf_fused_probe3(ppool, ptail, pn, r, 0, pcount, dp(tab), bbits, fbits, side_format, 0, int(swap),
+                               dp(pairs), maxp, dp(misc), dp(misc) + 4, self.tuning.fused_grid, sh), "cf_fused_probe")
         self._mark(marks, "probe")
         ck(lib.cf_check_pairs(dp(poolD), dp(poolI), dp(screen), r, dp(pairs), dp(misc), maxp, dp(res),
                               dp(misc) + 4, sh), "cf_check_pairs")

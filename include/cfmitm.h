@@ -153,9 +153,10 @@ int cf_join_part(const void* D, const uint32_t* dcount, uint32_t capD, const voi
  * D table: 2^bbits buckets of 16 slots, cf_dtab_bytes(bbits) bytes: first an
  * array of 32-byte fingerprint sectors (16 16-bit fingerprints per bucket, the
  * one sector a probe reads; cf_dtab_fp_bytes(bbits) bytes, L2-resident for
- * r <= 5), then per slot a second 32-bit fingerprint and the D rank, then a
- * 4-byte fill counter per bucket.  Before building, the caller zeroes the
- * fingerprint array and the fill counters (the last 4 * 2^bbits bytes).
+ * r <= 5), then a side area of 128 bytes per bucket (per slot more
+ * fingerprint bits and the D rank), then a 4-byte fill counter per bucket.
+ * Before building, the caller zeroes the fingerprint array and the fill
+ * counters (the last 4 * 2^bbits bytes).
  * cf_dtab_build inserts the D records of ranks [lo, lo+count), count < 2^32;
  * cf_fused_probe generates the I records of ranks [lo, lo+count) in
  * registers, probes the table and appends every {D rank, I rank} candidate
@@ -182,6 +183,19 @@ int cf_fused_probe2(const void* pool_dev, const void* tail, int n, int r, uint64
                     uint32_t max_pairs, uint32_t* npairs, uint32_t* err, uint32_t grid, void* stream);
 int cf_dtab_build(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count, void* tab,
                   int bbits, uint32_t* err, void* stream);
+/* The same with the side area's format chosen: side_format 0 = wide (per slot a
+ * 32-bit fingerprint and the rank, 8 bytes; what the variants above build and
+ * probe), 1 = compact (per slot one 32-bit word, rank << 8 | 8 more
+ * fingerprint bits; tables of at most 2^20 buckets and 2^24 records).  The
+ * compact side of an L2-sized table stays in L2 while it is built, so its
+ * sectors are written back whole once.  Build and probe must be given the same
+ * format. */
+int cf_dtab_build3(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count, void* tab,
+                   int bbits, int fbits, int side_format, uint32_t* err, void* stream);
+int cf_fused_probe3(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count,
+                    const void* tab, int bbits, int fbits, int side_format, uint64_t tab_rank0, int swap,
+                    void* pairs, uint32_t max_pairs, uint32_t* npairs, uint32_t* err, uint32_t grid,
+                    void* stream);
 int cf_fused_probe(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count,
                    const void* tab, int bbits, uint64_t d_rank0, void* pairs, uint32_t max_pairs,
                    uint32_t* npairs, uint32_t* err, uint32_t grid, void* stream);

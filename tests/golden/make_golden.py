@@ -356,19 +356,13 @@ def config4_bounded(target_i=200_000_000, threads=8):
     w = W.config4(0)
     M, r, B0, INS = w.M, w.r, list(w.B0), list(w.INS)
     P0 = W.product(B0)
-    # a first guess from the product quantile of random r-subsets, then bisection on exact counts
-    # (each count enumerates about target_i subsets) to the smallest cap, within 0.1%, that
-    # admits at least target_i records
-    import random
-    rng = random.Random(4)
-    frac = target_i / math.comb(len(INS), r)
-    logs = sorted(sum(math.log(p) for p in rng.sample(INS, r)) for _ in range(200_000))
-    guess = int(math.exp(logs[int(frac * len(logs))]))
-    lo, hi = guess * 2 // 3, guess * 3 // 2
-    while O.idump_count(INS, r, M, P0, lo) >= target_i:
-        lo = lo * 2 // 3
+    # grow the cap from the smallest product by factors of 1.5 while the exact count (which costs
+    # time in proportion to itself) stays below target_i, then bisect to the smallest cap, within
+    # 0.1%, that admits at least target_i records
+    lo = W.product(INS[:r])
+    hi = lo * 3 // 2
     while O.idump_count(INS, r, M, P0, hi) < target_i:
-        hi = hi * 3 // 2
+        lo, hi = hi, hi * 3 // 2
     while hi - lo > max(1, lo // 1000):
         mid = (lo + hi) // 2
         if O.idump_count(INS, r, M, P0, mid) >= target_i:
@@ -397,11 +391,17 @@ def config4_bounded(target_i=200_000_000, threads=8):
         D = np.frombuffer(buf, dtype=np.uint64).reshape(-1, 2)
         acc = O.record_digest_add(acc, D[:, 0], D[:, 1])
         nd += D.shape[0]
-        a = np.searchsorted(Ik, D[:, 0], side="left")
-        b = np.searchsorted(Ik, D[:, 0], side="right")
-        for j in np.nonzero(b > a)[0]:
+        od = np.argsort(D[:, 0], kind="stable")       # sorted queries: each search starts where the last ended
+        ks = D[od, 0]
+        a = np.searchsorted(Ik, ks, side="left")
+        hit = a < len(Ik)
+        hit[hit] = Ik[a[hit]] == ks[hit]
+        for jj in np.nonzero(hit)[0]:
+            j = od[jj]
+            b = np.searchsorted(Ik, ks[jj], side="right")
+            a_j = a[jj]
             dd = sorted(B0[(int(D[j, 1]) >> (6 * q)) & 63] for q in range(r))
-            for t in range(a[j], b[j]):
+            for t in range(a_j, b):
                 ii = [INS[x] for x in unrank_colex_py(Iid[t], r, len(INS))]
                 pairs.append([dd, ii])
     assert pd.wait() == 0
