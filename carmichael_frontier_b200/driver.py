@@ -138,6 +138,34 @@ def run_instance(tag, B0, INS, r: int, hmax: int, M: int, U: int, split: int, co
     return True
 
 
+def join_stream(D_chunks, blocks, device=None):
+    """Join sorted D chunks (build_D's) with I records arriving as host blocks -- a dumper's
+    stream read by records.DumperRun -- as the reference driver does for its idump path
+    (gpu/mitm_gpu_mstar_driver.py:249-262): each block is copied to the device, sorted with
+    sort_side and joined against every D chunk with join_sorted.  Returns (D id array, I id
+    array) of all equal-key pairs (numpy uint64) and the I records read."""
+    import numpy as np
+    import torch
+
+    from . import mitm_gpu2 as G
+    dev = torch.device(device if device is not None else "cuda")
+    pd_all, pi_all, n = [], [], 0
+    for a in blocks:
+        n += a.shape[0]
+        if a.shape[0] == 0 or not D_chunks:
+            continue
+        k = torch.from_numpy(np.ascontiguousarray(a[:, 0]).view(np.int64)).to(dev).view(torch.uint64)
+        i = torch.from_numpy(np.ascontiguousarray(a[:, 1]).view(np.int64)).to(dev).view(torch.uint64)
+        ks, is_ = G.sort_side(k, i)
+        for Dk, Did in D_chunks:
+            pd, pi = G.join_sorted(Dk, Did, ks, is_)
+            if pd.numel():
+                pd_all.append(pd.view(torch.int64).cpu().numpy().view(np.uint64))
+                pi_all.append(pi.view(torch.int64).cpu().numpy().view(np.uint64))
+    cat = lambda xs: np.concatenate(xs) if xs else np.zeros(0, np.uint64)  # noqa: E731
+    return cat(pd_all), cat(pi_all), n
+
+
 def decode_pair(B0, INS, r: int, d_colex: int, i_colex: int):
     """(D primes, I primes) of a pair of colex ids (the ids the bounded producers emit)."""
     B0s = sorted(B0)
