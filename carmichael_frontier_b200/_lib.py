@@ -103,9 +103,29 @@ SIGNATURES = [
     ("cf_sort_pairs", C.c_int, [vp, vp, u64, C.c_int, vp, sz, vp]),
     ("cf_sort_pairs_noalloc_max", u64, []),
     ("cf_sort_pairs_noalloc", C.c_int, [vp, vp, u64, C.c_int, vp]),
+    ("cf_join_tmp_bytes", sz, [u64]),
+    ("cf_join_count", C.c_int, [vp, u64, vp, u64, vp, sz, vp, vp]),
+    ("cf_join_emit", C.c_int, [vp, vp, u64, vp, vp, u64, vp, vp, vp, u64, vp]),
+    ("cf_igen_bounds_bytes", sz, [C.c_int, C.c_int]),
+    ("cf_igen_bounds", C.c_int, [vp, C.c_int, C.c_int, u64, u64, vp, sz]),
+    ("cf_igen_tmp_bytes", sz, [u64]),
+    ("cf_igen_count", C.c_int, [vp, vp, u64, u64, C.c_int, C.c_int, C.c_int, C.c_int, vp, sz, vp, vp, vp, vp]),
+    ("cf_igen_write", C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, vp, u64, u64, vp, vp, vp]),
+    ("cf_solve_batch", C.c_int, [vp, vp]),
     ("cf_merge_run_bytes", sz, []),
     ("cf_merge_join_runs", C.c_int, [vp, u64, vp, u64, vp, u64, vp, vp, vp, vp]),
 ]
+
+class CfBatchQueue(C.Structure):
+    """include/cfmitm.h CfBatchQueue: one prepared batch for cf_solve_batch."""
+    _fields_ = [("mods", vp), ("arena", vp), ("zero_bytes", u64), ("misc", vp), ("build_tickets", vp),
+                ("probe_tickets", vp), ("place_tickets", vp), ("scatter_tickets", vp), ("scatter_radius", vp),
+                ("ovf", vp), ("pairs", vp), ("pair_mods", vp), ("results", vp), ("nmod", u32), ("ticket", u32),
+                ("grid", u32), ("max_pairs", u32), ("ovf_cap", u32), ("n_scatter", u32), ("use_part", C.c_int),
+                ("part_lb", C.c_int)]
+
+
+assert C.sizeof(CfBatchQueue) == 136
 
 _lib = None
 _lock = threading.Lock()

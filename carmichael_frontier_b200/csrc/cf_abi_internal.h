@@ -30,3 +30,25 @@ static inline int cf_cuda_status(cudaError_t e, const char* where) {
     if (_e != cudaSuccess) return cf_cuda_status(_e, where); \
   } while (0)
 #endif
+
+// One prepared batch for cf_solve_batch.  The same layout is declared with
+// <stdint.h> types in include/cfmitm.h (CfBatchQueue); keep the two in step.
+struct CfBatchQueue {
+  const void* mods;                    // device CfBatchMod[nmod]
+  void* arena;                         // device table areas; the first zero_bytes are zeroed
+  u64 zero_bytes;
+  void* misc;                          // device, 64 bytes: queue heads, pair count, error word
+  const u64* build_tickets;            // device ticket prefix sums [nmod + 1] of the table builds
+  const u64* probe_tickets;            // ... of the probes
+  const u64* place_tickets;            // partitioned build: range placement tickets
+  const u64* const* scatter_tickets;   // host array [n_scatter] of device ticket prefix sums
+  const int* scatter_radius;           // host array [n_scatter]: the radius of each scatter launch
+  void* ovf;                           // device overflow records of the partitioned build
+  void* pairs;                         // device candidate pairs (16 bytes each)
+  void* pair_mods;                     // device u32 modulus index of each candidate
+  void* results;                       // device check results (cf_pair_result_bytes() each)
+  u32 nmod, ticket, grid, max_pairs;
+  u32 ovf_cap, n_scatter;
+  int use_part, part_lb;
+};
+static_assert(sizeof(CfBatchQueue) == 136, "CfBatchQueue layout");

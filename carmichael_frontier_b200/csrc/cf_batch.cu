@@ -647,3 +647,58 @@ extern "C" int cf_batch_part(int phase, const void* mods, const u64* tstart, u32
   CF_LAUNCH_CHECK("cf_batch_part");
   return CF_OK;
 }
+
+// ---------------------------------------------------------------------------
+// cf_solve_batch: the whole device sequence of one prepared batch in one call
+// (the per-instance loop of gpu/mitm_gpu_mstar_driver.py:296-320 that the
+// batch replaces): zero the arena's table prefix and the queue words, then --
+// when the batch builds some tables partitioned -- the scatter per radius, the
+// range placement and the overflow fix-up, then the table builds, the probes
+// and the exact checks.  Every launch goes to `stream` without a host wait, so
+// the call can be recorded into a CUDA graph and replayed.
+// ---------------------------------------------------------------------------
+extern "C" int cf_solve_batch(const CfBatchQueue* q, void* stream) {
+  if (!q || !q->mods || !q->misc || q->nmod == 0 || !q->build_tickets || !q->probe_tickets || !q->pairs ||
+      !q->pair_mods || !q->results || (q->zero_bytes && !q->arena) ||
+      (q->use_part && (!q->place_tickets || !q->ovf || (q->n_scatter && (!q->scatter_tickets || !q->scatter_radius))))) {
+    cf_set_error("cf_solve_batch: bad arguments%s", "");
+    return CF_EBADARG;
+  }
+  const cudaStream_t st = (cudaStream_t)stream;
+  unsigned char* m = (unsigned char*)q->misc;
+  // misc: +0 build queue, +8 probe queue, +16 npairs, +20 err, +24 overflow count, +32 scatter queue,
+  // +40 range queue
+  cudaError_t e = q->zero_bytes ? cudaMemsetAsync(q->arena, 0, q->zero_bytes, st) : cudaSuccess;
+  if (e == cudaSuccess) e = cudaMemsetAsync(m, 0, 64, st);
+  if (e != cudaSuccess) return cf_cuda_status(e, "cf_solve_batch: zero");
+  u32* npairs = (u32*)(m + 16);
+  u32* err = (u32*)(m + 20);
+  u32* novf = (u32*)(m + 24);
+  int rc = CF_OK;
+  if (q->use_part) {
+    for (u32 i = 0; i < q->n_scatter && rc == CF_OK; ++i) {
+      if (i) {
+        e = cudaMemsetAsync(m + 32, 0, 8, st);          // the scatter queue head, for the next radius
+        if (e != cudaSuccess) return cf_cuda_status(e, "cf_solve_batch: zero");
+      }
+      rc = cf_batch_part(0, q->mods, q->scatter_tickets[i], q->nmod, m + 32, nullptr, 0, novf, err, q->part_lb,
+                         q->scatter_radius[i], 0, stream);
+    }
+    if (rc == CF_OK)
+      rc = cf_batch_part(1, q->mods, q->place_tickets, q->nmod, m + 40, q->ovf, q->ovf_cap, novf, err, q->part_lb, 0,
+                         0, stream);
+    if (rc == CF_OK)
+      rc = cf_batch_part(2, q->mods, nullptr, q->nmod, nullptr, q->ovf, q->ovf_cap, novf, err, q->part_lb, 0, 0,
+                         stream);
+    if (rc != CF_OK) return rc;
+  }
+  rc = cf_batch_run(0, q->mods, q->build_tickets, q->nmod, q->ticket, m, q->pairs, (u32*)q->pair_mods, q->max_pairs,
+                    npairs, err, nullptr, q->grid, stream);
+  if (rc == CF_OK)
+    rc = cf_batch_run(1, q->mods, q->probe_tickets, q->nmod, q->ticket, m + 8, q->pairs, (u32*)q->pair_mods,
+                      q->max_pairs, npairs, err, nullptr, q->grid, stream);
+  if (rc == CF_OK)
+    rc = cf_batch_run(2, q->mods, nullptr, q->nmod, 0, nullptr, q->pairs, (u32*)q->pair_mods, q->max_pairs, npairs,
+                      err, q->results, 0, stream);
+  return rc;
+}

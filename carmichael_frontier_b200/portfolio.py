@@ -310,40 +310,28 @@ class BatchSolver:
 
     # -- running -------------------------------------------------------------
     def _enqueue(self, b: _Batch, maxp: int):
-        lib, dp, ck = self.lib, _lib.ptr, _lib.check
+        """Queue the batch's whole device sequence with one cf_solve_batch call."""
+        import ctypes as C
+        lib, dp = self.lib, _lib.ptr
         arena = self._bufs["arena"]
         misc = self._buf("misc", 64)
         ovf = self._buf("ovf", tu_ovf_bytes(self))
         pairs = self._buf("pairs", maxp * 16)
         pmod = self._buf("pmod", maxp * 4)
         res = self._buf("res", maxp * self.result_bytes)
-        sh = self._sh()
         tu = self.tuning
-        arena[: b.zero_bytes].zero_()
-        misc.zero_()
-        # misc: +0 build queue, +8 probe queue, +16 npairs, +20 err, +24 overflow count,
-        # +32 scatter queue, +40 range queue (partitioned build)
-        m = dp(misc)
-        nmod = len(b.idx)
         part = b.use_part and b.n_part > 0
-        if part:
-            oc = self.tuning.ovf_capacity
-            lb = self.tuning.part_lb
-            for i, (rr, ts) in enumerate(sorted(b.tsS.items())):
-                if i:
-                    misc[32:40].zero_()         # the scatter queue head, for the next radius
-                ck(lib.cf_batch_part(0, dp(b.mods), dp(ts), nmod, m + 32, None, 0, m + 24, m + 20, lb, rr, 0, sh),
-                   "cf_batch_part(scatter)")
-            ck(lib.cf_batch_part(1, dp(b.mods), dp(b.tsP), nmod, m + 40, dp(ovf), oc, m + 24, m + 20, lb, 0, 0,
-                                 sh), "cf_batch_part(place)")
-            ck(lib.cf_batch_part(2, dp(b.mods), None, nmod, None, dp(ovf), oc, m + 24, m + 20, lb, 0, 0, sh),
-               "cf_batch_part(fix)")
-        ck(lib.cf_batch_run(0, dp(b.mods), dp(b.tsD if part else b.tsD_all), nmod, tu.ticket, m, dp(pairs), dp(pmod),
-                            maxp, m + 16, m + 20, None, tu.grid, sh), "cf_batch_run(build)")
-        ck(lib.cf_batch_run(1, dp(b.mods), dp(b.tsI), nmod, tu.ticket, m + 8, dp(pairs), dp(pmod), maxp, m + 16,
-                            m + 20, None, tu.grid, sh), "cf_batch_run(probe)")
-        ck(lib.cf_batch_run(2, dp(b.mods), None, nmod, 0, None, dp(pairs), dp(pmod), maxp, m + 16, m + 20, dp(res),
-                            0, sh), "cf_batch_run(check)")
+        scat = sorted(b.tsS.items()) if part else []
+        s_ptrs = (C.c_void_p * max(1, len(scat)))(*[dp(ts) for _, ts in scat])
+        s_rad = (C.c_int * max(1, len(scat)))(*[int(rr) for rr, _ in scat])
+        q = _lib.CfBatchQueue(
+            mods=dp(b.mods), arena=dp(arena), zero_bytes=b.zero_bytes, misc=dp(misc),
+            build_tickets=dp(b.tsD if part else b.tsD_all), probe_tickets=dp(b.tsI),
+            place_tickets=dp(b.tsP) if part else None, scatter_tickets=C.addressof(s_ptrs),
+            scatter_radius=C.addressof(s_rad), ovf=dp(ovf), pairs=dp(pairs), pair_mods=dp(pmod), results=dp(res),
+            nmod=len(b.idx), ticket=tu.ticket, grid=tu.grid, max_pairs=maxp, ovf_cap=tu.ovf_capacity,
+            n_scatter=len(scat), use_part=int(part), part_lb=tu.part_lb)
+        _lib.check(lib.cf_solve_batch(C.byref(q), self._sh()), "cf_solve_batch")
 
     def _launch(self, b: _Batch, maxp: int, graphs: bool):
         torch = self.torch

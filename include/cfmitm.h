@@ -241,6 +241,25 @@ int cf_bgen_expand(int side, int d, int r, int n, uint64_t F, const void* pool, 
                    const uint64_t* offs, const uint32_t* xs, int split_idx, int bitmask, uint64_t c0, uint64_t cc,
                    uint64_t* okey, uint64_t* oalo, uint64_t* oahi, uint64_t* oid, uint32_t* ometa, void* stream);
 
+/* The bounded I side in two calls, as gpu/igen_gpu.py:113-162 counts and then
+ * writes its records: cf_igen_bounds computes the bound table H on the host
+ * (exact 128-bit, cf_igen_bounds_bytes(n, r) bytes; upload it); cf_igen_count
+ * expands the levels in the caller's workspace (pool_dev = cf_pool_prepare(ins,
+ * n, r, M, mult = P0 mod M) on the device) and returns the record count and a
+ * 64-byte host state, or CF_ENOMEM with the node count a level needs (size the
+ * retry with cf_igen_tmp_bytes); cf_igen_write writes records [c0, c0+cc) of
+ * the counted frontier, in src/mitm64_idump_stream2.cpp's order (colex ids).
+ * split_idx = n and hmax = r impose no stratum.  Moduli below 2^64. */
+size_t cf_igen_bounds_bytes(int n, int r);
+int cf_igen_bounds(const uint64_t* ins, int n, int r, uint64_t icap_lo, uint64_t icap_hi, void* out,
+                   size_t out_bytes);
+size_t cf_igen_tmp_bytes(uint64_t max_nodes);
+int cf_igen_count(const void* pool_dev, const void* bounds_dev, uint64_t M, uint64_t mult, int n, int r,
+                  int split_idx, int hmax, void* tmp, size_t tmp_bytes, uint64_t* total, uint64_t* need_nodes,
+                  void* state, void* stream);
+int cf_igen_write(const void* pool_dev, int n, int r, int split_idx, const void* tmp, const void* state,
+                  uint64_t c0, uint64_t cc, uint64_t* keys, uint64_t* ids, void* stream);
+
 /* Hash join of two materialised sides of {canonical key} records (the bounded
  * producers' output): cf_rec_build inserts the smaller side's keys into a table
  * of cf_dtab_bytes2(bbits, fbits) bytes (zeroed as for cf_dtab_build2);
@@ -336,6 +355,35 @@ int cf_batch_part(int phase, const void* mods, const uint64_t* tstart, uint32_t 
                   uint32_t ovf_cap, uint32_t* novf, uint32_t* err, int part_lb, int radius, uint32_t grid,
                   void* stream);
 
+/* One prepared batch (the descriptors, ticket sums and buffers a portfolio's
+ * prepare step lays out) and the call that runs it: zero the table areas and
+ * queue words, the partitioned builds (scatter per radius, range placement,
+ * overflow fix-up) when use_part, then cf_batch_run's build, probe and check --
+ * every launch on `stream`, with no host wait, so the call can be recorded in a
+ * CUDA graph.  misc (64 bytes): +0 build queue, +8 probe queue, +16 candidate
+ * count (u32), +20 error word (u32), +24 overflow count, +32 scatter queue,
+ * +40 range queue.  Replaces the reference's per-instance loop
+ * (gpu/mitm_gpu_mstar_driver.py:296-320). */
+typedef struct CfBatchQueue {
+  const void* mods;
+  void* arena;
+  uint64_t zero_bytes;
+  void* misc;
+  const uint64_t* build_tickets;
+  const uint64_t* probe_tickets;
+  const uint64_t* place_tickets;
+  const uint64_t* const* scatter_tickets;
+  const int* scatter_radius;
+  void* ovf;
+  void* pairs;
+  void* pair_mods;
+  void* results;
+  uint32_t nmod, ticket, grid, max_pairs;
+  uint32_t ovf_cap, n_scatter;
+  int use_part, part_lb;
+} CfBatchQueue;
+int cf_solve_batch(const CfBatchQueue* q, void* stream);
+
 /* ---- sorted-side drop-ins ------------------------------------------------ */
 
 /* Stable LSD radix sort of (keys, ids)[n] by key over key_bits bits, in place;
@@ -356,6 +404,18 @@ int cf_sort_pairs(uint64_t* keys, uint64_t* ids, uint64_t n, int key_bits, void*
  * reference. */
 uint64_t cf_sort_pairs_noalloc_max(void);
 int cf_sort_pairs_noalloc(uint64_t* keys, uint64_t* ids, uint64_t n, int key_bits, void* stream);
+
+/* The equal-key join of sorted Dk[nD] and sorted Ik[nI] with the pairs written
+ * on the device in join_sorted's order (I rows in order, D positions in order
+ * within a row; gpu/mitm_gpu2.py:107-119).  cf_join_count leaves per-row
+ * offsets in tmp (cf_join_tmp_bytes(nI) bytes) and the pair total in the device
+ * u64 *npairs; cf_join_emit then writes {Did, Iid} of the first max_pairs pairs
+ * to outD, outI. */
+size_t cf_join_tmp_bytes(uint64_t nI);
+int cf_join_count(const uint64_t* Dk, uint64_t nD, const uint64_t* Ik, uint64_t nI, void* tmp, size_t tmp_bytes,
+                  uint64_t* npairs, void* stream);
+int cf_join_emit(const uint64_t* Dk, const uint64_t* Did, uint64_t nD, const uint64_t* Ik, const uint64_t* Iid,
+                 uint64_t nI, const void* tmp, uint64_t* outD, uint64_t* outI, uint64_t max_pairs, void* stream);
 
 /* Equal-key runs between sorted Dk[nD] and sorted Ik[nI]: runs (24 bytes each,
  * {I row, first D position, count}), unordered, counted in the device u64

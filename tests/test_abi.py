@@ -167,3 +167,39 @@ def test_unrank_rank_lex_round_trip():
             assert tables.rank_lex(idx, n) == rank
     assert tables.unrank_lex(0, 10, 3) == (0, 1, 2)
     assert tables.unrank_lex(math.comb(10, 3) - 1, 10, 3) == (7, 8, 9)
+
+
+def test_igen_bound_table_equals_the_python_definition():
+    from carmichael_frontier_b200.bounded import _u128_pairs, quotient_table
+    lib = _lib.load()
+    rng = random.Random(5)
+    for _ in range(20):
+        n = rng.randint(3, 60)
+        r = rng.randint(1, min(n, 9))
+        INS = sorted(rng.sample(range(3, 50_000, 2), n))
+        Icap = rng.choice([1, 2, math.prod(INS[:r]), math.prod(INS[-r:]) + 1, (1 << 128) - 5, rng.randrange(1 << 100)])
+        nb = lib.cf_igen_bounds_bytes(n, r)
+        out = np.zeros(nb, dtype=np.uint8)
+        ins = np.asarray(INS, dtype=np.uint64)
+        _lib.check(lib.cf_igen_bounds(ins.ctypes.data, n, r, Icap & (2 ** 64 - 1), Icap >> 64, out.ctypes.data, nb),
+                   "cf_igen_bounds")
+        want = _u128_pairs(quotient_table(INS, r, Icap))
+        assert np.array_equal(out.view(np.uint64), want), (n, r, Icap)
+    bad = np.asarray([5, 3], dtype=np.uint64)
+    assert lib.cf_igen_bounds(bad.ctypes.data, 2, 1, 100, 0, out.ctypes.data, 64) == _lib.CF_EBADARG
+
+
+def test_named_entry_points_reject_bad_arguments_without_gpu():
+    lib = _lib.load()
+    assert lib.cf_join_count(None, 1, None, 1, None, 0, None, None) == _lib.CF_EBADARG
+    assert lib.cf_join_emit(None, None, 1, None, None, 1, None, None, None, 1, None) == _lib.CF_EBADARG
+    assert lib.cf_igen_count(None, None, 10, 1, 5, 2, 5, 2, None, 0, None, None, None, None) == _lib.CF_EBADARG
+    st = np.zeros(64, dtype=np.uint8)
+    assert lib.cf_igen_write(st.ctypes.data, 5, 2, 5, st.ctypes.data, st.ctypes.data, 0, 1, None, None, None) \
+        == _lib.CF_EBADARG                      # a state that cf_igen_count did not write
+    assert lib.cf_solve_batch(None, None) == _lib.CF_EBADARG
+    q = _lib.CfBatchQueue()
+    assert lib.cf_solve_batch(C.byref(q), None) == _lib.CF_EBADARG
+    assert lib.cf_igen_tmp_bytes(1 << 20) > lib.cf_igen_tmp_bytes(1 << 10) > 0
+    assert lib.cf_join_tmp_bytes(1000) >= 16 * 1000
+    assert lib.cf_dtab_build3(None, None, 5, 2, 0, 10, None, 10, 0, 1, None, None) == _lib.CF_EBADARG
