@@ -548,13 +548,83 @@ def measure_portfolio(dev, args, compact: bool = False) -> dict:
     return out
 
 
+def init_dist(dev):
+    """NCCL process group for torchrun launches (None for one process)."""
+    import datetime
+    import torch.distributed as dist
+    _, world, _ = dist_env()
+    if world == 1:
+        return None
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    return dist
+
+
+def run_portfolio_sharded(args, dev, dist):
+    """The portfolio split by modulus over the ranks (carmichael_frontier_b200.shard: balanced by
+    records, no data-path collective): each rank runs its share as one batch; the time is the max
+    over ranks of the device-timed batch, the value the whole portfolio's moduli over it."""
+    import torch
+    from carmichael_frontier_b200 import shard, workloads as W
+    from carmichael_frontier_b200.portfolio import BatchSolver
+    from carmichael_frontier_b200.solve import Instance
+    rank, world, _ = dist_env()
+    lim = args.i_limit
+    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config3(args.moduli)]
+    weights = [math.comb(len(x.B0), x.r) + min(math.comb(len(x.INS), x.r), lim) for x in insts]
+    mine = shard.assign(weights, world)[rank]
+    bs = BatchSolver(dev)
+    prep = bs.prepare([insts[i] for i in mine], lim)
+    clocks = ClockSampler(gpu_uuid(torch, dev))
+    clocks.start()
+    for _ in range(args.warmup):
+        bs.run(prep, graphs=True)
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    times = []
+    for _ in range(args.steps):
+        dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = bs.run(prep, graphs=True)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        t = torch.tensor([e0.elapsed_time(e1) / 1e3], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        times.append(float(t.item()))
+    clk = clocks.stop()
+    recs = torch.tensor([float(prep.records)], dtype=torch.float64, device=dev)
+    dist.all_reduce(recs, op=dist.ReduceOp.SUM)
+    g = [None] * world
+    dist.all_gather_object(g, [(i, x.residue_pairs, len(x.hits)) for i, x in zip(mine, res)])
+    t_b = statistics.median(times)
+    if rank == 0:
+        per = sorted(y for part in g for y in part)
+        line = {"metric": "portfolio moduli solved/s (batched persistent kernels)", "value": len(insts) / t_b,
+                "unit": "moduli/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * t_b, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "u64", "data": "synthetic (seeded moduli)",
+                "config": {"workload": "portfolio_1024_k64_r456", "moduli": len(insts), "i_limit": lim,
+                           "records": float(recs.item()), "parallelism": f"modulus-sharded x{world}",
+                           "sample": f"full D sides, I ranks [0, {lim}) per modulus"},
+                "records_per_s": float(recs.item()) / t_b, "moduli_solved": len(per),
+                "residue_pairs": sum(p for _, p, _ in per), "hits": sum(h for _, _, h in per),
+                "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"],
+                           "samples": clk["samples"]}}
+        print(json.dumps(line), flush=True)
+
+
 def run_portfolio(args):
     import torch
     rank, world, local = dist_env()
-    if rank != 0:
-        return
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if world > 1:
+        dist = init_dist(dev)
+        try:
+            run_portfolio_sharded(args, dev, dist)
+        finally:
+            dist.destroy_process_group()
+        return
     p = measure_portfolio(dev, args)
     line = {"metric": "portfolio moduli solved/s (batched persistent kernels)", "value": p["batched"]["moduli_per_s"],
             "unit": "moduli/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -646,10 +716,15 @@ def run_census(args):
     from carmichael_frontier_b200 import census as C
     from carmichael_frontier_b200.solve import Solver, Tuning
     rank, world, local = dist_env()
-    if rank != 0:
-        return
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if world > 1:
+        dist = init_dist(dev)
+        try:
+            run_census_sharded(args, dev, dist)
+        finally:
+            dist.destroy_process_group()
+        return
     gold = os.path.join(ROOT, "tests", "golden")
     with open(os.path.join(gold, "census_lambdaJ.json")) as f:
         fam = json.load(f)
@@ -696,6 +771,51 @@ def run_census(args):
                                  "instances_per_s": n2 / t_nb, "records_per_s": recs2 / t_nb,
                                  "completions_below_U": len(hits2)},
         "clocks": clk}))
+
+
+def run_census_sharded(args, dev, dist):
+    """The incumbent's divisor family (the census workload's first part) split by modulus over the
+    ranks: each rank runs its rows' family runs; instances are checked against the reference's
+    records on rank 0; the time is the max over ranks."""
+    import torch
+    from carmichael_frontier_b200 import census as C, shard
+    from carmichael_frontier_b200.solve import Solver, Tuning
+    rank, world, _ = dist_env()
+    with open(os.path.join(ROOT, "tests", "golden", "census_lambdaJ.json")) as f:
+        fam = json.load(f)
+    U = int(fam["U"])
+    rows = fam["survivors"]
+    weights = [sum(x["nD"] + x["nI"] for x in fam["runs"][str(r["D"])]["instances"]) + 1000 for r in rows]
+    s = Solver(dev, tuning=Tuning(strategy="bounded"))
+    C.family_run(rows[:3], U, r_max=3, solver=s)                # warm-up: tables, buffers
+    clocks = ClockSampler(gpu_uuid(torch, dev))
+    clocks.start()
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+
+    def solve_share(rws):
+        out, _hits = C.family_run(rws, U, r_max=10, solver=s)
+        return [out[r["D"]] for r in rws]
+    res, _mine = shard.run_sharded(rows, weights, solve_share)
+    torch.cuda.synchronize(dev)
+    t = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    clk = clocks.stop()
+    if rank == 0:
+        n_inst = sum(len(x["instances"]) for x in res)
+        same = all(x["instances"] == [y for y in fam["runs"][str(r["D"])]["instances"]
+                                      if y["r"] in {z["r"] for z in x["instances"]}] for r, x in zip(rows, res))
+        tt = float(t.item())
+        print(json.dumps({
+            "metric": "census family instances/s (bounded runs below the incumbent U)", "value": n_inst / tt,
+            "unit": "instances/s", "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": 1e3 * tt,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u128 products, u64 keys",
+            "data": "the reference's incumbent U (148 digits) and its census",
+            "config": {"workload": "census_lambdaJ_family_r1-10", "survivors": len(rows),
+                       "parallelism": f"modulus-sharded x{world}"},
+            "family": {"instances": n_inst, "same_as_reference_records": same, "s": tt},
+            "clocks": clk}), flush=True)
 
 
 # ------------------------------------------------------------------ large radius (r = 7, pool 160)

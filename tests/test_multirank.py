@@ -1,6 +1,10 @@
-"""The multi-GPU path on the CPU: two gloo ranks shard moduli the way `bench.py --gpus N`
-does (no data-path collective), reduce time by max and records by sum, and gather the
-per-modulus results -- which must equal the single-process results."""
+"""The multi-GPU path on the CPU: two gloo ranks run the product's sharding code.
+
+carmichael_frontier_b200.shard assigns moduli to ranks and gathers the per-modulus results (the
+only collectives besides the max-over-ranks of the device time); bench.py's step schedule gives each
+rank its own moduli.  Here each rank solves its share with the CPU oracle in place of its GPU (the
+only part that needs a device), and the gathered results must equal a single-process run, in input
+order, with every modulus solved exactly once."""
 import datetime
 import os
 import socket
@@ -25,13 +29,24 @@ def _small():
     from carmichael_frontier_b200 import workloads as W
     rng = random.Random(5)
     out = []
-    for j in range(6):
+    for j in range(7):
         M = W.draw_modulus(700 + j)
         Q = W.eligible_pool(M, 5518)
         k = rng.randint(8, 14)
         Qs = Q[: k + rng.randint(3, 20)]
         out.append((M, Qs, Qs[:k], rng.randint(1, 3), W.product(Qs[:k]) * 10 ** 6))
     return out
+
+
+def _solve_on_this_rank(items):
+    import oracle as O
+    return [sorted((tuple(D), tuple(I)) for D, I in O.solve_exhaustive(M, Q, B0, r, B)[0])
+            for M, Q, B0, r, B in items]
+
+
+def _weights(items):
+    import math
+    return [math.comb(len(B0), r) + math.comb(len(Q) - len(B0), r) for _, Q, B0, r, _ in items]
 
 
 def _rank(rank, world, port, out):
@@ -44,23 +59,34 @@ def _rank(rank, world, port, out):
     import torch.distributed as dist
 
     import bench
-    import oracle as O
+    from carmichael_frontier_b200 import shard
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
         sched = [w.name for w in bench.step_seeds(5, world, rank)]
-        mine = _small()[rank::world]                       # this rank's moduli
-        res = [(M, sorted((tuple(D), tuple(I)) for D, I in O.solve_exhaustive(M, Q, B0, r, B)[0]))
-               for M, Q, B0, r, B in mine]
+        items = _small()
+        res, mine = shard.run_sharded(items, _weights(items), _solve_on_this_rank)
         t = torch.tensor([0.5 + rank], dtype=torch.float64)   # per-rank "device seconds"
         n = torch.tensor([1000.0 * (rank + 1)], dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.all_reduce(n, op=dist.ReduceOp.SUM)
         g = [None] * world
-        dist.all_gather_object(g, (sched, res))
-        if rank == 0:
-            out.put((float(t.item()), float(n.item()), g))
+        dist.all_gather_object(g, (sched, mine))
+        out.put((rank, float(t.item()), float(n.item()), g, res))
     finally:
         dist.destroy_process_group()
+
+
+def test_assignment_is_balanced_and_covers_every_item_once():
+    import sys
+    sys.path.insert(0, ROOT)
+    from carmichael_frontier_b200 import shard
+    w = [5, 1, 1, 1, 1, 1, 3, 2, 8, 1]
+    for world in (1, 2, 3, 4, 16):
+        sh = shard.assign(w, world)
+        assert sorted(i for s in sh for i in s) == list(range(len(w)))
+        loads = [sum(w[i] for i in s) for s in sh]
+        assert max(loads) - min(loads) <= max(w)
+        assert sh == shard.assign(w, world)                 # every rank computes the same shares
 
 
 @pytest.mark.timeout(600)
@@ -69,25 +95,27 @@ def test_two_gloo_ranks_shard_moduli():
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import bench
-    import oracle as O
+    from carmichael_frontier_b200 import shard
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _port()
     procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
     for p in procs:
         p.start()
-    tmax, nsum, gathered = q.get(timeout=500)
+    got = sorted(q.get(timeout=500) for _ in range(2))
     for p in procs:
         p.join(60)
         assert p.exitcode == 0
-    assert tmax == 1.5 and nsum == 3000.0                 # max over ranks, sum over ranks
-    s0, s1 = gathered[0][0], gathered[1][0]
-    # every step gives each rank a different modulus; together they are the two-rank schedule
-    assert len(s0) == len(s1) == 5 and all(a != b for a, b in zip(s0, s1))
-    both = [w.name for w in bench.step_seeds(5, 2, 0)] + [w.name for w in bench.step_seeds(5, 2, 1)]
-    assert sorted(both) == sorted(s0 + s1)
-    # the sharded results are the single-process results
-    sharded = {M: pairs for _, res in gathered for M, pairs in res}
-    for M, Q, B0, r, B in _small():
-        want = sorted((tuple(D), tuple(I)) for D, I in O.solve_exhaustive(M, Q, B0, r, B)[0])
-        assert sharded[M] == want
+    items = _small()
+    want = _solve_on_this_rank(items)                     # one process, every modulus
+    for rank, tmax, nsum, gathered, res in got:
+        assert tmax == 1.5 and nsum == 3000.0             # max over ranks, sum over ranks
+        assert res == want                                # every rank holds all results, in input order
+        s0, s1 = gathered[0][0], gathered[1][0]
+        # every step gives each rank a different modulus; together they are the two-rank schedule
+        assert len(s0) == len(s1) == 5 and all(a != b for a, b in zip(s0, s1))
+        both = [w.name for w in bench.step_seeds(5, 2, 0)] + [w.name for w in bench.step_seeds(5, 2, 1)]
+        assert sorted(both) == sorted(s0 + s1)
+        m0, m1 = gathered[0][1], gathered[1][1]           # each modulus solved by exactly one rank
+        assert sorted(m0 + m1) == list(range(len(items))) and not set(m0) & set(m1)
+        assert (m0, m1) == tuple(shard.assign(_weights(items), 2))
