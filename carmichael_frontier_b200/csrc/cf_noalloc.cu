@@ -16,7 +16,9 @@
 //  * n <= CF_NOALLOC_MAX_RECORDS (131072 records); larger n is rejected.
 //  * The first call on a device looks up the array's device address on that
 //    device (cudaGetSymbolAddress, with that device current); make that first
-//    call before any stream capture on the device.
+//    call before any stream capture on the device.  The address is kept for the
+//    life of the process, so it goes stale if the caller resets the device
+//    (cudaDeviceReset); the entry point is not for use after a reset.
 //  * All calls share the one scratch array and it keeps whatever the last call
 //    left there; the parts that must start at zero are cleared on every call.
 //    Calls whose device work overlaps (different streams, or different host

@@ -399,7 +399,10 @@ int cf_sort_pairs(uint64_t* keys, uint64_t* ids, uint64_t n, int key_bits, void*
  * held by every GPU that loads the library).  n is limited to
  * cf_sort_pairs_noalloc_max() = 131072 records; larger n returns CF_EBADARG.
  * The first call on a device looks up the array's address on that device
- * (make it before any stream capture).  Calls share the array: device work of
+ * (make it before any stream capture) and keeps it for the life of the process:
+ * after cudaDeviceReset on that device the kept address is stale, so do not use
+ * this entry point after a reset.  Like cf_sort_pairs it waits on `stream` once
+ * (it reads the digit histogram back).  Calls share the array: device work of
  * two calls must not overlap.  This entry point has no counterpart in the
  * reference. */
 uint64_t cf_sort_pairs_noalloc_max(void);
