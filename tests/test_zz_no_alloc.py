@@ -21,7 +21,7 @@ def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint64).view(np.int64)).cuda()
 
 
-@pytest.mark.parametrize("key_bits", [64, 62, 16])
+@pytest.mark.parametrize("key_bits", [64, 24, 16])      # 8, 3 and 2 digit passes
 def test_noalloc_sort_equals_workspace_sort_on_two_calls(cuda, key_bits):
     lib = _lib.load()
     limit = lib.cf_sort_pairs_noalloc_max()
