@@ -166,20 +166,21 @@ def cpu_model() -> str:
 
 def cpu_sample(w, cores: int, seconds: float):
     """Bounded sample of one modulus for the CPU engine: the r-subsets of the nb largest base
-    primes against those of the n' smallest insertion primes.  mitm64 builds its D side on one
-    thread before its I threads start (src/mitm64.cpp:50-71, 137-140), so nb is chosen to keep that
-    build near D_BUILD_SHARE of the step (~4M D leaves/s on one core) and n' to fill the rest of
-    `seconds` at ~4M I leaves/s per core."""
+    primes against those of the n' smallest insertion primes.  n' fills `seconds` at ~4M I leaves/s
+    per core (all of the pool when it is smaller); mitm64 builds its D side on one thread before its
+    I threads start (src/mitm64.cpp:50-71, 137-140), so nb is then chosen to keep that build near
+    D_BUILD_SHARE of the step (~2.5M D leaves/s on one core)."""
     r = w.r
     base, ins = sorted(w.B0), list(w.INS)
-    d_budget = max(10_000, int(D_BUILD_SHARE * seconds * 4.0e6))
-    nb = r
-    while nb < len(base) and math.comb(nb + 1, r) <= d_budget:
-        nb += 1
     i_budget = max(1_000_000, int((1 - D_BUILD_SHARE) * seconds * 4.0e6 * cores))
     n2 = r
     while n2 < len(ins) and math.comb(n2 + 1, r) <= i_budget:
         n2 += 1
+    i_seconds = math.comb(n2, r) / (4.0e6 * cores)
+    d_budget = max(10_000, int(D_BUILD_SHARE / (1 - D_BUILD_SHARE) * i_seconds * 2.5e6))
+    nb = r
+    while nb < len(base) and math.comb(nb + 1, r) <= d_budget:
+        nb += 1
     return base[-nb:], ins[:n2]
 
 

@@ -112,6 +112,10 @@ SIGNATURES = [
     ("cf_igen_count", C.c_int, [vp, vp, u64, u64, C.c_int, C.c_int, C.c_int, C.c_int, vp, sz, vp, vp, vp, vp]),
     ("cf_igen_write", C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, vp, u64, u64, vp, vp, vp]),
     ("cf_solve_batch", C.c_int, [vp, vp]),
+    ("cf_ddump_bounds_bytes", sz, [C.c_int, C.c_int]),
+    ("cf_ddump_bounds", C.c_int, [vp, C.c_int, C.c_int, u64, u64, vp, sz]),
+    ("cf_bounded_join", C.c_int, [vp, vp, C.c_int, vp, vp, C.c_int, C.c_int, u64, u64, C.c_int, C.c_int, C.c_int,
+                                  C.c_int, vp, sz, vp, u64, vp, vp, vp, vp]),
     ("cf_merge_run_bytes", sz, []),
     ("cf_merge_join_runs", C.c_int, [vp, u64, vp, u64, vp, u64, vp, vp, vp, vp]),
 ]

@@ -90,6 +90,9 @@ class BoundedSolve:
         self.torch = solver.torch
         self.lib = solver.lib
         self.gen = BoundedGenerator(solver.device, max_nodes=solver.tuning.max_nodes)
+        self.native = True                  # one C call per instance (cf_bounded_join) where it applies
+        self._native_bytes = 256 << 20
+        self._native_out = 1 << 12
 
     def _table(self, keys, n: int, plan: dict):
         from .solve import dtab_shape
@@ -145,7 +148,75 @@ class BoundedSolve:
         with self.torch.cuda.stream(self.s._torch_stream()):
             return self._join_on_stream(inst, Icap, Dmin, split, hmax)
 
+    NATIVE_MAX_BYTES = 24 << 30     # one-call joins whose workspace would exceed this take the level loop here
+
+    def _join_native(self, inst, Icap, Dmin, split, hmax):
+        """The whole instance through cf_bounded_join (one C call: D records, table, I leaves probed,
+        candidates back); None when the instance is outside its limits (modulus of 2^64 or more, caps
+        of 2^128 or more, a workspace above NATIVE_MAX_BYTES), which the level loop below handles."""
+        import ctypes as C
+        torch, lib, dp = self.torch, self.lib, _lib.ptr
+        r, M = inst.r, inst.M
+        B0, INS = list(inst.B0), list(inst.INS)
+        if wide_modulus(M) or Icap - 1 >= U128 or Dmin >= U128 or Icap <= 1 or len(B0) < r or len(INS) < r:
+            return None
+        nb, ni = len(B0), len(INS)
+        g = self.gen
+        poolD = g.tables.pool(B0, r, M, 1)
+        poolI = g.tables.pool(INS, r, M, inst.P0 % M)
+
+        def host_table(fn, primes, bound):
+            n = len(primes)
+            nbytes = lib.cf_igen_bounds_bytes(n, r)
+            out = np.zeros(nbytes, dtype=np.uint8)
+            pr = np.asarray(primes, dtype=np.uint64)
+            _lib.check(fn(pr.ctypes.data, n, r, bound & (2 ** 64 - 1), bound >> 64, out.ctypes.data, nbytes), "bounds")
+            return out
+        G = g.tables.get(("ddumpGc", tuple(B0), r, int(Dmin)), lambda: host_table(lib.cf_ddump_bounds, B0, int(Dmin)))
+        H = g.tables.get(("igenHc", tuple(INS), r, int(Icap)), lambda: host_table(lib.cf_igen_bounds, INS, int(Icap)))
+        split_idx = ni if split is None else next((i for i, p in enumerate(INS) if p > split), ni)
+        hmax = r if hmax is None else int(hmax)
+        if hmax < 0:
+            return None
+        sh = self.s._sh()
+        n_out, need = C.c_uint64(0), C.c_uint64(0)
+        sizes = (C.c_uint64 * 2)()
+        while True:
+            nbytes = self._native_bytes
+            tmp = self.s._buf("bjoin", nbytes)
+            out = np.zeros(3 * self._native_out, dtype=np.uint64)
+            rc = lib.cf_bounded_join(dp(poolD), dp(G), nb, dp(poolI), dp(H), ni, r, M, inst.P0 % M, split_idx, hmax,
+                                     0, 0, dp(tmp), nbytes, out.ctypes.data, self._native_out, C.byref(n_out), sizes,
+                                     C.byref(need), sh)
+            if rc == _lib.CF_ENOMEM:
+                grow = max(2 * nbytes, need.value + need.value // 4)
+                if grow > self.NATIVE_MAX_BYTES:
+                    return None
+                self._native_bytes = grow
+                continue
+            if rc == _lib.CF_EOVERFLOW and n_out.value > self._native_out:
+                self._native_out = 2 * n_out.value
+                continue
+            _lib.check(rc, "cf_bounded_join")
+            break
+        g.launches += 4 * r + 4
+        nD, nI, k = int(sizes[0]), int(sizes[1]), int(n_out.value)
+        mo = self._native_out
+        did, dkey, iid = out[:k], out[mo:mo + k], out[2 * mo:2 * mo + k]
+        P0m = inst.P0 % M
+        pairs = []
+        for j in range(k):
+            ii = unrank_colex(int(iid[j]), r, ni)
+            if (P0m * math.prod(INS[x] for x in ii)) % M != int(dkey[j]):
+                continue                       # fingerprint collision, not an equal-residue pair
+            pairs.append((unrank_colex(int(did[j]), r, nb), ii))
+        return pairs, nD, nI, dict(strategy="bounded", Icap=Icap, Dmin=Dmin, table="D", native=True)
+
     def _join_on_stream(self, inst, Icap, Dmin, split, hmax):
+        if self.native:
+            got = self._join_native(inst, Icap, Dmin, split, hmax)
+            if got is not None:
+                return got
         torch, lib, dp = self.torch, self.lib, _lib.ptr
         r, M = inst.r, inst.M
         plan = dict(strategy="bounded", Icap=Icap, Dmin=Dmin)

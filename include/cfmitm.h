@@ -260,6 +260,28 @@ int cf_igen_count(const void* pool_dev, const void* bounds_dev, uint64_t M, uint
 int cf_igen_write(const void* pool_dev, int n, int r, int split_idx, const void* tmp, const void* state,
                   uint64_t c0, uint64_t cc, uint64_t* keys, uint64_t* ids, void* stream);
 
+/* One product-bounded exchange instance in one call (the device part of the
+ * reference driver's run_instance, gpu/mitm_gpu_mstar_driver.py:184-286):
+ * cf_ddump_bounds computes the D side's bound table G (exact 128-bit,
+ * cf_ddump_bounds_bytes(n, r) bytes; upload it); cf_bounded_join then expands
+ * the D side (prod >= Dmin, colex ids), builds a record table of it, expands the
+ * I side (prod < Icap, at most hmax primes at indices >= split_idx) to its last
+ * inner level, probes every leaf in registers and returns in out (host,
+ * 3 * max_out u64: D colex ids | D keys | I colex ids) the candidates -- the
+ * equal-key pairs and rare fingerprint collisions, which the caller drops by
+ * recomputing the I key -- and sizes[2] = {nD, nI}.  poolD = cf_pool_prepare(B0,
+ * nb, r, M, 1), poolI = cf_pool_prepare(INS, ni, r, M, P0 mod M), both on the
+ * device; bbits = 0 picks the table shape.  CF_ENOMEM: retry with at least
+ * *need bytes of workspace; CF_EOVERFLOW with *n_out > max_out: retry with a
+ * larger out.  Moduli below 2^64, caps below 2^128.  Waits on `stream` once per
+ * level. */
+size_t cf_ddump_bounds_bytes(int n, int r);
+int cf_ddump_bounds(const uint64_t* b, int n, int r, uint64_t dmin_lo, uint64_t dmin_hi, void* out, size_t out_bytes);
+int cf_bounded_join(const void* poolD, const void* boundsD, int nb, const void* poolI, const void* boundsI, int ni,
+                    int r, uint64_t M, uint64_t p0_mod_m, int split_idx, int hmax, int bbits, int fbits, void* tmp,
+                    size_t tmp_bytes, uint64_t* out, uint64_t max_out, uint64_t* n_out, uint64_t* sizes,
+                    uint64_t* need, void* stream);
+
 /* Hash join of two materialised sides of {canonical key} records (the bounded
  * producers' output): cf_rec_build inserts the smaller side's keys into a table
  * of cf_dtab_bytes2(bbits, fbits) bytes (zeroed as for cf_dtab_build2);

@@ -203,3 +203,24 @@ def test_named_entry_points_reject_bad_arguments_without_gpu():
     assert lib.cf_igen_tmp_bytes(1 << 20) > lib.cf_igen_tmp_bytes(1 << 10) > 0
     assert lib.cf_join_tmp_bytes(1000) >= 16 * 1000
     assert lib.cf_dtab_build3(None, None, 5, 2, 0, 10, None, 10, 0, 1, None, None) == _lib.CF_EBADARG
+
+
+def test_ddump_bound_table_equals_the_python_definition():
+    from carmichael_frontier_b200.bounded import _u128_pairs, dmin_table
+    lib = _lib.load()
+    rng = random.Random(6)
+    for _ in range(20):
+        n = rng.randint(3, 64)
+        r = rng.randint(1, min(n, 10))
+        B = sorted(rng.sample(range(3, 5_000, 2), n))
+        Dmin = rng.choice([0, 1, math.prod(B[:r]), math.prod(B[-r:]), math.prod(B[-r:]) + 1,
+                           rng.randrange(1, 1 << 100)])
+        nb = lib.cf_ddump_bounds_bytes(n, r)
+        out = np.zeros(nb, dtype=np.uint8)
+        b = np.asarray(B, dtype=np.uint64)
+        _lib.check(lib.cf_ddump_bounds(b.ctypes.data, n, r, Dmin & (2 ** 64 - 1), Dmin >> 64, out.ctypes.data, nb),
+                   "cf_ddump_bounds")
+        want = _u128_pairs(dmin_table(B, r, Dmin)).reshape(r, n, 2)
+        got = out.view(np.uint64).reshape(r, n, 2)
+        for t in range(r):                              # entries x < t are never read
+            assert np.array_equal(got[t, t:], want[t, t:]), (n, r, Dmin, t)
