@@ -126,10 +126,10 @@ class CfBatchQueue(C.Structure):
                 ("probe_tickets", vp), ("place_tickets", vp), ("scatter_tickets", vp), ("scatter_radius", vp),
                 ("ovf", vp), ("pairs", vp), ("pair_mods", vp), ("results", vp), ("nmod", u32), ("ticket", u32),
                 ("grid", u32), ("max_pairs", u32), ("ovf_cap", u32), ("n_scatter", u32), ("use_part", C.c_int),
-                ("part_lb", C.c_int)]
+                ("part_lb", C.c_int), ("n_probe", u32), ("pad0", u32), ("probe_tickets_r", vp), ("probe_radius", vp)]
 
 
-assert C.sizeof(CfBatchQueue) == 136
+assert C.sizeof(CfBatchQueue) == 160
 
 _lib = None
 _lock = threading.Lock()

@@ -50,5 +50,8 @@ struct CfBatchQueue {
   u32 nmod, ticket, grid, max_pairs;
   u32 ovf_cap, n_scatter;
   int use_part, part_lb;
+  u32 n_probe, pad0;                   // n_probe > 0: one probe launch per radius instead of probe_tickets
+  const u64* const* probe_tickets_r;   // host array [n_probe] of device ticket prefix sums (one radius each)
+  const int* probe_radius;             // host array [n_probe]: the radius of each probe launch
 };
-static_assert(sizeof(CfBatchQueue) == 136, "CfBatchQueue layout");
+static_assert(sizeof(CfBatchQueue) == 160, "CfBatchQueue layout");

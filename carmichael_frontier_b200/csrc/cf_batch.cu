@@ -114,8 +114,11 @@ __device__ __forceinline__ bool batch_ticket(const CfBatchMod& md, u32 mod, u64 
   return ok;
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kBatchBlock)
+// RF = 0: any radius (a switch into the radius-templated code); RF > 0: every
+// modulus of the launch has radius RF (its ticket sums hold only those), so the
+// kernel carries only that radius's code and registers.
+template <int MODE, int RF>
+__global__ void __launch_bounds__(kBatchBlock, (MODE == 1 && RF > 0) ? 4 : 1)   // one-radius probes: 4 CTAs per SM
 k_batch(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart /*[nmod+1]*/, u32 nmod, u32 ticket,
         unsigned long long* __restrict__ queue, CfPair* __restrict__ pairs, u32* __restrict__ pmod, u32 max_pairs,
         u32* __restrict__ npairs, u32* __restrict__ err) {
@@ -148,7 +151,14 @@ k_batch(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart /*[n
     const u32 left = (u32)((n_side - first) < ticket ? (n_side - first) : ticket);
     const u64 rank0 = first + (d_side ? 0 : md.i_lo);
     bool good;
-    switch (md.r) {
+    if constexpr (RF > 0) {
+      if (md.r == RF) {
+        good = batch_ticket<RF, MODE>(md, lo, rank0, left, lane, sink);
+      } else {
+        good = true;
+        badarg = true;
+      }
+    } else switch (md.r) {
       case 1: good = batch_ticket<1, MODE>(md, lo, rank0, left, lane, sink); break;
       case 2: good = batch_ticket<2, MODE>(md, lo, rank0, left, lane, sink); break;
       case 3: good = batch_ticket<3, MODE>(md, lo, rank0, left, lane, sink); break;
@@ -519,6 +529,9 @@ k_batch_check(const CfBatchMod* __restrict__ mods, const CfPair* __restrict__ pa
 extern "C" size_t cf_batch_mod_bytes(void) { return sizeof(CfBatchMod); }
 extern "C" int cf_batch_max_r(void) { return kBatchMaxR; }
 
+static int batch_launch(int mode, int rf, const void* mods, const u64* tstart, u32 nmod, u32 ticket, void* queue,
+                        void* pairs, u32* pmod, u32 max_pairs, u32* npairs, u32* err, u32 grid, cudaStream_t st);
+
 // mode 0: build the table of every modulus (from its smaller side); mode 1:
 // probe it with the other side; mode 2: check every candidate pair.
 //   mods    device array of nmod CfBatchMod descriptors (radius 1..8 each)
@@ -549,30 +562,53 @@ extern "C" int cf_batch_run(int mode, const void* mods, const u64* tstart, u32 n
     CF_LAUNCH_CHECK("cf_batch_run(check)");
     return CF_OK;
   }
-  if (grid == 0) {                           // every CTA resident: one wave of persistent CTAs
-    static int s_grid[2][64];                 // per mode and device; benign race (same value)
+  return batch_launch(mode, 0, mods, tstart, nmod, ticket, queue, pairs, pmod, max_pairs, npairs, err, grid, st);
+}
+
+// (definitions of the launch helpers declared above cf_batch_run)
+// Launch k_batch<mode, rf> as a persistent wave (grid 0: as many CTAs as are
+// resident at once, looked up once per mode, radius and device).
+template <int MODE, int RF>
+static int batch_launch_t(const void* mods, const u64* tstart, u32 nmod, u32 ticket, void* queue, void* pairs,
+                          u32* pmod, u32 max_pairs, u32* npairs, u32* err, u32 grid, cudaStream_t st) {
+  if (grid == 0) {
+    static int s_grid[64];                    // per device; benign race (same value)
     int dev = 0;
     cudaGetDevice(&dev);
-    int* slot = (dev >= 0 && dev < 64) ? &s_grid[mode][dev] : nullptr;
+    int* slot = (dev >= 0 && dev < 64) ? &s_grid[dev] : nullptr;
     if (slot && *slot) {
       grid = (u32)*slot;
     } else {
       int sms = 148, per_sm = 0;
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      if (mode == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<0>, kBatchBlock, 0);
-      else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<1>, kBatchBlock, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<MODE, RF>, kBatchBlock, 0);
       grid = (u32)sms * (u32)(per_sm > 0 ? per_sm : 1);
       if (slot) *slot = (int)grid;
     }
   }
-  if (mode == 0)
-    k_batch<0><<<grid, kBatchBlock, 0, st>>>((const CfBatchMod*)mods, tstart, nmod, ticket,
-                                             (unsigned long long*)queue, (CfPair*)pairs, pmod, max_pairs, npairs, err);
-  else
-    k_batch<1><<<grid, kBatchBlock, 0, st>>>((const CfBatchMod*)mods, tstart, nmod, ticket,
-                                             (unsigned long long*)queue, (CfPair*)pairs, pmod, max_pairs, npairs, err);
+  k_batch<MODE, RF><<<grid, kBatchBlock, 0, st>>>((const CfBatchMod*)mods, tstart, nmod, ticket,
+                                                  (unsigned long long*)queue, (CfPair*)pairs, pmod, max_pairs,
+                                                  npairs, err);
   CF_LAUNCH_CHECK("cf_batch_run");
   return CF_OK;
+}
+
+static int batch_launch(int mode, int rf, const void* mods, const u64* tstart, u32 nmod, u32 ticket, void* queue,
+                        void* pairs, u32* pmod, u32 max_pairs, u32* npairs, u32* err, u32 grid, cudaStream_t st) {
+#define CF_BL(M, R) batch_launch_t<M, R>(mods, tstart, nmod, ticket, queue, pairs, pmod, max_pairs, npairs, err, grid, st)
+  if (mode == 0) return CF_BL(0, 0);
+  switch (rf) {
+    case 1: return CF_BL(1, 1);
+    case 2: return CF_BL(1, 2);
+    case 3: return CF_BL(1, 3);
+    case 4: return CF_BL(1, 4);
+    case 5: return CF_BL(1, 5);
+    case 6: return CF_BL(1, 6);
+    case 7: return CF_BL(1, 7);
+    case 8: return CF_BL(1, 8);
+    default: return CF_BL(1, 0);
+  }
+#undef CF_BL
 }
 
 extern "C" u32 cf_batch_part_buckets(int lb) { return lb >= kPlbMin && lb <= kPlbMax ? 1u << lb : 0u; }
@@ -660,7 +696,8 @@ extern "C" int cf_batch_part(int phase, const void* mods, const u64* tstart, u32
 extern "C" int cf_solve_batch(const CfBatchQueue* q, void* stream) {
   if (!q || !q->mods || !q->misc || q->nmod == 0 || !q->build_tickets || !q->probe_tickets || !q->pairs ||
       !q->pair_mods || !q->results || (q->zero_bytes && !q->arena) ||
-      (q->use_part && (!q->place_tickets || !q->ovf || (q->n_scatter && (!q->scatter_tickets || !q->scatter_radius))))) {
+      (q->use_part && (!q->place_tickets || !q->ovf || (q->n_scatter && (!q->scatter_tickets || !q->scatter_radius)))) ||
+      (q->n_probe && (!q->probe_tickets_r || !q->probe_radius))) {
     cf_set_error("cf_solve_batch: bad arguments%s", "");
     return CF_EBADARG;
   }
@@ -694,9 +731,17 @@ extern "C" int cf_solve_batch(const CfBatchQueue* q, void* stream) {
   }
   rc = cf_batch_run(0, q->mods, q->build_tickets, q->nmod, q->ticket, m, q->pairs, (u32*)q->pair_mods, q->max_pairs,
                     npairs, err, nullptr, q->grid, stream);
-  if (rc == CF_OK)
+  if (rc == CF_OK && q->n_probe == 0)
     rc = cf_batch_run(1, q->mods, q->probe_tickets, q->nmod, q->ticket, m + 8, q->pairs, (u32*)q->pair_mods,
                       q->max_pairs, npairs, err, nullptr, q->grid, stream);
+  for (u32 i = 0; i < q->n_probe && rc == CF_OK; ++i) {       // one probe launch per radius present
+    e = cudaMemsetAsync(m + 8, 0, 8, st);
+    if (e != cudaSuccess) return cf_cuda_status(e, "cf_solve_batch: zero");
+    const int rr = q->probe_radius[i];
+    if (rr < 1 || rr > kBatchMaxR) { cf_set_error("cf_solve_batch: probe radius out of range%s", ""); return CF_EBADARG; }
+    rc = batch_launch(1, rr, q->mods, q->probe_tickets_r[i], q->nmod, q->ticket, m + 8, q->pairs, (u32*)q->pair_mods,
+                      q->max_pairs, npairs, err, q->grid, st);
+  }
   if (rc == CF_OK)
     rc = cf_batch_run(2, q->mods, nullptr, q->nmod, 0, nullptr, q->pairs, (u32*)q->pair_mods, q->max_pairs, npairs,
                       err, q->results, 0, stream);

@@ -61,6 +61,7 @@ class BatchTuning:
     part_lb: int = 10                  # log2 buckets per range of the partitioned build (9 or 10)
     part_sigma: float = 8.0            # bucket-range capacity = mean + sigma*sqrt(mean) + 32
     ovf_capacity: int = 1 << 16        # records that ran past their bucket range (per batch)
+    probe_per_radius: bool = True      # one probe launch per radius (kernels carry one radius's code)
 
 
 @dataclass
@@ -69,6 +70,7 @@ class _Batch:
     mods: object = None                # device CfBatchMod[nmod]
     tsD: object = None                 # device u64[nmod+1] ticket prefix sums, table sides (build)
     tsI: object = None                 # device u64[nmod+1] ticket prefix sums, probing sides
+    tsIr: object = None                # the same per radius {r: prefix sums over that radius's moduli}
     tsD_all: object = None             # table-side tickets with every modulus built in place
     tsS: object = None                 # scatter tickets of the partitioned build per radius {r: prefix sums}
     tsP: object = None                 # bucket ranges of the partitioned build (0 for in-place moduli)
@@ -270,6 +272,9 @@ class BatchSolver:
             b.tsD_all = _prefix(build)
             b.tsD = _prefix([0 if j in b._part else v for j, v in enumerate(build)])
             b.tsI = _prefix([-(-max(nD[k], nI[k]) // t) for k in b.idx])
+            # the probe runs one launch per radius present, each over its radius's moduli only
+            b.tsIr = {rr: _prefix([-(-max(nD[k], nI[k]) // t) if insts[k].r == rr else 0 for k in b.idx])
+                      for rr in sorted({insts[k].r for k in b.idx})}
             # one scatter launch per radius present, each with a generator specialised for it
             b.tsS = {}
             for rr in sorted({insts[k].r for j, k in enumerate(b.idx) if j in b._part}):
@@ -324,13 +329,17 @@ class BatchSolver:
         scat = sorted(b.tsS.items()) if part else []
         s_ptrs = (C.c_void_p * max(1, len(scat)))(*[dp(ts) for _, ts in scat])
         s_rad = (C.c_int * max(1, len(scat)))(*[int(rr) for rr, _ in scat])
+        prb = sorted(b.tsIr.items()) if (tu.probe_per_radius and b.tsIr) else []
+        p_ptrs = (C.c_void_p * max(1, len(prb)))(*[dp(ts) for _, ts in prb])
+        p_rad = (C.c_int * max(1, len(prb)))(*[int(rr) for rr, _ in prb])
         q = _lib.CfBatchQueue(
             mods=dp(b.mods), arena=dp(arena), zero_bytes=b.zero_bytes, misc=dp(misc),
             build_tickets=dp(b.tsD if part else b.tsD_all), probe_tickets=dp(b.tsI),
             place_tickets=dp(b.tsP) if part else None, scatter_tickets=C.addressof(s_ptrs),
             scatter_radius=C.addressof(s_rad), ovf=dp(ovf), pairs=dp(pairs), pair_mods=dp(pmod), results=dp(res),
             nmod=len(b.idx), ticket=tu.ticket, grid=tu.grid, max_pairs=maxp, ovf_cap=tu.ovf_capacity,
-            n_scatter=len(scat), use_part=int(part), part_lb=tu.part_lb)
+            n_scatter=len(scat), use_part=int(part), part_lb=tu.part_lb, n_probe=len(prb),
+            probe_tickets_r=C.addressof(p_ptrs), probe_radius=C.addressof(p_rad))
         _lib.check(lib.cf_solve_batch(C.byref(q), self._sh()), "cf_solve_batch")
 
     def _launch(self, b: _Batch, maxp: int, graphs: bool):
@@ -424,7 +433,7 @@ class BatchSolver:
         """Drop a prepared portfolio's graphs and device tables."""
         for b in prep.batches:
             b.graph = None
-            b.mods = b.tsD = b.tsI = b.tsD_all = b.tsS = b.tsP = None
+            b.mods = b.tsD = b.tsI = b.tsD_all = b.tsS = b.tsP = b.tsIr = None
         prep.tables = prep.tails = None
         live = getattr(self, "_live", [])
         self._live = [p for p in live if p is not prep]

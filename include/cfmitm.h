@@ -403,6 +403,9 @@ typedef struct CfBatchQueue {
   uint32_t nmod, ticket, grid, max_pairs;
   uint32_t ovf_cap, n_scatter;
   int use_part, part_lb;
+  uint32_t n_probe, pad0;                   /* n_probe > 0: one probe launch per radius present, */
+  const uint64_t* const* probe_tickets_r;   /* each with the ticket sums of that radius's moduli only */
+  const int* probe_radius;
 } CfBatchQueue;
 int cf_solve_batch(const CfBatchQueue* q, void* stream);
 
