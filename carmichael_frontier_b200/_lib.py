@@ -73,8 +73,7 @@ SIGNATURES = [
     ("cf_fused_probe2", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, C.c_int, u64, C.c_int, vp, u32,
                                   vp, vp, u32, vp]),
     ("cf_dtab_build", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, vp, vp]),
-    ("cf_dtab_build3", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp,
-                                 vp]),
+    ("cf_dtab_build3", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, C.c_int, C.c_int, vp, vp]),
     ("cf_fused_probe3", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, C.c_int, C.c_int, u64, C.c_int,
                                   vp, u32, vp, vp, u32, vp]),
     ("cf_fused_probe", C.c_int, [vp, vp, C.c_int, C.c_int, u64, u64, vp, C.c_int, u64, vp, u32, vp, vp, u32, vp]),

@@ -64,7 +64,6 @@ struct DTab {
   int bbits;
   int fbits;
   u32 xb;         // 0: wide side entries; 8: compact side words
-  u32 blo, bhi;   // k_fused's build: insert only the records whose bucket lies in [blo, bhi)
 };
 
 constexpr u32 kCompactXb = 8;

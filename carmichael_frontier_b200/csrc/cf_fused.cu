@@ -119,8 +119,6 @@ k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo
               u64 X;
               u32 x2;
               cf_fuse_res(q, tail[j], ar.md, minv, X, x2);
-              const CfFuseKey fk = cf_fuse_key(X, x2, tab.bbits);
-              if (fk.bucket < tab.blo || fk.bucket >= tab.bhi) continue;   // another pass's buckets
               if (tab.bloom) {
                 const CfBloomKey bl = cf_bloom_key(X, x2, tab.fbits);
                 u32* blk = tab.bloom + (u64)bl.block * 8;
@@ -128,6 +126,7 @@ k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo
                 atomicOr(blk + bl.w1, bl.m1);
                 atomicOr(blk + bl.w2, bl.m2);
               }
+              const CfFuseKey fk = cf_fuse_key(X, x2, tab.bbits);
               bk[u] = fk.bucket;
               f16[u] = fk.f16;
               f32[u] = fk.f32;
@@ -198,8 +197,6 @@ void dispatch_fused(int mode, const u64* pool, const CfTailEnt* tail, int n, u64
 DTab make_tab(void* tab, int bbits, int fbits, u64 rank0, int compact) {
   DTab t;
   t.xb = compact ? kCompactXb : 0u;
-  t.blo = 0;
-  t.bhi = 0xffffffffu;
   t.nb = 1ull << bbits;
   t.fpw = (u32*)tab;
   t.side = (uint2*)((unsigned char*)tab + t.nb * 32);
@@ -231,18 +228,13 @@ extern "C" size_t cf_dtab_fp_bytes(int bbits) {
 // Build: insert the D-side records of ranks [lo, lo+count), count < 2^32, slots
 // claimed by fill counter.  side_format 0: wide side entries; 1: compact side
 // words (tables of at most 2^20 buckets; the probe must be told the same
-// format).  passes: the side is generated `passes` times, each pass inserting
-// the records of one 1/passes slice of the buckets, so that the table areas a
-// pass writes stay in L2 (0: as many passes as keep that area near
-// kBuildPassBytes).  The caller zeroes the fingerprint array (the first
+// format).  The caller zeroes the fingerprint array (the first
 // cf_dtab_fp_bytes(bbits) bytes), the fill counters (4 * 2^bbits bytes from
 // offset 160 * 2^bbits) and the Bloom filter (when fbits > 0) first.
-constexpr u64 kBuildPassBytes = 48ull << 20;
-
 extern "C" int cf_dtab_build3(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count, void* tab,
-                              int bbits, int fbits, int side_format, int passes, u32* err, void* stream) {
+                              int bbits, int fbits, int side_format, u32* err, void* stream) {
   if (!pool_dev || !tail || !tab || !err || n < 1 || n > CF_MAX_POOL || r < 1 || r > CF_MAX_DISPATCH_R ||
-      bbits < 1 || bbits > 28 || (side_format != 0 && side_format != 1) || passes < 0 || passes > 64) {
+      bbits < 1 || bbits > 28 || (side_format != 0 && side_format != 1)) {
     cf_set_error("cf_dtab_build: bad arguments%s", "");
     return CF_EBADARG;
   }
@@ -253,33 +245,23 @@ extern "C" int cf_dtab_build3(const void* pool_dev, const void* tail, int n, int
     cf_set_error("cf_dtab_build: compact side words need at most 2^20 buckets and 2^24 records%s", "");
     return CF_EBADARG;
   }
-  DTab t = make_tab(tab, bbits, fbits, lo, side_format);
-  if (passes == 0) {
-    const u64 area = t.nb * (32 + (side_format ? 64 : 128) + 4);
-    passes = (int)((area + kBuildPassBytes - 1) / kBuildPassBytes);
-    if (passes < 1) passes = 1;
-    if ((u64)passes > t.nb) passes = (int)t.nb;
-  }
-  for (int p = 0; p < passes; ++p) {
-    t.blo = (u32)(t.nb * (u64)p / (u64)passes);
-    t.bhi = p + 1 == passes ? 0xffffffffu : (u32)(t.nb * (u64)(p + 1) / (u64)passes);
-    int rc = CF_OK;
-    CF_DISPATCH_R(r, dispatch_fused, 0, (const u64*)pool_dev, (const CfTailEnt*)tail, n, lo, count, t, nullptr, 0u,
-                  nullptr, err, 0u, 0u, (cudaStream_t)stream, &rc);
-    if (rc != CF_OK) return rc;
-    CF_LAUNCH_CHECK("cf_dtab_build");
-  }
+  const DTab t = make_tab(tab, bbits, fbits, lo, side_format);
+  int rc = CF_OK;
+  CF_DISPATCH_R(r, dispatch_fused, 0, (const u64*)pool_dev, (const CfTailEnt*)tail, n, lo, count, t, nullptr, 0u,
+                nullptr, err, 0u, 0u, (cudaStream_t)stream, &rc);
+  if (rc != CF_OK) return rc;
+  CF_LAUNCH_CHECK("cf_dtab_build");
   return CF_OK;
 }
 
 extern "C" int cf_dtab_build2(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count, void* tab,
                               int bbits, int fbits, u32* err, void* stream) {
-  return cf_dtab_build3(pool_dev, tail, n, r, lo, count, tab, bbits, fbits, 0, 1, err, stream);
+  return cf_dtab_build3(pool_dev, tail, n, r, lo, count, tab, bbits, fbits, 0, err, stream);
 }
 
 extern "C" int cf_dtab_build(const void* pool_dev, const void* tail, int n, int r, u64 lo, u64 count, void* tab,
                              int bbits, u32* err, void* stream) {
-  return cf_dtab_build3(pool_dev, tail, n, r, lo, count, tab, bbits, 0, 0, 1, err, stream);
+  return cf_dtab_build3(pool_dev, tail, n, r, lo, count, tab, bbits, 0, 0, err, stream);
 }
 
 // Probe: generate the records of ranks [lo, lo+count) of the probing side in

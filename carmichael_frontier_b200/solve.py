@@ -103,7 +103,6 @@ class Tuning:
     max_nodes: int = 1 << 27        # bounded strategy: frontier nodes per block of first indices
     part_build: bool = True         # fused: partitioned table build for tables of part_min_buckets or more
     part_min_buckets: int = 1 << 21 # smaller tables stay in L2 while built alone: built in place
-    build_passes: int = 0           # in-place build: bucket-range passes (0 = from the table size)
     part_lb: int = 10               # log2 buckets per range of the partitioned build (9 or 10)
     part_sigma: float = 8.0         # bucket-range capacity = mean + sigma*sqrt(mean) + 32
 
@@ -349,7 +348,7 @@ class Solver:
             # the build side's tables first: the table build runs while the host prepares the other side
             bpool, btail = self._side_tables(inst, bside)
             ck(lib.cf_dtab_build3(dp(bpool), dp(btail), bn, r, 0, bcount, dp(tab), bbits, fbits, side_format,
-                                  tu.build_passes, dp(misc) + 4, sh), "cf_dtab_build")
+                                  dp(misc) + 4, sh), "cf_dtab_build")
             ppool, ptail = self._side_tables(inst, pside)
             screen = self.tables.screen(inst.P0, inst.B, 1e-6)
             poolD, poolI = (bpool, ppool) if bside == "D" else (ppool, bpool)

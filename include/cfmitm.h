@@ -187,12 +187,11 @@ int cf_dtab_build(const void* pool_dev, const void* tail, int n, int r, uint64_t
  * 32-bit fingerprint and the rank, 8 bytes; what the variants above build and
  * probe), 1 = compact (per slot one 32-bit word, rank << 8 | 8 more
  * fingerprint bits; tables of at most 2^20 buckets and 2^24 records).  The
- * compact side of an L2-sized table stays in L2 while it is built.  Build and
- * probe must be given the same format.  passes: the side is generated that many
- * times, each pass inserting the records of one slice of the buckets, so the
- * table area a pass writes stays in L2 (0 = chosen from the table size). */
+ * compact side of an L2-sized table stays in L2 while it is built, so its
+ * sectors are written back whole once.  Build and probe must be given the same
+ * format. */
 int cf_dtab_build3(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count, void* tab,
-                   int bbits, int fbits, int side_format, int passes, uint32_t* err, void* stream);
+                   int bbits, int fbits, int side_format, uint32_t* err, void* stream);
 int cf_fused_probe3(const void* pool_dev, const void* tail, int n, int r, uint64_t lo, uint64_t count,
                     const void* tab, int bbits, int fbits, int side_format, uint64_t tab_rank0, int swap,
                     void* pairs, uint32_t max_pairs, uint32_t* npairs, uint32_t* err, uint32_t grid,

@@ -202,7 +202,7 @@ def test_named_entry_points_reject_bad_arguments_without_gpu():
     assert lib.cf_solve_batch(C.byref(q), None) == _lib.CF_EBADARG
     assert lib.cf_igen_tmp_bytes(1 << 20) > lib.cf_igen_tmp_bytes(1 << 10) > 0
     assert lib.cf_join_tmp_bytes(1000) >= 16 * 1000
-    assert lib.cf_dtab_build3(None, None, 5, 2, 0, 10, None, 10, 0, 1, 0, None, None) == _lib.CF_EBADARG
+    assert lib.cf_dtab_build3(None, None, 5, 2, 0, 10, None, 10, 0, 1, None, None) == _lib.CF_EBADARG
 
 
 def test_ddump_bound_table_equals_the_python_definition():
