@@ -26,7 +26,7 @@ import numpy as np
 from . import _lib
 from .bounded import U128
 from .certify import verify_certificate
-from .tables import unrank_colex, wide_modulus
+from .tables import pool_table_host, unrank_colex, wide_modulus
 
 RANK_LIMIT = 1 << 32          # positions in the join table are 32-bit
 
@@ -93,6 +93,7 @@ class BoundedSolve:
         self.native = True                  # one C call per instance (cf_bounded_join) where it applies
         self._native_bytes = 256 << 20
         self._native_out = 1 << 12
+        self._stage = None                  # page-locked staging of one instance's tables
 
     def _table(self, keys, n: int, plan: dict):
         from .solve import dtab_shape
@@ -161,23 +162,30 @@ class BoundedSolve:
         if wide_modulus(M) or Icap - 1 >= U128 or Dmin >= U128 or Icap <= 1 or len(B0) < r or len(INS) < r:
             return None
         nb, ni = len(B0), len(INS)
-        g = self.gen
-        poolD = g.tables.pool(B0, r, M, 1)
-        poolI = g.tables.pool(INS, r, M, inst.P0 % M)
-
-        def host_table(fn, primes, bound):
-            n = len(primes)
-            nbytes = lib.cf_igen_bounds_bytes(n, r)
-            out = np.zeros(nbytes, dtype=np.uint8)
-            pr = np.asarray(primes, dtype=np.uint64)
-            _lib.check(fn(pr.ctypes.data, n, r, bound & (2 ** 64 - 1), bound >> 64, out.ctypes.data, nbytes), "bounds")
-            return out
-        G = g.tables.get(("ddumpGc", tuple(B0), r, int(Dmin)), lambda: host_table(lib.cf_ddump_bounds, B0, int(Dmin)))
-        H = g.tables.get(("igenHc", tuple(INS), r, int(Icap)), lambda: host_table(lib.cf_igen_bounds, INS, int(Icap)))
         split_idx = ni if split is None else next((i for i, p in enumerate(INS) if p > split), ni)
         hmax = r if hmax is None else int(hmax)
         if hmax < 0:
             return None
+        g = self.gen
+        # the instance's four tables (two pool tables, two bound tables) go up in ONE copy: each is
+        # built on the host by the library, packed at 256-byte offsets into a page-locked buffer
+        parts = [pool_table_host(B0, r, M, 1), pool_table_host(INS, r, M, inst.P0 % M),
+                 self._bound_table(lib.cf_ddump_bounds, B0, r, int(Dmin)),
+                 self._bound_table(lib.cf_igen_bounds, INS, r, int(Icap))]
+        offs, total = [], 0
+        for a in parts:
+            offs.append(total)
+            total += (a.nbytes + 255) // 256 * 256
+        if self._stage is None or self._stage.numel() < total:
+            self._stage = torch.empty(max(total, 1 << 20), dtype=torch.uint8, pin_memory=True)
+        host = self._stage.numpy()
+        for o, a in zip(offs, parts):
+            host[o:o + a.nbytes] = a.view(np.uint8)
+        dev = self.s._buf("bjtab", max(total, 1 << 20))
+        with torch.cuda.stream(self.s._torch_stream()):
+            dev[:total].copy_(self._stage[:total], non_blocking=True)
+        base = dp(dev)
+        poolD, poolI, G, H = (base + o for o in offs)
         sh = self.s._sh()
         n_out, need = C.c_uint64(0), C.c_uint64(0)
         sizes = (C.c_uint64 * 2)()
@@ -185,7 +193,7 @@ class BoundedSolve:
             nbytes = self._native_bytes
             tmp = self.s._buf("bjoin", nbytes)
             out = np.zeros(3 * self._native_out, dtype=np.uint64)
-            rc = lib.cf_bounded_join(dp(poolD), dp(G), nb, dp(poolI), dp(H), ni, r, M, inst.P0 % M, split_idx, hmax,
+            rc = lib.cf_bounded_join(poolD, G, nb, poolI, H, ni, r, M, inst.P0 % M, split_idx, hmax,
                                      0, 0, dp(tmp), nbytes, out.ctypes.data, self._native_out, C.byref(n_out), sizes,
                                      C.byref(need), sh)
             if rc == _lib.CF_ENOMEM:
@@ -211,6 +219,15 @@ class BoundedSolve:
                 continue                       # fingerprint collision, not an equal-residue pair
             pairs.append((unrank_colex(int(did[j]), r, nb), ii))
         return pairs, nD, nI, dict(strategy="bounded", Icap=Icap, Dmin=Dmin, table="D", native=True)
+
+    def _bound_table(self, fn, primes, r: int, bound: int) -> np.ndarray:
+        """A bound table (cf_ddump_bounds / cf_igen_bounds) of the primes, on the host."""
+        n = len(primes)
+        nbytes = self.lib.cf_igen_bounds_bytes(n, r)
+        out = np.zeros(nbytes, dtype=np.uint8)
+        pr = np.asarray(primes, dtype=np.uint64)
+        _lib.check(fn(pr.ctypes.data, n, r, bound & (2 ** 64 - 1), bound >> 64, out.ctypes.data, nbytes), "bounds")
+        return out
 
     def _join_on_stream(self, inst, Icap, Dmin, split, hmax):
         if self.native:
