@@ -104,10 +104,11 @@ def footprint(inst: Instance, tu: Tuning) -> dict:
         # most min(nI, nD) of them) or on the D records (I leaves probed, never written)
         m = min(nI, nD)
         side = max(16 * m + _dtab_bytes(m, tu), _dtab_bytes(nD, tu))
-        return dict(bytes=fixed + 16 * nD + frontier * 2 + side, strategy="bounded", nD=nD, nI=nI)
+        return dict(bytes=fixed + 16 * nD + frontier * 2 + side, strategy="bounded", nD=nD, nI=nI, work=nD + nI)
     small = min(math.comb(nB, r), math.comb(nI_full, r))
     tails = 16 * (math.comb(nB, 2) + math.comb(nI_full, 2))
-    return dict(bytes=fixed + _dtab_bytes(small, tu) + tails, strategy="fused")
+    return dict(bytes=fixed + _dtab_bytes(small, tu) + tails, strategy="fused",
+                work=math.comb(nB, r) + math.comb(nI_full, r))
 
 
 # -- admission and workers ---------------------------------------------------------
@@ -118,6 +119,7 @@ class Ticket:
     inst: Instance
     arrival: float
     need: int = 0
+    work: int = 0                       # estimated records (footprint()["work"])
     admitted: float = 0.0
     finished: float = 0.0
     result: SolveResult | None = None
@@ -201,11 +203,16 @@ class Server:
     slots: concurrent requests (one worker thread and CUDA stream each);
     budget: device bytes that admitted requests may hold together (default: 60%
     of the free device memory at start); solve_fn(worker_state, inst) may replace
-    the GPU solve (used by CPU tests of the admission logic)."""
+    the GPU solve (used by CPU tests of the admission logic).
+    large_work: requests whose estimated records (footprint()["work"]) reach this run on their
+    worker's high-priority stream, so that the largest requests -- the tail of the latency
+    distribution -- are not slowed by the small ones sharing the GPU with them (the small ones
+    still fill the SMs the large one leaves free)."""
 
     def __init__(self, device=None, slots: int = 4, budget: int | None = None, strategy: str = "auto",
-                 solve_fn=None, clock=time.perf_counter):
+                 solve_fn=None, clock=time.perf_counter, large_work: float = 2e9):
         self.slots = slots
+        self.large_work = large_work
         self.clock = clock
         self.tuning = Tuning(strategy=strategy, max_nodes=1 << 22)
         self.solve_fn = solve_fn
@@ -239,7 +246,11 @@ class Server:
             rid = self._rid
             self._rid += 1
         t = Ticket(rid, inst, self.clock() if arrival is None else arrival)
-        t.need = footprint(inst, self.tuning)["bytes"] if self.solve_fn is None else getattr(inst, "need", 1)
+        if self.solve_fn is None:
+            fp = footprint(inst, self.tuning)
+            t.need, t.work = fp["bytes"], fp.get("work", 0)
+        else:
+            t.need, t.work = getattr(inst, "need", 1), getattr(inst, "work", 0)
         self.tickets.append(t)
         self.adm.put(t)
         return t
@@ -253,7 +264,7 @@ class Server:
                 return
             t.admitted = self.clock()
             try:
-                t.result = self._solve(state, t.inst)
+                t.result = self._solve(state, t.inst, t.work >= self.large_work)
             except Exception as e:                     # noqa: BLE001 - reported per request
                 t.error = f"{type(e).__name__}: {e}"
             finally:
@@ -268,23 +279,28 @@ class Server:
         import torch
         from .solve import Solver
         dev = torch.device(self.device if self.device is not None else "cuda")
+        lo, hi = torch.cuda.Stream.priority_range()
         stream = torch.cuda.Stream(dev)
-        return {"worker": w, "stream": stream, "solver": Solver(dev, stream=stream, tuning=self.tuning)}
+        fast = torch.cuda.Stream(dev, priority=hi)           # the highest priority the device offers
+        return {"worker": w, "stream": stream, "solver": Solver(dev, stream=stream, tuning=self.tuning),
+                "fast_stream": fast, "fast_solver": Solver(dev, stream=fast, tuning=self.tuning)}
 
-    def _solve(self, state, inst: Instance) -> SolveResult:
+    def _solve(self, state, inst: Instance, large: bool = False) -> SolveResult:
         if self.solve_fn is not None:
             return self.solve_fn(state, inst)
         import torch
-        with torch.cuda.stream(state["stream"]):
-            res = state["solver"].solve_instance(inst)
-            state["stream"].synchronize()
+        st, solver = (state["fast_stream"], state["fast_solver"]) if large else (state["stream"], state["solver"])
+        with torch.cuda.stream(st):
+            res = solver.solve_instance(inst)
+            st.synchronize()
         return res
 
     def _trim(self, state):
         """Drop the worker's per-request device buffers (pool tables stay resident)."""
-        s = state.get("solver")
-        if s is not None:
-            s._bufs.clear()
+        for key in ("solver", "fast_solver"):
+            s = state.get(key)
+            if s is not None:
+                s._bufs.clear()
 
 
 # -- drivers ------------------------------------------------------------------------

@@ -83,3 +83,32 @@ def test_poisson_stats_shape():
     srv.stop()
     assert st["requests"] == 20 and st["errors"] == 0
     assert st["p50_ms"] <= st["p99_ms"] and st["throughput_rps"] > 0
+
+
+def test_footprint_reports_work_and_large_requests_take_the_fast_path():
+    # the footprint's record estimate is at least the records the solve will touch, and the server
+    # sends requests at or above large_work to the worker's high-priority path
+    import math
+
+    from carmichael_frontier_b200 import serve, workloads as W
+    from carmichael_frontier_b200.solve import Instance, Tuning
+    insts = [Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in W.config5_requests(12)]
+    for x in insts:
+        fp = serve.footprint(x, Tuning(strategy="auto"))
+        assert fp["work"] > 0
+        if fp["strategy"] == "fused":
+            assert fp["work"] == math.comb(len(x.B0), x.r) + math.comb(len(x.INS), x.r)
+    seen = []
+
+    class Job:
+        def __init__(self, work):
+            self.need, self.work = 1, work
+
+    srv = serve.Server(slots=2, budget=10, solve_fn=lambda st, inst: None, large_work=100)
+    orig = srv._solve
+    srv._solve = lambda state, inst, large=False: seen.append((inst.work, large)) or orig(state, inst, large)
+    srv.start()
+    for w in (5, 100, 7, 5000):
+        srv.submit(Job(w)).done.wait()
+    srv.stop()
+    assert sorted(seen) == [(5, False), (7, False), (100, True), (5000, True)]
