@@ -25,7 +25,10 @@ without it.  Sources of truth, all the reference's own code:
     sub-instance of 6.2e8 D and about 2e8 I records, joined from the reference
     dumpers' records in numpy (config4_bounded).
 
-Usage: CF_REFERENCE_ROOT=<reference tree> python tests/golden/make_golden.py [--quick | --m0-large | --config4]
+  * Whole moduli of the seeded portfolio (config3_pins): every D against every I
+    subset through the reference's mitm64.
+
+Usage: CF_REFERENCE_ROOT=<reference tree> python tests/golden/make_golden.py [--quick | --m0-large | --config4 | --config3]
 (the reference tree defaults to oracle/build.py's REF_SRC).
 """
 from __future__ import annotations
@@ -409,7 +412,31 @@ def config4_bounded(target_i=200_000_000, threads=8):
                 d_records=nd, i_digest=i_dig, d_digest=O.record_digest_hex(acc), pairs=sorted(pairs))
 
 
+CONFIG3_PINS = (0, 2, 3, 5, 13, 14)      # seeded portfolio moduli whose whole join the reference finishes in seconds
+
+
+def config3_pins():
+    """Whole moduli of the seeded 1024-modulus portfolio (radii 4, 5 and 6, pools of 121-272 primes), every
+    D against every I subset, joined by the reference's mitm64."""
+    ws = W.config3(1024)
+    out = []
+    for k in CONFIG3_PINS:
+        row = mitm64_case(ws[k], timeout=1800)
+        row["index"] = k
+        out.append(row)
+        print("config3", k, ws[k].r, row["d_leaves"], row["i_leaves"], row["matches"], row["d_res"], flush=True)
+    return out
+
+
 def main():
+    if "--config3" in sys.argv:
+        obuild.build_oracle()
+        obuild.build_reference()
+        gold = json.load(open(OUT))
+        gold["config3_pins"] = config3_pins()
+        json.dump(gold, open(OUT, "w"), indent=0)
+        print("wrote", OUT)
+        return
     if "--config4" in sys.argv:
         obuild.build_oracle()
         obuild.build_reference()
@@ -460,6 +487,7 @@ def main():
     if not quick:
         gold["m0_kat_large"] = m0_kat_large()
         gold["config4_bounded"] = config4_bounded()
+        gold["config3_pins"] = config3_pins()
     print("m0", [(x["r"], x["d_records"], x["i_records"]) for x in gold["m0_kat"]["rows"]])
     json.dump(gold, open(OUT, "w"), indent=0)
     print("wrote", OUT)

@@ -167,3 +167,24 @@ def test_batched_partitioned_build_with_bloom_level(cuda):
     ref = BatchSolver(cuda, tuning=BatchTuning(part_build=False)).solve(insts, i_limit=lim)
     for a, b in zip(got, ref):
         assert summary(a) == summary(b)
+
+
+def test_whole_portfolio_moduli_match_reference_mitm64(cuda, golden):
+    # whole moduli of the seeded 1024-modulus portfolio (radii 4, 5, 6; pools of 121-272 primes): every
+    # D against every I subset, in one batch and one modulus at a time, against the reference's mitm64
+    # (its pair set is complete where no two D subsets share a residue: d_res == d_leaves)
+    pins = golden["config3_pins"]
+    ws = W.config3(1024)
+    insts = [Instance.build(ws[g["index"]].M, ws[g["index"]].Q, ws[g["index"]].B0, ws[g["index"]].r, ws[g["index"]].B)
+             for g in pins]
+    batched = BatchSolver(cuda).solve(insts, graphs=True)
+    single = run_per_modulus(insts, solver=Solver(cuda))
+    assert {g["r"] for g in pins} == {4, 5, 6}
+    for g, a, b in zip(pins, batched, single):
+        assert (a.n_D, a.n_I) == (g["d_leaves"], g["i_leaves"])
+        assert as_lists(a.pairs) == as_lists(b.pairs)
+        if g["d_res"] == g["d_leaves"]:
+            assert as_lists(a.pairs) == g["pairs"] and a.residue_pairs == g["matches"]
+        else:                                   # mitm64 keeps one D per residue: compare the projection
+            assert {tuple(map(tuple, p))[1] for p in as_lists(a.pairs)} == {tuple(p[1]) for p in g["pairs"]}
+        assert sorted([list(h.D), list(h.I), str(h.n)] for h in a.hits) == g["hits"]
