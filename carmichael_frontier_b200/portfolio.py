@@ -443,13 +443,11 @@ class BatchSolver:
 
 def run_per_modulus(instances: list, i_limit: int | None = None, verify: bool = True, device=None,
                     solver: Solver | None = None) -> list[SolveResult]:
-    """This library's single-modulus fused solve, one modulus at a time."""
+    """This library's single-modulus fused solve, one modulus at a time on the device (the host
+    collects each solve while the next one runs: Solver.solve_many)."""
     s = solver or Solver(device)
-    out = []
-    for w in instances:
-        x = w if isinstance(w, Instance) else Instance.build(w.M, w.Q, w.B0, w.r, w.B)
-        out.append(s.solve_instance(x, verify=verify, i_limit=i_limit))
-    return out
+    xs = [w if isinstance(w, Instance) else Instance.build(w.M, w.Q, w.B0, w.r, w.B) for w in instances]
+    return s.solve_many(xs, verify=verify, i_limit=i_limit)
 
 
 def run_plain(instances: list, i_limit: int | None = None, verify: bool = True, chunk: int = 1 << 27,

@@ -244,16 +244,30 @@ class Solver:
         self.tuning = tuning or Tuning()
         self.tables = DeviceTables(self.device, stream=stream, async_upload=True)
         self._bufs: dict[str, object] = {}
+        self._bufset = 0                 # which of two buffer sets the next enqueue uses (solve_many)
+        self.d2h_bytes = 0               # bytes read back from the device by collect()
+        self._pinned: dict = {}
         self._bounded = None
         self.result_bytes = self.lib.cf_pair_result_bytes()
         assert self.result_bytes == RESULT_DTYPE.itemsize
 
     # -- buffers -----------------------------------------------------------
     def _buf(self, name: str, nbytes: int):
-        t = self._bufs.get(name)
+        key = (name, self._bufset)
+        t = self._bufs.get(key)
         if t is None or t.numel() < nbytes:
             t = self.torch.empty(max(nbytes, 16), dtype=self.torch.uint8, device=self.device)
-            self._bufs[name] = t
+            self._bufs[key] = t
+        return t
+
+    def _pinned_buf(self, name: str, nbytes: int):
+        """Page-locked host buffer of the current buffer set (rewritten only after the solve that
+        last used it has been collected)."""
+        key = (name, self._bufset)
+        t = self._pinned.get(key)
+        if t is None or t.numel() < nbytes:
+            t = self.torch.empty(max(nbytes, 64), dtype=self.torch.uint8, pin_memory=True)
+            self._pinned[key] = t
         return t
 
     def _sh(self):
@@ -397,13 +411,12 @@ class Solver:
         host[: MOD_DTYPE.itemsize // 8] = row.view(np.uint64)
         k = MOD_DTYPE.itemsize // 8
         host[k:k + 4] = (0, -(-n_build // tile), 0, nparts)        # scatter and range ticket prefix sums
-        # pinned staging, rewritten only after the previous solve has been collected
-        if getattr(self, "_pdesc_host", None) is None or self._pdesc_host.numel() < host.nbytes:
-            self._pdesc_host = torch.empty(host.nbytes, dtype=torch.uint8, pin_memory=True)
-        self._pdesc_host[: host.nbytes].numpy()[:] = host.view(np.uint8)
+        # pinned staging of this buffer set, rewritten only after its previous solve has been collected
+        stage = self._pinned_buf("pdesc", host.nbytes)
+        stage[: host.nbytes].numpy()[:] = host.view(np.uint8)
         hdev = self._buf("pdesc", host.nbytes)
         with torch.cuda.stream(self._torch_stream()):
-            hdev[: host.nbytes].copy_(self._pdesc_host[: host.nbytes], non_blocking=True)
+            hdev[: host.nbytes].copy_(stage[: host.nbytes], non_blocking=True)
         self.h2d_desc_bytes = getattr(self, "h2d_desc_bytes", 0) + host.nbytes
         mods, tsS, tsP = dp(hdev), dp(hdev) + 8 * k, dp(hdev) + 8 * k + 16
         scr[: up(nparts * 4) + 64].zero_()
@@ -469,8 +482,15 @@ class Solver:
 
     def collect(self, inst: Instance, h: dict, verify: bool = True) -> tuple[SolveResult | None, dict | None]:
         """Synchronise, read counters; returns (result, None) or (None, bigger plan) on overflow."""
-        self._torch_stream().synchronize()
-        misc = h["misc"][:2].cpu().numpy().view(np.uint32)
+        ev = h.get("ev")
+        if ev is None:
+            self._torch_stream().synchronize()
+            misc = h["misc"][:2].cpu().numpy().view(np.uint32)
+            self.d2h_bytes += 8
+        else:                                      # staged by _stage_readback: wait for this solve only
+            ev.synchronize()
+            misc = h["hread"][:8].numpy().view(np.uint32).copy()
+            self.d2h_bytes += 8 + h["hrows"] * self.result_bytes
         npairs, err = int(misc[0]), int(misc[1])
         plan = h["plan"]
         if err & _lib.ERR_TABLE_FULL:
@@ -493,34 +513,71 @@ class Solver:
             raise _lib.CfError(_lib.CF_EBADARG, "solve", "a kernel rejected its arguments (pool primes >= 2^31?)")
         if err & _lib.ERR_KEY_MISMATCH:
             raise _lib.CfError(_lib.CF_EBADARG, "solve", "checked pair with unequal residues (internal error)")
-        res = np.frombuffer(h["res"][: npairs * self.result_bytes].cpu().numpy().tobytes(), dtype=RESULT_DTYPE)
+        nb = npairs * self.result_bytes
+        if ev is not None and npairs <= h["hrows"]:
+            res = np.frombuffer(h["hread"][8:8 + nb].numpy().tobytes(), dtype=RESULT_DTYPE)
+        else:
+            res = np.frombuffer(h["res"][:nb].cpu().numpy().tobytes(), dtype=RESULT_DTYPE)
+            self.d2h_bytes += nb
         return self._finish(inst, h, res, verify), None
 
     def _finish(self, inst: Instance, h: dict, res: np.ndarray, verify: bool) -> SolveResult:
         return finish_rows(inst, res, h["nD"], h["nI"], h["plan"], verify)
 
-    def solve_instance(self, inst: Instance, verify: bool = True, timed: bool = False,
-                       marks: list | None = None, i_limit: int | None = None) -> SolveResult:
-        """Join one instance.  i_limit: join only the I ranks [0, i_limit) (a bounded
-        sample of the instance; every pair with such an I rank is found)."""
+    def _direct_plan(self, inst: Instance, i_limit: int | None) -> dict | None:
+        """The device plan of a fused or partition join of inst, or None when inst takes another
+        path (radius 0, the bounded strategy, an empty side)."""
         if inst.r == 0:
-            return self._solve_r0(inst)
+            return None
         st = self.tuning.strategy
         if i_limit is None and (st == "bounded" or st == "auto"):
             from . import bsolve
             if bsolve.applicable(inst) and (st == "bounded" or bsolve.prunes(inst)):
-                if self._bounded is None:
-                    self._bounded = bsolve.BoundedSolve(self)
-                return self._bounded.solve(inst, verify)
+                return None
         nD, nI = ncomb(len(inst.B0), inst.r), ncomb(len(inst.INS), inst.r)
         if i_limit is not None:
             nI = min(nI, int(i_limit))
         if nI == 0 or nD == 0:
-            return SolveResult([], nD, nI, 0, 0, 0, 0)
+            return None
         plan = self.plan(nD, nI)
         plan["i_limit"] = i_limit
         if min(nD, nI) >= 1 << 32:        # ranks in the fused table are 32-bit
             plan["strategy"] = "partition"
+        return plan
+
+    def _replan(self, inst: Instance, newp: dict) -> dict:
+        """The plan after an overflow: the capacities collect() asked for."""
+        nD, nI = ncomb(len(inst.B0), inst.r), _i_window(inst, newp)
+        plan = self.plan(nD, nI, newp["capD"], newp["capI"], newp["pairs"])
+        plan["strategy"] = newp.get("strategy", plan["strategy"])
+        plan["i_limit"] = newp.get("i_limit")
+        plan["no_part"] = newp.get("no_part", False)
+        return plan
+
+    def solve_instance(self, inst: Instance, verify: bool = True, timed: bool = False,
+                       marks: list | None = None, i_limit: int | None = None) -> SolveResult:
+        """Join one instance.  i_limit: join only the I ranks [0, i_limit) (a bounded
+        sample of the instance; every pair with such an I rank is found)."""
+        plan = self._direct_plan(inst, i_limit)
+        if plan is None:
+            if inst.r == 0:
+                return self._solve_r0(inst)
+            st = self.tuning.strategy
+            if i_limit is None and (st == "bounded" or st == "auto"):
+                from . import bsolve
+                if bsolve.applicable(inst) and (st == "bounded" or bsolve.prunes(inst)):
+                    if self._bounded is None:
+                        self._bounded = bsolve.BoundedSolve(self)
+                    return self._bounded.solve(inst, verify)
+            nD, nI = ncomb(len(inst.B0), inst.r), ncomb(len(inst.INS), inst.r)
+            if i_limit is not None:
+                nI = min(nI, int(i_limit))
+            return SolveResult([], nD, nI, 0, 0, 0, 0)
+        return self._run_plan(inst, plan, verify, timed, marks)
+
+    def _run_plan(self, inst: Instance, plan: dict, verify: bool, timed: bool = False,
+                  marks: list | None = None) -> SolveResult:
+        """Enqueue, collect, and re-run with larger capacities while a buffer overflows."""
         for _attempt in range(6):
             ev0 = ev1 = None
             if timed:
@@ -538,11 +595,65 @@ class Solver:
                     out.device_ms = ev0.elapsed_time(ev1)
                 out.launches = h["launches"]
                 return out
-            plan = self.plan(nD, nI, newp["capD"], newp["capI"], newp["pairs"])
-            plan["strategy"] = newp.get("strategy", plan["strategy"])
-            plan["i_limit"] = i_limit
-            plan["no_part"] = newp.get("no_part", False)
+            plan = self._replan(inst, newp)
         raise _lib.CfError(_lib.CF_EOVERFLOW, "solve", "capacities kept overflowing")
+
+    def _stage_readback(self, h: dict, rows: int):
+        """Queue, behind a solve's kernels, the copy of its counters and of its first `rows`
+        checked rows into page-locked memory, and an event after them: collect() then waits
+        for this solve alone, not for work queued after it."""
+        torch = self.torch
+        rb = self.result_bytes
+        rows = max(0, min(int(rows), int(h["plan"]["pairs"])))
+        hm = self._pinned_buf("readback", 8 + rows * rb)
+        st = self._torch_stream()
+        with torch.cuda.stream(st):
+            hm[:8].copy_(h["misc"][:2].view(torch.uint8), non_blocking=True)
+            if rows:
+                hm[8:8 + rows * rb].copy_(h["res"][: rows * rb], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(st)
+        h.update(ev=ev, hread=hm, hrows=rows)
+
+    def solve_many(self, insts: list, verify: bool = True, marks_list: list | None = None,
+                   i_limit: int | None = None, readback_rows: int = 256) -> list[SolveResult]:
+        """Solve instances one after another, each with its own build, probe and check, while
+        the host collects and certifies each one as the device runs the next: two buffer sets
+        alternate, and every solve's counters and first checked rows come back behind its own
+        kernels.  The results equal solve_instance's on each instance.  marks_list (optional
+        list) receives one marks list per instance (see enqueue)."""
+        out: list = [None] * len(insts)
+        pending = None
+        try:
+            for i in range(len(insts) + 1):
+                cur = None
+                if i < len(insts):
+                    inst = insts[i]
+                    marks = None
+                    if marks_list is not None:
+                        marks = []
+                        marks_list.append(marks)
+                    self._bufset = i & 1          # the set the solve in flight does not use
+                    plan = self._direct_plan(inst, i_limit)
+                    if plan is None:
+                        out[i] = self.solve_instance(inst, verify=verify, marks=marks, i_limit=i_limit)
+                    else:
+                        h = self.enqueue(inst, plan, marks)
+                        self._stage_readback(h, readback_rows)
+                        cur = (i, h, marks)
+                if pending is not None:
+                    j, h, marks = pending
+                    self._bufset = j & 1
+                    res, newp = self.collect(insts[j], h, verify)
+                    if res is None:                # an overflow: run it again alone, larger
+                        res = self._run_plan(insts[j], self._replan(insts[j], newp), verify, marks=marks)
+                    else:
+                        res.launches = h["launches"]
+                    out[j] = res
+                pending = cur
+        finally:
+            self._bufset = 0
+        return out
 
     def _torch_stream(self):
         return self.stream if self.stream is not None else self.torch.cuda.current_stream(self.device)
@@ -578,6 +689,24 @@ def solve(M: int, Q, B0, r: int, B: int, device=None, verify: bool = True, strat
     if s is None:
         s = _default_solvers[key] = Solver(dev, tuning=Tuning(strategy=strategy))
     return s.solve(M, Q, B0, r, B, verify=verify)
+
+
+def solve_many(instances, device=None, verify: bool = True, strategy: str = "fused") -> list[SolveResult]:
+    """solve() over a list of (M, Q, B0, r, B) tuples (or objects with those attributes), in order:
+    each instance is joined on its own on the device, while the host prepares the next one's
+    tables and collects and certifies the previous one.  Returns one SolveResult per instance,
+    equal to solve()'s."""
+    import torch
+    dev = torch.device(device if device is not None else "cuda")
+    key = (dev.type, dev.index, strategy)
+    s = _default_solvers.get(key)
+    if s is None:
+        s = _default_solvers[key] = Solver(dev, tuning=Tuning(strategy=strategy))
+    xs = []
+    for w in instances:
+        M, Q, B0, r, B = (w.M, w.Q, w.B0, w.r, w.B) if hasattr(w, "M") else w
+        xs.append(Instance.build(M, Q, B0, r, B))
+    return s.solve_many(xs, verify=verify)
 
 
 def decode_pair(inst: Instance, d_rank: int, i_rank: int):
