@@ -217,13 +217,17 @@ class _Pools:
 
 
 def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: int = 4000, k: int = 64,
-               sieve_bound: int = SIEVE_BOUND, consider=None, log=None, solver=None) -> dict:
+               sieve_bound: int = SIEVE_BOUND, consider=None, log=None, solver=None, workers: int = 2) -> dict:
     """Run every survivor row as gpu/run_mstar_family.py:66-94 drives the reference's GPU driver: the
     k smallest primes of the capped pool checked as a Carmichael number below U (radius 0), then each
     radius r_min..min(rmax, r_max) at the driver's h-stratum bound, through ``driver.run_instance`` (the
     driver's Icap/Dmin/affordable-pool bounds, product-bounded producers and record join on the GPU).
     Radii 1..16 are run; radii whose bounds need more than 128-bit products (or colex ids of 2^64 and
     more) are reported as skipped.
+
+    With workers > 1 the instances' GPU joins run ahead on that many worker threads, each with its own
+    solver and CUDA stream (one instance's kernels overlap another's host work), while the exact
+    checks, consider() and log() run here in the order above, exactly as with one worker.
 
     Returns (runs, completions): runs = {D: {"base_carmichael", "base_below_U", "instances": [per-radius
     counts], "skipped": [r]}}; completions = the (key, factors, label) of every completion below U that
@@ -240,6 +244,8 @@ def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: in
     solver = solver or Solver(tuning=Tuning(strategy="bounded"))
     out = {}
     pools = _Pools([int(r["D"]) for r in rows if _searchable(int(r["D"]))], sieve_bound)
+    # host pass: every row's base and the instances to join, in the reference's order
+    steps = []                     # ("base", D, base) or ("inst", rec, (base, INS, r, h, D))
     for row in rows:
         D, cap, rmax = int(row["D"]), int(row["cap"]), int(row["rmax"])
         if not _searchable(D):
@@ -251,7 +257,7 @@ def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: in
         ok, n, _ = verify_certificate(base)
         rec = {"base_carmichael": bool(ok), "base_below_U": bool(ok and n < U), "instances": [], "skipped": []}
         if ok and n < U:
-            consider((D, "ksmall", 0, 0), base, "census_base")
+            steps.append(("base", D, base))
         hi = rmax if r_max is None else min(rmax, r_max)
         for r in range(max(1, r_min), hi + 1):
             h = driver.hmax_for(base, INS, r, U, split)
@@ -261,11 +267,58 @@ def family_run(rows, U: int, r_min: int = 1, r_max: int | None = None, split: in
             if len(aff) >= r and not bsolve.bounds_fit(base, aff, r, Icap):
                 rec["skipped"].append(r)
                 continue
-            st: dict = {}
-            driver.run_instance("ksmall", base, INS, r, h, D, U, split, consider, log, st, solver)
-            rec["instances"].append(st["last"])
+            steps.append(("inst", rec, (base, INS, r, h, D)))
         out[D] = rec
+    jobs = [a for kind, _, a in steps if kind == "inst"]
+    joined = _join_ahead(jobs, U, split, solver, workers)
+    for kind, x, a in steps:
+        if kind == "base":
+            consider((x, "ksmall", 0, 0), a, "census_base")
+            continue
+        base, INS, r, h, D = a
+        st: dict = {}
+        driver.run_instance("ksmall", base, INS, r, h, D, U, split, consider, log, st, solver,
+                            joined=next(joined))
+        x["instances"].append(st["last"])
     return out, hits
+
+
+def _join_ahead(jobs, U: int, split: int, solver, workers: int):
+    """Iterator over driver.instance_join's results for jobs (base, INS, r, h, M), in order.  With
+    workers > 1 the joins run on worker threads, each with a solver on its own CUDA stream (the
+    library's C calls release the interpreter lock while they wait for the device)."""
+    from . import driver
+    if workers <= 1 or len(jobs) < 2:
+        for base, INS, r, h, M in jobs:
+            yield driver.instance_join(base, INS, r, h, M, U, split, solver)
+        return
+    import queue
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    from .solve import Solver
+    # the worker solvers live on the caller's solver, so later runs reuse their streams and buffers
+    ws = getattr(solver, "_join_workers", None)
+    if ws is None or len(ws) < workers:
+        ws = solver._join_workers = [Solver(solver.device, stream=torch.cuda.Stream(solver.device),
+                                            tuning=solver.tuning) for _ in range(workers)]
+    free: queue.Queue = queue.Queue()
+    for w in ws[:workers]:
+        free.put(w)
+    local = threading.local()
+
+    def run(job):
+        if getattr(local, "solver", None) is None:
+            local.solver = free.get()
+        base, INS, r, h, M = job
+        return driver.instance_join(base, INS, r, h, M, U, split, local.solver)
+
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        futs = [ex.submit(run, j) for j in jobs]
+        for f in futs:
+            yield f.result()
 
 
 # -- lambda-neighbourhood census ------------------------------------------------------------

@@ -78,13 +78,30 @@ def build_D(B0, M: int, r: int, Dmin=None, nchunks: int = 1, device=None):
     return chunks, nD
 
 
+def instance_join(B0, INS, r: int, hmax: int, M: int, U: int, split: int, solver=None):
+    """The GPU part of run_instance: the filtered sides joined under the driver's bounds.
+    Returns (pairs as (D index tuple, I index tuple), nD, nI, seconds), or None when the
+    affordable pool holds fewer than r primes (nothing to search)."""
+    from .solve import Solver, Tuning
+    Icap, Dmin, _cap_r, INS_aff = instance_bounds(B0, INS, r, U)
+    if len(INS_aff) < r:
+        return None
+    s = solver or Solver(tuning=Tuning(strategy="bounded"))
+    if s._bounded is None:
+        from .bsolve import BoundedSolve
+        s._bounded = BoundedSolve(s)
+    t0 = time.time()
+    pairs_idx, nD, nI, _plan = s._bounded.join(sorted(B0), INS_aff, r, M, math.prod(B0), Icap, Dmin, split, hmax)
+    return pairs_idx, nD, nI, time.time() - t0
+
+
 def run_instance(tag, B0, INS, r: int, hmax: int, M: int, U: int, split: int, consider, log,
-                 state: dict | None = None, solver=None) -> bool:
+                 state: dict | None = None, solver=None, joined=None) -> bool:
     """One exchange instance below the bound U, as the driver's run_instance: returns True
     when the instance is complete.  consider(key, factors, label) receives every completion
     below U (the driver's incumbent update and oracle); log(str) writes the instance line
-    (None: no line)."""
-    from .solve import Solver, Tuning
+    (None: no line).  joined: instance_join's result for these arguments, when the join has
+    already run (family runs join ahead on worker streams)."""
     B0s = sorted(B0)
     B0set = set(B0)
     P0 = math.prod(B0)
@@ -96,13 +113,9 @@ def run_instance(tag, B0, INS, r: int, hmax: int, M: int, U: int, split: int, co
         st["instances"] = st.get("instances", 0) + 1
         st["last"] = dict(r=r, hmax=hmax, ins=len(INS_aff), nD=0, nI=0, pairs=0, below_U=0)
         return True
-    s = solver or Solver(tuning=Tuning(strategy="bounded"))
-    if s._bounded is None:
-        from .bsolve import BoundedSolve
-        s._bounded = BoundedSolve(s)
-    t0 = time.time()
-    pairs_idx, nD, nI, plan = s._bounded.join(B0s, INS_aff, r, M, P0, Icap, Dmin, split, hmax)
-    dt = time.time() - t0
+    if joined is None:
+        joined = instance_join(B0, INS, r, hmax, M, U, split, solver)
+    pairs_idx, nD, nI, dt = joined
     below = nb = 0
     rmin = None
     for di, ii in pairs_idx:

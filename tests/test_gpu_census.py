@@ -59,3 +59,20 @@ def test_family_run_on_a_modulus_above_2_64(cuda):
                  if math.prod(c) < Icap and sum(p > 4000 for p in c) <= h)
         assert (x["nD"], x["nI"]) == (nD, nI), r
         assert 0 < nD < math.comb(len(base), r) or 0 < nI < math.comb(len(aff), r)
+
+
+def test_family_run_same_with_any_number_of_join_workers(cuda):
+    # the joins run ahead on worker threads and streams; the runs and their order do not change
+    with open(GOLD) as f:
+        fam = json.load(f)
+    U = int(fam["U"])
+    rows = fam["survivors"][:12]
+    s = Solver(cuda, tuning=Tuning(strategy="bounded"))
+    seen = {1: [], 3: []}
+    outs = {}
+    for w in (1, 3):
+        outs[w] = C.family_run(rows, U, r_max=8, solver=s, workers=w,
+                               consider=lambda key, fac, label, w=w: seen[w].append(key) or True)
+    assert outs[1] == outs[3]
+    assert seen[1] == seen[3]
+    assert sum(len(v["instances"]) for v in outs[1][0].values()) > 40
