@@ -616,13 +616,32 @@ class Solver:
         h.update(ev=ev, hread=hm, hrows=rows)
 
     def solve_many(self, insts: list, verify: bool = True, marks_list: list | None = None,
-                   i_limit: int | None = None, readback_rows: int = 256) -> list[SolveResult]:
+                   i_limit: int | None = None, readback_rows: int = 256, streams: int = 2) -> list[SolveResult]:
         """Solve instances one after another, each with its own build, probe and check, while
         the host collects and certifies each one as the device runs the next: two buffer sets
         alternate, and every solve's counters and first checked rows come back behind its own
-        kernels.  The results equal solve_instance's on each instance.  marks_list (optional
-        list) receives one marks list per instance (see enqueue)."""
+        kernels.  With streams = 2 the two buffer sets also have a CUDA stream each, so one
+        solve's table build can run beside the previous solve's probe.  The results equal
+        solve_instance's on each instance.  marks_list (optional list) receives one marks list
+        per instance (see enqueue)."""
+        torch = self.torch
         out: list = [None] * len(insts)
+        base = self._torch_stream()
+        saved = (self.stream, self.tables.stream)
+        if getattr(self, "_many_streams", None) is None:
+            self._many_streams = [torch.cuda.Stream(self.device), torch.cuda.Stream(self.device)]
+        sts = self._many_streams[:2] if streams > 1 else [base]
+        for st in sts:
+            if st is not base:
+                st.wait_stream(base)               # after everything queued before the call
+
+        def use(k):
+            self._bufset = k & 1
+            st = sts[k & 1] if len(sts) > 1 else sts[0]
+            self.stream = st
+            self.tables.stream = st
+            return torch.cuda.stream(st)
+
         pending = None
         try:
             for i in range(len(insts) + 1):
@@ -633,26 +652,30 @@ class Solver:
                     if marks_list is not None:
                         marks = []
                         marks_list.append(marks)
-                    self._bufset = i & 1          # the set the solve in flight does not use
-                    plan = self._direct_plan(inst, i_limit)
-                    if plan is None:
-                        out[i] = self.solve_instance(inst, verify=verify, marks=marks, i_limit=i_limit)
-                    else:
-                        h = self.enqueue(inst, plan, marks)
-                        self._stage_readback(h, readback_rows)
-                        cur = (i, h, marks)
+                    with use(i):                   # the set (and stream) the solve in flight does not use
+                        plan = self._direct_plan(inst, i_limit)
+                        if plan is None:
+                            out[i] = self.solve_instance(inst, verify=verify, marks=marks, i_limit=i_limit)
+                        else:
+                            h = self.enqueue(inst, plan, marks)
+                            self._stage_readback(h, readback_rows)
+                            cur = (i, h, marks)
                 if pending is not None:
                     j, h, marks = pending
-                    self._bufset = j & 1
-                    res, newp = self.collect(insts[j], h, verify)
-                    if res is None:                # an overflow: run it again alone, larger
-                        res = self._run_plan(insts[j], self._replan(insts[j], newp), verify, marks=marks)
-                    else:
-                        res.launches = h["launches"]
+                    with use(j):
+                        res, newp = self.collect(insts[j], h, verify)
+                        if res is None:            # an overflow: run it again alone, larger
+                            res = self._run_plan(insts[j], self._replan(insts[j], newp), verify, marks=marks)
+                        else:
+                            res.launches = h["launches"]
                     out[j] = res
                 pending = cur
         finally:
             self._bufset = 0
+            self.stream, self.tables.stream = saved
+            for st in sts:
+                if st is not base:
+                    base.wait_stream(st)           # work queued after the call follows every solve
         return out
 
     def _torch_stream(self):

@@ -97,9 +97,11 @@ class DeviceTables:
 
     stream: the torch stream of the uploads and tail builds (None: the current stream).  With
     async_upload a table is staged in page-locked memory and copied without waiting for the
-    device, so kernels queued before it keep running; the consumer must then launch on the same
-    stream (the single-modulus solver does).  Otherwise the copy returns when the data is on the
-    device, which any stream may use."""
+    device, so kernels queued before it keep running.  An entry remembers the stream it was made
+    on and an event after it; a later lookup from another stream (the one the lookup's kernels
+    will use: `stream`, or the current stream) makes that stream wait for the event and marks the
+    tensor as used there, so entries can be shared by solves on two streams.  Otherwise the copy
+    returns when the data is on the device, which any stream may use."""
 
     RING_BYTES = 4 << 20
 
@@ -110,27 +112,61 @@ class DeviceTables:
         self.async_upload = async_upload
         self._ring = None
         self._cache: dict = {}
+        self._made: dict = {}          # key -> (raw stream it was made on, event after it)
+
+    def _stream_now(self):
+        import torch
+        return self.stream if self.stream is not None else torch.cuda.current_stream(self.device)
+
+    def _made_on(self, key, t, s):
+        import torch
+        ev = torch.cuda.Event()
+        ev.record(s)
+        self._made[key] = (s.cuda_stream, ev)
+
+    def _use(self, key, t):
+        """Order the current stream after the making of entry `key` when it was made on another."""
+        made = self._made.get(key)
+        if made is None:
+            return t
+        s = self._stream_now()
+        if made[0] != s.cuda_stream:
+            s.wait_event(made[1])
+            t.record_stream(s)
+        return t
+
+    def _insert(self, key, t):
+        if len(self._cache) >= self.max_entries:
+            old = next(iter(self._cache))
+            self._cache.pop(old)
+            self._made.pop(old, None)
+        self._cache[key] = t
 
     def get(self, key, make):
         import torch
         t = self._cache.get(key)
-        if t is None:
-            host = make()
-            if self.async_upload:
-                s = self.stream if self.stream is not None else torch.cuda.current_stream(self.device)
+        if t is not None:
+            return self._use(key, t)
+        host = make()
+        if self.async_upload:
+            s = self._stream_now()
+            with _on_stream(s):
+                t = torch.empty(host.shape, dtype=torch.from_numpy(host[:0]).dtype, device=self.device)
+            if self._ring is None:
+                self._ring = _PinnedRing(self.RING_BYTES)
+            if not self._ring.upload(host, t, s):
                 with _on_stream(s):
-                    t = torch.empty(host.shape, dtype=torch.from_numpy(host[:0]).dtype, device=self.device)
-                if self._ring is None:
-                    self._ring = _PinnedRing(self.RING_BYTES)
-                if not self._ring.upload(host, t, s):
-                    with _on_stream(s):
-                        t.copy_(torch.from_numpy(host), non_blocking=False)
-            else:
-                t = torch.from_numpy(host).to(self.device, non_blocking=False)
-            if len(self._cache) >= self.max_entries:
-                self._cache.pop(next(iter(self._cache)))
-            self._cache[key] = t
+                    t.copy_(torch.from_numpy(host), non_blocking=False)
+            self._made_on(key, t, s)
+        else:
+            t = torch.from_numpy(host).to(self.device, non_blocking=False)
+        self._insert(key, t)
         return t
+
+    def clear(self):
+        """Drop every entry (the next lookups make and upload their tables again)."""
+        self._cache.clear()
+        self._made.clear()
 
     def pool(self, primes, r: int, M: int, mult: int):
         key = ("pool", tuple(int(p) for p in primes), r, M, int(mult) % M)
@@ -141,16 +177,17 @@ class DeviceTables:
         import torch
         key = ("tail", tuple(int(p) for p in primes), r, M, int(mult) % M)
         t = self._cache.get(key)
-        if t is None:
-            lib = _lib.load()
-            nbytes = lib.cf_tail_bytes(len(primes), r)
-            with _on_stream(self.stream if self.stream is not None else torch.cuda.current_stream(self.device)):
-                t = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=self.device)
-            _lib.check(lib.cf_build_tail(pool_dev.data_ptr(), len(primes), r, t.data_ptr(),
-                                         _lib.stream_handle(self.stream)), "cf_build_tail")
-            if len(self._cache) >= self.max_entries:
-                self._cache.pop(next(iter(self._cache)))
-            self._cache[key] = t
+        if t is not None:
+            return self._use(key, t)
+        lib = _lib.load()
+        nbytes = lib.cf_tail_bytes(len(primes), r)
+        s = self._stream_now()
+        with _on_stream(s):
+            t = torch.empty(max(nbytes, 16), dtype=torch.uint8, device=self.device)
+        _lib.check(lib.cf_build_tail(pool_dev.data_ptr(), len(primes), r, t.data_ptr(),
+                                     _lib.stream_handle(self.stream)), "cf_build_tail")
+        self._made_on(key, t, s)
+        self._insert(key, t)
         return t
 
     def screen(self, P0: int, B: int, eps: float):
