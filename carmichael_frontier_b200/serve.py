@@ -125,6 +125,7 @@ class Ticket:
     result: SolveResult | None = None
     error: str | None = None
     exclusive: bool = False
+    large: bool = False                 # runs in the large lane (one at a time, high priority)
     done: threading.Event = field(default_factory=threading.Event)
 
     @property
@@ -136,12 +137,18 @@ class Admission:
     """Byte budget and FIFO queue with bounded bypass: a worker takes the oldest
     waiting request whose footprint fits; a request that has been passed over
     `max_bypass` times blocks younger ones until it fits.  A request larger than
-    the budget runs alone."""
+    the budget runs alone.  Large requests (Ticket.large) run one at a time in
+    arrival order -- the tail of the latency distribution is theirs, and two of
+    them sharing the GPU both finish late -- while younger small ones pass a large
+    request that waits for the lane; while a large request runs, at most
+    `beside_large` small ones (None: any number) run beside it."""
 
-    def __init__(self, budget: int, max_bypass: int = 8):
+    def __init__(self, budget: int, max_bypass: int = 8, beside_large: int | None = None):
         self.budget = int(budget)
         self.used = 0
         self.running = 0
+        self.large_running = 0
+        self.beside_large = beside_large      # small requests admitted while a large one runs (None: any)
         self.peak = 0
         self.max_bypass = max_bypass
         self.q: deque = deque()
@@ -162,6 +169,11 @@ class Admission:
 
     def _pick(self):
         for i, t in enumerate(self.q):
+            if t.large and not t.exclusive and self.large_running:
+                continue             # the large lane is busy: younger requests may pass, not counted as bypass
+            if (not t.large and self.large_running and self.beside_large is not None
+                    and self.running - self.large_running >= self.beside_large):
+                return None          # a large request runs: only beside_large small ones share the GPU with it
             if t.exclusive:
                 ok = self.running == 0
             else:
@@ -183,6 +195,7 @@ class Admission:
                     # a request larger than the budget takes all of it: nothing runs beside it
                     self.used += self.budget if t.exclusive else t.need
                     self.running += 1
+                    self.large_running += int(t.large)
                     self.peak = max(self.peak, self.used)
                     self.bypassed.pop(t.rid, None)
                     return t
@@ -194,6 +207,7 @@ class Admission:
         with self.cv:
             self.used -= self.budget if t.exclusive else t.need
             self.running -= 1
+            self.large_running -= int(t.large)
             self.cv.notify_all()
 
 
@@ -204,13 +218,18 @@ class Server:
     budget: device bytes that admitted requests may hold together (default: 60%
     of the free device memory at start); solve_fn(worker_state, inst) may replace
     the GPU solve (used by CPU tests of the admission logic).
-    large_work: requests whose estimated records (footprint()["work"]) reach this run on their
-    worker's high-priority stream, so that the largest requests -- the tail of the latency
-    distribution -- are not slowed by the small ones sharing the GPU with them (the small ones
-    still fill the SMs the large one leaves free)."""
+    large_work: requests whose estimated records (footprint()["work"]) reach this are large: they
+    run one at a time (Admission), each on its worker's high-priority stream, so that the largest
+    requests -- the tail of the latency distribution -- neither share the GPU with one another
+    nor wait behind the small ones' kernels (the small ones still fill the SMs a large one leaves
+    free); beside_large caps the small requests that run while a large one does (None: any).
+    The default large_work is the measured knee of the seeded serving stream: its requests above
+    3e9 estimated records take 0.2-1.7 s alone and are about a sixth of the stream, those below
+    take milliseconds."""
 
     def __init__(self, device=None, slots: int = 4, budget: int | None = None, strategy: str = "auto",
-                 solve_fn=None, clock=time.perf_counter, large_work: float = 2e9):
+                 solve_fn=None, clock=time.perf_counter, large_work: float = 3e9,
+                 beside_large: int | None = None):
         self.slots = slots
         self.large_work = large_work
         self.clock = clock
@@ -221,7 +240,7 @@ class Server:
             import torch
             free, _total = torch.cuda.mem_get_info(torch.device(device if device is not None else "cuda"))
             budget = int(free * 0.6)
-        self.adm = Admission(budget)
+        self.adm = Admission(budget, beside_large=beside_large)
         self.tickets: list[Ticket] = []
         self._rid = 0
         self._threads: list[threading.Thread] = []
@@ -251,6 +270,7 @@ class Server:
             t.need, t.work = fp["bytes"], fp.get("work", 0)
         else:
             t.need, t.work = getattr(inst, "need", 1), getattr(inst, "work", 0)
+        t.large = t.work >= self.large_work
         self.tickets.append(t)
         self.adm.put(t)
         return t
@@ -264,7 +284,7 @@ class Server:
                 return
             t.admitted = self.clock()
             try:
-                t.result = self._solve(state, t.inst, t.work >= self.large_work)
+                t.result = self._solve(state, t.inst, t.large)
             except Exception as e:                     # noqa: BLE001 - reported per request
                 t.error = f"{type(e).__name__}: {e}"
             finally:

@@ -112,3 +112,56 @@ def test_footprint_reports_work_and_large_requests_take_the_fast_path():
         srv.submit(Job(w)).done.wait()
     srv.stop()
     assert sorted(seen) == [(5, False), (7, False), (100, True), (5000, True)]
+
+
+def test_large_requests_run_one_at_a_time_in_order():
+    # requests at or above large_work share a one-request lane in arrival order; small ones run
+    # beside a large one and pass a large one that waits for the lane
+    active, log = [], []
+    lock = threading.Lock()
+
+    def solve(state, inst):
+        with lock:
+            active.append(inst)
+            log.append((inst.rid, [a.rid for a in active if a.work >= 100]))
+        time.sleep(inst.dt)
+        with lock:
+            active.remove(inst)
+        return types.SimpleNamespace(hits=[], rid=inst.rid)
+
+    srv = Server(slots=4, budget=1000, solve_fn=solve, large_work=100).start()
+    big = [types.SimpleNamespace(rid=i, need=1, work=500, dt=0.03) for i in range(3)]
+    small = [types.SimpleNamespace(rid=10 + i, need=1, work=5, dt=0.002) for i in range(12)]
+    ts = [srv.submit(q) for q in (big[0], big[1], small[0], big[2], *small[1:])]
+    for t in ts:
+        assert t.done.wait(20)
+    srv.stop()
+    assert all(len(larges) <= 1 for _rid, larges in log)
+    starts = [rid for rid, _ in log]
+    assert [r for r in starts if r < 10] == [0, 1, 2]
+    assert starts.index(10) < starts.index(1)                 # a small one passed the waiting large one
+    assert srv.adm.large_running == 0 and srv.adm.used == 0
+
+
+def test_small_requests_beside_a_large_one_are_capped():
+    active, log = [], []
+    lock = threading.Lock()
+
+    def solve(state, inst):
+        with lock:
+            active.append(inst)
+            log.append((inst.rid, sum(1 for a in active if a.work >= 100), sum(1 for a in active if a.work < 100)))
+        time.sleep(inst.dt)
+        with lock:
+            active.remove(inst)
+        return types.SimpleNamespace(hits=[], rid=inst.rid)
+
+    srv = Server(slots=4, budget=1000, solve_fn=solve, large_work=100, beside_large=1).start()
+    big = types.SimpleNamespace(rid=0, need=1, work=500, dt=0.05)
+    small = [types.SimpleNamespace(rid=1 + i, need=1, work=5, dt=0.005) for i in range(10)]
+    ts = [srv.submit(big)] + [srv.submit(q) for q in small]
+    for t in ts:
+        assert t.done.wait(20)
+    srv.stop()
+    assert all(nsmall <= 1 for _rid, nlarge, nsmall in log if nlarge)
+    assert any(nlarge and nsmall for _rid, nlarge, nsmall in log)    # one small ran beside the large one
