@@ -107,7 +107,7 @@ __device__ __forceinline__ bool batch_ticket(const CfBatchMod& md, u32 mod, u64 
                           (cf_word8(a, c, bk.w2) & bk.m2);
           if (!in) continue;
         }
-        dtab_probe(tab, cf_fuse_key(X, x2, tab.bbits), rank_base + off, sink);
+        dtab_probe(tab, X, x2, rank_base + off, sink);
       }
     }
   }

@@ -48,7 +48,7 @@ k_bgen_probe(int r, int n, u64 F, const u64* __restrict__ pool, const u64* __res
       if (!((cf_word8(u, v, bk.w0) & bk.m0) && (cf_word8(u, v, bk.w1) & bk.m1) && (cf_word8(u, v, bk.w2) & bk.m2)))
         continue;
     }
-    dtab_probe(tab, cf_fuse_key(X, 0u, tab.bbits), iid, sink);
+    dtab_probe(tab, X, 0u, iid, sink);
   }
 }
 

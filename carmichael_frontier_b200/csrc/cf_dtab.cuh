@@ -25,13 +25,19 @@ constexpr size_t kBinomSmemMaxF = 24 * 1024;
 struct CfFuseKey {
   u32 bucket, f16, f32;
 };
-__device__ __forceinline__ CfFuseKey cf_fuse_key(u64 X, u32 x2, int bbits) {
+__device__ __forceinline__ u32 cf_fuse_f32(u64 X, u32 x2) {
+  return (u32)X ^ ((u32)(X >> 32) * 0x85EBCA6Bu) ^ (x2 * 0xC2B2AE35u);
+}
+__device__ __forceinline__ void cf_fuse_bucket(u64 X, u32 x2, int bbits, u32& bucket, u32& f16) {
   const u64 h = (X ^ ((u64)x2 << 32)) * CF_HASH_MULT;
-  CfFuseKey k;
-  k.bucket = (u32)(h >> (64 - bbits));
+  bucket = (u32)(h >> (64 - bbits));
   const u32 f = (u32)(h >> (48 - bbits)) & 0xffffu;
-  k.f16 = f ? f : 1u;                       // 0 marks an empty slot
-  k.f32 = (u32)X ^ ((u32)(X >> 32) * 0x85EBCA6Bu) ^ (x2 * 0xC2B2AE35u);
+  f16 = f ? f : 1u;                         // 0 marks an empty slot
+}
+__device__ __forceinline__ CfFuseKey cf_fuse_key(u64 X, u32 x2, int bbits) {
+  CfFuseKey k;
+  cf_fuse_bucket(X, x2, bbits, k.bucket, k.f16);
+  k.f32 = cf_fuse_f32(X, x2);
   return k;
 }
 
@@ -241,11 +247,14 @@ __device__ __forceinline__ u32 cf_zero_half(u32 w) { return (w - 0x00010001u) & 
 // words).  Slots are claimed in order, so the bucket is full exactly when its
 // last slot (the high half of the last word) is occupied.
 __device__ __forceinline__ bool probe_match(uint4 r0, uint4 r1, u32 f16) {
+  // (t - 0x00010001) & ~t per word, OR-ed over the words before the one mask: the same
+  // bits as OR-ing the eight masked tests, one three-input logic op per word
   const u32 ff = f16 * 0x10001u;
-  const u32 eq = cf_zero_half(r0.x ^ ff) | cf_zero_half(r0.y ^ ff) | cf_zero_half(r0.z ^ ff) |
-                 cf_zero_half(r0.w ^ ff) | cf_zero_half(r1.x ^ ff) | cf_zero_half(r1.y ^ ff) |
-                 cf_zero_half(r1.z ^ ff) | cf_zero_half(r1.w ^ ff);
-  return eq != 0u;
+  const u32 w[8] = {r0.x ^ ff, r0.y ^ ff, r0.z ^ ff, r0.w ^ ff, r1.x ^ ff, r1.y ^ ff, r1.z ^ ff, r1.w ^ ff};
+  u32 acc = 0u;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc |= (w[i] - 0x00010001u) & ~w[i];
+  return (acc & 0x80008000u) != 0u;
 }
 
 // Probe the table for one residue.  The bucket's fingerprint row is tested in
@@ -271,16 +280,19 @@ __device__ __forceinline__ void dtab_row(const u32* row, bool wide, uint4& r0, u
   }
 }
 
-__device__ __forceinline__ void dtab_probe(const DTab& t, const CfFuseKey& fk, u64 rank, const CfPairSink& o) {
-  u64 b = fk.bucket;
+// Probe for the residue (X, x2) (x2 = 0 for keys that carry the whole residue in X).
+__device__ __forceinline__ void dtab_probe(const DTab& t, u64 X, u32 x2, u64 rank, const CfPairSink& o) {
+  u32 bucket, f16;
+  cf_fuse_bucket(X, x2, t.bbits, bucket, f16);
+  u64 b = bucket;
   const bool wide = ((uintptr_t)t.fpw & 31u) == 0u;
 #pragma unroll 1
   for (int hop = 0;; ++hop) {
     uint4 r0, r1;
     dtab_row(t.fpw + b * 8, wide, r0, r1);
     const bool full = (r1.w >> 16) != 0u;
-    if (probe_match(r0, r1, fk.f16) || (full && hop == kProbeHops - 1)) {
-      probe_slow(t, b, fk.f16, fk.f32, rank, o);
+    if (probe_match(r0, r1, f16) || (full && hop == kProbeHops - 1)) {
+      probe_slow(t, b, f16, cf_fuse_f32(X, x2), rank, o);   // the side fingerprint: cold path only
       return;
     }
     if (!full) return;

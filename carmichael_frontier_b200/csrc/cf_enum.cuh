@@ -216,7 +216,7 @@ struct CfTailWalker {
   static constexpr int A = R - B;
   int idx[A > 0 ? A : 1];        // prefix indices
   CfElt32 Q[A + 1];              // Q[j] = start * p[idx[0]] ... p[idx[j-1]] (lazy, 32-bit radix)
-  u64 cur, tend;                 // position in the tail table and its end
+  u32 cur, tend;                 // position in the tail table and its end (C(n, B) <= 523,776 entries)
 
   __device__ __forceinline__ void init(u64 rank, int n, const u64* __restrict__ binom, const CfArithFast& ar,
                                        CfElt32 start, u64 tail_n) {
@@ -227,8 +227,8 @@ struct CfTailWalker {
     Q[0] = start;
 #pragma unroll
     for (int j = 1; j <= A; ++j) Q[j] = ar.mul(Q[j - 1], idx[j - 1]);
-    cur = cf_rank_lex<B, R>(full + A, n, binom);
-    tend = tail_n;
+    cur = (u32)cf_rank_lex<B, R>(full + A, n, binom);
+    tend = (u32)tail_n;
   }
 
   __device__ __forceinline__ bool next_prefix(int n, const u64* __restrict__ binom, const CfArithFast& ar) {
@@ -254,7 +254,7 @@ struct CfTailWalker {
         for (int t = 1; t <= A; ++t)
           if (t > j) Q[t] = ar.mul(Q[t - 1], idx[t - 1]);
       }
-      cur = tend - cf_binom(binom, R, n - idx[A - 1] - 1, B);
+      cur = tend - (u32)cf_binom(binom, R, n - idx[A - 1] - 1, B);
       return true;
     }
   }
@@ -264,10 +264,10 @@ struct CfTailWalker {
   template <bool WANT_IDX>
   __device__ __forceinline__ void step(int n, const u64* __restrict__ binom, const CfArithFast& ar, int lane,
                                        CfElt32& myQ, u64& myj, int (&myidx)[A > 0 ? A : 1]) {
-    if (tend - cur >= 32) {                       // common case: the whole step lies in one tail
+    if (tend - cur >= 32u) {                      // common case: the whole step lies in one tail
       myQ = Q[A];
-      myj = cur + (u64)lane;
-      cur += 32;
+      myj = (u64)(cur + (u32)lane);
+      cur += 32u;
       if (WANT_IDX) {
 #pragma unroll
         for (int j = 0; j < A; ++j) myidx[j] = idx[j];
@@ -278,18 +278,18 @@ struct CfTailWalker {
     myj = ~0ull;
     do {
       if (cur >= tend && !next_prefix(n, binom, ar)) break;
-      const u64 avail = tend - cur;
-      const int take = avail < (u64)(32 - f) ? (int)avail : 32 - f;
+      const u32 avail = tend - cur;
+      const int take = avail < (u32)(32 - f) ? (int)avail : 32 - f;
       if ((unsigned)(lane - f) < (unsigned)take) {
         myQ = Q[A];
-        myj = cur + (u64)(lane - f);
+        myj = (u64)(cur + (u32)(lane - f));
         if (WANT_IDX) {
 #pragma unroll
           for (int j = 0; j < A; ++j) myidx[j] = idx[j];
         }
       }
       f += take;
-      cur += (u64)take;
+      cur += (u32)take;
     } while (f < 32);
   }
 };

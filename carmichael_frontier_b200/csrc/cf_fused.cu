@@ -62,7 +62,7 @@ __device__ __forceinline__ const u64* fuse_setup(const u64* __restrict__ pool, u
 //         bound by the latency of the claims, not by their number).
 // MODE 1: probe every record of [lo, lo+count) against the D table.
 template <int R, int MODE, bool BLOOM>
-__global__ void __launch_bounds__(kFuseBlock)
+__global__ void __launch_bounds__(kFuseBlock, 4)   // 64 registers: four CTAs per SM
 k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo, u64 count, DTab tab,
         CfPair* __restrict__ pairs, u32 max_pairs, u32* __restrict__ npairs, u32* __restrict__ err, u32 steps,
         u32 swap) {
@@ -160,7 +160,7 @@ k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo
                             (cf_word8(a, c, bk.w2) & bk.m2);
             if (!in) continue;
           }
-          dtab_probe(tab, cf_fuse_key(X, x2, tab.bbits), rank_base + off, sink);
+          dtab_probe(tab, X, x2, rank_base + off, sink);
         }
       }
     }

@@ -46,7 +46,7 @@ k_rec_probe(const u64* __restrict__ keys, u64 n, DTab tab, CfPairSink sink) {
       if (!((cf_word8(a, c, bk.w0) & bk.m0) && (cf_word8(a, c, bk.w1) & bk.m1) && (cf_word8(a, c, bk.w2) & bk.m2)))
         continue;
     }
-    dtab_probe(tab, cf_fuse_key(X, 0u, tab.bbits), i, sink);
+    dtab_probe(tab, X, 0u, i, sink);
   }
 }
 
