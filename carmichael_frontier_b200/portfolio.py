@@ -62,6 +62,7 @@ class BatchTuning:
     part_sigma: float = 8.0            # bucket-range capacity = mean + sigma*sqrt(mean) + 32
     ovf_capacity: int = 1 << 16        # records that ran past their bucket range (per batch)
     probe_per_radius: bool = True      # one probe launch per radius (kernels carry one radius's code)
+    overlap: bool = True               # consecutive batches alternate between two arenas and streams
 
 
 @dataclass
@@ -80,6 +81,7 @@ class _Batch:
     arena_bytes: int = 0
     records: int = 0
     graph: object = None
+    bset: int = 0                      # buffer set (arena, counters, pair buffers, stream) of the batch
 
 
 @dataclass
@@ -119,16 +121,32 @@ class BatchSolver:
         self.max_r = self.lib.cf_batch_max_r()
         self.result_bytes = self.lib.cf_pair_result_bytes()
         self._bufs: dict = {}
+        self._set = 0                  # buffer set of the batch being queued or collected
+        self._set_streams: list = []
+        self._capture = None           # the stream a CUDA graph is being captured on
         self._single: Solver | None = None
 
     # -- buffers -------------------------------------------------------------
     def _buf(self, name: str, nbytes: int):
-        t = self._bufs.get(name)
+        key = (name, self._set)
+        t = self._bufs.get(key)
         if t is None or t.numel() < nbytes:
             self._drop_graphs()
-            t = self.torch.empty(max(nbytes, 16), dtype=self.torch.uint8, device=self.device)
-            self._bufs[name] = t
+            with self.torch.cuda.stream(self._torch_stream()):
+                t = self.torch.empty(max(nbytes, 16), dtype=self.torch.uint8, device=self.device)
+            self._bufs[key] = t
         return t
+
+    def _nsets(self) -> int:
+        return 2 if self.tuning.overlap else 1
+
+    def _stream_of(self, k: int):
+        """The stream of buffer set k: the solver's stream for one set, else one of two own streams."""
+        if self._nsets() == 1:
+            return self.stream if self.stream is not None else self.torch.cuda.current_stream(self.device)
+        while len(self._set_streams) < 2:
+            self._set_streams.append(self.torch.cuda.Stream(self.device))
+        return self._set_streams[k]
 
     def _drop_graphs(self):
         for prep in getattr(self, "_live", []):
@@ -136,9 +154,16 @@ class BatchSolver:
                 b.graph = None
 
     def _sh(self):
-        return _lib.stream_handle(self.stream)
+        return _lib.stream_handle(self._torch_stream())
 
     def _torch_stream(self):
+        if self._capture is not None:
+            return self._capture
+        if self._nsets() > 1 and self._set_streams:
+            return self._set_streams[self._set]
+        return self.stream if self.stream is not None else self.torch.cuda.current_stream(self.device)
+
+    def _base_stream(self):
         return self.stream if self.stream is not None else self.torch.cuda.current_stream(self.device)
 
     # -- preparation ---------------------------------------------------------
@@ -288,37 +313,48 @@ class BatchSolver:
         return prep
 
     def _place(self, prep: PreparedPortfolio):
-        """Point every batch's descriptors into the shared arena and upload them."""
+        """Point every batch's descriptors into the arena of its buffer set and upload them
+        (with overlap, consecutive batches alternate between two sets)."""
         torch = self.torch
         if not prep.batches:
             return
-        need = max(b.arena_bytes for b in prep.batches)
-        arena = self._buf("arena", need)
-        abase = arena.data_ptr()
-        for b in prep.batches:
-            rows = b._rows.copy()
-            for j, k in enumerate(b.idx):
-                bb, fb = prep.shapes[k]
-                z = abase + b._zl[j]
-                rows[j]["fpw"] = z
-                rows[j]["fill"] = z + (32 << bb)
-                rows[j]["bloom"] = z + _up(36 << bb) if fb else 0
-                rows[j]["side"] = abase + b.zero_bytes + b._sl[j]
-                if j in b._part:
-                    npt, cap = b._part[j]
-                    rows[j]["pcnt"] = z + _up(36 << bb) + (_up(32 << fb) if fb else 0)
-                    pk = abase + b.zero_bytes + b._side_bytes + b._pl[j]
-                    rows[j]["pkw"] = pk
-                    rows[j]["psd"] = pk + _up(npt * cap * 4)
-            b.mods = torch.from_numpy(rows.view(np.uint8).copy()).to(self.device)
-            b._arena_ptr = abase
+        nsets = self._nsets()
+        saved = self._set
+        try:
+            for k in range(nsets):
+                mine = [bt for i, bt in enumerate(prep.batches) if i % nsets == k]
+                if not mine:
+                    continue
+                self._set = k
+                arena = self._buf("arena", max(bt.arena_bytes for bt in mine))
+                abase = arena.data_ptr()
+                for bt in mine:
+                    bt.bset = k
+                    rows = bt._rows.copy()
+                    for j, kk in enumerate(bt.idx):
+                        bb, fb = prep.shapes[kk]
+                        z = abase + bt._zl[j]
+                        rows[j]["fpw"] = z
+                        rows[j]["fill"] = z + (32 << bb)
+                        rows[j]["bloom"] = z + _up(36 << bb) if fb else 0
+                        rows[j]["side"] = abase + bt.zero_bytes + bt._sl[j]
+                        if j in bt._part:
+                            npt, cap = bt._part[j]
+                            rows[j]["pcnt"] = z + _up(36 << bb) + (_up(32 << fb) if fb else 0)
+                            pk = abase + bt.zero_bytes + bt._side_bytes + bt._pl[j]
+                            rows[j]["pkw"] = pk
+                            rows[j]["psd"] = pk + _up(npt * cap * 4)
+                    bt.mods = torch.from_numpy(rows.view(np.uint8).copy()).to(self.device)
+                    bt._arena_ptr = abase
+        finally:
+            self._set = saved
 
     # -- running -------------------------------------------------------------
     def _enqueue(self, b: _Batch, maxp: int):
         """Queue the batch's whole device sequence with one cf_solve_batch call."""
         import ctypes as C
         lib, dp = self.lib, _lib.ptr
-        arena = self._bufs["arena"]
+        arena = self._bufs[("arena", self._set)]
         misc = self._buf("misc", 64)
         ovf = self._buf("ovf", tu_ovf_bytes(self))
         pairs = self._buf("pairs", maxp * 16)
@@ -343,79 +379,126 @@ class BatchSolver:
         _lib.check(lib.cf_solve_batch(C.byref(q), self._sh()), "cf_solve_batch")
 
     def _launch(self, b: _Batch, maxp: int, graphs: bool):
+        """Queue batch b on the stream of its buffer set (replaying its CUDA graph when graphs)."""
         torch = self.torch
+        self._set = b.bset
         if not graphs:
             self._enqueue(b, maxp)
             return
-        if b.graph is None or b._graph_maxp != maxp or b._arena_ptr != self._bufs["arena"].data_ptr():
+        if b.graph is None or b._graph_maxp != maxp or b._arena_ptr != self._bufs[("arena", b.bset)].data_ptr():
             for nm, nb in (("misc", 64), ("ovf", tu_ovf_bytes(self)), ("pairs", maxp * 16), ("pmod", maxp * 4),
                            ("res", maxp * self.result_bytes)):
                 self._buf(nm, nb)            # allocate outside the capture
             g = torch.cuda.CUDAGraph()
+            home = self._torch_stream()
             s = torch.cuda.Stream(self.device)
-            s.wait_stream(self._torch_stream())
+            s.wait_stream(home)
             with torch.cuda.stream(s):
-                prev, self.stream = self.stream, s
+                self._capture = s
                 try:
                     with torch.cuda.graph(g, stream=s):
                         self._enqueue(b, maxp)
                 finally:
-                    self.stream = prev
-            self._torch_stream().wait_stream(s)
+                    self._capture = None
+            home.wait_stream(s)
             b.graph, b._graph_maxp = g, maxp
         with torch.cuda.stream(self._torch_stream()):
             b.graph.replay()
 
+    def _drain(self):
+        for k in range(self._nsets()):
+            self._stream_of(k).synchronize()
+
     def run(self, prep: PreparedPortfolio, verify: bool = True, graphs: bool = False,
             marks: list | None = None) -> list[SolveResult]:
-        """Every result of the portfolio, in input order."""
+        """Every result of the portfolio, in input order.  With overlap, batch i + 1 is queued on
+        the other buffer set and stream before batch i is collected: its table builds run beside
+        batch i's probes, and the host's certification of batch i beside its kernels."""
         torch = self.torch
         out: list = [None] * len(prep.instances)
         for k in prep.trivial:
             out[k] = self._trivial(prep, k, verify)
-        for b in prep.batches:
-            if b._arena_ptr != self._bufs["arena"].data_ptr():
-                self._place(prep)
-            for _attempt in range(8):
-                maxp = prep.pairs_cap
-                self._launch(b, maxp, graphs)
+        base = self._base_stream()
+        for k in range(self._nsets()):
+            st = self._stream_of(k)
+            if st is not base:
+                st.wait_stream(base)            # after the preparation's uploads and tail builds
+        saved = self._set
+        pending = None
+        try:
+            for b in prep.batches:
+                if pending is not None and pending.bset == b.bset:
+                    self._collect(prep, pending, graphs, verify, out, marks)   # b reuses its buffers
+                    pending = None
+                if b._arena_ptr != self._bufs[("arena", b.bset)].data_ptr():
+                    self._drain()               # another portfolio moved the arenas: place this one again
+                    self._place(prep)
+                self._launch(b, prep.pairs_cap, graphs)
                 if marks is not None:
                     ev = torch.cuda.Event(enable_timing=True)
                     ev.record(self._torch_stream())
                     marks.append(("batch", ev))
-                self._torch_stream().synchronize()
-                misc = self._bufs["misc"][:32].cpu().numpy().view(np.uint32)
-                npairs, err = int(misc[4]), int(misc[5])
-                if err & _lib.ERR_PART_OVERFLOW and b.use_part and b.n_part:
-                    b.use_part, b.graph = False, None       # a bucket range overflowed: build in place
-                    continue
-                if err & _lib.ERR_PAIR_OVERFLOW:
-                    prep.pairs_cap = 1 << max(npairs + 16, 2 * maxp).bit_length()
-                    continue
-                if err & _lib.ERR_TABLE_FULL:
-                    raise _lib.CfError(_lib.CF_EOVERFLOW, "batch", "D table full (internal error)")
-                if err:
-                    raise _lib.CfError(_lib.CF_EBADARG, "batch", f"a batched kernel rejected its work (err {err:#x})")
-                break
-            else:
-                raise _lib.CfError(_lib.CF_EOVERFLOW, "batch", "pair buffer kept overflowing")
-            rows = np.frombuffer(self._bufs["res"][: npairs * self.result_bytes].cpu().numpy().tobytes(),
-                                 dtype=RESULT_DTYPE)
-            mods = self._bufs["pmod"][: npairs * 4].cpu().numpy().view(np.uint32)
-            order = np.argsort(mods, kind="stable")
-            rows, mods = rows[order], mods[order]
-            cuts = np.searchsorted(mods, np.arange(len(b.idx) + 1))
-            for j, k in enumerate(b.idx):
-                bb, fb = prep.shapes[k]
-                plan = dict(strategy="fused", batched=True, bbits=bb, fbits=fb, i_limit=prep.i_limit)
-                out[k] = finish_rows(prep.instances[k], rows[cuts[j]:cuts[j + 1]], prep.nD[k], prep.nI[k], plan,
-                                     verify)
+                if pending is not None:
+                    self._collect(prep, pending, graphs, verify, out, marks)
+                pending = b
+            if pending is not None:
+                self._collect(prep, pending, graphs, verify, out, marks)
+        finally:
+            self._set = saved
+            for k in range(self._nsets()):
+                st = self._stream_of(k)
+                if st is not base:
+                    base.wait_stream(st)        # work queued after run() follows every batch
         if prep.fallback:
             if self._single is None:
                 self._single = Solver(self.device, self.stream, self.tuning.dtab)
             for k in prep.fallback:
                 out[k] = self._single.solve_instance(prep.instances[k], verify=verify, i_limit=prep.i_limit)
         return out
+
+    def _collect(self, prep: PreparedPortfolio, b: _Batch, graphs: bool, verify: bool, out: list, marks):
+        """Read batch b's counters on its own stream (the other batch keeps running), re-run it on
+        an overflow (after draining both streams: buffers may grow), and finish its moduli."""
+        torch = self.torch
+        for _attempt in range(8):
+            self._set = b.bset
+            with torch.cuda.stream(self._torch_stream()):
+                misc = self._bufs[("misc", b.bset)][:32].cpu().numpy().view(np.uint32)
+            npairs, err = int(misc[4]), int(misc[5])
+            retry = False
+            if err & _lib.ERR_PART_OVERFLOW and b.use_part and b.n_part:
+                b.use_part, b.graph = False, None       # a bucket range overflowed: build in place
+                retry = True
+            elif err & _lib.ERR_PAIR_OVERFLOW:
+                prep.pairs_cap = 1 << max(npairs + 16, 2 * prep.pairs_cap).bit_length()
+                retry = True
+            elif err & _lib.ERR_TABLE_FULL:
+                raise _lib.CfError(_lib.CF_EOVERFLOW, "batch", "D table full (internal error)")
+            elif err:
+                raise _lib.CfError(_lib.CF_EBADARG, "batch", f"a batched kernel rejected its work (err {err:#x})")
+            if not retry:
+                break
+            if _attempt == 7:
+                raise _lib.CfError(_lib.CF_EOVERFLOW, "batch", "pair buffer kept overflowing")
+            self._drain()
+            self._launch(b, prep.pairs_cap, graphs)
+            if marks is not None:
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record(self._torch_stream())
+                marks.append(("batch", ev))
+        self._set = b.bset
+        with torch.cuda.stream(self._torch_stream()):
+            rows = np.frombuffer(self._bufs[("res", b.bset)][: npairs * self.result_bytes].cpu().numpy().tobytes(),
+                                 dtype=RESULT_DTYPE)
+            mods = self._bufs[("pmod", b.bset)][: npairs * 4].cpu().numpy().view(np.uint32)
+        order = np.argsort(mods, kind="stable")
+        rows, mods = rows[order], mods[order]
+        cuts = np.searchsorted(mods, np.arange(len(b.idx) + 1))
+        for j, k in enumerate(b.idx):
+            bb, fb = prep.shapes[k]
+            plan = dict(strategy="fused", batched=True, bbits=bb, fbits=fb, i_limit=prep.i_limit)
+            out[k] = finish_rows(prep.instances[k], rows[cuts[j]:cuts[j + 1]], prep.nD[k], prep.nI[k], plan,
+                                 verify)
 
     def _trivial(self, prep: PreparedPortfolio, k: int, verify: bool) -> SolveResult:
         x = prep.instances[k]

@@ -75,13 +75,16 @@ def test_batched_portfolio_sample_equals_per_modulus_and_plain(cuda):
         assert a.above_bound == c.above_bound
 
 
-def test_batched_split_budget_graphs_and_overflow(cuda):
-    # many small batches (tiny budget), a pair buffer of 16 that must grow, CUDA-graph replay
+@pytest.mark.parametrize("overlap", [True, False])
+def test_batched_split_budget_graphs_and_overflow(cuda, overlap):
+    # many small batches (tiny budget), a pair buffer of 16 that must grow, CUDA-graph replay; with
+    # overlap the batches alternate between two arenas and streams, a batch queued before the
+    # previous one is collected
     M = 2 ** 5 * 3 ** 2 * 5 * 7 * 11 * 13          # tiny modulus: residues collide massively
     Q = W.eligible_pool(M)
     insts = [Instance.build(M, Q, Q[:20], 3, 1 << 2040)] + small_portfolio(7, 10)
-    ref = [summary(x) for x in BatchSolver(cuda).solve(insts)]
-    bs = BatchSolver(cuda, tuning=BatchTuning(mem_budget=4096, pair_capacity=16, ticket=64))
+    ref = [summary(x) for x in BatchSolver(cuda, tuning=BatchTuning(overlap=False)).solve(insts)]
+    bs = BatchSolver(cuda, tuning=BatchTuning(mem_budget=4096, pair_capacity=16, ticket=64, overlap=overlap))
     prep = bs.prepare(insts)
     assert len(prep.batches) > 3
     for graphs in (False, True, True):
