@@ -280,16 +280,12 @@ __device__ __forceinline__ void dtab_row(const u32* row, bool wide, uint4& r0, u
   }
 }
 
-// Probe for the residue (X, x2) (x2 = 0 for keys that carry the whole residue in X).
-__device__ __forceinline__ void dtab_probe(const DTab& t, u64 X, u32 x2, u64 rank, const CfPairSink& o) {
-  u32 bucket, f16;
-  cf_fuse_bucket(X, x2, t.bbits, bucket, f16);
-  u64 b = bucket;
-  const bool wide = ((uintptr_t)t.fpw & 31u) == 0u;
+// The rest of a probe whose first row (bucket b) is already in registers: test it and, while
+// the bucket is full, the rows after it.
+__device__ __forceinline__ void dtab_probe_rows(const DTab& t, u64 b, u32 f16, uint4 r0, uint4 r1, u64 X, u32 x2,
+                                                u64 rank, const CfPairSink& o, bool wide) {
 #pragma unroll 1
   for (int hop = 0;; ++hop) {
-    uint4 r0, r1;
-    dtab_row(t.fpw + b * 8, wide, r0, r1);
     const bool full = (r1.w >> 16) != 0u;
     if (probe_match(r0, r1, f16) || (full && hop == kProbeHops - 1)) {
       probe_slow(t, b, f16, cf_fuse_f32(X, x2), rank, o);   // the side fingerprint: cold path only
@@ -297,6 +293,17 @@ __device__ __forceinline__ void dtab_probe(const DTab& t, u64 X, u32 x2, u64 ran
     }
     if (!full) return;
     b = (b + 1) & (t.nb - 1);
+    dtab_row(t.fpw + b * 8, wide, r0, r1);
   }
+}
+
+// Probe for the residue (X, x2) (x2 = 0 for keys that carry the whole residue in X).
+__device__ __forceinline__ void dtab_probe(const DTab& t, u64 X, u32 x2, u64 rank, const CfPairSink& o) {
+  u32 bucket, f16;
+  cf_fuse_bucket(X, x2, t.bbits, bucket, f16);
+  const bool wide = ((uintptr_t)t.fpw & 31u) == 0u;
+  uint4 r0, r1;
+  dtab_row(t.fpw + (u64)bucket * 8, wide, r0, r1);
+  dtab_probe_rows(t, bucket, f16, r0, r1, X, x2, rank, o, wide);
 }
 
