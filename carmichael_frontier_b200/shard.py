@@ -11,6 +11,15 @@ the gather of the (small) per-modulus results and the max-over-ranks of the devi
   run_sharded(items, weights, solve_share, group)
                                 this rank solves its share with solve_share(list of items) and gets
                                 back every rank's results, in the input order
+
+One modulus too large for one GPU's time splits the other way (the I-rank range; the D table is
+built on every rank, it is the small side):
+
+  windows(n_I, world)           contiguous I-rank windows of near-equal size, one per rank
+  run_split(solve_window, n_I, group)
+                                this rank joins its window with solve_window(lo, hi) -> SolveResult,
+                                and every rank gets the merged result: the whole instance's pairs and
+                                hits, as one solve over all I ranks gives them
 """
 from __future__ import annotations
 
@@ -56,3 +65,52 @@ def run_sharded(items, weights, solve_share, group=None) -> tuple[list, list[int
         for i, x in zip(shares[r], res):
             out[i] = x
     return out, mine
+
+
+def windows(n: int, world: int) -> list[tuple[int, int]]:
+    """[lo, hi) I-rank windows covering [0, n), one per rank, sizes differing by at most one."""
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    q, rem = divmod(int(n), world)
+    out, lo = [], 0
+    for r in range(world):
+        hi = lo + q + (1 if r < rem else 0)
+        out.append((lo, hi))
+        lo = hi
+    return out
+
+
+def merge_windows(parts: list):
+    """One SolveResult from the SolveResults of disjoint I-rank windows of one instance: counts
+    added, pairs and hits merged in the order a single solve reports them."""
+    from .solve import SolveResult
+    parts = [p for p in parts if p is not None]
+    if not parts:
+        raise ValueError("no window results to merge")
+    hits = sorted((h for p in parts for h in p.hits), key=lambda h: (h.n, h.D, h.I))
+    pairs = sorted(x for p in parts for x in p.pairs)
+    first = parts[0]
+    return SolveResult(hits=hits, n_D=first.n_D, n_I=sum(p.n_I for p in parts),
+                       residue_pairs=sum(p.residue_pairs for p in parts), screened=sum(p.screened for p in parts),
+                       above_bound=sum(p.above_bound for p in parts), rejected=sum(p.rejected for p in parts),
+                       plan=dict(first.plan), pairs=pairs, launches=sum(p.launches for p in parts))
+
+
+def run_split(solve_window, n_I: int, group=None):
+    """Join this rank's I-rank window of one instance and gather the whole result.
+
+    solve_window(lo, hi) -> SolveResult of the I ranks [lo, hi) (the D side complete).  With no
+    process group (or world size 1) the whole range is joined here.  Returns (merged SolveResult,
+    this rank's window)."""
+    import torch.distributed as dist
+    if group is None and not (dist.is_available() and dist.is_initialized()):
+        world, rank = 1, 0
+    else:
+        world, rank = dist.get_world_size(group), dist.get_rank(group)
+    win = windows(n_I, world)[rank]
+    mine = solve_window(*win)
+    if world == 1:
+        return mine, win
+    gathered: list = [None] * world
+    dist.all_gather_object(gathered, mine, group=group)
+    return merge_windows(gathered), win

@@ -124,10 +124,17 @@ def dtab_shape(nD: int, tu: Tuning) -> tuple[int, int]:
 
 
 def _i_window(inst: "Instance", plan: dict) -> int:
-    """I ranks joined: [0, C(|INS|, r)) or its prefix [0, plan["i_limit"])."""
+    """Number of I ranks joined: the window [plan["i_lo"], plan["i_limit"]) of [0, C(|INS|, r)), where
+    i_lo defaults to 0 and i_limit to C(|INS|, r)."""
     nI = ncomb(len(inst.INS), inst.r)
     lim = plan.get("i_limit")
-    return nI if lim is None else min(nI, int(lim))
+    hi = nI if lim is None else min(nI, int(lim))
+    return max(0, hi - _i_lo(plan))
+
+
+def _i_lo(plan: dict) -> int:
+    """First I rank of the window joined."""
+    return int(plan.get("i_lo") or 0)
 
 
 def _pow2ceil(x: int) -> int:
@@ -353,6 +360,7 @@ class Solver:
         # L2-resident while built); partitioned builds and larger tables the wide entries
         side_format = 1 if pshape is None and bbits <= 20 else 0
         self._mark(marks, "start")
+        ilo = _i_lo(plan)                          # first I rank of the window
         if pshape is not None:
             tables = self._tables_for(inst)
             self._part_build(inst, plan, pshape, tables, tab, nD, nIt, swap, misc)
@@ -361,15 +369,16 @@ class Solver:
         else:
             # the build side's tables first: the table build runs while the host prepares the other side
             bpool, btail = self._side_tables(inst, bside)
-            ck(lib.cf_dtab_build3(dp(bpool), dp(btail), bn, r, 0, bcount, dp(tab), bbits, fbits, side_format,
-                                  dp(misc) + 4, sh), "cf_dtab_build")
+            ck(lib.cf_dtab_build3(dp(bpool), dp(btail), bn, r, ilo if swap else 0, bcount, dp(tab), bbits, fbits,
+                                  side_format, dp(misc) + 4, sh), "cf_dtab_build")
             ppool, ptail = self._side_tables(inst, pside)
             screen = self.tables.screen(inst.P0, inst.B, 1e-6)
             poolD, poolI = (bpool, ppool) if bside == "D" else (ppool, bpool)
         ppool, ptail = dp(ppool), dp(ptail)
         self._mark(marks, "gen_D")
-        ck(lib.cf_fused_probe3(ppool, ptail, pn, r, 0, pcount, dp(tab), bbits, fbits, side_format, 0, int(swap),
-                               dp(pairs), maxp, dp(misc), dp(misc) + 4, self.tuning.fused_grid, sh), "cf_fused_probe")
+        ck(lib.cf_fused_probe3(ppool, ptail, pn, r, 0 if swap else ilo, pcount, dp(tab), bbits, fbits, side_format,
+                               ilo if swap else 0, int(swap), dp(pairs), maxp, dp(misc), dp(misc) + 4,
+                               self.tuning.fused_grid, sh), "cf_fused_probe")
         self._mark(marks, "probe")
         ck(lib.cf_check_pairs(dp(poolD), dp(poolI), dp(screen), r, dp(pairs), dp(misc), maxp, dp(res),
                               dp(misc) + 4, sh), "cf_check_pairs")
@@ -404,7 +413,7 @@ class Solver:
         t0 = dp(tab)
         row["fpw"], row["side"], row["fill"] = t0, t0 + 32 * nb, t0 + 160 * nb
         row["bloom"] = t0 + 164 * nb if fbits else 0
-        row["nD"], row["i_lo"], row["nI"] = nD, 0, nIt
+        row["nD"], row["i_lo"], row["nI"] = nD, _i_lo(plan), nIt
         row["bbits"], row["fbits"], row["r"], row["swap"] = bbits, fbits, inst.r, int(swap)
         row["pkw"], row["psd"], row["pcnt"], row["pcap"], row["plb"] = pkw, psd, pcnt, cap, self.tuning.part_lb
         host = np.zeros(MOD_DTYPE.itemsize // 8 + 4, dtype=np.uint64)
@@ -462,9 +471,11 @@ class Solver:
                            dp(misc) + 4, shape, sh), "cf_gen_part(D)")
         launches += 1
         self._mark(marks, "gen_D")
-        for lo in range(0, nIt, chunk):
-            cnt = min(chunk, nIt - lo)
-            if lo:
+        ilo = _i_lo(plan)
+        for off in range(0, nIt, chunk):
+            cnt = min(chunk, nIt - off)
+            lo = ilo + off
+            if off:
                 icnt.zero_()
             ck(lib.cf_gen_part(dp(poolI), dp(tailI), len(inst.INS), r, lo, cnt, pbits, capI, dp(icnt), dp(Ibuf),
                                dp(misc) + 4, shape, sh), "cf_gen_part(I)")
@@ -524,23 +535,23 @@ class Solver:
     def _finish(self, inst: Instance, h: dict, res: np.ndarray, verify: bool) -> SolveResult:
         return finish_rows(inst, res, h["nD"], h["nI"], h["plan"], verify)
 
-    def _direct_plan(self, inst: Instance, i_limit: int | None) -> dict | None:
-        """The device plan of a fused or partition join of inst, or None when inst takes another
-        path (radius 0, the bounded strategy, an empty side)."""
+    def _direct_plan(self, inst: Instance, i_limit: int | None, i_lo: int = 0) -> dict | None:
+        """The device plan of a fused or partition join of inst over the I ranks [i_lo, i_limit), or
+        None when inst takes another path (radius 0, the bounded strategy, an empty window)."""
         if inst.r == 0:
             return None
         st = self.tuning.strategy
-        if i_limit is None and (st == "bounded" or st == "auto"):
+        if i_limit is None and not i_lo and (st == "bounded" or st == "auto"):
             from . import bsolve
             if bsolve.applicable(inst) and (st == "bounded" or bsolve.prunes(inst)):
                 return None
-        nD, nI = ncomb(len(inst.B0), inst.r), ncomb(len(inst.INS), inst.r)
-        if i_limit is not None:
-            nI = min(nI, int(i_limit))
+        nD = ncomb(len(inst.B0), inst.r)
+        nI = _i_window(inst, {"i_limit": i_limit, "i_lo": i_lo})
         if nI == 0 or nD == 0:
             return None
         plan = self.plan(nD, nI)
         plan["i_limit"] = i_limit
+        plan["i_lo"] = int(i_lo)
         if min(nD, nI) >= 1 << 32:        # ranks in the fused table are 32-bit
             plan["strategy"] = "partition"
         return plan
@@ -551,28 +562,30 @@ class Solver:
         plan = self.plan(nD, nI, newp["capD"], newp["capI"], newp["pairs"])
         plan["strategy"] = newp.get("strategy", plan["strategy"])
         plan["i_limit"] = newp.get("i_limit")
+        plan["i_lo"] = _i_lo(newp)
         plan["no_part"] = newp.get("no_part", False)
         return plan
 
     def solve_instance(self, inst: Instance, verify: bool = True, timed: bool = False,
-                       marks: list | None = None, i_limit: int | None = None) -> SolveResult:
-        """Join one instance.  i_limit: join only the I ranks [0, i_limit) (a bounded
-        sample of the instance; every pair with such an I rank is found)."""
-        plan = self._direct_plan(inst, i_limit)
+                       marks: list | None = None, i_limit: int | None = None, i_lo: int = 0) -> SolveResult:
+        """Join one instance.  i_lo, i_limit: join only the I ranks [i_lo, i_limit) (a bounded
+        sample of the instance, or one device's share of it; every pair with such an I rank
+        is found).  n_I of the result is the window's size."""
+        if i_lo < 0 or (i_limit is not None and i_limit < 0):
+            raise ValueError("the I-rank window must not start or end below 0")
+        plan = self._direct_plan(inst, i_limit, i_lo)
         if plan is None:
             if inst.r == 0:
                 return self._solve_r0(inst)
             st = self.tuning.strategy
-            if i_limit is None and (st == "bounded" or st == "auto"):
+            if i_limit is None and not i_lo and (st == "bounded" or st == "auto"):
                 from . import bsolve
                 if bsolve.applicable(inst) and (st == "bounded" or bsolve.prunes(inst)):
                     if self._bounded is None:
                         self._bounded = bsolve.BoundedSolve(self)
                     return self._bounded.solve(inst, verify)
-            nD, nI = ncomb(len(inst.B0), inst.r), ncomb(len(inst.INS), inst.r)
-            if i_limit is not None:
-                nI = min(nI, int(i_limit))
-            return SolveResult([], nD, nI, 0, 0, 0, 0)
+            nD = ncomb(len(inst.B0), inst.r)
+            return SolveResult([], nD, _i_window(inst, {"i_limit": i_limit, "i_lo": i_lo}), 0, 0, 0, 0)
         return self._run_plan(inst, plan, verify, timed, marks)
 
     def _run_plan(self, inst: Instance, plan: dict, verify: bool, timed: bool = False,
@@ -616,7 +629,8 @@ class Solver:
         h.update(ev=ev, hread=hm, hrows=rows)
 
     def solve_many(self, insts: list, verify: bool = True, marks_list: list | None = None,
-                   i_limit: int | None = None, readback_rows: int = 256, streams: int = 2) -> list[SolveResult]:
+                   i_limit: int | None = None, readback_rows: int = 256, streams: int = 2,
+                   i_lo: int = 0) -> list[SolveResult]:
         """Solve instances one after another, each with its own build, probe and check, while
         the host collects and certifies each one as the device runs the next: two buffer sets
         alternate, and every solve's counters and first checked rows come back behind its own
@@ -653,9 +667,10 @@ class Solver:
                         marks = []
                         marks_list.append(marks)
                     with use(i):                   # the set (and stream) the solve in flight does not use
-                        plan = self._direct_plan(inst, i_limit)
+                        plan = self._direct_plan(inst, i_limit, i_lo)
                         if plan is None:
-                            out[i] = self.solve_instance(inst, verify=verify, marks=marks, i_limit=i_limit)
+                            out[i] = self.solve_instance(inst, verify=verify, marks=marks, i_limit=i_limit,
+                                                         i_lo=i_lo)
                         else:
                             h = self.enqueue(inst, plan, marks)
                             self._stage_readback(h, readback_rows)

@@ -304,3 +304,25 @@ def test_table_uploads_through_the_staging_ring(cuda):
     for i, a in want.items():
         assert np.array_equal(dt.get(("t", i), None).cpu().numpy(), a)
     assert np.array_equal(dt.get(("big",), None).cpu().numpy(), big)
+
+
+@pytest.mark.parametrize("strategy,parts", [("fused", 3), ("fused", 100), ("partition", 3)])
+def test_i_rank_windows_add_up_to_the_whole_join(cuda, golden, strategy, parts):
+    # one modulus split by I-rank window, as shard.run_split splits it over GPUs: the D side complete in
+    # every window, the windows' pairs together the reference mitm64's pair set; with 100 windows each
+    # (5.9M I ranks) is smaller than the D side (7.6M), so the table is built on the I window (ranks
+    # offset by its first rank) and the D side probes it
+    from carmichael_frontier_b200 import shard
+    g = golden["config2"][1]
+    x = Instance.build(g["M"], g["Q"], g["B0"], g["r"], int(g["B"]))
+    s = Solver(cuda, tuning=Tuning(strategy=strategy))
+    win = shard.windows(g["i_leaves"], parts)
+    got = [s.solve_instance(x, i_lo=lo, i_limit=hi) for lo, hi in win]
+    assert [r.n_I for r in got] == [hi - lo for lo, hi in win]
+    if parts == 100:
+        assert all(r.plan["swap"] for r in got)
+    m = shard.merge_windows(got)
+    assert m.n_D == g["d_leaves"] and m.n_I == g["i_leaves"]
+    assert m.residue_pairs == g["matches"] and as_lists(m.pairs) == g["pairs"]
+    assert sorted([list(h.D), list(h.I), str(h.n)] for h in m.hits) == g["hits"]
+    assert s.solve_instance(x, i_lo=g["i_leaves"], i_limit=g["i_leaves"] + 5).n_I == 0   # an empty window

@@ -4,7 +4,8 @@ carmichael_frontier_b200.shard assigns moduli to ranks and gathers the per-modul
 only collectives besides the max-over-ranks of the device time); bench.py's step schedule gives each
 rank its own moduli.  Here each rank solves its share with the CPU oracle in place of its GPU (the
 only part that needs a device), and the gathered results must equal a single-process run, in input
-order, with every modulus solved exactly once."""
+order, with every modulus solved exactly once.  One instance split over the ranks by I-rank window
+(shard.run_split, every rank with the whole D side) must give the whole instance's pair set."""
 import datetime
 import os
 import socket
@@ -44,6 +45,30 @@ def _solve_on_this_rank(items):
             for M, Q, B0, r, B in items]
 
 
+def _window_solve(item, lo, hi):
+    """The join of one instance over its I ranks [lo, hi), by brute force on the CPU (lexicographic
+    ranks: itertools.combinations order), as a SolveResult like the GPU solve's."""
+    import itertools
+    import math
+
+    from carmichael_frontier_b200.solve import SolveResult
+    M, Q, B0, r, B = item
+    B0 = sorted(B0)
+    INS = sorted(set(Q) - set(B0))
+    P0 = math.prod(B0)
+    byres: dict = {}
+    for D in itertools.combinations(B0, r):
+        byres.setdefault(math.prod(D) % M, []).append(D)
+    pairs = []
+    for i, I in enumerate(itertools.combinations(INS, r)):
+        if i >= hi:
+            break
+        if i >= lo:
+            pairs += [(D, I) for D in byres.get(P0 * math.prod(I) % M, [])]
+    return SolveResult(hits=[], n_D=math.comb(len(B0), r), n_I=hi - lo, residue_pairs=len(pairs), screened=0,
+                       above_bound=0, rejected=0, pairs=sorted(pairs))
+
+
 def _weights(items):
     import math
     return [math.comb(len(B0), r) + math.comb(len(Q) - len(B0), r) for _, Q, B0, r, _ in items]
@@ -71,9 +96,28 @@ def _rank(rank, world, port, out):
         dist.all_reduce(n, op=dist.ReduceOp.SUM)
         g = [None] * world
         dist.all_gather_object(g, (sched, mine))
-        out.put((rank, float(t.item()), float(n.item()), g, res))
+        # one instance split over the ranks by I-rank window (the D side on every rank)
+        import math
+        splits = []
+        for item in items[:3]:
+            nI = math.comb(len(item[1]) - len(item[2]), item[3])
+            merged, win = shard.run_split(lambda lo, hi, item=item: _window_solve(item, lo, hi), nI)
+            splits.append((merged.pairs, merged.n_I, merged.residue_pairs, win))
+        out.put((rank, float(t.item()), float(n.item()), g, res, splits))
     finally:
         dist.destroy_process_group()
+
+
+def test_windows_cover_the_rank_range_once():
+    import sys
+    sys.path.insert(0, ROOT)
+    from carmichael_frontier_b200 import shard
+    for n in (0, 1, 7, 100, 12345):
+        for world in (1, 2, 3, 8):
+            w = shard.windows(n, world)
+            assert len(w) == world and w[0][0] == 0 and w[-1][1] == n
+            assert all(a[1] == b[0] for a, b in zip(w, w[1:]))
+            assert max(hi - lo for lo, hi in w) - min(hi - lo for lo, hi in w) <= 1
 
 
 def test_assignment_is_balanced_and_covers_every_item_once():
@@ -108,7 +152,12 @@ def test_two_gloo_ranks_shard_moduli():
         assert p.exitcode == 0
     items = _small()
     want = _solve_on_this_rank(items)                     # one process, every modulus
-    for rank, tmax, nsum, gathered, res in got:
+    import math
+    for rank, tmax, nsum, gathered, res, splits in got:
+        for item, (pairs, n_i, npairs, win) in zip(items[:3], splits):
+            whole = _window_solve(item, 0, math.comb(len(item[1]) - len(item[2]), item[3]))
+            assert pairs == whole.pairs and n_i == whole.n_I and npairs == whole.residue_pairs
+            assert win == shard.windows(whole.n_I, 2)[rank]
         assert tmax == 1.5 and nsum == 3000.0             # max over ranks, sum over ranks
         assert res == want                                # every rank holds all results, in input order
         s0, s1 = gathered[0][0], gathered[1][0]
