@@ -64,3 +64,20 @@ def test_i_limit_and_repeated_instances(cuda, golden):
     ref = summary(s.solve_instance(x, i_limit=lim))
     out = s.solve_many([x, x, x], i_limit=lim)
     assert [summary(r) for r in out] == [ref] * 3
+
+
+def test_partitioned_builds_pipelined(cuda, golden):
+    # the partitioned table build (its descriptor staged in page-locked memory per buffer set) in the
+    # pipelined, two-stream sequence, with I windows, against one solve at a time
+    gs = golden["config2"][:3]
+    insts = [Instance.build(g["M"], g["Q"], g["B0"], g["r"], int(g["B"])) for g in gs]
+    insts = insts + insts[::-1]
+    lim = 1 << 22
+    one = [summary(Solver(cuda, tuning=Tuning(part_build=False)).solve_instance(x, i_limit=lim)) for x in insts]
+    s = Solver(cuda, tuning=Tuning(part_min_buckets=16))
+    assert [summary(r) for r in s.solve_many(insts, i_limit=lim)] == one
+    # a window that starts inside the I side: the pairs with I ranks in [2^21, 2^22) only
+    half = [summary(r) for r in s.solve_many(insts, i_limit=lim, i_lo=1 << 21)]
+    low = [summary(r) for r in s.solve_many(insts, i_limit=1 << 21)]
+    for h, l, o in zip(half, low, one):
+        assert h[1] + l[1] == o[1] and sorted(h[6] + l[6]) == o[6]
