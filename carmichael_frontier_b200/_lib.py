@@ -89,6 +89,9 @@ SIGNATURES = [
     ("cf_rec_probe", C.c_int, [vp, u64, vp, C.c_int, C.c_int, C.c_int, vp, u32, vp, vp, vp]),
     ("cf_bgen_probe", C.c_int, [C.c_int, C.c_int, u64, vp, vp, vp, vp, vp, u64, u64, vp, C.c_int, C.c_int, vp, u32,
                                 vp, vp, vp]),
+    ("cf_rec_build_keyform", C.c_int, [vp, u64, vp, C.c_int, C.c_int, vp, vp, vp]),
+    ("cf_bgen_probe_keyform", C.c_int, [C.c_int, C.c_int, u64, vp, vp, vp, vp, vp, u64, u64, vp, C.c_int, C.c_int,
+                                        vp, u32, vp, vp, vp]),
     ("cf_part_hist", C.c_int, [vp, u64, u64, C.c_int, vp, vp]),
     ("cf_part_scatter", C.c_int, [vp, vp, u64, u64, C.c_int, vp, vp, vp, vp]),
     ("cf_batch_mod_bytes", sz, []),

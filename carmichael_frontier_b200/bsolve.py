@@ -95,7 +95,9 @@ class BoundedSolve:
         self._native_out = 1 << 12
         self._stage = None                  # page-locked staging of one instance's tables
 
-    def _table(self, keys, n: int, plan: dict):
+    def _table(self, keys, n: int, plan: dict, keyform_pool=None):
+        """Record table of keys[0..n): canonical residues, or, with keyform_pool (a device pool table),
+        their key forms under that pool's modulus (probed by cf_bgen_probe_keyform)."""
         from .solve import dtab_shape
         torch, lib, dp = self.torch, self.lib, _lib.ptr
         if n >= RANK_LIMIT:
@@ -108,8 +110,12 @@ class BoundedSolve:
         tab[: 32 * nbk].zero_()
         tab[160 * nbk: tbytes].zero_()
         self.misc.zero_()
-        _lib.check(lib.cf_rec_build(dp(keys), n, dp(tab), bbits, fbits, dp(self.misc) + 4, self.s._sh()),
-                   "cf_rec_build")
+        if keyform_pool is not None:
+            _lib.check(lib.cf_rec_build_keyform(dp(keys), n, dp(tab), bbits, fbits, dp(keyform_pool),
+                                                dp(self.misc) + 4, self.s._sh()), "cf_rec_build_keyform")
+        else:
+            _lib.check(lib.cf_rec_build(dp(keys), n, dp(tab), bbits, fbits, dp(self.misc) + 4, self.s._sh()),
+                       "cf_rec_build")
         return tab, bbits, fbits
 
     def _probe(self, launch, maxp: int):
@@ -271,11 +277,13 @@ class BoundedSolve:
                     pv[:, 1] = iid.cpu().numpy().view(np.uint64)
                     cands.append(pv)
         else:
-            # the table holds the D records; every I leaf probes it without being written
+            # the table holds the D records; every I leaf probes it without being written (under the
+            # leaves' key form, so that no leaf is converted to a canonical residue; wide moduli write
+            # their leaves and probe a table of canonical keys)
             plan["table"] = "D"
-            tab, bb, fb = self._table(Dk, nD, plan)
-            chain = [first] + ([second] if second is not None else [])
             wide = wide_modulus(M)
+            tab, bb, fb = self._table(Dk, nD, plan, keyform_pool=None if wide else poolI)
+            chain = [first] + ([second] if second is not None else [])
             chunk = self.WIDE_LEAF_CHUNK if wide else self.LEAF_CHUNK
             for fr in _chain(chain, blocks):
                 total = fr["total"]
@@ -298,9 +306,10 @@ class BoundedSolve:
                             pv[:, 1] = iid.cpu().numpy().view(np.uint64)
                     else:
                         pv, maxp = self._probe(lambda pairs, mp, fr=fr, c0=c0, cc=cc: _lib.check(
-                            lib.cf_bgen_probe(r, len(inst.INS), fr["F"], dp(poolI), dp(fr["key"]), dp(fr["ids"]),
-                                              dp(fr["offs"]), dp(fr["xs"]), c0, cc, dp(tab), bb, fb, dp(pairs), mp,
-                                              dp(self.misc), dp(self.misc) + 4, sh), "cf_bgen_probe"), maxp)
+                            lib.cf_bgen_probe_keyform(r, len(inst.INS), fr["F"], dp(poolI), dp(fr["key"]),
+                                                      dp(fr["ids"]), dp(fr["offs"]), dp(fr["xs"]), c0, cc, dp(tab),
+                                                      bb, fb, dp(pairs), mp, dp(self.misc), dp(self.misc) + 4, sh),
+                            "cf_bgen_probe_keyform"), maxp)
                     if pv is not None:
                         cands.append(pv)
         pairs = []

@@ -14,8 +14,11 @@
 
 namespace {
 
-constexpr int kLeavesPerThread = 8;
+constexpr int kLeavesPerThread = 32;       // consecutive leaves per thread: one parent search each
 
+// KEYFORM: the table holds key forms (cf_rec_build_keyform) and the leaves probe with theirs; else the
+// table holds canonical residues and every leaf is converted first (two Montgomery products).
+template <bool KEYFORM>
 __global__ void __launch_bounds__(256)
 k_bgen_probe(int r, int n, u64 F, const u64* __restrict__ pool, const u64* __restrict__ key,
              const u64* __restrict__ id, const u64* __restrict__ offs, const u32* __restrict__ xs, u64 c0, u64 cc,
@@ -39,7 +42,7 @@ k_bgen_probe(int r, int n, u64 F, const u64* __restrict__ pool, const u64* __res
     while (p + 1 < F && offs[p + 1] <= c) ++p;  // consecutive leaves share or follow their parent
     const int x = (int)(xs[p] + (c - offs[p]));
     const u64 kk = cf_mul_key(key[p], pkey[x], md);
-    const u64 X = cf_key_to_canon(kk, md, hd->inv2a, hd->inv2aR);
+    const u64 X = KEYFORM ? kk : cf_key_to_canon(kk, md, hd->inv2a, hd->inv2aR);
     const u64 iid = id[p] + binom[(size_t)x * (r + 1) + r];      // colex: + C(x, r)
     if (tab.bloom) {
       const CfBloomKey bk = cf_bloom_key(X, 0u, tab.fbits);
@@ -58,9 +61,9 @@ k_bgen_probe(int r, int n, u64 F, const u64* __restrict__ pool, const u64* __res
 // cf_scan_u64 at d = r-1, as for cf_bgen_expand) against a table built by
 // cf_rec_build from D records.  Candidates {D position, I colex id} go to pairs
 // through *npairs (zeroed by the caller).
-extern "C" int cf_bgen_probe(int r, int n, u64 F, const void* pool, const u64* key, const u64* id, const u64* offs,
-                             const u32* xs, u64 c0, u64 cc, const void* tab, int bbits, int fbits, void* pairs,
-                             u32 max_pairs, u32* npairs, u32* err, void* stream) {
+static int bgen_probe(bool keyform, int r, int n, u64 F, const void* pool, const u64* key, const u64* id,
+                      const u64* offs, const u32* xs, u64 c0, u64 cc, const void* tab, int bbits, int fbits,
+                      void* pairs, u32 max_pairs, u32* npairs, u32* err, void* stream) {
   if (r < 1 || r > CF_MAX_R || n < 1 || n > CF_MAX_POOL || F == 0 || !pool || !key || !id || !offs || !xs || !tab ||
       !npairs || !err || (max_pairs && !pairs) || bbits < 1 || bbits > 28 || fbits < 0 || fbits > 26) {
     cf_set_error("cf_bgen_probe: bad arguments%s", "");
@@ -86,8 +89,25 @@ extern "C" int cf_bgen_probe(int r, int n, u64 F, const void* pool, const u64* k
   sink.mod = 0;
   sink.swap = 0;
   const u64 threads = (cc + kLeavesPerThread - 1) / kLeavesPerThread;
-  k_bgen_probe<<<(unsigned)((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
-      r, n, F, (const u64*)pool, key, id, offs, xs, c0, cc, t, sink);
+  auto kern = keyform ? k_bgen_probe<true> : k_bgen_probe<false>;
+  kern<<<(unsigned)((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(r, n, F, (const u64*)pool, key, id, offs,
+                                                                          xs, c0, cc, t, sink);
   CF_LAUNCH_CHECK("cf_bgen_probe");
   return CF_OK;
+}
+
+extern "C" int cf_bgen_probe(int r, int n, u64 F, const void* pool, const u64* key, const u64* id, const u64* offs,
+                             const u32* xs, u64 c0, u64 cc, const void* tab, int bbits, int fbits, void* pairs,
+                             u32 max_pairs, u32* npairs, u32* err, void* stream) {
+  return bgen_probe(false, r, n, F, pool, key, id, offs, xs, c0, cc, tab, bbits, fbits, pairs, max_pairs, npairs,
+                    err, stream);
+}
+
+// The same probe of a table built by cf_rec_build_keyform with the same pool's modulus: the leaves
+// probe with their key forms, without the conversion to canonical residues.
+extern "C" int cf_bgen_probe_keyform(int r, int n, u64 F, const void* pool, const u64* key, const u64* id,
+                                     const u64* offs, const u32* xs, u64 c0, u64 cc, const void* tab, int bbits,
+                                     int fbits, void* pairs, u32 max_pairs, u32* npairs, u32* err, void* stream) {
+  return bgen_probe(true, r, n, F, pool, key, id, offs, xs, c0, cc, tab, bbits, fbits, pairs, max_pairs, npairs,
+                    err, stream);
 }

@@ -26,7 +26,6 @@ extern "C" size_t cf_scan_tmp_bytes(u64 n);
 extern "C" int cf_scan_u64(const u64* in, u64 n, u64* out, void* tmp, size_t tmp_bytes, void* stream);
 extern "C" u64 cf_key_of(u64 M, u64 v);
 extern "C" size_t cf_dtab_bytes2(int bbits, int fbits);
-extern "C" int cf_rec_build(const u64* keys, u64 n, void* tab, int bbits, int fbits, u32* err, void* stream);
 extern "C" int cf_bgen_count(int side, int d, int r, int n, u64 F, const u64* alo, const u64* ahi, const u32* meta,
                              const u64* bounds, int split_idx, int hmax, int xa, int xb, u64* cnt, u32* xs,
                              void* stream);
@@ -34,9 +33,11 @@ extern "C" int cf_bgen_expand(int side, int d, int r, int n, u64 F, const void* 
                               const u64* ahi, const u64* id, const u32* meta, const u64* offs, const u32* xs,
                               int split_idx, int bitmask, u64 c0, u64 cc, u64* okey, u64* oalo, u64* oahi, u64* oid,
                               u32* ometa, void* stream);
-extern "C" int cf_bgen_probe(int r, int n, u64 F, const void* pool, const u64* key, const u64* id, const u64* offs,
-                             const u32* xs, u64 c0, u64 cc, const void* tab, int bbits, int fbits, void* pairs,
-                             u32 max_pairs, u32* npairs, u32* err, void* stream);
+extern "C" int cf_rec_build_keyform(const u64* keys, u64 n, void* tab, int bbits, int fbits, const void* pool,
+                                    u32* err, void* stream);
+extern "C" int cf_bgen_probe_keyform(int r, int n, u64 F, const void* pool, const u64* key, const u64* id,
+                                     const u64* offs, const u32* xs, u64 c0, u64 cc, const void* tab, int bbits,
+                                     int fbits, void* pairs, u32 max_pairs, u32* npairs, u32* err, void* stream);
 
 namespace {
 
@@ -259,14 +260,16 @@ extern "C" int cf_bounded_join(const void* poolD, const void* boundsD, int nb, c
   if (e == cudaSuccess) e = cudaMemsetAsync(tab + nbk * 160, 0, tb - nbk * 160, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(misc, 0, 8, st);
   if (e != cudaSuccess) return cf_cuda_status(e, "cf_bounded_join: zero");
-  rc = cf_rec_build(Dk, nD, tab, bbits, fbits, misc + 1, st);
+  // the D records go in under the key form of the I pool's modulus, the form the I leaves are computed
+  // in: the leaves probe without a conversion to canonical residues
+  rc = cf_rec_build_keyform(Dk, nD, tab, bbits, fbits, poolI, misc + 1, st);
   if (rc != CF_OK) return rc;
   // ---- probe every I leaf, in launches of at most 2^30 leaves
   constexpr u64 kChunk = 1ull << 30;
   for (u64 c0 = 0; c0 < nI; c0 += kChunk) {
     const u64 cc = nI - c0 < kChunk ? nI - c0 : kChunk;
-    rc = cf_bgen_probe(r, ni, fi.F, poolI, fi.key, fi.id, fi.offs, fi.xs, c0, cc, tab, bbits, fbits, pairs, cap, misc,
-                       misc + 1, st);
+    rc = cf_bgen_probe_keyform(r, ni, fi.F, poolI, fi.key, fi.id, fi.offs, fi.xs, c0, cc, tab, bbits, fbits, pairs,
+                               cap, misc, misc + 1, st);
     if (rc != CF_OK) return rc;
   }
   e = cudaMemcpyAsync(hostw, misc, 8, cudaMemcpyDeviceToHost, st);

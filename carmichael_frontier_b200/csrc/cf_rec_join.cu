@@ -35,6 +35,23 @@ k_rec_build(const u64* __restrict__ keys, u64 n, DTab tab, u32* __restrict__ err
   if (!ok) atomicOr(err, CF_ERR_TABLE_FULL);
 }
 
+// Insert canonical residues keys[0..n) under their key form of the pool's modulus: the odd part in
+// Montgomery form (x * 2^64 mod m, one product with 2^128 mod m) over the 2-adic part -- the form in
+// which the bounded producers' nodes carry products, so that their leaves probe without converting.
+__global__ void __launch_bounds__(256)
+k_rec_build_keyform(const u64* __restrict__ keys, u64 n, DTab tab, const u64* __restrict__ pool, u32* __restrict__ err) {
+  const CfPoolHdr* hd = (const CfPoolHdr*)pool;
+  const CfMod md = cf_mod_from_hdr(hd);
+  const u64 r2 = hd->r2;
+  bool ok = true;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+    const u64 k = keys[i];
+    const u64 kf = (cf_redc_mul(k, r2, md.m, md.minv) << md.a) | (k & md.mask2);   // k * r2 < 2^64 * m
+    ok &= dtab_insert(tab, kf, 0u, i);
+  }
+  if (!ok) atomicOr(err, CF_ERR_TABLE_FULL);
+}
+
 __global__ void __launch_bounds__(256)
 k_rec_probe(const u64* __restrict__ keys, u64 n, DTab tab, CfPairSink sink) {
   for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
@@ -68,6 +85,22 @@ extern "C" int cf_rec_build(const u64* keys, u64 n, void* tab, int bbits, int fb
   if (n == 0) return CF_OK;
   k_rec_build<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(keys, n, rec_tab(tab, bbits, fbits), err);
   CF_LAUNCH_CHECK("cf_rec_build");
+  return CF_OK;
+}
+
+// The same table from canonical residues inserted under the key form of the modulus of `pool` (a
+// pool table on the device): the table a probe by key-form leaves (cf_bgen_probe_keyform) reads.
+extern "C" int cf_rec_build_keyform(const u64* keys, u64 n, void* tab, int bbits, int fbits, const void* pool,
+                                    u32* err, void* stream) {
+  if (!tab || !err || !pool || (n && !keys) || bbits < 1 || bbits > 28 || fbits < 0 || fbits > 26 ||
+      n >= (1ull << 32)) {
+    cf_set_error("cf_rec_build_keyform: bad arguments%s", "");
+    return CF_EBADARG;
+  }
+  if (n == 0) return CF_OK;
+  k_rec_build_keyform<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(keys, n, rec_tab(tab, bbits, fbits),
+                                                                       (const u64*)pool, err);
+  CF_LAUNCH_CHECK("cf_rec_build_keyform");
   return CF_OK;
 }
 

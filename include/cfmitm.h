@@ -305,6 +305,19 @@ int cf_bgen_probe(int r, int n, uint64_t F, const void* pool, const uint64_t* ke
                   const uint64_t* offs, const uint32_t* xs, uint64_t c0, uint64_t cc, const void* tab, int bbits,
                   int fbits, void* pairs, uint32_t max_pairs, uint32_t* npairs, uint32_t* err, void* stream);
 
+/* The same pair for a table of D records under their key form (odd part in Montgomery form
+ * over the 2-adic part, the form the bounded producers' nodes carry): cf_rec_build_keyform
+ * inserts canonical D keys converted with the modulus of `pool` (the I pool table on the
+ * device, M < 2^64), and cf_bgen_probe_keyform probes it with the leaves' key forms, with no
+ * conversion per leaf.  Same candidates as cf_rec_build + cf_bgen_probe.  No counterpart in
+ * the reference. */
+int cf_rec_build_keyform(const uint64_t* keys, uint64_t n, void* tab, int bbits, int fbits, const void* pool,
+                         uint32_t* err, void* stream);
+int cf_bgen_probe_keyform(int r, int n, uint64_t F, const void* pool, const uint64_t* key, const uint64_t* id,
+                          const uint64_t* offs, const uint32_t* xs, uint64_t c0, uint64_t cc, const void* tab,
+                          int bbits, int fbits, void* pairs, uint32_t max_pairs, uint32_t* npairs, uint32_t* err,
+                          void* stream);
+
 /* ---- streamed (out-of-core) join --------------------------------------------- */
 
 /* Range partitioning of canonical {key, id} records (key < M) for sides larger than

@@ -203,6 +203,11 @@ def test_named_entry_points_reject_bad_arguments_without_gpu():
     assert lib.cf_igen_tmp_bytes(1 << 20) > lib.cf_igen_tmp_bytes(1 << 10) > 0
     assert lib.cf_join_tmp_bytes(1000) >= 16 * 1000
     assert lib.cf_dtab_build3(None, None, 5, 2, 0, 10, None, 10, 0, 1, None, None) == _lib.CF_EBADARG
+    buf = np.zeros(64, dtype=np.uint8)
+    assert lib.cf_rec_build_keyform(buf.ctypes.data, 4, buf.ctypes.data, 10, 0, None, buf.ctypes.data, None) \
+        == _lib.CF_EBADARG                      # no pool to take the modulus from
+    assert lib.cf_bgen_probe_keyform(2, 10, 0, None, None, None, None, None, 0, 1, None, 10, 0, None, 0, None, None,
+                                     None) == _lib.CF_EBADARG
 
 
 def test_ddump_bound_table_equals_the_python_definition():

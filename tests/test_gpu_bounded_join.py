@@ -60,8 +60,13 @@ def test_one_call_join_against_the_oracle(cuda):
         inst = Instance.build(M, Q, B0, r, B)
         Icap, Dmin = bsolve.caps(inst)
         s = Solver(cuda, tuning=Tuning(strategy="bounded"))
-        got, nD, nI, plan = bsolve.BoundedSolve(s).join(inst.B0, inst.INS, r, M, P0, Icap, Dmin)
+        bs = bsolve.BoundedSolve(s)
+        got, nD, nI, plan = bs.join(inst.B0, inst.INS, r, M, P0, Icap, Dmin)
         assert plan.get("native")
         want = {(D, I) for D, I in ((tuple(D), tuple(I)) for D, I in pairs)
                 if math.prod(I) < Icap and math.prod(D) >= Dmin}
         assert {(tuple(inst.B0[x] for x in d), tuple(inst.INS[x] for x in i)) for d, i in got} == want
+        bs.native = False                       # the level loop (its D table also under key forms)
+        got2, _nD, _nI, plan2 = bs.join(inst.B0, inst.INS, r, M, P0, Icap, Dmin)
+        assert not plan2.get("native")
+        assert {(tuple(inst.B0[x] for x in d), tuple(inst.INS[x] for x in i)) for d, i in got2} == want
