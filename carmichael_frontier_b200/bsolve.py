@@ -26,7 +26,7 @@ import numpy as np
 from . import _lib
 from .bounded import U128
 from .certify import verify_certificate
-from .tables import pool_table_host, unrank_colex, wide_modulus
+from .tables import pool_table_host, unrank_colex_batch, wide_modulus
 
 RANK_LIMIT = 1 << 32          # positions in the join table are 32-bit
 
@@ -217,13 +217,8 @@ class BoundedSolve:
         nD, nI, k = int(sizes[0]), int(sizes[1]), int(n_out.value)
         mo = self._native_out
         did, dkey, iid = out[:k], out[mo:mo + k], out[2 * mo:2 * mo + k]
-        P0m = inst.P0 % M
-        pairs = []
-        for j in range(k):
-            ii = unrank_colex(int(iid[j]), r, ni)
-            if (P0m * math.prod(INS[x] for x in ii)) % M != int(dkey[j]):
-                continue                       # fingerprint collision, not an equal-residue pair
-            pairs.append((unrank_colex(int(did[j]), r, nb), ii))
+        pairs = _confirmed_pairs(unrank_colex_batch(did, r, nb), unrank_colex_batch(iid, r, ni), dkey, INS,
+                                 inst.P0 % M, M)
         return pairs, nD, nI, dict(strategy="bounded", Icap=Icap, Dmin=Dmin, table="D", native=True)
 
     def _bound_table(self, fn, primes, r: int, bound: int) -> np.ndarray:
@@ -318,17 +313,15 @@ class BoundedSolve:
             dpos = torch.from_numpy(pv[:, 0].astype(np.int64)).to(self.s.device)
             dk = Dk.view(torch.int64)[dpos].cpu().numpy().view(np.uint64)
             di = Did.view(torch.int64)[dpos].cpu().numpy().view(np.uint64)
-            P0m = inst.P0 % M
-            wide = wide_modulus(M)             # keys taken mod 2^64: compare the residues themselves
-            for j in range(len(pv)):
-                ii = unrank_colex(int(pv[j, 1]), r, len(inst.INS))
-                dd = unrank_colex(int(di[j]), r, len(inst.B0))
-                if wide:
+            ii_all = unrank_colex_batch(pv[:, 1], r, len(inst.INS))
+            dd_all = unrank_colex_batch(di, r, len(inst.B0))
+            if wide_modulus(M):                # keys taken mod 2^64: compare the residues themselves
+                for dd, ii in zip(map(tuple, dd_all.tolist()), map(tuple, ii_all.tolist())):
                     if (inst.P0 * math.prod(inst.INS[x] for x in ii) - math.prod(inst.B0[x] for x in dd)) % M:
                         continue
-                elif (P0m * math.prod(inst.INS[x] for x in ii)) % M != int(dk[j]):
-                    continue                   # fingerprint collision, not an equal-residue pair
-                pairs.append((dd, ii))
+                    pairs.append((dd, ii))
+            else:
+                pairs = _confirmed_pairs(dd_all, ii_all, dk, inst.INS, inst.P0 % M, M)
         return pairs, nD, nI, plan
 
     def _finish(self, inst, pairs, nD, nI, plan, verify):
@@ -337,10 +330,14 @@ class BoundedSolve:
         hits, pairs_out, above, rejected, screened = [], [], 0, 0, 0
         if pairs:
             B0, INS = inst.B0, inst.INS
-            for di_, ii_ in pairs:
+            near = log2_screen(inst.P0, B0, INS, pairs, inst.B)
+            for (di_, ii_), maybe in zip(pairs, near.tolist()):
                 D = tuple(B0[x] for x in di_)
                 I = tuple(INS[x] for x in ii_)
                 pairs_out.append((D, I))
+                if not maybe:                  # log2 n is above log2 B by more than the screen's margin
+                    above += 1
+                    continue
                 dset = set(D)
                 fac = tuple(sorted([p for p in B0 if p not in dset] + list(I)))
                 n = math.prod(fac)
@@ -360,6 +357,34 @@ class BoundedSolve:
         pairs_out.sort()
         return SolveResult(hits, nD, nI, len(pairs_out), screened, above, rejected, plan=plan, pairs=pairs_out,
                            launches=self.gen.launches)
+
+
+def _confirmed_pairs(dd_all: np.ndarray, ii_all: np.ndarray, dkeys, INS, P0m: int, M: int) -> list:
+    """(D index tuple, I index tuple) of every candidate whose residues are equal, P0 * prod(I) == the
+    D key (mod M): the table's fingerprint collisions are dropped."""
+    pairs = []
+    for dd, ii, kd in zip(dd_all.tolist(), ii_all.tolist(), np.asarray(dkeys, dtype=np.uint64).tolist()):
+        v = P0m
+        for x in ii:
+            v = v * INS[x] % M
+        if v == kd:
+            pairs.append((tuple(dd), tuple(ii)))
+    return pairs
+
+
+def log2_screen(P0: int, B0, INS, pairs, bound: int) -> np.ndarray:
+    """Which pairs (D index tuple, I index tuple) may have n = P0 * prod(I) / prod(D) at or below
+    bound: a float64 screen of log2 n with a margin far above its rounding
+    error (sums of at most 32 logarithms of numbers below 2^64), so every pair it rejects is
+    certainly above the bound; the pairs it keeps are decided exactly by the caller."""
+    if len(pairs) < 64:                        # a few pairs: the exact check alone is cheaper
+        return np.ones(len(pairs), dtype=bool)
+    dd = np.array([d for d, _ in pairs], dtype=np.int64)
+    ii = np.array([i for _, i in pairs], dtype=np.int64)
+    lgB = np.log2(np.asarray(B0, dtype=np.float64))
+    lgI = np.log2(np.asarray(INS, dtype=np.float64))
+    lg = math.log2(P0) - lgB[dd].sum(axis=1) + lgI[ii].sum(axis=1)
+    return lg <= math.log2(bound) + 1e-6
 
 
 class _Sides:

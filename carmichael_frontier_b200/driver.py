@@ -21,6 +21,7 @@ import math
 import time
 
 from .bounded import generator
+from .bsolve import log2_screen
 from .tables import unrank_colex
 
 
@@ -118,7 +119,10 @@ def run_instance(tag, B0, INS, r: int, hmax: int, M: int, U: int, split: int, co
     pairs_idx, nD, nI, dt = joined
     below = nb = 0
     rmin = None
-    for di, ii in pairs_idx:
+    near = log2_screen(P0, B0s, INS_aff, pairs_idx, U).tolist()   # False: n certainly above U
+    for (di, ii), maybe in zip(pairs_idx, near):
+        if not maybe:
+            continue
         D = [B0s[x] for x in di]
         I = [INS_aff[x] for x in ii]
         prodD, prodI = math.prod(D), math.prod(I)

@@ -251,6 +251,32 @@ def rank_lex(idx, n: int) -> int:
     return rank
 
 
+@lru_cache(maxsize=64)
+def _colex_columns(r: int, n: int) -> np.ndarray:
+    """C(x, t) for x < n, t = 1..r as uint64 columns [r, n] (every colex rank below 2^64)."""
+    out = np.zeros((r, n), dtype=np.uint64)
+    for t in range(1, r + 1):
+        out[t - 1] = np.array([min(comb(x, t), (1 << 64) - 1) for x in range(n)], dtype=np.uint64)
+    return out
+
+
+def unrank_colex_batch(ids, r: int, n: int) -> np.ndarray:
+    """unrank_colex of every id in the array ids (ranks below C(n, r) < 2^64): an int64 array
+    [len(ids), r] of ascending indices.  Each column is one vectorised search: the largest x with
+    C(x, t) <= the remaining rank, t = r .. 1 (C(x, t) increases with x)."""
+    v = np.ascontiguousarray(np.asarray(ids, dtype=np.uint64)).copy()
+    out = np.zeros((len(v), r), dtype=np.int64)
+    cols = _colex_columns(r, n)
+    for t in range(r, 0, -1):
+        col = cols[t - 1]
+        x = np.searchsorted(col, v, side="right").astype(np.int64) - 1
+        out[:, t - 1] = x
+        v = v - col[x]
+    if len(v) and v.any():
+        raise ValueError("not a colex rank")
+    return out
+
+
 def unrank_colex(v: int, r: int, n: int) -> tuple[int, ...]:
     """Inverse of the colex rank sum_j C(i_j, j+1) (src/mitm64_idump_stream2.cpp:26-29)."""
     v = int(v)

@@ -42,3 +42,27 @@ def test_bound_tables_match_their_definitions():
             for x in range(n):
                 want = (Icap - 1) // math.prod(P[x:x + t + 1]) if x + t < n else 0
                 assert H[t * n + x] == want
+
+
+def test_log2_screen_keeps_every_pair_at_or_below_the_bound():
+    # the float screen may keep pairs above the bound (decided exactly later) but never drops one
+    # at or below it, including pairs whose n equals the bound or sits one unit on either side
+    import math
+    import random
+
+    from carmichael_frontier_b200 import workloads as W
+    from carmichael_frontier_b200.bsolve import log2_screen
+    rng = random.Random(11)
+    Q = W.eligible_pool(W.draw_modulus(4242), 20000)
+    B0, INS = Q[:40], Q[40:90]
+    P0 = math.prod(B0)
+    r = 3
+    pairs = [(tuple(sorted(rng.sample(range(len(B0)), r))), tuple(sorted(rng.sample(range(len(INS)), r))))
+             for _ in range(3000)]
+    ns = [P0 * math.prod(INS[x] for x in i) // math.prod(B0[x] for x in d) for d, i in pairs]
+    for bound in [sorted(ns)[len(ns) // 2], ns[0], ns[0] - 1, ns[0] + 1, min(ns), max(ns)]:
+        keep = log2_screen(P0, B0, INS, pairs, bound)
+        assert all(k for k, n in zip(keep, ns) if n <= bound)
+        assert sum(keep) <= sum(1 for n in ns if n <= bound) + 5      # and drops all but a few above it
+    assert len(log2_screen(P0, B0, INS, [], 10)) == 0
+    assert log2_screen(P0, B0, INS, pairs[:10], 1).all()               # short lists go to the exact check
