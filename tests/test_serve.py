@@ -6,6 +6,8 @@ import threading
 import time
 import types
 
+import pytest
+
 from carmichael_frontier_b200 import serve, workloads as W
 from carmichael_frontier_b200.serve import Server, count_ge_upper, count_lt_upper
 
@@ -85,9 +87,10 @@ def test_poisson_stats_shape():
     assert st["p50_ms"] <= st["p99_ms"] and st["throughput_rps"] > 0
 
 
-def test_footprint_reports_work_and_large_requests_take_the_fast_path():
+def test_footprint_reports_work_and_the_priority_class_takes_the_fast_path():
     # the footprint's record estimate is at least the records the solve will touch, and the server
-    # sends requests at or above large_work to the worker's high-priority path
+    # sends the chosen class (requests at or above large_work, those below, or neither) to the
+    # worker's high-priority path
     import math
 
     from carmichael_frontier_b200 import serve, workloads as W
@@ -104,14 +107,22 @@ def test_footprint_reports_work_and_large_requests_take_the_fast_path():
         def __init__(self, work):
             self.need, self.work = 1, work
 
-    srv = serve.Server(slots=2, budget=10, solve_fn=lambda st, inst: None, large_work=100)
-    orig = srv._solve
-    srv._solve = lambda state, inst, large=False: seen.append((inst.work, large)) or orig(state, inst, large)
-    srv.start()
-    for w in (5, 100, 7, 5000):
-        srv.submit(Job(w)).done.wait()
-    srv.stop()
-    assert sorted(seen) == [(5, False), (7, False), (100, True), (5000, True)]
+    want = {"large": [(5, False), (7, False), (100, True), (5000, True)],
+            "small": [(5, True), (7, True), (100, False), (5000, False)],
+            "none": [(5, False), (7, False), (100, False), (5000, False)]}
+    for prio, expect in want.items():
+        seen = []
+        srv = serve.Server(slots=2, budget=10, solve_fn=lambda st, inst: None, large_work=100, priority=prio)
+        orig = srv._solve
+        srv._solve = lambda state, inst, fast=False, orig=orig, seen=seen: seen.append((inst.work, fast)) or \
+            orig(state, inst, fast)
+        srv.start()
+        for w in (5, 100, 7, 5000):
+            srv.submit(Job(w)).done.wait()
+        srv.stop()
+        assert sorted(seen) == expect, prio
+    with pytest.raises(ValueError):
+        serve.Server(slots=1, budget=10, solve_fn=lambda st, inst: None, priority="fastest")
 
 
 def test_large_requests_run_one_at_a_time_in_order():
