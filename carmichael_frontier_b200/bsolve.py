@@ -26,7 +26,7 @@ import numpy as np
 from . import _lib
 from .bounded import U128
 from .certify import verify_certificate
-from .tables import pool_table_host, unrank_colex_batch, wide_modulus
+from .tables import pool_table_host, unrank_colex, unrank_colex_batch, wide_modulus
 
 RANK_LIMIT = 1 << 32          # positions in the join table are 32-bit
 
@@ -217,8 +217,12 @@ class BoundedSolve:
         nD, nI, k = int(sizes[0]), int(sizes[1]), int(n_out.value)
         mo = self._native_out
         did, dkey, iid = out[:k], out[mo:mo + k], out[2 * mo:2 * mo + k]
-        pairs = _confirmed_pairs(unrank_colex_batch(did, r, nb), unrank_colex_batch(iid, r, ni), dkey, INS,
-                                 inst.P0 % M, M)
+        if k <= 32:                            # a few candidates (most family instances): no array set-up
+            dd_all = [unrank_colex(int(v), r, nb) for v in did]
+            ii_all = [unrank_colex(int(v), r, ni) for v in iid]
+        else:
+            dd_all, ii_all = unrank_colex_batch(did, r, nb).tolist(), unrank_colex_batch(iid, r, ni).tolist()
+        pairs = _confirmed_pairs(dd_all, ii_all, dkey, INS, inst.P0 % M, M)
         return pairs, nD, nI, dict(strategy="bounded", Icap=Icap, Dmin=Dmin, table="D", native=True)
 
     def _bound_table(self, fn, primes, r: int, bound: int) -> np.ndarray:
@@ -321,7 +325,7 @@ class BoundedSolve:
                         continue
                     pairs.append((dd, ii))
             else:
-                pairs = _confirmed_pairs(dd_all, ii_all, dk, inst.INS, inst.P0 % M, M)
+                pairs = _confirmed_pairs(dd_all.tolist(), ii_all.tolist(), dk, inst.INS, inst.P0 % M, M)
         return pairs, nD, nI, plan
 
     def _finish(self, inst, pairs, nD, nI, plan, verify):
@@ -359,11 +363,11 @@ class BoundedSolve:
                            launches=self.gen.launches)
 
 
-def _confirmed_pairs(dd_all: np.ndarray, ii_all: np.ndarray, dkeys, INS, P0m: int, M: int) -> list:
+def _confirmed_pairs(dd_all, ii_all, dkeys, INS, P0m: int, M: int) -> list:
     """(D index tuple, I index tuple) of every candidate whose residues are equal, P0 * prod(I) == the
-    D key (mod M): the table's fingerprint collisions are dropped."""
+    D key (mod M): the table's fingerprint collisions are dropped.  dd_all, ii_all: index rows."""
     pairs = []
-    for dd, ii, kd in zip(dd_all.tolist(), ii_all.tolist(), np.asarray(dkeys, dtype=np.uint64).tolist()):
+    for dd, ii, kd in zip(dd_all, ii_all, np.asarray(dkeys, dtype=np.uint64).tolist()):
         v = P0m
         for x in ii:
             v = v * INS[x] % M
