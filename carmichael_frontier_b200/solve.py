@@ -636,8 +636,9 @@ class Solver:
         alternate, and every solve's counters and first checked rows come back behind its own
         kernels.  With streams = 2 the two buffer sets also have a CUDA stream each, so one
         solve's table build can run beside the previous solve's probe.  The results equal
-        solve_instance's on each instance.  marks_list (optional list) receives one marks list
-        per instance (see enqueue)."""
+        solve_instance's on each instance (i_lo, i_limit: the same I-rank window for every
+        instance).  marks_list (optional list) receives one marks list per instance (see
+        enqueue)."""
         torch = self.torch
         out: list = [None] * len(insts)
         base = self._torch_stream()
