@@ -104,6 +104,8 @@ SIGNATURES = [
     ("cf_batch_part", C.c_int, [C.c_int, vp, vp, u32, vp, vp, u32, vp, vp, C.c_int, C.c_int, u32, vp]),
     ("cf_sort_tmp_bytes", sz, [u64]),
     ("cf_sort_pairs", C.c_int, [vp, vp, u64, C.c_int, vp, sz, vp]),
+    ("cf_sort_digits_tmp_bytes", sz, [u64, C.c_int, C.c_int]),
+    ("cf_sort_pairs_digits", C.c_int, [vp, vp, u64, C.c_int, C.c_int, vp, sz, vp]),
     ("cf_sort_pairs_noalloc_max", u64, []),
     ("cf_sort_pairs_noalloc", C.c_int, [vp, vp, u64, C.c_int, vp]),
     ("cf_join_tmp_bytes", sz, [u64]),

@@ -9,6 +9,10 @@ representative instance; results cached in memory and optionally in a JSON file.
 ``tune_batch``: for the batched portfolio kernels, the work-queue ticket size
 (records a warp takes per queue pop) and the persistent grid, by timing whole
 batch runs of a prepared portfolio.
+
+``tune_sort``: the radix digit width (8 or 9 bits) of the materialised join's
+sort (sort_side) per size class, by timing whole sorts of random keys of the
+class's size and key width.
 """
 from __future__ import annotations
 
@@ -104,6 +108,56 @@ def tune_batch(prep, device=None, reps: int = 3, tickets=TICKETS, grids=GRID_PER
             best = (ms, tu)
         bs.release(p2)
     return best[1], rows
+
+
+def tune_sort(sizes, key_bits: int = 64, device=None, widths=None, reps: int = 3, seed: int = 0,
+              apply: bool = True, verbose: bool = False) -> list[dict]:
+    """Radix digit width of sort_side per size class (bit length of n) among `sizes`: for each
+    class, the largest size in it is sorted with every candidate width on random keys below
+    2^key_bits (the residue keys of a modulus M lie below 2^bit_length(M)), timed whole with CUDA
+    events (median of `reps` after one warm-up).  The fastest width is recorded for the class
+    (mitm_gpu2.set_sort_digit_bits) unless apply=False.  Returns one row per class and width."""
+    import torch
+
+    from . import mitm_gpu2 as G
+    widths = G.SORT_DIGIT_WIDTHS if widths is None else tuple(widths)
+    if not 1 <= key_bits <= 64:
+        raise ValueError("key_bits must be 1..64")
+    dev = torch.device(device if device is not None else "cuda")
+    largest: dict[int, int] = {}
+    for n in sizes:
+        n = int(n)
+        if n > 1:
+            c = n.bit_length()
+            largest[c] = max(largest.get(c, 0), n)
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    rows = []
+    for c, n in sorted(largest.items()):
+        keys = torch.from_numpy(rng.integers(0, 1 << key_bits, size=n, dtype=np.uint64)).to(dev)
+        ids = torch.arange(n, device=dev, dtype=torch.int64).view(torch.uint64)
+        best = None
+        for db in widths:
+            G.sort_side(keys, ids, digit_bits=db)
+            ts = []
+            for _ in range(reps):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record()
+                G.sort_side(keys, ids, digit_bits=db)
+                b.record()
+                b.synchronize()
+                ts.append(a.elapsed_time(b))
+            ms = sorted(ts)[len(ts) // 2]
+            rows.append(dict(size_class=c, n=n, key_bits=key_bits, digit_bits=db, ms=ms))
+            if verbose:
+                print(f"  n={n} key_bits={key_bits} digit_bits={db}: {ms:.3f} ms", flush=True)
+            if best is None or ms < best[0]:
+                best = (ms, db)
+        if apply:
+            G.set_sort_digit_bits(n, best[1])
+        del keys, ids
+    return rows
 
 
 class TuningCache:

@@ -3,65 +3,76 @@
 // (gpu/mitm_gpu2.py:101-104, a stable argsort plus two gathers) and
 // join_sorted (gpu/mitm_gpu2.py:107-119).
 //
-// Sort: one histogram kernel reads every key once and counts all 8-bit digits
-// of all passes; each pass is then ONE kernel (onesweep): a CTA takes the next
-// tile ticket, ranks its keys stably in shared memory (per warp, item by item
-// over a warp-striped tile, lanes of one digit matched through a shared mask,
-// so equal digits keep input order),
-// publishes its per-digit counts, resolves its global digit offsets by
-// decoupled look-back over the tiles before it (bounded spin), and scatters
-// keys, then ids.  Passes whose digit is equal for every key are skipped by the
-// host, so keys below M cost at most ceil(log2 M / 8) passes.
+// Sort: one histogram kernel reads every key once and counts all digits of all
+// passes; each pass is then ONE kernel (onesweep): a CTA takes the next tile
+// ticket, ranks its keys stably in shared memory (per warp, item by item over a
+// warp-striped tile, lanes of one digit matched through a shared mask, so equal
+// digits keep input order), publishes its per-digit counts, resolves its global
+// digit offsets by decoupled look-back over the tiles before it (bounded spin),
+// and scatters keys, then ids.  The digit is 8 or 9 bits wide (one width for all
+// passes of a sort; the autotuner picks it per size class).  Passes whose digit
+// is equal for every key are skipped by the host, so keys below M cost at most
+// ceil(log2 M / width) passes.
 //
 // Merge join: every thread takes a run of consecutive sorted I keys, finds the
 // first D key >= its first key by binary search and then gallops forward;
 // every I row with at least one equal D key is appended as (row, first D
 // position, count) to a compact run list (pairs are rare).  The host expands
 // runs into pairs in I-row order, which is join_sorted's output order.
+#include <type_traits>
+#include <vector>
 #include "cf_abi_internal.h"
 
 namespace {
 
+using u16 = unsigned short;
+
 constexpr int kSortBlock = 512;
 constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortBlock * kSortItems;  // 4096
-constexpr int kRadix = 256;
 constexpr int kWarps = kSortBlock / 32;
+constexpr int kMaxPasses = 8;                       // 64 bits at 8 or 9 bits per digit
 constexpr u64 kFlagAgg = 1ull << 62;
 constexpr u64 kFlagInc = 2ull << 62;
 constexpr u64 kValMask = (1ull << 62) - 1;
 constexpr u32 kSpinLimit = 1u << 24;
 
+// Digit counts of every pass, one read of the keys: hist[p][d] for the digit of
+// width db at bit p * db, p < np.  Dynamic shared memory: np << db counters.
 __global__ void __launch_bounds__(kSortBlock)
-k_sort_hist(const u64* __restrict__ keys, u64 n, u64* __restrict__ hist /*[8][256]*/) {
-  __shared__ u32 s_h[8][kRadix];
-  for (int i = threadIdx.x; i < 8 * kRadix; i += kSortBlock) (&s_h[0][0])[i] = 0;
+k_sort_hist(const u64* __restrict__ keys, u64 n, u64* __restrict__ hist /*[np][1 << db]*/, int np, int db) {
+  extern __shared__ u32 s_h[];
+  const int bins = np << db;
+  const u64 mask = (1ull << db) - 1;
+  for (int i = threadIdx.x; i < bins; i += kSortBlock) s_h[i] = 0;
   __syncthreads();
   for (u64 i = (u64)blockIdx.x * kSortBlock + threadIdx.x; i < n; i += (u64)gridDim.x * kSortBlock) {
     const u64 k = keys[i];
 #pragma unroll
-    for (int p = 0; p < 8; ++p) atomicAdd(&s_h[p][(k >> (8 * p)) & 0xff], 1u);
+    for (int p = 0; p < kMaxPasses; ++p)
+      if (p < np) atomicAdd(&s_h[(p << db) + (int)((k >> (p * db)) & mask)], 1u);
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < 8 * kRadix; i += kSortBlock) {
-    const u32 v = (&s_h[0][0])[i];
+  for (int i = threadIdx.x; i < bins; i += kSortBlock) {
+    const u32 v = s_h[i];
     if (v) atomicAdd((unsigned long long*)&hist[i], (unsigned long long)v);
   }
 }
 
-// exclusive scan of each pass's 256-bin histogram (one warp per pass)
-__global__ void k_sort_hist_scan(const u64* __restrict__ hist, u64* __restrict__ excl) {
+// exclusive scan of each pass's histogram of 1 << db bins (one warp per pass)
+__global__ void k_sort_hist_scan(const u64* __restrict__ hist, u64* __restrict__ excl, int db) {
   const int p = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bins = 1 << db;
   u64 run = 0;
-  for (int c = 0; c < kRadix; c += 32) {
-    const u64 v = hist[p * kRadix + c + lane];
+  for (int c = 0; c < bins; c += 32) {
+    const u64 v = hist[p * bins + c + lane];
     u64 incl = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const u64 x = __shfl_up_sync(0xffffffffu, incl, o);
       if (lane >= o) incl += x;
     }
-    excl[p * kRadix + c + lane] = run + incl - v;
+    excl[p * bins + c + lane] = run + incl - v;
     run += __shfl_sync(0xffffffffu, incl, 31);
   }
 }
@@ -105,13 +116,14 @@ __device__ __forceinline__ bool mbar_wait(u64* bar, u32 parity, u32 limit) {
 
 // Write a staged tile (staged element j has digit s_dj[j]) to its global places,
 // kSortItems elements per thread with their shared-memory loads issued together.
-__device__ __forceinline__ void write_tile(const u64* s_v, const unsigned char* s_dj, const u64* s_gbase,
+template <typename Dig>
+__device__ __forceinline__ void write_tile(const u64* s_v, const Dig* s_dj, const u64* s_gbase,
                                            u64* __restrict__ out, int tv) {
   u32 d[kSortItems];
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
     const int j = threadIdx.x + k * kSortBlock;
-    d[k] = j < tv ? s_dj[j] : 0u;
+    d[k] = j < tv ? (u32)s_dj[j] : 0u;
   }
   u64 dst[kSortItems], v[kSortItems];
 #pragma unroll
@@ -127,29 +139,57 @@ __device__ __forceinline__ void write_tile(const u64* s_v, const unsigned char* 
 
 constexpr int kLookWin = 8;           // predecessor tiles read per look-back round trip
 constexpr u32 kMbarLimit = 1u << 22;  // try_wait rounds (each suspends for a while) before giving up
-constexpr size_t kPassSmem = (size_t)kSortTile * 16 + (size_t)kSortTile + (size_t)kWarps * kRadix * 8;
 
-// One onesweep pass over the digit at bit `shift`.  Two CTAs per SM.  BULK: the
-// tile's keys and ids are brought into shared memory by two bulk copies at the
-// start (every pointer 16-byte aligned), so the id load overlaps the ranking;
-// otherwise by plain coalesced loads.  Each item's digit (9 bits, 0x100 = no
+// Dynamic shared memory of one pass with DB-bit digits (R = 2^DB bins):
+//   tile keys [4096] u64 | tile ids [4096] u64 | warp digit counters [16][R] Cnt |
+//   union { peer masks [16][R] u32 (ranking only),
+//           staged digits [4096] Dig, gbase [R] u64, dcnt [R] u32, doff [R] u32 (after ranking) }.
+// A warp's count of one digit is at most 256 and the exclusive over warps at most 4096, so the
+// 9-bit pass keeps its counters in 16 bits; with the union that keeps it at 112 KB, two CTAs per SM.
+template <int DB>
+struct PassLayout {
+  static constexpr int R = 1 << DB;
+  using Cnt = typename std::conditional<DB == 8, u32, u16>::type;
+  using Dig = typename std::conditional<DB == 8, unsigned char, u16>::type;
+  static constexpr size_t kTile = (size_t)kSortTile * 16;
+  static constexpr size_t kWc = (size_t)kWarps * R * sizeof(Cnt);
+  static constexpr size_t kMm = (size_t)kWarps * R * 4;
+  static constexpr size_t kDj = (size_t)kSortTile * sizeof(Dig);
+  static constexpr size_t kAfter = kDj + (size_t)R * 16;
+  static constexpr size_t kUnion = kMm > kAfter ? kMm : kAfter;
+  static constexpr size_t kSmem = kTile + kWc + kUnion;
+  static_assert(R <= kSortBlock, "one thread per digit in the scan and look-back");
+  static_assert(kWc % 16 == 0 && kDj % 16 == 0, "aligned sub-arrays");
+  static_assert(2 * (kSmem + 1024 + 256) <= 233472, "two CTAs per SM");
+};
+
+// One onesweep pass over the DB-bit digit at bit `shift`.  Two CTAs per SM.  BULK:
+// the tile's keys and ids are brought into shared memory by two bulk copies at
+// the start (every pointer 16-byte aligned), so the id load overlaps the ranking;
+// otherwise by plain coalesced loads.  Each item's digit (DB + 1 bits, R = no
 // item) rides in the top bits of its local offset.
-template <bool BULK>
+template <int DB, bool BULK>
 __global__ void __launch_bounds__(kSortBlock, 2)
 k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __restrict__ kout,
-            u64* __restrict__ iout, u64 n, int shift, const u64* __restrict__ gexcl /*[256]*/,
-            u64* __restrict__ status /*[tiles][256]*/, u32* __restrict__ ticket, u32* __restrict__ err) {
+            u64* __restrict__ iout, u64 n, int shift, const u64* __restrict__ gexcl /*[R]*/,
+            u64* __restrict__ status /*[tiles][R]*/, u32* __restrict__ ticket, u32* __restrict__ err) {
+  using L = PassLayout<DB>;
+  using Cnt = typename L::Cnt;
+  using Dig = typename L::Dig;
+  constexpr int R = L::R;
+  constexpr u32 kNone = (u32)R;
   extern __shared__ __align__(128) unsigned char smem[];
   u64* s_kin = (u64*)smem;                                   // tile keys; later the staging area
   u64* s_iin = s_kin + kSortTile;                            // tile ids
-  unsigned char* s_dj = (unsigned char*)(s_iin + kSortTile); // digit of staged element j
-  u32* s_wc = (u32*)(s_dj + kSortTile);                      // [kWarps][256] warp digit counts
-  u32* s_mm = s_wc + kWarps * kRadix;                        // [kWarps][256] lanes holding each digit
+  Cnt* s_wc = (Cnt*)(smem + L::kTile);                       // [kWarps][R] warp digit counts
+  unsigned char* s_un = smem + L::kTile + L::kWc;
+  u32* s_mm = (u32*)s_un;                                    // [kWarps][R] lanes holding each digit
+  Dig* s_dj = (Dig*)s_un;                                    // digit of staged element j
+  u64* s_gbase = (u64*)(s_un + L::kDj);  // global position of staged element j of digit d: s_gbase[d] + j
+  u32* s_dcnt = (u32*)(s_gbase + R);
+  u32* s_doff = s_dcnt + R;
   __shared__ __align__(8) u64 s_bar[2];
   __shared__ u32 s_tile;
-  __shared__ u32 s_dcnt[kRadix];
-  __shared__ u32 s_doff[kRadix];
-  __shared__ u64 s_gbase[kRadix];   // global position of staged element j of digit d: s_gbase[d] + j
   __shared__ u32 s_scan[kWarps];
 
   if (threadIdx.x == 0) {
@@ -183,7 +223,8 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
       s_iin[j] = iin[base + j];
     }
   }
-  for (int i = threadIdx.x; i < 2 * kWarps * kRadix; i += kSortBlock) s_wc[i] = 0;   // s_wc and s_mm
+  for (int i = threadIdx.x; i < (int)((L::kWc + L::kMm) / 4); i += kSortBlock)   // counters and masks
+    ((u32*)(smem + L::kTile))[i] = 0;
   __syncthreads();
   // A tile whose keys never arrived (both bounded waits ran out, practically unreachable) is
   // ranked as empty: it publishes zero counts, so its successors' look-back still ends and
@@ -203,8 +244,8 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
   u64 key[kSortItems];
   u32 loc[kSortItems];                      // local offset (low 16 bits) | digit << 16
   const u32 lt = lanemask_lt();
-  u32* wc = s_wc + wid * kRadix;
-  u32* mm = s_mm + wid * kRadix;
+  Cnt* wc = s_wc + wid * R;
+  u32* mm = s_mm + wid * R;
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
     const int e = wid * 32 * kSortItems + it * 32 + lane;
@@ -217,8 +258,8 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
     const int e = wid * 32 * kSortItems + it * 32 + lane;
-    const u32 d = e < tr ? (u32)((key[it] >> shift) & 0xff) : 0x100u;
-    const bool valid = d < 0x100u;
+    const u32 d = e < tr ? (u32)((key[it] >> shift) & (u64)(R - 1)) : kNone;
+    const bool valid = d < kNone;
     if (valid) atomicOr(&mm[d], 1u << lane);
     __syncwarp();
     const u32 peers = valid ? mm[d] : 0u;
@@ -227,7 +268,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
     u32 base = 0;
     if (valid && lane == leader) {
       base = wc[d];
-      wc[d] = base + __popc(peers);
+      wc[d] = (Cnt)(base + __popc(peers));
       mm[d] = 0u;
     }
     base = __shfl_sync(0xffffffffu, base, leader);
@@ -235,22 +276,22 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
     loc[it] = (d << 16) | (base + __popc(peers & lt));
   }
   __syncthreads();
-  if (threadIdx.x < kRadix) {                 // per digit: exclusive over warps, tile total
+  if (threadIdx.x < R) {                      // per digit: exclusive over warps, tile total
     const int d = threadIdx.x;
     u32 v[kWarps];
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) v[w] = s_wc[w * kRadix + d];
+    for (int w = 0; w < kWarps; ++w) v[w] = s_wc[w * R + d];
     u32 run = 0;
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) {
-      s_wc[w * kRadix + d] = run;
+      s_wc[w * R + d] = (Cnt)run;
       run += v[w];
     }
     s_dcnt[d] = run;
     // flag and count share one 64-bit word and readers read nothing else that this
     // tile writes, so the status store needs no fence before it
     const u64 pub = (tile == 0) ? (kFlagInc | (u64)run) : (kFlagAgg | (u64)run);
-    ((volatile u64*)status)[(u64)tile * kRadix + d] = pub;
+    ((volatile u64*)status)[(u64)tile * R + d] = pub;
     u32 incl = run;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -261,7 +302,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
     s_doff[d] = incl - run;
   }
   __syncthreads();
-  if (threadIdx.x < kRadix) {
+  if (threadIdx.x < R) {
     const int d = threadIdx.x;
     u32 add = 0;
     for (int w = 0; w < wid; ++w) add += s_scan[w];
@@ -276,7 +317,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
         u64 v[kLookWin];
 #pragma unroll
         for (int w = 0; w < kLookWin; ++w)
-          v[w] = (j - w >= 0) ? ((volatile const u64*)status)[(u64)(j - w) * kRadix + d] : kFlagInc;
+          v[w] = (j - w >= 0) ? ((volatile const u64*)status)[(u64)(j - w) * R + d] : kFlagInc;
         int used = 0;
         bool stop = false, stall = false;
 #pragma unroll
@@ -295,7 +336,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
           __nanosleep(64);
         }
       }
-      ((volatile u64*)status)[(u64)tile * kRadix + d] = kFlagInc | (excl + s_dcnt[d]);
+      ((volatile u64*)status)[(u64)tile * R + d] = kFlagInc | (excl + s_dcnt[d]);
     }
     s_gbase[d] = gexcl[d] + excl - s_doff[d];   // wraps mod 2^64; j >= s_doff[d] brings it back
   }
@@ -305,16 +346,16 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
 #pragma unroll
     for (int it = 0; it < kSortItems; ++it) {
       const u32 d = loc[it] >> 16;
-      add[it] = d < 0x100u ? s_doff[d] + wc[d] : 0u;
+      add[it] = d < kNone ? s_doff[d] + (u32)wc[d] : 0u;
     }
 #pragma unroll
     for (int it = 0; it < kSortItems; ++it) {
       const u32 d = loc[it] >> 16;
-      if (d < 0x100u) {
+      if (d < kNone) {
         const u32 l = (loc[it] & 0xffffu) + add[it];
         loc[it] = l | (d << 16);
         s_kin[l] = key[it];
-        s_dj[l] = (unsigned char)d;
+        s_dj[l] = (Dig)d;
       }
     }
   }
@@ -343,11 +384,11 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
 #pragma unroll
     for (int it = 0; it < kSortItems; ++it) {
       const int e = wid * 32 * kSortItems + it * 32 + lane;
-      idv[it] = (loc[it] >> 16) < 0x100u ? s_iin[e] : 0ull;
+      idv[it] = (loc[it] >> 16) < kNone ? s_iin[e] : 0ull;
     }
 #pragma unroll
     for (int it = 0; it < kSortItems; ++it)
-      if ((loc[it] >> 16) < 0x100u) s_kin[loc[it] & 0xffffu] = idv[it];
+      if ((loc[it] >> 16) < kNone) s_kin[loc[it] & 0xffffu] = idv[it];
   }
   __syncthreads();
   write_tile(s_kin, s_dj, s_gbase, iout, tr);
@@ -407,65 +448,82 @@ k_merge_runs(const u64* __restrict__ Dk, u64 nD, const u64* __restrict__ Ik, u64
 
 }  // namespace
 
-// Workspace of one sort of n records: second key/id buffers, histograms, the
-// look-back status words of every pass and the tile tickets.
-extern "C" size_t cf_sort_tmp_bytes(u64 n) {
+// Workspace of one sort of n records with np passes of db-bit digits: second
+// key/id buffers, histograms, the look-back status words of every pass and the
+// tile tickets.
+static size_t sort_tmp_bytes(u64 n, int np, int db) {
   const u64 tiles = (n + kSortTile - 1) / kSortTile;
-  return (size_t)(2 * n * 8) + 2 * 8 * kRadix * 8 + (size_t)(8 * tiles * kRadix * 8) + 8 * 4 + 64;
+  const u64 bins = (u64)np << db;
+  return (size_t)(2 * n * 8) + (size_t)(2 * bins * 8) + (size_t)(tiles * bins * 8) + kMaxPasses * 4 + 64;
 }
 
-// Sort (keys, ids) of length n by key, stably, in place (results end in the
-// caller's arrays).  key_bits: bits of the largest key (1..64); passes whose
-// digit is constant are skipped.  Synchronises the stream once (to read the
-// digit histogram).
-extern "C" int cf_sort_pairs(u64* keys, u64* ids, u64 n, int key_bits, void* tmp, size_t tmp_bytes, void* stream) {
-  if (n <= 1) return CF_OK;
-  if (!keys || !ids || !tmp) { cf_set_error("cf_sort_pairs: null buffer%s", ""); return CF_EBADARG; }
-  if (key_bits < 1 || key_bits > 64) { cf_set_error("cf_sort_pairs: key_bits must be 1..64%s", ""); return CF_EBADARG; }
-  if (n > (1ull << 40)) { cf_set_error("cf_sort_pairs: n too large%s", ""); return CF_EBADARG; }
-  if (tmp_bytes < cf_sort_tmp_bytes(n)) { cf_set_error("cf_sort_pairs: workspace too small%s", ""); return CF_ENOMEM; }
-  cudaStream_t st = (cudaStream_t)stream;
+static int sort_passes(int key_bits, int db) { return (key_bits + db - 1) / db; }
+
+template <int DB>
+static cudaError_t sort_pass_attrs() {
+  cudaError_t e = cudaFuncSetAttribute(k_sort_pass<DB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)PassLayout<DB>::kSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sort_pass<DB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)PassLayout<DB>::kSmem);
+  return e;
+}
+
+template <int DB>
+static void sort_pass_launch(bool bulk, unsigned tiles, cudaStream_t st, const u64* ka, const u64* ia, u64* kb,
+                             u64* ib, u64 n, int shift, const u64* excl, u64* status, u32* ticket, u32* errw) {
+  if (bulk)
+    k_sort_pass<DB, true><<<tiles, kSortBlock, PassLayout<DB>::kSmem, st>>>(ka, ia, kb, ib, n, shift, excl, status,
+                                                                          ticket, errw);
+  else
+    k_sort_pass<DB, false><<<tiles, kSortBlock, PassLayout<DB>::kSmem, st>>>(ka, ia, kb, ib, n, shift, excl,
+                                                                           status, ticket, errw);
+}
+
+// The sort behind cf_sort_pairs and cf_sort_pairs_digits: np = ceil(key_bits / db)
+// passes of db-bit digits (8 or 9), passes whose digit is constant skipped.
+static int sort_pairs(u64* keys, u64* ids, u64 n, int key_bits, int db, void* tmp, size_t tmp_bytes, size_t need,
+                      cudaStream_t st) {
+  const int np = sort_passes(key_bits, db);
+  const int bins = 1 << db;
   const u64 tiles = (n + kSortTile - 1) / kSortTile;
+  if (tmp_bytes < need) { cf_set_error("cf_sort_pairs: workspace too small%s", ""); return CF_ENOMEM; }
   unsigned char* w = (unsigned char*)tmp;
   u64* k2 = (u64*)w; w += n * 8;
   u64* i2 = (u64*)w; w += n * 8;
-  u64* hist = (u64*)w; w += 8 * kRadix * 8;
-  u64* excl = (u64*)w; w += 8 * kRadix * 8;
-  u64* status = (u64*)w; w += 8 * tiles * kRadix * 8;
-  u32* tickets = (u32*)w; w += 8 * 4;
+  u64* hist = (u64*)w; w += (size_t)np * bins * 8;
+  u64* excl = (u64*)w; w += (size_t)np * bins * 8;
+  u64* status = (u64*)w; w += (size_t)np * tiles * bins * 8;
+  u32* tickets = (u32*)w; w += kMaxPasses * 4;
   u32* errw = (u32*)w;
-  const int npass = (key_bits + 7) / 8;
-  cudaError_t e = cudaMemsetAsync(hist, 0, 8 * kRadix * 8, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, (size_t)8 * tiles * kRadix * 8, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(tickets, 0, 8 * 4 + 4, st);
+  cudaError_t e = cudaMemsetAsync(hist, 0, (size_t)np * bins * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, (size_t)np * tiles * bins * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(tickets, 0, kMaxPasses * 4 + 4, st);
   if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: memset");
   const unsigned hgrid = (unsigned)((n + kSortBlock * 8 - 1) / (kSortBlock * 8));
-  k_sort_hist<<<hgrid < 2048 ? hgrid : 2048, kSortBlock, 0, st>>>(keys, n, hist);
-  k_sort_hist_scan<<<1, 256, 0, st>>>(hist, excl);
+  k_sort_hist<<<hgrid < 2048 ? hgrid : 2048, kSortBlock, (size_t)(np << db) * 4, st>>>(keys, n, hist, np, db);
+  k_sort_hist_scan<<<1, 32 * np, 0, st>>>(hist, excl, db);
   CF_LAUNCH_CHECK("cf_sort_pairs: histogram");
-  u64 hh[8 * kRadix];
-  e = cudaMemcpyAsync(hh, hist, sizeof hh, cudaMemcpyDeviceToHost, st);
+  std::vector<u64> hh((size_t)np * bins);
+  e = cudaMemcpyAsync(hh.data(), hist, hh.size() * 8, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: histogram read");
-  e = cudaFuncSetAttribute(k_sort_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPassSmem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_sort_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPassSmem);
+  e = db == 8 ? sort_pass_attrs<8>() : sort_pass_attrs<9>();
   if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: smem attribute");
   u64 *ka = keys, *ia = ids, *kb = k2, *ib = i2;
   int done = 0;
-  for (int p = 0; p < npass; ++p) {
+  for (int p = 0; p < np; ++p) {
     bool trivial = false;
-    for (int d = 0; d < kRadix; ++d) if (hh[p * kRadix + d] == n) trivial = true;
+    for (int d = 0; d < bins; ++d) if (hh[(size_t)p * bins + d] == n) trivial = true;
     if (trivial) continue;
     // bulk copies read 16-byte units from 16-byte boundaries: every tile starts at
     // a multiple of 4096 records, so aligned source arrays suffice
     const bool bulk = ((((uintptr_t)ka) | ((uintptr_t)ia)) & 15u) == 0;
-    if (bulk)
-      k_sort_pass<true><<<(unsigned)tiles, kSortBlock, kPassSmem, st>>>(
-          ka, ia, kb, ib, n, 8 * p, excl + p * kRadix, status + (u64)p * tiles * kRadix, tickets + p, errw);
+    u64* pst = status + (u64)p * tiles * bins;
+    if (db == 8)
+      sort_pass_launch<8>(bulk, (unsigned)tiles, st, ka, ia, kb, ib, n, 8 * p, excl + p * bins, pst, tickets + p, errw);
     else
-      k_sort_pass<false><<<(unsigned)tiles, kSortBlock, kPassSmem, st>>>(
-          ka, ia, kb, ib, n, 8 * p, excl + p * kRadix, status + (u64)p * tiles * kRadix, tickets + p, errw);
+      sort_pass_launch<9>(bulk, (unsigned)tiles, st, ka, ia, kb, ib, n, 9 * p, excl + p * bins, pst, tickets + p, errw);
     CF_LAUNCH_CHECK("cf_sort_pairs: pass");
     u64* t = ka; ka = kb; kb = t;
     t = ia; ia = ib; ib = t;
@@ -482,6 +540,49 @@ extern "C" int cf_sort_pairs(u64* keys, u64* ids, u64 n, int key_bits, void* tmp
   if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: error word");
   if (herr & CF_ERR_SPIN_LIMIT) { cf_set_error("cf_sort_pairs: look-back wait exceeded its limit%s", ""); return CF_ETIMEOUT; }
   return CF_OK;
+}
+
+static int sort_args_ok(const u64* keys, const u64* ids, u64 n, int key_bits, const void* tmp, const char* who) {
+  if (!keys || !ids || !tmp) { cf_set_error("%s: null buffer", who); return CF_EBADARG; }
+  if (key_bits < 1 || key_bits > 64) { cf_set_error("%s: key_bits must be 1..64", who); return CF_EBADARG; }
+  if (n > (1ull << 40)) { cf_set_error("%s: n too large", who); return CF_EBADARG; }
+  return CF_OK;
+}
+
+extern "C" size_t cf_sort_tmp_bytes(u64 n) { return sort_tmp_bytes(n, kMaxPasses, 8); }
+
+// Sort (keys, ids) of length n by key, stably, in place (results end in the
+// caller's arrays), 8-bit digits.  key_bits: bits of the largest key (1..64);
+// passes whose digit is constant are skipped.  Synchronises the stream once (to
+// read the digit histogram).
+extern "C" int cf_sort_pairs(u64* keys, u64* ids, u64 n, int key_bits, void* tmp, size_t tmp_bytes, void* stream) {
+  if (n <= 1) return CF_OK;
+  const int rc = sort_args_ok(keys, ids, n, key_bits, tmp, "cf_sort_pairs");
+  if (rc != CF_OK) return rc;
+  return sort_pairs(keys, ids, n, key_bits, 8, tmp, tmp_bytes, cf_sort_tmp_bytes(n), (cudaStream_t)stream);
+}
+
+// Workspace of cf_sort_pairs_digits; 0 for a digit width other than 8 or 9 or
+// key_bits outside 1..64.
+extern "C" size_t cf_sort_digits_tmp_bytes(u64 n, int key_bits, int digit_bits) {
+  if ((digit_bits != 8 && digit_bits != 9) || key_bits < 1 || key_bits > 64) return 0;
+  return sort_tmp_bytes(n, sort_passes(key_bits, digit_bits), digit_bits);
+}
+
+// cf_sort_pairs with the digit width chosen by the caller (8 or 9 bits):
+// ceil(key_bits / digit_bits) passes, constant-digit passes skipped.  Same
+// result for every width.
+extern "C" int cf_sort_pairs_digits(u64* keys, u64* ids, u64 n, int key_bits, int digit_bits, void* tmp,
+                                    size_t tmp_bytes, void* stream) {
+  if (digit_bits != 8 && digit_bits != 9) {
+    cf_set_error("cf_sort_pairs_digits: digit_bits must be 8 or 9%s", "");
+    return CF_EBADARG;
+  }
+  if (n <= 1) return CF_OK;
+  const int rc = sort_args_ok(keys, ids, n, key_bits, tmp, "cf_sort_pairs_digits");
+  if (rc != CF_OK) return rc;
+  return sort_pairs(keys, ids, n, key_bits, digit_bits, tmp, tmp_bytes,
+                    cf_sort_digits_tmp_bytes(n, key_bits, digit_bits), (cudaStream_t)stream);
 }
 
 extern "C" size_t cf_merge_run_bytes(void) { return sizeof(CfRun); }

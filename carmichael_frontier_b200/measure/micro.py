@@ -2,7 +2,8 @@
 and the rates of the LSD radix sort (the materialised join's sort_side) and of generation.
 
     python -m carmichael_frontier_b200.measure.micro            # ceilings, one JSON line
-    python -m carmichael_frontier_b200.measure.micro sort N     # cf_sort_pairs on N random 62-bit keys
+    python -m carmichael_frontier_b200.measure.micro sort N [KEY_BITS [DIGIT_BITS]]
+                                     # the radix sort on N random keys (default 62 bits, 8-bit digits)
     python -m carmichael_frontier_b200.measure.micro gen N      # linear generator, bounded D producer
 bench.py measures the L2 figure in its own run as the fused probe's ceiling.  The ceiling kernels
 live in libcfmicro.so (measure/cf_micro.cu), apart from the library's C ABI.
@@ -69,32 +70,47 @@ def montgomery_products(iters: int = 4096, reps: int = 3) -> float:
     return best
 
 
-def sort_rate(n: int, key_bits: int = 62, reps: int = 3) -> dict:
-    """cf_sort_pairs on n random (key, id) records: records/s and the HBM bytes per second
-    of its passes (each 8-bit digit pass reads and writes 16 bytes per record)."""
+def sort_rate(n: int, key_bits: int = 62, digit_bits: int = 8, reps: int = 3, library: bool = True) -> dict:
+    """cf_sort_pairs_digits on n random (key, id) records below 2^key_bits: records/s and the HBM
+    bytes per second of its passes (each digit pass reads and writes 16 bytes per record, the
+    histogram reads the keys once).  library=True adds the stable torch.sort of the same keys
+    (the CUDA library's radix sort of (key, 64-bit index) pairs over all 64 key bits) for context."""
     import torch
     lib = _lib.load()
     g = torch.Generator(device="cuda").manual_seed(7)
     k0 = torch.randint(0, 1 << key_bits, (n,), dtype=torch.int64, device="cuda", generator=g)
     keys, ids = torch.empty_like(k0), torch.arange(n, dtype=torch.int64, device="cuda")
-    nb = lib.cf_sort_tmp_bytes(n)
+    nb = lib.cf_sort_digits_tmp_bytes(n, key_bits, digit_bits)
+    if nb == 0:
+        raise ValueError(f"digit width {digit_bits} or key_bits {key_bits} not supported")
     tmp = torch.empty(nb, dtype=torch.uint8, device="cuda")
     sh = torch.cuda.current_stream().cuda_stream
-    best = None
-    for _ in range(reps + 1):
-        keys.copy_(k0)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        _lib.check(lib.cf_sort_pairs(keys.data_ptr(), ids.data_ptr(), n, key_bits, tmp.data_ptr(), nb, sh), "sort")
-        e1.record()
-        torch.cuda.synchronize()
-        t = e0.elapsed_time(e1) * 1e-3
-        best = t if best is None else min(best, t)
+
+    def timed(fn):
+        best = None
+        for _ in range(reps + 1):
+            keys.copy_(k0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) * 1e-3
+            best = t if best is None else min(best, t)
+        return best
+
+    best = timed(lambda: _lib.check(lib.cf_sort_pairs_digits(keys.data_ptr(), ids.data_ptr(), n, key_bits,
+                                                             digit_bits, tmp.data_ptr(), nb, sh), "sort"))
     assert bool((keys[1:] >= keys[:-1]).all())
-    passes = (key_bits + 7) // 8
-    return {"n": n, "s": best, "records_per_s": n / best, "passes": passes,
-            "GB_s": (32 * passes + 8) * n / best / 1e9}     # passes + one histogram read of the keys
+    passes = (key_bits + digit_bits - 1) // digit_bits
+    out = {"n": n, "key_bits": key_bits, "digit_bits": digit_bits, "s": best, "records_per_s": n / best,
+           "passes": passes, "GB_s": (32 * passes + 8) * n / best / 1e9}
+    if library:
+        del tmp
+        t_lib = timed(lambda: torch.sort(keys, stable=True))
+        out["torch_sort"] = {"s": t_lib, "records_per_s": n / t_lib}
+    return out
 
 
 def generation_rate(n: int, dmin_bits: int = 40, reps: int = 3) -> dict:
@@ -134,7 +150,9 @@ def generation_rate(n: int, dmin_bits: int = 40, reps: int = 3) -> dict:
 def main() -> None:
     import sys
     if len(sys.argv) > 2 and sys.argv[1] == "sort":
-        print(json.dumps(sort_rate(int(sys.argv[2]))))
+        kb = int(sys.argv[3]) if len(sys.argv) > 3 else 62
+        db = int(sys.argv[4]) if len(sys.argv) > 4 else 8
+        print(json.dumps(sort_rate(int(sys.argv[2]), kb, db)))
         return
     if len(sys.argv) > 2 and sys.argv[1] == "gen":
         print(json.dumps(generation_rate(int(sys.argv[2]))))

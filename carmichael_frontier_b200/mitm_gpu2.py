@@ -6,7 +6,7 @@ CuPy arrays.  Every function runs hand-written sm_100a kernels through the C ABI
 (``include/cfmitm.h``):
 
   generate    -> cf_gen_subsets   (lexicographic rank ranges, canonical residues)
-  sort_side   -> cf_sort_pairs    (stable LSD onesweep radix sort, keys and ids)
+  sort_side   -> cf_sort_pairs_digits (stable LSD onesweep radix sort, keys and ids, tuned digit width)
   join_sorted -> cf_merge_join_runs + host expansion of the (rare) equal runs
 """
 from __future__ import annotations
@@ -81,20 +81,43 @@ def generate(primes, r: int, M: int, mult: int = 1, bits: int = 10, lo: int = 0,
     return keys, ids
 
 
-def sort_side(keys, ids):
-    """Sort one side by key (stable LSD radix sort). Returns (sorted_keys, sorted_ids)."""
-    torch = _torch()
+SORT_DIGIT_WIDTHS = (8, 9)
+_sort_digits: dict[int, int] = {}     # size class (bit length of n) -> digit width picked by the autotuner
+
+
+def sort_digit_bits(n: int) -> int:
+    """Radix digit width sort_side uses for n records: the autotuner's pick for n's size class
+    (autotune.tune_sort), else 8."""
+    return _sort_digits.get(int(n).bit_length(), 8)
+
+
+def set_sort_digit_bits(n: int, bits: int | None) -> None:
+    """Record the digit width for n's size class (None forgets the class's pick)."""
+    if bits is None:
+        _sort_digits.pop(int(n).bit_length(), None)
+        return
+    if bits not in SORT_DIGIT_WIDTHS:
+        raise ValueError(f"digit width {bits} not in {SORT_DIGIT_WIDTHS}")
+    _sort_digits[int(n).bit_length()] = int(bits)
+
+
+def sort_side(keys, ids, digit_bits: int | None = None):
+    """Sort one side by key (stable LSD radix sort). Returns (sorted_keys, sorted_ids).
+    digit_bits (8 or 9) overrides the tuned radix digit width; the result is the same."""
     n = keys.numel()
     ko = keys.contiguous().clone()
     io = ids.contiguous().clone()
     if n <= 1:
         return ko, io
+    db = sort_digit_bits(n) if digit_bits is None else int(digit_bits)
+    if db not in SORT_DIGIT_WIDTHS:
+        raise ValueError(f"digit width {db} not in {SORT_DIGIT_WIDTHS}")
     dev = ko.device
     lib = _lib.load()
-    nbytes = lib.cf_sort_tmp_bytes(n)
+    nbytes = lib.cf_sort_digits_tmp_bytes(n, 64, db)
     tmp = _workspace(dev, "sort", nbytes)
-    _lib.check(lib.cf_sort_pairs(_lib.ptr(ko), _lib.ptr(io), n, 64, _lib.ptr(tmp), nbytes, _lib.stream_handle()),
-               "sort_side")
+    _lib.check(lib.cf_sort_pairs_digits(_lib.ptr(ko), _lib.ptr(io), n, 64, db, _lib.ptr(tmp), nbytes,
+                                        _lib.stream_handle()), "sort_side")
     return ko, io
 
 

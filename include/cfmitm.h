@@ -431,6 +431,17 @@ size_t cf_sort_tmp_bytes(uint64_t n);
 int cf_sort_pairs(uint64_t* keys, uint64_t* ids, uint64_t n, int key_bits, void* tmp, size_t tmp_bytes,
                   void* stream);
 
+/* The same sort with the digit width chosen by the caller: digit_bits 8 or 9
+ * (other widths return CF_EBADARG), ceil(key_bits / digit_bits) passes, passes
+ * whose digit is constant skipped; the result does not depend on the width.
+ * Workspace cf_sort_digits_tmp_bytes(n, key_bits, digit_bits) (0 for a bad
+ * width or key_bits).  The width is the radix digit width that the autotuner
+ * picks per size class for sort_side (gpu/mitm_gpu2.py:101-104), whose call
+ * has no such argument. */
+size_t cf_sort_digits_tmp_bytes(uint64_t n, int key_bits, int digit_bits);
+int cf_sort_pairs_digits(uint64_t* keys, uint64_t* ids, uint64_t n, int key_bits, int digit_bits, void* tmp,
+                         size_t tmp_bytes, void* stream);
+
 /* The same sort for callers that cannot allocate device memory (for example
  * when all device memory belongs to another allocator): no workspace argument;
  * the scratch is a fixed array inside this library's own device memory (3 MiB,

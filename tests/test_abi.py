@@ -210,6 +210,28 @@ def test_named_entry_points_reject_bad_arguments_without_gpu():
                                      None) == _lib.CF_EBADARG
 
 
+def test_sort_digit_widths_workspace_and_arguments():
+    # the workspace of the digit-width sort: ceil(key_bits / width) passes of 2^width bins each;
+    # the 8-bit workspace over 64 bits is cf_sort_pairs' own
+    lib = _lib.load()
+    n = 1 << 20
+    tiles = n // 4096
+    for bits, width in ((64, 8), (64, 9), (52, 9), (52, 8), (1, 9)):
+        npass = -(-bits // width)
+        want = 16 * n + 16 * (npass << width) + 8 * tiles * (npass << width) + 8 * 4 + 64
+        assert lib.cf_sort_digits_tmp_bytes(n, bits, width) == want
+    assert lib.cf_sort_digits_tmp_bytes(n, 64, 8) == lib.cf_sort_tmp_bytes(n)
+    assert lib.cf_sort_digits_tmp_bytes(n, 64, 10) == 0 and lib.cf_sort_digits_tmp_bytes(n, 0, 8) == 0
+    buf = np.zeros(64, dtype=np.uint8)
+    p = buf.ctypes.data
+    assert lib.cf_sort_pairs_digits(p, p, 100, 64, 7, p, 64, None) == _lib.CF_EBADARG
+    assert b"digit_bits" in lib.cf_last_error_string()
+    assert lib.cf_sort_pairs_digits(None, p, 100, 64, 9, p, 64, None) == _lib.CF_EBADARG
+    assert lib.cf_sort_pairs_digits(p, p, 100, 65, 9, p, 64, None) == _lib.CF_EBADARG
+    assert lib.cf_sort_pairs_digits(p, p, 100, 64, 9, p, 64, None) == _lib.CF_ENOMEM   # before any device work
+    assert lib.cf_sort_pairs_digits(p, p, 1, 64, 9, p, 64, None) == _lib.CF_OK          # nothing to sort
+
+
 def test_ddump_bound_table_equals_the_python_definition():
     from carmichael_frontier_b200.bounded import _u128_pairs, dmin_table
     lib = _lib.load()

@@ -34,11 +34,53 @@ def test_sort_side_is_numpy_stable_sort(cuda, n, bits):
     assert np.array_equal(host(is_), ei)    # stability: ties keep input order
 
 
+@pytest.mark.parametrize("width", [8, 9])
+@pytest.mark.parametrize("n,bits", [(2, 9), (4095, 10), (4097, 52), (12_289, 18), (1_000_001, 62), (777_777, 64),
+                                    (65_536, 27)])
+def test_digit_widths_give_the_numpy_stable_sort(cuda, width, n, bits):
+    # every width: odd n (the workspace arrays of odd passes are not 16-byte aligned, so both
+    # tile-load variants run), ragged last tiles, a last digit narrower than the width, and
+    # passes over constant digits that are skipped
+    rng = np.random.default_rng(n * 131 + bits)
+    keys = rng.integers(0, 1 << bits, size=n, dtype=np.uint64)
+    keys[rng.integers(0, n, size=n // 3)] = keys[0]                  # long runs of one key
+    ids = np.arange(n, dtype=np.uint64) ^ np.uint64(0x5DEECE66D)
+    ks, is_ = G.sort_side(to_dev(keys), to_dev(ids), digit_bits=width)
+    ek, ei = O.sort_side(keys, ids)
+    assert np.array_equal(host(ks), ek)
+    assert np.array_equal(host(is_), ei)
+
+
+def test_tuned_digit_width_is_used_and_changes_nothing(cuda):
+    from carmichael_frontier_b200 import autotune
+    sizes = [3000, 70_000, 1 << 20]
+    rows = autotune.tune_sort(sizes, key_bits=52, reps=2)
+    assert sorted({r["size_class"] for r in rows}) == [n.bit_length() for n in sizes]
+    assert all(r["ms"] > 0 and r["digit_bits"] in G.SORT_DIGIT_WIDTHS for r in rows)
+    for n in sizes:
+        picked = G.sort_digit_bits(n)
+        best = min((r for r in rows if r["size_class"] == n.bit_length()), key=lambda r: r["ms"])
+        assert picked == best["digit_bits"]
+        rng = np.random.default_rng(n)
+        keys = rng.integers(0, 1 << 52, size=n, dtype=np.uint64)
+        ids = np.arange(n, dtype=np.uint64)
+        ks, is_ = G.sort_side(to_dev(keys), to_dev(ids))
+        ek, ei = O.sort_side(keys, ids)
+        assert np.array_equal(host(ks), ek) and np.array_equal(host(is_), ei)
+        G.set_sort_digit_bits(n, None)
+        assert G.sort_digit_bits(n) == 8
+    with pytest.raises(ValueError):
+        G.set_sort_digit_bits(10, 11)
+    with pytest.raises(ValueError):
+        G.sort_side(to_dev(np.arange(10, dtype=np.uint64)), to_dev(np.arange(10, dtype=np.uint64)), digit_bits=10)
+
+
 def test_sort_side_all_equal_keys(cuda):
     keys = np.full(50_000, 123456789, dtype=np.uint64)
     ids = np.arange(50_000, dtype=np.uint64)
-    ks, is_ = G.sort_side(to_dev(keys), to_dev(ids))
-    assert np.array_equal(host(is_), ids)
+    for width in G.SORT_DIGIT_WIDTHS:
+        ks, is_ = G.sort_side(to_dev(keys), to_dev(ids), digit_bits=width)
+        assert np.array_equal(host(is_), ids) and np.array_equal(host(ks), keys)
 
 
 def test_join_sorted_config1_and_random(cuda):
