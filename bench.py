@@ -531,6 +531,14 @@ def measure_portfolio(dev, args, compact: bool = False) -> dict:
     torch.cuda.synchronize(dev)
     t_p = time.perf_counter() - t0
     npl = len(insts) if compact else min(args.plain_moduli, len(insts))
+    # the plain form's sort: radix digit width per size class of its sides, by the autotuner
+    from carmichael_frontier_b200 import autotune, mitm_gpu2
+    sides = [n for k in range(npl) for n in (prep.nD[k], min(prep.nI[k], 1 << 27))]
+    key_bits = max(x.M.bit_length() for x in insts[:npl])
+    t0 = time.perf_counter()
+    autotune.tune_sort(sides, key_bits=key_bits, device=dev, reps=2)
+    t_tune = time.perf_counter() - t0
+    digit_bits = {n.bit_length(): mitm_gpu2.sort_digit_bits(n) for n in sides if n > 1}
     run_plain(insts[:1], i_limit=1 << 16, device=dev)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -560,7 +568,9 @@ def measure_portfolio(dev, args, compact: bool = False) -> dict:
         "per_modulus_fused": {"moduli_per_s": len(insts) / t_p, "records_per_s": recs / t_p, "s": t_p,
                               "same_results": same},
         "plain_mitm_gpu2": {"moduli": npl, "moduli_per_s": npl / t_pl, "records_per_s": rec_pl / t_pl, "s": t_pl,
-                            "same_results": same_plain},
+                            "same_results": same_plain,
+                            "sort_digit_bits": {f"2^{c - 1}..2^{c}": b for c, b in sorted(digit_bits.items())},
+                            "sort_key_bits": key_bits, "sort_tune_s": t_tune},
         "batched_over_plain": (len(insts) / t_b) / (npl / t_pl),
         "mitm64_all_cores": cpu,
         "batched_over_mitm64": ((recs / t_b) / cpu["records_per_s"]) if cpu and cpu.get("records_per_s") else None,
