@@ -71,7 +71,7 @@ def tune(inst: Instance, device=None, reps: int = 3, shapes=None, d_per_part=D_P
     return best[1], rows
 
 
-TICKETS = (2048, 8192, 32768)
+TICKETS = (2048, 4096, 8192, 32768)
 GRID_PER_SM = (0, 2, 4)                 # 0 = one resident wave (the occupancy limit)
 
 

@@ -51,7 +51,9 @@ def tu_ovf_bytes(solver) -> int:
 @dataclass
 class BatchTuning:
     """Launch shape of the batched kernels (chosen by autotune.tune_batch when tuned)."""
-    ticket: int = 8192                 # records per work-queue ticket (multiple of 32)
+    ticket: int = 4096                 # records per work-queue ticket (multiple of 32; tune_batch's pick on
+                                       # the 1024-modulus portfolio: 512 ms against 520 / 529 / 566 ms at
+                                       # 2048 / 8192 / 16384)
     grid: int = 0                      # persistent CTAs per launch (0 = one resident wave)
     mem_budget: int = 24 << 30         # D-table bytes of one batch
     pair_capacity: int = 1 << 16       # initial candidate buffer (grown on overflow)
