@@ -51,6 +51,29 @@ def test_digit_widths_give_the_numpy_stable_sort(cuda, width, n, bits):
     assert np.array_equal(host(is_), ei)
 
 
+@pytest.mark.parametrize("width", [8, 9])
+@pytest.mark.parametrize("key_bits", [9, 45, 52, 63])
+def test_c_entry_with_narrow_key_bits(cuda, width, key_bits):
+    # cf_sort_pairs_digits over key_bits bits only (ceil(key_bits / width) passes, no pass above
+    # them): keys below 2^key_bits come out in numpy's stable order; the workspace it asks for
+    # is the one it needs
+    from carmichael_frontier_b200 import _lib
+    lib = _lib.load()
+    n = 300_007
+    rng = np.random.default_rng(key_bits * 10 + width)
+    keys = rng.integers(0, 1 << key_bits, size=n, dtype=np.uint64)
+    ids = rng.permutation(n).astype(np.uint64)
+    kd, idd = to_dev(keys), to_dev(ids)
+    nb = lib.cf_sort_digits_tmp_bytes(n, key_bits, width)
+    tmp = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    _lib.check(lib.cf_sort_pairs_digits(kd.data_ptr(), idd.data_ptr(), n, key_bits, width, tmp.data_ptr(), nb,
+                                        _lib.stream_handle()), "sort")
+    ek, ei = O.sort_side(keys, ids)
+    assert np.array_equal(host(kd), ek) and np.array_equal(host(idd), ei)
+    assert lib.cf_sort_pairs_digits(kd.data_ptr(), idd.data_ptr(), n, key_bits, width, tmp.data_ptr(), nb - 1,
+                                    _lib.stream_handle()) == _lib.CF_ENOMEM
+
+
 def test_tuned_digit_width_is_used_and_changes_nothing(cuda):
     from carmichael_frontier_b200 import autotune
     sizes = [3000, 70_000, 1 << 20]
