@@ -143,7 +143,6 @@ __device__ __forceinline__ void write_tile(const u64* s_v, const u64 (&dst)[kSor
     if (threadIdx.x + k * kSortBlock < tv) out[dst[k]] = v[k];
 }
 
-constexpr int kLookWin = 8;           // predecessor tiles read per look-back round trip
 constexpr u32 kMbarLimit = 1u << 22;  // try_wait rounds (each suspends for a while) before giving up
 
 // Dynamic shared memory of one pass with DB-bit digits (R = 2^DB bins):
@@ -184,6 +183,9 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
   using Dig = typename L::Dig;
   constexpr int R = L::R;
   constexpr u32 kNone = (u32)R;
+  // predecessor tiles read per look-back round trip: every round reads R status words per tile, so
+  // narrow windows win (measured at 2^28 records: 8-bit digits 5 > 4, 6 > 8 > 12; 9-bit 2 > 3, 4 > 8)
+  constexpr int kLookWin = DB == 8 ? 5 : 2;
   extern __shared__ __align__(128) unsigned char smem[];
   u64* s_kin = (u64*)smem;                                   // tile keys; later the staging area
   u64* s_iin = s_kin + kSortTile;                            // tile ids
