@@ -32,9 +32,15 @@ constexpr int kSortItems = 8;
 constexpr int kSortTile = kSortBlock * kSortItems;  // 4096
 constexpr int kWarps = kSortBlock / 32;
 constexpr int kMaxPasses = 8;                       // 64 bits at 8 or 9 bits per digit
-constexpr u64 kFlagAgg = 1ull << 62;
-constexpr u64 kFlagInc = 2ull << 62;
-constexpr u64 kValMask = (1ull << 62) - 1;
+// Look-back status word of one digit of one tile: flag (aggregate / inclusive) in the top two bits,
+// count below.  32-bit words when n < 2^30 (half the status traffic), 64-bit words otherwise.
+template <typename SW>
+struct Status {
+  static constexpr int kBits = (int)sizeof(SW) * 8;
+  static constexpr SW kAgg = (SW)1 << (kBits - 2);
+  static constexpr SW kInc = (SW)2 << (kBits - 2);
+  static constexpr SW kVal = ((SW)1 << (kBits - 2)) - 1;
+};
 constexpr u32 kSpinLimit = 1u << 24;
 
 // Digit counts of every pass, one read of the keys: hist[p][d] for the digit of
@@ -173,11 +179,12 @@ struct PassLayout {
 // the start (every pointer 16-byte aligned), so the id load overlaps the ranking;
 // otherwise by plain coalesced loads.  Each item's digit (DB + 1 bits, R = no
 // item) rides in the top bits of its local offset.
-template <int DB, bool BULK>
+template <int DB, bool BULK, typename SW>
 __global__ void __launch_bounds__(kSortBlock, 2)
 k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __restrict__ kout,
             u64* __restrict__ iout, u64 n, int shift, const u64* __restrict__ gexcl /*[R]*/,
-            u64* __restrict__ status /*[tiles][R]*/, u32* __restrict__ ticket, u32* __restrict__ err) {
+            SW* __restrict__ status /*[tiles][R]*/, u32* __restrict__ ticket, u32* __restrict__ err) {
+  using St = Status<SW>;
   using L = PassLayout<DB>;
   using Cnt = typename L::Cnt;
   using Dig = typename L::Dig;
@@ -298,8 +305,8 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
     s_dcnt[d] = run;
     // flag and count share one 64-bit word and readers read nothing else that this
     // tile writes, so the status store needs no fence before it
-    const u64 pub = (tile == 0) ? (kFlagInc | (u64)run) : (kFlagAgg | (u64)run);
-    ((volatile u64*)status)[(u64)tile * R + d] = pub;
+    const SW pub = (tile == 0) ? (St::kInc | (SW)run) : (St::kAgg | (SW)run);
+    ((volatile SW*)status)[(u64)tile * R + d] = pub;
     u32 incl = run;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -322,20 +329,20 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
       int j = (int)tile - 1;
       u32 spins = 0;
       for (;;) {
-        u64 v[kLookWin];
+        SW v[kLookWin];
 #pragma unroll
         for (int w = 0; w < kLookWin; ++w)
-          v[w] = (j - w >= 0) ? ((volatile const u64*)status)[(u64)(j - w) * R + d] : kFlagInc;
+          v[w] = (j - w >= 0) ? ((volatile const SW*)status)[(u64)(j - w) * R + d] : St::kInc;
         int used = 0;
         bool stop = false, stall = false;
 #pragma unroll
         for (int w = 0; w < kLookWin; ++w) {
           if (stop || stall) continue;
-          const u64 f = v[w] & ~kValMask;
+          const SW f = v[w] & (SW)~St::kVal;
           if (f == 0) { stall = true; continue; }
-          excl += v[w] & kValMask;
+          excl += (u64)(v[w] & St::kVal);
           ++used;
-          if (f == kFlagInc) stop = true;
+          if (f == St::kInc) stop = true;
         }
         if (stop) break;
         j -= used;
@@ -344,7 +351,7 @@ k_sort_pass(const u64* __restrict__ kin, const u64* __restrict__ iin, u64* __res
           __nanosleep(64);
         }
       }
-      ((volatile u64*)status)[(u64)tile * R + d] = kFlagInc | (excl + s_dcnt[d]);
+      ((volatile SW*)status)[(u64)tile * R + d] = St::kInc | (SW)(excl + s_dcnt[d]);
     }
     s_gbase[d] = gexcl[d] + excl - s_doff[d];   // wraps mod 2^64; j >= s_doff[d] brings it back
   }
@@ -472,26 +479,29 @@ static size_t sort_tmp_bytes(u64 n, int np, int db) {
 
 static int sort_passes(int key_bits, int db) { return (key_bits + db - 1) / db; }
 
-template <int DB>
+template <int DB, typename SW>
 static cudaError_t sort_pass_attrs() {
-  cudaError_t e = cudaFuncSetAttribute(k_sort_pass<DB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_sort_pass<DB, true, SW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)PassLayout<DB>::kSmem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_sort_pass<DB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_sort_pass<DB, false, SW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)PassLayout<DB>::kSmem);
   return e;
 }
 
-template <int DB>
+template <int DB, typename SW>
 static void sort_pass_launch(bool bulk, unsigned tiles, cudaStream_t st, const u64* ka, const u64* ia, u64* kb,
-                             u64* ib, u64 n, int shift, const u64* excl, u64* status, u32* ticket, u32* errw) {
+                             u64* ib, u64 n, int shift, const u64* excl, SW* status, u32* ticket, u32* errw) {
   if (bulk)
-    k_sort_pass<DB, true><<<tiles, kSortBlock, PassLayout<DB>::kSmem, st>>>(ka, ia, kb, ib, n, shift, excl, status,
-                                                                          ticket, errw);
+    k_sort_pass<DB, true, SW><<<tiles, kSortBlock, PassLayout<DB>::kSmem, st>>>(ka, ia, kb, ib, n, shift, excl,
+                                                                              status, ticket, errw);
   else
-    k_sort_pass<DB, false><<<tiles, kSortBlock, PassLayout<DB>::kSmem, st>>>(ka, ia, kb, ib, n, shift, excl,
-                                                                           status, ticket, errw);
+    k_sort_pass<DB, false, SW><<<tiles, kSortBlock, PassLayout<DB>::kSmem, st>>>(ka, ia, kb, ib, n, shift, excl,
+                                                                               status, ticket, errw);
 }
+
+template <typename SW>
+static cudaError_t sort_passes_attrs(int db) { return db == 8 ? sort_pass_attrs<8, SW>() : sort_pass_attrs<9, SW>(); }
 
 // The sort behind cf_sort_pairs and cf_sort_pairs_digits: np = ceil(key_bits / db)
 // passes of db-bit digits (8 or 9), passes whose digit is constant skipped.
@@ -506,11 +516,12 @@ static int sort_pairs(u64* keys, u64* ids, u64 n, int key_bits, int db, void* tm
   u64* i2 = (u64*)w; w += n * 8;
   u64* hist = (u64*)w; w += (size_t)np * bins * 8;
   u64* excl = (u64*)w; w += (size_t)np * bins * 8;
-  u64* status = (u64*)w; w += (size_t)np * tiles * bins * 8;
+  const bool narrow = n < (1ull << 30);           // 32-bit status words hold every count
+  unsigned char* status = w; w += (size_t)np * tiles * bins * 8;   // room for 64-bit words
   u32* tickets = (u32*)w; w += kMaxPasses * 4;
   u32* errw = (u32*)w;
   cudaError_t e = cudaMemsetAsync(hist, 0, (size_t)np * bins * 8, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, (size_t)np * tiles * bins * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, (size_t)np * tiles * bins * (narrow ? 4 : 8), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(tickets, 0, kMaxPasses * 4 + 4, st);
   if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: memset");
   const unsigned hgrid = (unsigned)((n + kSortBlock * 8 - 1) / (kSortBlock * 8));
@@ -521,7 +532,7 @@ static int sort_pairs(u64* keys, u64* ids, u64 n, int key_bits, int db, void* tm
   e = cudaMemcpyAsync(hh.data(), hist, hh.size() * 8, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: histogram read");
-  e = db == 8 ? sort_pass_attrs<8>() : sort_pass_attrs<9>();
+  e = narrow ? sort_passes_attrs<u32>(db) : sort_passes_attrs<u64>(db);
   if (e != cudaSuccess) return cf_cuda_status(e, "cf_sort_pairs: smem attribute");
   u64 *ka = keys, *ia = ids, *kb = k2, *ib = i2;
   int done = 0;
@@ -532,11 +543,17 @@ static int sort_pairs(u64* keys, u64* ids, u64 n, int key_bits, int db, void* tm
     // bulk copies read 16-byte units from 16-byte boundaries: every tile starts at
     // a multiple of 4096 records, so aligned source arrays suffice
     const bool bulk = ((((uintptr_t)ka) | ((uintptr_t)ia)) & 15u) == 0;
-    u64* pst = status + (u64)p * tiles * bins;
-    if (db == 8)
-      sort_pass_launch<8>(bulk, (unsigned)tiles, st, ka, ia, kb, ib, n, 8 * p, excl + p * bins, pst, tickets + p, errw);
-    else
-      sort_pass_launch<9>(bulk, (unsigned)tiles, st, ka, ia, kb, ib, n, 9 * p, excl + p * bins, pst, tickets + p, errw);
+    const u64 pw = (u64)p * tiles * bins;           // this pass's status words
+    const u64* pex = excl + p * bins;
+    if (narrow) {
+      u32* pst = (u32*)status + pw;
+      if (db == 8) sort_pass_launch<8, u32>(bulk, (unsigned)tiles, st, ka, ia, kb, ib, n, 8 * p, pex, pst, tickets + p, errw);
+      else sort_pass_launch<9, u32>(bulk, (unsigned)tiles, st, ka, ia, kb, ib, n, 9 * p, pex, pst, tickets + p, errw);
+    } else {
+      u64* pst = (u64*)status + pw;
+      if (db == 8) sort_pass_launch<8, u64>(bulk, (unsigned)tiles, st, ka, ia, kb, ib, n, 8 * p, pex, pst, tickets + p, errw);
+      else sort_pass_launch<9, u64>(bulk, (unsigned)tiles, st, ka, ia, kb, ib, n, 9 * p, pex, pst, tickets + p, errw);
+    }
     CF_LAUNCH_CHECK("cf_sort_pairs: pass");
     u64* t = ka; ka = kb; kb = t;
     t = ia; ia = ib; ib = t;

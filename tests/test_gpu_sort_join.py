@@ -74,6 +74,33 @@ def test_c_entry_with_narrow_key_bits(cuda, width, key_bits):
                                     _lib.stream_handle()) == _lib.CF_ENOMEM
 
 
+@pytest.mark.parametrize("width", [8, 9])
+def test_more_than_2_30_records(cuda, width):
+    # past 2^30 records the look-back's status words are 64-bit (32-bit below): a ragged, odd n with
+    # 2^20 distinct keys, so every key repeats about 1000 times and stability is tested everywhere
+    free, _ = torch.cuda.mem_get_info()
+    if free < (80 << 30):
+        pytest.skip("needs about 60 GB of free device memory")
+    n = (1 << 30) + 4099
+    g = torch.Generator(device="cuda").manual_seed(width)
+    keys = torch.randint(0, 1 << 20, (n,), device="cuda", generator=g, dtype=torch.int64)
+    ids = torch.arange(n, device="cuda", dtype=torch.int64)
+    ks, is_ = G.sort_side(keys.view(torch.uint64), ids.view(torch.uint64), digit_bits=width)
+    ks, is_ = ks.view(torch.int64), is_.view(torch.int64)
+    assert bool((ks[1:] >= ks[:-1]).all())
+    seen = torch.zeros(n, dtype=torch.bool, device="cuda")
+    seen[is_] = True
+    assert bool(seen.all())                                       # the ids are a permutation
+    del seen
+    assert torch.equal(ks, keys[is_])                             # each key travelled with its id
+    del keys
+    eq = ks[1:] == ks[:-1]
+    assert bool((is_[1:] > is_[:-1])[eq].all())                  # ties keep input order
+    G._ws.clear()                                                 # the 21 GB sort workspace
+    del ks, is_, eq
+    torch.cuda.empty_cache()
+
+
 def test_tuned_digit_width_is_used_and_changes_nothing(cuda):
     from carmichael_frontier_b200 import autotune
     sizes = [3000, 70_000, 1 << 20]
