@@ -114,6 +114,20 @@ __device__ __forceinline__ bool batch_ticket(const CfBatchMod& md, u32 mod, u64 
   return ok;
 }
 
+// The modulus of ticket t (tstart[lo] <= t < tstart[lo + 1]).  `hint` is the modulus of the caller's
+// previous ticket, 0 before the first: tickets from the queue only grow, so tstart[hint] <= t, and the
+// ticket usually falls in that modulus or the next; a binary search over the rest otherwise.
+__device__ __forceinline__ u32 ticket_mod(const u64* __restrict__ tstart, u32 nmod, u64 t, u32 hint) {
+  if (tstart[hint + 1] > t) return hint;
+  u32 lo = hint + 1, hi = nmod;                // tstart[lo] <= t < tstart[hi]
+  if (tstart[lo + 1] > t) return lo;
+  while (hi - lo > 1) {
+    const u32 mid = (lo + hi) >> 1;
+    if (tstart[mid] <= t) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
 // RF = 0: any radius (a switch into the radius-templated code); RF > 0: every
 // modulus of the launch has radius RF (its ticket sums hold only those), so the
 // kernel carries only that radius's code and registers.
@@ -133,16 +147,13 @@ k_batch(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart /*[n
   sink.mod = 0;
   sink.swap = 0;
   bool ok = true, badarg = false;
+  u32 lo = 0;                                 // modulus of the warp's ticket
   for (;;) {
     u64 t = 0;
     if (lane == 0) t = atomicAdd(queue, 1ull);
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= total) break;
-    u32 lo = 0, hi = nmod;                    // the modulus with tstart[lo] <= t < tstart[lo + 1]
-    while (hi - lo > 1) {
-      const u32 mid = (lo + hi) >> 1;
-      if (tstart[mid] <= t) lo = mid; else hi = mid;
-    }
+    lo = ticket_mod(tstart, nmod, t, lo);
     const CfBatchMod& md = mods[lo];
     const bool d_side = (MODE == 0) == (md.swap == 0);
     const u64 n_side = d_side ? md.nD : md.nI;
@@ -297,16 +308,13 @@ k_bscatter(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart, 
   __shared__ u64 s_t;
   const u64 total = tstart[nmod];
   bool ok = true;
+  u32 lo = 0;                                    // modulus of the CTA's ticket
   for (;;) {
     if (threadIdx.x == 0) s_t = atomicAdd(queue, 1ull);
     __syncthreads();
     const u64 t = s_t;
     if (t >= total) break;
-    u32 lo = 0, hi = nmod;                       // the modulus with tstart[lo] <= t < tstart[lo + 1]
-    while (hi - lo > 1) {
-      const u32 mid = (lo + hi) >> 1;
-      if (tstart[mid] <= t) lo = mid; else hi = mid;
-    }
+    lo = ticket_mod(tstart, nmod, t, lo);
     const CfBatchMod& md = mods[lo];
     const u64 n_side = md.swap ? md.nI : md.nD;
     const u64 first = (t - tstart[lo]) * (u64)kScTile;
@@ -408,16 +416,13 @@ k_bplace(const CfBatchMod* __restrict__ mods, const u64* __restrict__ tstart, u3
   u32* s_fill = (u32*)(s_side + kPartBuckets * 16);          // [kPartBuckets] slots claimed
   __shared__ u64 s_t;
   const u64 total = tstart[nmod];
+  u32 lo = 0;                                    // modulus of the CTA's ticket
   for (;;) {
     if (threadIdx.x == 0) s_t = atomicAdd(queue, 1ull);
     __syncthreads();
     const u64 t = s_t;
     if (t >= total) break;
-    u32 lo = 0, hi = nmod;
-    while (hi - lo > 1) {
-      const u32 mid = (lo + hi) >> 1;
-      if (tstart[mid] <= t) lo = mid; else hi = mid;
-    }
+    lo = ticket_mod(tstart, nmod, t, lo);
     const CfBatchMod& md = mods[lo];
     const u32 p = (u32)(t - tstart[lo]);
     if (md.plb != (u32)PLB) {                    // the launch's range size must be the modulus's
