@@ -110,6 +110,18 @@ def tune_batch(prep, device=None, reps: int = 3, tickets=TICKETS, grids=GRID_PER
     return best[1], rows
 
 
+def sort_size_classes(sizes) -> dict[int, int]:
+    """{size class: largest size in it} over the sizes above 1; a size n is in class bit_length(n),
+    the key under which sort_side looks up its digit width."""
+    largest: dict[int, int] = {}
+    for n in sizes:
+        n = int(n)
+        if n > 1:
+            c = n.bit_length()
+            largest[c] = max(largest.get(c, 0), n)
+    return dict(sorted(largest.items()))
+
+
 def tune_sort(sizes, key_bits: int = 64, device=None, widths=None, reps: int = 3, seed: int = 0,
               apply: bool = True, verbose: bool = False) -> list[dict]:
     """Radix digit width of sort_side per size class (bit length of n) among `sizes`: for each
@@ -117,23 +129,19 @@ def tune_sort(sizes, key_bits: int = 64, device=None, widths=None, reps: int = 3
     2^key_bits (the residue keys of a modulus M lie below 2^bit_length(M)), timed whole with CUDA
     events (median of `reps` after one warm-up).  The fastest width is recorded for the class
     (mitm_gpu2.set_sort_digit_bits) unless apply=False.  Returns one row per class and width."""
+    import numpy as np
     import torch
 
     from . import mitm_gpu2 as G
     widths = G.SORT_DIGIT_WIDTHS if widths is None else tuple(widths)
     if not 1 <= key_bits <= 64:
         raise ValueError("key_bits must be 1..64")
+    if any(w not in G.SORT_DIGIT_WIDTHS for w in widths):
+        raise ValueError(f"digit widths must be among {G.SORT_DIGIT_WIDTHS}")
     dev = torch.device(device if device is not None else "cuda")
-    largest: dict[int, int] = {}
-    for n in sizes:
-        n = int(n)
-        if n > 1:
-            c = n.bit_length()
-            largest[c] = max(largest.get(c, 0), n)
-    import numpy as np
     rng = np.random.default_rng(seed)
     rows = []
-    for c, n in sorted(largest.items()):
+    for c, n in sort_size_classes(sizes).items():
         keys = torch.from_numpy(rng.integers(0, 1 << key_bits, size=n, dtype=np.uint64)).to(dev)
         ids = torch.arange(n, device=dev, dtype=torch.int64).view(torch.uint64)
         best = None

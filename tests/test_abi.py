@@ -251,3 +251,21 @@ def test_ddump_bound_table_equals_the_python_definition():
         got = out.view(np.uint64).reshape(r, n, 2)
         for t in range(r):                              # entries x < t are never read
             assert np.array_equal(got[t, t:], want[t, t:]), (n, r, Dmin, t)
+
+
+def test_sort_digit_width_classes_without_gpu():
+    # the tuner groups side sizes by bit length (sort_side's lookup key) and times the largest of each
+    from carmichael_frontier_b200 import autotune, mitm_gpu2 as G
+    assert autotune.sort_size_classes([0, 1, 3000, 4000, 70_000, 65_536, 1 << 20, (1 << 21) - 1]) == \
+        {12: 4000, 17: 70_000, 21: (1 << 21) - 1}
+    assert autotune.sort_size_classes([]) == {}
+    n = 123_457
+    assert G.sort_digit_bits(n) == 8                      # untuned classes use 8-bit digits
+    G.set_sort_digit_bits(n, 9)
+    assert G.sort_digit_bits(n + 1000) == 9 and G.sort_digit_bits(2 * n) == 8
+    G.set_sort_digit_bits(n, None)
+    assert G.sort_digit_bits(n) == 8
+    with pytest.raises(ValueError):
+        G.set_sort_digit_bits(n, 10)
+    with pytest.raises(ValueError):
+        autotune.tune_sort([n], widths=(8, 10))
