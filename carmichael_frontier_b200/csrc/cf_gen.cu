@@ -160,8 +160,10 @@ __host__ __device__ inline GenPartSmem gen_part_layout(int block, int steps, int
   return L;
 }
 
+// Tiles of 4096 records leave room for two CTAs per SM in shared memory; the register budget is
+// held to that too (512 threads: 64 registers, 1.36x the single-CTA rate on the k=64 r=5 I side).
 template <int R, int BLOCK, int STEPS>
-__global__ void __launch_bounds__(BLOCK)
+__global__ void __launch_bounds__(BLOCK, BLOCK * STEPS <= 4096 ? 2 : 1)
 k_gen_part(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo, u64 count, int pbits,
            u32 cap, u32* __restrict__ counts, CfRec* __restrict__ out, u32* __restrict__ err) {
   constexpr int T = BLOCK * STEPS;
@@ -207,8 +209,7 @@ k_gen_part(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64
   const u64 tile0 = (u64)blockIdx.x * T;
   const u64 wbase = tile0 + (u64)(threadIdx.x >> 5) * (32u * STEPS);
   u64 key[STEPS];
-  u32 pos[STEPS];
-  u32 part[STEPS];
+  u32 pp[STEPS];                                // partition << 13 | position in it (T <= 8192)
   if (wbase < count) {
     CfTailWalker<R, B> w;
     w.init(lo + wbase, n, binom, ar, st, hd->tail_n);
@@ -222,8 +223,8 @@ k_gen_part(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64
         w.template step<false>(n, binom, ar, lane, q, j, unused);
         if (t0 + lane < count) {
           key[s] = cf_tail_key(q, tail[j], ar.md, minv);
-          part[s] = cf_part_of(cf_hash(key[s]), pbits);
-          pos[s] = atomicAdd(&s_hist[part[s]], 1u);
+          const u32 pt = cf_part_of(cf_hash(key[s]), pbits);
+          pp[s] = (pt << 13) | atomicAdd(&s_hist[pt], 1u);
         }
       }
     }
@@ -255,12 +256,12 @@ k_gen_part(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64
   for (int s = 0; s < STEPS; ++s) {
     const u64 t = wbase + (u64)s * 32 + lane;
     if (t < count) {
-      const u32 slot = s_loff[part[s]] + pos[s];
+      const u32 slot = s_loff[pp[s] >> 13] + (pp[s] & 0x1fffu);
       CfRec rc;
       rc.key = key[s];
       rc.id = lo + t;
       s_stage[slot] = rc;
-      s_part[slot] = (unsigned short)part[s];
+      s_part[slot] = (unsigned short)(pp[s] >> 13);
     }
   }
   __syncthreads();
