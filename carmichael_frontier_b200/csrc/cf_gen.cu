@@ -167,6 +167,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK * STEPS <= 4096 ? 2 : 1)
 k_gen_part(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo, u64 count, int pbits,
            u32 cap, u32* __restrict__ counts, CfRec* __restrict__ out, u32* __restrict__ err) {
   constexpr int T = BLOCK * STEPS;
+  static_assert(T <= 8192, "positions within a partition are packed into 13 bits");
   constexpr int B = R < 2 ? R : 2;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ u32 s_warp[BLOCK / 32];
