@@ -146,12 +146,37 @@ __device__ __forceinline__ bool dtab_claim(const DTab& t, u64 b, u32 f16, uint2 
   return false;
 }
 
+// L2 eviction policy of the in-place build's claims and stores.  For tables of at most
+// 2^20 buckets (fingerprints, compact side words and fill counters about 100 MB, inside the
+// 126 MB L2) it is evict-last, so that the table's partly written sectors stay in L2 until
+// the build has filled them instead of leaving for DRAM half written and coming back for the
+// next slot (config-2 tables: build 16% faster); larger tables keep the normal priority.
+__device__ __forceinline__ u64 cf_l2_build_policy(u64 nb) {
+  u64 last, normal;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(last));
+  asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(normal));
+  return nb <= (1ull << kCompactMaxBbits) ? last : normal;
+}
+__device__ __forceinline__ u32 cf_atom_add_keep(u32* a, u32 v, u64 pol) {
+  u32 old;
+  asm volatile("atom.global.add.L2::cache_hint.u32 %0, [%1], %2, %3;" : "=r"(old) : "l"(a), "r"(v), "l"(pol)
+               : "memory");
+  return old;
+}
+__device__ __forceinline__ void cf_st_keep_u16(unsigned short* a, unsigned short v, u64 pol) {
+  asm volatile("st.global.L2::cache_hint.b16 [%0], %1, %2;" ::"l"(a), "h"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void cf_st_keep_u32(u32* a, u32 v, u64 pol) {
+  asm volatile("st.global.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(a), "r"(v), "l"(pol) : "memory");
+}
+
 // Fill a claimed slot s of bucket b: its 16-bit fingerprint (a 16-bit store into
 // the bucket's row) and its side entry in the table's format.
-__device__ __forceinline__ void dtab_place(const DTab& t, u64 b, u32 s, u32 f16, u32 f32, u32 rel) {
-  reinterpret_cast<unsigned short*>(t.fpw)[b * 16 + s] = (unsigned short)f16;
+__device__ __forceinline__ void dtab_place(const DTab& t, u64 b, u32 s, u32 f16, u32 f32, u32 rel, u64 pol) {
+  cf_st_keep_u16(reinterpret_cast<unsigned short*>(t.fpw) + b * 16 + s, (unsigned short)f16, pol);
   if (t.xb)
-    reinterpret_cast<u32*>(t.side)[b * 16 + s] = (rel << kCompactXb) | (f32 & ((1u << kCompactXb) - 1u));
+    cf_st_keep_u32(reinterpret_cast<u32*>(t.side) + b * 16 + s,
+                   (rel << kCompactXb) | (f32 & ((1u << kCompactXb) - 1u)), pol);
   else
     t.side[b * 16 + s] = make_uint2(f32, rel);
 }
@@ -162,15 +187,16 @@ __device__ __forceinline__ void dtab_place(const DTab& t, u64 b, u32 s, u32 f16,
 // occupied slots of a bucket are a prefix and "bucket full" is "last slot
 // occupied" -- the layout the probe expects.  Returns false if every bucket was
 // full.
-__device__ __forceinline__ bool dtab_claim_fill(const DTab& t, u64 b, u32 first_slot, u32 f16, u32 f32, u32 rel) {
+__device__ __forceinline__ bool dtab_claim_fill(const DTab& t, u64 b, u32 first_slot, u32 f16, u32 f32, u32 rel,
+                                                u64 pol) {
   u32 s = first_slot;
   for (u64 tries = 0; tries < t.nb; ++tries) {
     if (s < 16u) {
-      dtab_place(t, b, s, f16, f32, rel);
+      dtab_place(t, b, s, f16, f32, rel, pol);
       return true;
     }
     b = (b + 1) & (t.nb - 1);
-    s = atomicAdd(t.fill + b, 1u);
+    s = cf_atom_add_keep(t.fill + b, 1u, pol);
   }
   return false;
 }

@@ -96,6 +96,7 @@ k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo
   const u64 per_warp = 32ull * steps;
   const u64 nwarps = (u64)gridDim.x * (kFuseBlock / 32);
   bool bad = false;
+  const u64 keep = MODE == 0 ? cf_l2_build_policy(tab.nb) : 0ull;   // build: L2 priority of claims and stores
   for (u64 wbase = ((u64)blockIdx.x * (kFuseBlock / 32) + (threadIdx.x >> 5)) * per_warp; wbase < count;
        wbase += nwarps * per_warp) {
     const u32 left = (u32)((count - wbase) < per_warp ? (count - wbase) : per_warp);
@@ -137,10 +138,10 @@ k_fused(const u64* __restrict__ pool, const CfTailEnt* __restrict__ tail, u64 lo
         }
         u32 slot[kBuildU];
 #pragma unroll
-        for (int u = 0; u < kBuildU; ++u) slot[u] = v[u] ? atomicAdd(tab.fill + bk[u], 1u) : 16u;
+        for (int u = 0; u < kBuildU; ++u) slot[u] = v[u] ? cf_atom_add_keep(tab.fill + bk[u], 1u, keep) : 16u;
 #pragma unroll
         for (int u = 0; u < kBuildU; ++u)
-          if (v[u]) bad |= !dtab_claim_fill(tab, bk[u], slot[u], f16[u], f32[u], rel[u]);
+          if (v[u]) bad |= !dtab_claim_fill(tab, bk[u], slot[u], f16[u], f32[u], rel[u], keep);
       }
     } else {
       for (u32 off = 0; off < left; off += 32) {    // uniform across the warp
